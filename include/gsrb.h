@@ -1,0 +1,179 @@
+/* gsrb.h -- C ABI of libgsrb, a B200 (sm_100a) implementation of the TPDS'22
+ * GPU synchronization layer (multi-level sense-reversing grid barrier, mutexes,
+ * priority semaphore) and of the persistent barrier-stepped kernels that run on
+ * it (reduce, scan, Lonestar BFS / SSSP / PageRank).
+ *
+ * Conventions
+ *   - Every entry point returns gsrb_status_t (0 = success, negative = error);
+ *     nothing calls exit() or traps.  Device-side failures (a bounded wait that
+ *     ran out) are sticky in the context until gsrb_ctx_status() reads and
+ *     clears them.
+ *   - Pointers named d_* are device pointers, h_* host pointers.  No torch or
+ *     C++ types cross this boundary.
+ *   - Work is issued on the context's stream.  Entry points documented as
+ *     "synchronous" wait for their work; the others only enqueue it.
+ *   - One context may be used by one host thread at a time (calls serialize on
+ *     an internal mutex).
+ */
+#ifndef GSRB_H_
+#define GSRB_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t gsrb_status_t;
+enum {
+  GSRB_OK = 0,
+  GSRB_ERR_ARG = -1,             /* invalid argument */
+  GSRB_ERR_CUDA = -2,            /* a CUDA runtime call failed */
+  GSRB_ERR_NOT_CORESIDENT = -3,  /* persistent grid larger than the co-resident capacity: refused */
+  GSRB_ERR_TIMEOUT = -4,         /* a device-side bounded wait ran out */
+  GSRB_ERR_NOMEM = -5,
+  GSRB_ERR_STATE = -6,           /* context in a bad state (e.g. sticky device error) */
+  GSRB_ERR_UNSUPPORTED = -7,
+  GSRB_ERR_OVERFLOW = -8,        /* a device worklist / scratch area would overflow */
+  GSRB_ERR_LOCK_TIMEOUT = -9,    /* a mutex / semaphore wait ran out */
+  GSRB_ERR_INVARIANT = -10       /* a device-checked invariant failed */
+};
+
+typedef struct gsrb_ctx* gsrb_ctx_t;
+
+/* Barrier variants (gsrb_cfg_t.variant). */
+enum {
+  GSRB_BAR_CLUSTER = 0,          /* 3-level: HW cluster barrier -> L2 counter -> HW cluster release */
+  GSRB_BAR_CLUSTER_ALLPOLL = 1,  /* 3-level: HW cluster arrival, every CTA polls the L2 generation */
+  GSRB_BAR_DSMEM = 2,            /* 3-level: DSMEM arrival counter / DSMEM release flags */
+  GSRB_BAR_SOFT2 = 3,            /* reference GSRB: software per-group counters -> global */
+  GSRB_BAR_FLAT = 4,             /* reference GCPUSRB: one counter for all CTAs */
+  GSRB_BAR_TREE = 5,             /* HeteroSync atomic tree barrier (paper baseline) */
+  GSRB_BAR_CCG = 6,              /* cooperative_groups grid.sync() (library baseline) */
+  GSRB_BAR_CLUSTER_RED = 7,      /* 3-level with red.release arrivals and a polling master */
+  GSRB_BAR_NONE = 99             /* no barrier (phase-only timing baseline) */
+};
+
+/* Launch / schedule configuration.  Zero-initialise and call gsrb_cfg_default. */
+typedef struct gsrb_cfg {
+  int32_t variant;       /* GSRB_BAR_* */
+  int32_t cluster;       /* CTAs per cluster for the cluster variants (1,2,4,8,16) */
+  int32_t ctas_per_sm;   /* persistent CTAs per SM (grid = ctas_per_sm * #SMs) */
+  int32_t threads;       /* threads per CTA */
+  int32_t fanin_groups;  /* global fan-in groups (0 = arrive at the root directly) */
+  int32_t spin_ns;       /* __nanosleep between polls (0 = hot spin) */
+  uint32_t timeout_ms;   /* per-wait device deadline */
+  int32_t tile;          /* elements per tile / segment hint (0 = auto) */
+  int32_t grid_override; /* exact grid size (0 = ctas_per_sm * #SMs) */
+  int32_t reserved[7];
+} gsrb_cfg_t;
+
+void gsrb_cfg_default(gsrb_cfg_t* cfg);
+const char* gsrb_status_string(gsrb_status_t s);
+
+/* ---- context ---------------------------------------------------------------- */
+gsrb_status_t gsrb_ctx_create(int device, gsrb_ctx_t* out);
+gsrb_status_t gsrb_ctx_destroy(gsrb_ctx_t ctx);
+/* Use an existing cudaStream_t (passed as void*); NULL = the context's own stream. */
+gsrb_status_t gsrb_ctx_set_stream(gsrb_ctx_t ctx, void* stream);
+/* Device facts: number of SMs, L2 bytes, device ordinal. */
+gsrb_status_t gsrb_ctx_info(gsrb_ctx_t ctx, int32_t* num_sms, int64_t* l2_bytes, int32_t* device);
+/* Synchronous: wait for the context's stream, read the sticky device status and
+ * clear it.  Returns GSRB_OK or the mapped error; `dev_code`, `where`
+ * (episode) and `who` (block) describe the first device error (may be NULL). */
+gsrb_status_t gsrb_ctx_status(gsrb_ctx_t ctx, uint32_t* dev_code, uint32_t* where, uint32_t* who);
+gsrb_status_t gsrb_ctx_synchronize(gsrb_ctx_t ctx);
+/* Largest co-resident grid for a barrier configuration (CTAs), for a given kernel family:
+ * 0 = barrier microbenchmark, 1 = reduce, 2 = scan, 3 = graph traversal. */
+gsrb_status_t gsrb_max_coresident(gsrb_ctx_t ctx, const gsrb_cfg_t* cfg, int32_t family, int32_t* ctas);
+
+/* ---- memory plumbing (device, pinned host) ----------------------------------- */
+gsrb_status_t gsrb_malloc(void** d_ptr, size_t bytes);
+gsrb_status_t gsrb_free(void* d_ptr);
+gsrb_status_t gsrb_host_alloc(void** h_ptr, size_t bytes);   /* pinned */
+gsrb_status_t gsrb_host_free(void* h_ptr);
+gsrb_status_t gsrb_memcpy_h2d(gsrb_ctx_t ctx, void* d_dst, const void* h_src, size_t bytes);   /* async */
+gsrb_status_t gsrb_memcpy_d2h(gsrb_ctx_t ctx, void* h_dst, const void* d_src, size_t bytes);   /* async */
+gsrb_status_t gsrb_memset(gsrb_ctx_t ctx, void* d_ptr, int value, size_t bytes);               /* async */
+
+/* ---- timing helpers (CUDA events recorded on the context stream) -------------- */
+gsrb_status_t gsrb_event_record(gsrb_ctx_t ctx, int32_t slot);        /* slot 0..63 */
+gsrb_status_t gsrb_event_elapsed_ms(gsrb_ctx_t ctx, int32_t a, int32_t b, float* ms); /* synchronous */
+/* Write a buffer larger than L2 to evict the inputs of the next timed launch. */
+gsrb_status_t gsrb_l2_flush(gsrb_ctx_t ctx);
+/* Number of kernels this library has launched in this process (for launch accounting). */
+uint64_t gsrb_launch_count(void);
+
+/* ---- grid barrier microbenchmark -------------------
+ * One persistent launch of grid = cfg->ctas_per_sm * #SMs CTAs of cfg->threads
+ * threads; each CTA runs `episodes` times: `fma_per_episode` dependent FP32 FMAs
+ * per thread, then one grid barrier of cfg->variant.  d_episode_count (uint32,
+ * zeroed by the caller) receives the sum over CTAs of completed episodes
+ * (must equal episodes * grid).  d_sink: >= grid*threads floats, written with
+ * the FMA results.  Reference: kernelAtomicTreeBarrierUniqSRB,
+ * Heterosync/main.cu:188-226, launched by invokeAtomicTreeBarrierSRB :1532-1562. */
+gsrb_status_t gsrb_barrier_bench(gsrb_ctx_t ctx, const gsrb_cfg_t* cfg, int32_t episodes,
+                                 int32_t fma_per_episode, float* d_sink, uint32_t* d_episode_count);
+/* Message-passing litmus test across the barrier: every episode each thread writes
+ * a stamp, barrier, reads another CTA's stamp, barrier.  d_buf: grid*threads
+ * uint32; d_stale (uint64, zeroed by caller) receives the number of stale reads. */
+gsrb_status_t gsrb_barrier_litmus(gsrb_ctx_t ctx, const gsrb_cfg_t* cfg, int32_t episodes,
+                                  uint32_t* d_buf, unsigned long long* d_stale);
+/* Fault test: launch a barrier kernel whose expected arrival count is one more
+ * than the grid, so every wait must run out after cfg->timeout_ms and report
+ * GSRB_ERR_TIMEOUT (synchronous).  The context stays usable afterwards. */
+gsrb_status_t gsrb_barrier_fault_short_grid(gsrb_ctx_t ctx, const gsrb_cfg_t* cfg);
+
+/* L2 atomic probes (synchronous, ms via CUDA events): mode 0 = `ctas` CTAs each
+ * issue `iters` red.add to one address from one thread (same-address throughput);
+ * mode 1 = one thread issues `iters` dependent atom.add (round-trip latency). */
+gsrb_status_t gsrb_probe_l2_atomics(gsrb_ctx_t ctx, int32_t ctas, int32_t iters, int32_t mode, float* ms);
+
+/* ---- reduce ----------------------------------------
+ * Sum of n int32 into *d_out (int64), one persistent launch: each CTA reduces a
+ * contiguous chunk with 128-bit loads, one grid barrier, CTA 0 combines the
+ * partials.  Replaces reduce_kernel/reduce() of Reduce/reduce_gsrb.cu:289-404
+ * (API Reduce/reduce.cuh:47).  Asynchronous. */
+gsrb_status_t gsrb_reduce_i32(gsrb_ctx_t ctx, const int32_t* d_in, size_t n, int64_t* d_out,
+                              const gsrb_cfg_t* cfg);
+
+/* ---- host-side graphs and synthetic inputs ----------------------------------------
+ * CSR in the layout of the reference CSRGraph (row_start[n+1], edge_dst[m],
+ * edge_data[m]; LONESTAR/rt/include/csr_graph.h.prehip:20-103).  Host memory
+ * allocated by the library; release with gsrb_host_csr_free. */
+typedef struct gsrb_host_csr {
+  uint32_t nnodes;
+  uint32_t _pad;
+  uint64_t nedges;
+  uint32_t* row_start;
+  uint32_t* edge_dst;
+  int32_t* edge_data;
+} gsrb_host_csr_t;
+
+void gsrb_host_csr_free(gsrb_host_csr_t* g);
+/* Seeded uniform integers in [lo, hi] / floats in [0, 1) (splitmix64-seeded
+ * xoshiro256**, one stream per 65536-element block: independent of thread count). */
+gsrb_status_t gsrb_gen_uniform_i32(uint64_t seed, size_t n, int32_t lo, int32_t hi, int32_t* h_out);
+gsrb_status_t gsrb_gen_uniform_f32(uint64_t seed, size_t n, float* h_out);
+/* Symmetric weight of the unordered pair {u, v}, uniform in [lo, hi]. */
+uint32_t gsrb_edge_weight(uint32_t u, uint32_t v, uint64_t seed, int32_t lo, int32_t hi);
+/* CSR with sorted, duplicate-free rows and no self loops from an edge list
+ * (symmetrize != 0 inserts both directions); weights from gsrb_edge_weight. */
+gsrb_status_t gsrb_csr_from_edges(uint32_t n, uint64_t m, const uint32_t* h_src, const uint32_t* h_dst,
+                                  int symmetrize, uint64_t weight_seed, int32_t wlo, int32_t whi,
+                                  gsrb_host_csr_t* out);
+/* R-MAT (scale, edge factor, a, b, c), symmetrised and deduplicated. */
+gsrb_status_t gsrb_gen_rmat(int32_t scale, int32_t edgefactor, double a, double b, double c, uint64_t seed,
+                            int32_t wlo, int32_t whi, gsrb_host_csr_t* out);
+/* width x height 4-neighbour grid (vertex id = row * width + col). */
+gsrb_status_t gsrb_gen_grid2d(int32_t width, int32_t height, uint64_t seed, int32_t wlo, int32_t whi,
+                              gsrb_host_csr_t* out);
+/* Galois `.gr` version 1 reader / writer (LONESTAR/rt/src/csr_graph.cu:152-237). */
+gsrb_status_t gsrb_gr_read(const char* path, gsrb_host_csr_t* out);
+gsrb_status_t gsrb_gr_write(const char* path, const gsrb_host_csr_t* g, int32_t with_weights);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GSRB_H_ */

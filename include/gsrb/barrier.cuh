@@ -1,0 +1,492 @@
+// gsrb/barrier.cuh -- grid barriers for persistent kernels on sm_100a.
+//
+// Reference algorithms restated here (behaviour, not code):
+//   * GSRB, the two-level sense-reversing barrier of the TPDS'22 artifact:
+//     Heterosync/cudaLocksBarrierAtomicSRB.cu:63-236 and its application copy
+//     Reduce/reduce_gsrb.cu:198-269 (group = blockIdx % min(grid, NUM_SM); the
+//     last arriver of a group joins the global counter; everyone waits for the
+//     global sense to flip).
+//   * GCPUSRB, the one-level "CPU style" sense-reversing barrier:
+//     Heterosync/cudaLocksBarrierAtomicSRB.cu:17-61 (naive = true in the apps,
+//     e.g. Reduce/reduce_gcpusrb.cu).
+//   * the HeteroSync atomic tree barrier used as the paper's baseline:
+//     Heterosync/cudaLocksBarrierAtomic.cu:6-170 (two counters per level, no sense).
+//   * CUDA cooperative groups grid.sync(): Heterosync/main.cu:127-133.
+//
+// The B200-native barrier (GSRB_CLUSTER and its siblings) has three levels:
+//   CTA      -> __syncthreads (implied by the cluster barrier, which every thread joins)
+//   cluster  -> hardware `barrier.cluster.arrive.release / wait.acquire`, or a
+//               distributed-shared-memory arrival counter in the cluster leader
+//   global   -> one arriving thread per cluster does `atom.acq_rel.gpu.add` (or
+//               `red.release.gpu.add`) on an L2-resident counter, optionally
+//               through a layer of sub-group counters (fan-in), and the barrier
+//               completes when the generation word ("sense", kept as an epoch
+//               counter so it never needs resetting) is bumped with a
+//               `st.release.gpu`; waiters poll it with `ld.acquire.gpu`.
+//
+// Every wait is bounded by a %globaltimer deadline.  A wait that runs out records
+// GSRB_DEV_TIMEOUT in the slot's status word (first error wins) and returns
+// false; every other waiter notices the status word within 32 polls and returns
+// false too, so all CTAs leave the kernel and the host reads the error.  Nothing
+// traps, nothing spins forever.
+#pragma once
+#include <stdint.h>
+#include <cooperative_groups.h>
+#include "gsrb/ptx.cuh"
+
+namespace gsrb {
+
+// Device status codes written into BarrierSlot::status.
+enum : uint32_t {
+  GSRB_DEV_OK = 0,
+  GSRB_DEV_TIMEOUT = 1,        // a bounded wait ran out
+  GSRB_DEV_BAD_CONFIG = 2,     // kernel saw a launch shape it cannot serve
+  GSRB_DEV_OVERFLOW = 3,       // a worklist or scratch area would overflow
+  GSRB_DEV_LOCK_TIMEOUT = 4,   // mutex / semaphore wait ran out
+  GSRB_DEV_INVARIANT = 5,      // a checked invariant failed (e.g. semaphore over-post)
+};
+
+// Barrier variants.  The numeric values are part of the C ABI (include/gsrb.h).
+enum Variant : int {
+  V_CLUSTER = 0,         // HW cluster barrier -> leader global -> HW cluster barrier release
+  V_CLUSTER_ALLPOLL = 1, // HW cluster barrier -> leader global arrive; every CTA polls
+  V_DSMEM = 2,           // DSMEM arrival counter -> leader global -> DSMEM release flags
+  V_SOFT2 = 3,           // reference GSRB: software group counters -> global; all poll
+  V_FLAT = 4,            // reference GCPUSRB: every CTA arrives at one counter; all poll
+  V_TREE = 5,            // HeteroSync atomic tree barrier (two counters per level)
+  V_CCG = 6,             // cooperative_groups::this_grid().sync()
+  V_CLUSTER_RED = 7,     // HW cluster barrier -> red.release arrivals, master polls count
+  V_COUNT = 8
+};
+
+// One global barrier slot: four 128-byte lines so that the arrival counter, the
+// generation word and the status word never share an L2 line.
+struct __align__(128) BarrierSlot {
+  uint32_t count;      // arrivals at the global level (reset by the completer)
+  uint32_t _p0[31];
+  uint32_t epoch;      // generation; bumped once per completed episode
+  uint32_t _p1[31];
+  uint32_t status;     // GSRB_DEV_* (first error wins)
+  uint32_t where;      // episode index of the first error
+  uint32_t who;        // block index that recorded it
+  uint32_t _p2[29];
+  uint32_t count2;     // second counter for the tree barrier
+  uint32_t _p3[31];
+};
+static_assert(sizeof(BarrierSlot) == 512, "slot layout");
+
+// A sub-group counter for fan-in combining (and for the per-SM level of the
+// reference-style barriers).  Two lines: counter and a private generation.
+struct __align__(128) GroupSlot {
+  uint32_t count;
+  uint32_t _p0[31];
+  uint32_t count2;     // second counter (tree barrier local level)
+  uint32_t _p1[31];
+};
+static_assert(sizeof(GroupSlot) == 256, "group layout");
+
+// Launch-time parameters of one grid barrier (passed by value to kernels).
+struct GridBarrier {
+  BarrierSlot* slot;
+  GroupSlot* groups;      // >= ngroups entries when ngroups > 0
+  uint32_t nparticipants; // CTAs taking part (gridDim.x for whole-grid barriers)
+  uint32_t first_cta;     // first participating block index (sub-grid barriers)
+  uint32_t ngroups;       // global fan-in groups (0 = arrive directly at the root)
+  uint32_t spin_ns;       // __nanosleep between polls (0 = hot spin)
+  uint64_t timeout_ns;    // per-wait deadline
+};
+
+// Shared-memory words a CTA needs for the cluster / DSMEM levels.
+struct BarrierShared {
+  uint32_t arrive;   // DSMEM arrival counter (used in the cluster leader)
+  uint32_t release;  // DSMEM release flag (epoch broadcast into every CTA)
+  uint32_t ok;       // result broadcast
+  uint32_t pad;
+};
+
+namespace detail {
+
+__device__ __forceinline__ void record_error(const GridBarrier& gb, uint32_t code,
+                                             uint32_t episode) {
+  if (ptx::atom_cas_acq_rel_gpu(&gb.slot->status, 0u, code) == 0u) {
+    ptx::st_relaxed_gpu(&gb.slot->where, episode);
+    ptx::st_relaxed_gpu(&gb.slot->who, blockIdx.x);
+  }
+}
+
+// Poll `*word` until it differs from `old`.  Bounded: returns false after the
+// deadline (recording a timeout) or when another CTA has recorded an error.
+__device__ __forceinline__ bool wait_ne(const uint32_t* word, uint32_t old,
+                                        const GridBarrier& gb, uint32_t episode) {
+  uint64_t t0 = 0;
+  for (uint32_t it = 0;; ++it) {
+    if (ptx::ld_acquire_gpu(word) != old) return true;
+    if ((it & 31u) == 31u) {
+      if (ptx::ld_relaxed_gpu(&gb.slot->status) != 0u) return false;
+      const uint64_t now = ptx::globaltimer_ns();
+      if (t0 == 0) {
+        t0 = now;
+      } else if (now - t0 > gb.timeout_ns) {
+        record_error(gb, GSRB_DEV_TIMEOUT, episode);
+        return false;
+      }
+    }
+    if (gb.spin_ns) __nanosleep(gb.spin_ns);
+  }
+}
+
+// Poll until `*word == want` (used by the red-arrival master and the tree barrier).
+__device__ __forceinline__ bool wait_eq(const uint32_t* word, uint32_t want,
+                                        const GridBarrier& gb, uint32_t episode) {
+  uint64_t t0 = 0;
+  for (uint32_t it = 0;; ++it) {
+    if (ptx::ld_acquire_gpu(word) == want) return true;
+    if ((it & 31u) == 31u) {
+      if (ptx::ld_relaxed_gpu(&gb.slot->status) != 0u) return false;
+      const uint64_t now = ptx::globaltimer_ns();
+      if (t0 == 0) {
+        t0 = now;
+      } else if (now - t0 > gb.timeout_ns) {
+        record_error(gb, GSRB_DEV_TIMEOUT, episode);
+        return false;
+      }
+    }
+    if (gb.spin_ns) __nanosleep(gb.spin_ns);
+  }
+}
+
+// Number of arrivals (among `n` participants numbered 0..n-1) that land in
+// fan-in group g when participant i belongs to group i % ngroups.
+__device__ __forceinline__ uint32_t group_size(uint32_t n, uint32_t ngroups, uint32_t g) {
+  return n / ngroups + (g < n % ngroups ? 1u : 0u);
+}
+
+// Global level, atom flavour: participant `idx` of `n` arrives; the completing
+// arrival resets the counter(s) and bumps the epoch.  Returns true if this
+// caller completed the episode (it need not wait).
+__device__ __forceinline__ bool global_arrive_atom(const GridBarrier& gb, uint32_t idx,
+                                                   uint32_t n, uint32_t epoch) {
+  if (gb.ngroups > 1 && n > gb.ngroups) {
+    const uint32_t g = idx % gb.ngroups;
+    uint32_t* gc = &gb.groups[g].count;
+    const uint32_t gs = group_size(n, gb.ngroups, g);
+    if (ptx::atom_add_acq_rel_gpu(gc, 1u) != gs - 1u) return false;
+    ptx::st_relaxed_gpu(gc, 0u);
+    n = gb.ngroups;  // the root counts groups
+  }
+  if (ptx::atom_add_acq_rel_gpu(&gb.slot->count, 1u) != n - 1u) return false;
+  ptx::st_relaxed_gpu(&gb.slot->count, 0u);
+  ptx::st_release_gpu(&gb.slot->epoch, epoch + 1u);
+  return true;
+}
+
+// Global level, red flavour: arrivals are fire-and-forget `red.release.gpu.add`;
+// participant 0 polls the counter, resets it and bumps the epoch.
+__device__ __forceinline__ bool global_arrive_red(const GridBarrier& gb, uint32_t idx,
+                                                  uint32_t n, uint32_t epoch,
+                                                  uint32_t episode) {
+  ptx::red_add_release_gpu(&gb.slot->count, 1u);
+  if (idx != 0) return true;
+  if (!wait_eq(&gb.slot->count, n, gb, episode)) return false;
+  ptx::st_relaxed_gpu(&gb.slot->count, 0u);
+  ptx::st_release_gpu(&gb.slot->epoch, epoch + 1u);
+  return true;
+}
+
+}  // namespace detail
+
+// Per-CTA barrier handle.  All member functions are whole-CTA collectives:
+// every thread of the CTA (and, for the cluster variants, of its cluster) must
+// call them in the same order.
+template <int V>
+struct GridSync {
+  GridBarrier gb;
+  BarrierShared* sh;
+  uint32_t epoch;    // meaningful in thread 0
+  uint32_t episode;  // meaningful in thread 0
+
+  // Index of this CTA among the participants and of its arrival unit.
+  __device__ __forceinline__ uint32_t my_index() const { return blockIdx.x - gb.first_cta; }
+
+  // Reads the current generation and refuses to start after a recorded error.
+  // For the cluster variants the verdict is taken by the cluster leader and
+  // broadcast, so that every CTA of a cluster takes the same path (a hardware
+  // cluster barrier must see the same number of arrivals from all of them).
+  __device__ bool init(const GridBarrier& g, BarrierShared* s) {
+    gb = g;
+    sh = s;
+    episode = 0;
+    if (threadIdx.x == 0) {
+      epoch = ptx::ld_acquire_gpu(&gb.slot->epoch);
+      sh->arrive = 0;
+      sh->release = epoch;
+      sh->ok = 0;
+    }
+    if (V == V_CLUSTER || V == V_CLUSTER_ALLPOLL || V == V_DSMEM || V == V_CLUSTER_RED) {
+      ptx::cluster_sync();  // peers' shared words are initialised
+      if (threadIdx.x == 0 && ptx::cluster_ctarank() == 0) {
+        const uint32_t ok = (ptx::ld_relaxed_gpu(&gb.slot->status) == 0u) ? 1u : 0u;
+        const uint32_t n = ptx::cluster_nctarank();
+        const uint32_t sa = ptx::smem_u32(&sh->ok);
+        for (uint32_t r = 0; r < n; ++r) ptx::st_cluster_relaxed_u32(ptx::mapa_shared(sa, r), ok);
+      }
+      ptx::cluster_sync();
+    } else {
+      if (threadIdx.x == 0) sh->ok = (ptx::ld_relaxed_gpu(&gb.slot->status) == 0u) ? 1u : 0u;
+      __syncthreads();
+    }
+    return sh->ok != 0u;
+  }
+
+  // Cluster variants must not leave while a peer may still touch their shared
+  // memory; every CTA calls finish() once, on every exit path.
+  __device__ void finish() {
+    if (V == V_CLUSTER || V == V_CLUSTER_ALLPOLL || V == V_DSMEM || V == V_CLUSTER_RED) {
+      ptx::cluster_sync();
+    }
+  }
+
+  __device__ bool sync();
+};
+
+// ---------------------------------------------------------------------------
+// V_CLUSTER: level 2 = hardware cluster barrier; level 3 = the cluster leader's
+// thread 0 arrives (optionally through fan-in groups) and waits for the epoch;
+// the cluster is released by a second hardware cluster barrier.  The leader
+// writes the verdict into every peer's shared memory before releasing them.
+template <>
+__device__ __forceinline__ bool GridSync<V_CLUSTER>::sync() {
+  ptx::cluster_sync();
+  const uint32_t crank = ptx::cluster_ctarank();
+  if (crank == 0 && threadIdx.x == 0) {
+    const uint32_t ncl = gb.nparticipants / ptx::cluster_nctarank();
+    const uint32_t cid = my_index() / ptx::cluster_nctarank();
+    bool ok = true;
+    if (!detail::global_arrive_atom(gb, cid, ncl, epoch))
+      ok = detail::wait_ne(&gb.slot->epoch, epoch, gb, episode);
+    const uint32_t n = ptx::cluster_nctarank();
+    const uint32_t sa = ptx::smem_u32(&sh->ok);
+    for (uint32_t r = 0; r < n; ++r) ptx::st_cluster_relaxed_u32(ptx::mapa_shared(sa, r), ok ? 1u : 0u);
+  }
+  ptx::cluster_sync();
+  if (threadIdx.x == 0) { ++epoch; ++episode; }
+  return sh->ok != 0u;
+}
+
+// V_CLUSTER_RED: as V_CLUSTER but arrivals are `red.release.gpu.add` and the
+// leader of cluster 0 polls the counter and publishes the new epoch.
+template <>
+__device__ __forceinline__ bool GridSync<V_CLUSTER_RED>::sync() {
+  ptx::cluster_sync();
+  const uint32_t crank = ptx::cluster_ctarank();
+  if (crank == 0 && threadIdx.x == 0) {
+    const uint32_t ncl = gb.nparticipants / ptx::cluster_nctarank();
+    const uint32_t cid = my_index() / ptx::cluster_nctarank();
+    bool ok = detail::global_arrive_red(gb, cid, ncl, epoch, episode);
+    if (ok && cid != 0) ok = detail::wait_ne(&gb.slot->epoch, epoch, gb, episode);
+    const uint32_t n = ptx::cluster_nctarank();
+    const uint32_t sa = ptx::smem_u32(&sh->ok);
+    for (uint32_t r = 0; r < n; ++r) ptx::st_cluster_relaxed_u32(ptx::mapa_shared(sa, r), ok ? 1u : 0u);
+  }
+  ptx::cluster_sync();
+  if (threadIdx.x == 0) { ++epoch; ++episode; }
+  return sh->ok != 0u;
+}
+
+// V_CLUSTER_ALLPOLL: one hardware cluster barrier for arrival; the leader
+// arrives globally; every CTA's thread 0 then polls the epoch itself.  The
+// verdict is per CTA (not cluster-uniform), so a kernel using this variant must
+// keep calling sync() the same number of times on every CTA even after a
+// failure (the library's kernels only use it in fixed-count loops).
+template <>
+__device__ __forceinline__ bool GridSync<V_CLUSTER_ALLPOLL>::sync() {
+  ptx::cluster_sync();
+  if (threadIdx.x == 0) {
+    bool ok = true;
+    bool done = false;
+    if (ptx::cluster_ctarank() == 0) {
+      const uint32_t ncl = gb.nparticipants / ptx::cluster_nctarank();
+      const uint32_t cid = my_index() / ptx::cluster_nctarank();
+      done = detail::global_arrive_atom(gb, cid, ncl, epoch);
+    }
+    if (!done) ok = detail::wait_ne(&gb.slot->epoch, epoch, gb, episode);
+    sh->ok = ok ? 1u : 0u;
+    ++epoch;
+    ++episode;
+  }
+  __syncthreads();
+  return sh->ok != 0u;
+}
+
+// V_DSMEM: every CTA's thread 0 adds one to the leader's shared-memory arrival
+// counter (red.release.cluster); the leader polls it, arrives globally, waits,
+// and writes the new epoch into every peer's release word; peers poll their own
+// shared memory.  No hardware cluster barrier per episode.
+template <>
+__device__ __forceinline__ bool GridSync<V_DSMEM>::sync() {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const uint32_t n = ptx::cluster_nctarank();
+    const uint32_t crank = ptx::cluster_ctarank();
+    const uint32_t next = epoch + 1u;
+    bool ok = true;
+    if (crank == 0) {
+      // wait for the n-1 peers (bounded; a shared-memory poll)
+      uint64_t t0 = 0;
+      for (uint32_t it = 0;; ++it) {
+        if (ptx::ld_shared_acquire_cluster_u32(&sh->arrive) == n - 1u) break;
+        if ((it & 255u) == 255u) {
+          if (ptx::ld_relaxed_gpu(&gb.slot->status) != 0u) { ok = false; break; }
+          const uint64_t now = ptx::globaltimer_ns();
+          if (t0 == 0) t0 = now;
+          else if (now - t0 > gb.timeout_ns) {
+            detail::record_error(gb, GSRB_DEV_TIMEOUT, episode);
+            ok = false;
+            break;
+          }
+        }
+      }
+      sh->arrive = 0;
+      if (ok) {
+        const uint32_t ncl = gb.nparticipants / n;
+        const uint32_t cid = my_index() / n;
+        if (!detail::global_arrive_atom(gb, cid, ncl, epoch))
+          ok = detail::wait_ne(&gb.slot->epoch, epoch, gb, episode);
+      }
+      // broadcast: ok -> next epoch; failure -> next epoch with the top bit set
+      const uint32_t msg = ok ? next : (next | 0x80000000u);
+      const uint32_t sa = ptx::smem_u32(&sh->release);
+      for (uint32_t r = 1; r < n; ++r) ptx::st_cluster_release_u32(ptx::mapa_shared(sa, r), msg);
+      sh->release = msg;
+    } else {
+      ptx::red_cluster_release_add_u32(ptx::mapa_shared(ptx::smem_u32(&sh->arrive), 0), 1u);
+      uint64_t t0 = 0;
+      for (uint32_t it = 0;; ++it) {
+        const uint32_t v = ptx::ld_shared_acquire_cluster_u32(&sh->release);
+        if ((v & 0x7fffffffu) == (next & 0x7fffffffu)) { ok = (v & 0x80000000u) == 0u; break; }
+        if ((it & 255u) == 255u) {
+          const uint64_t now = ptx::globaltimer_ns();
+          if (t0 == 0) t0 = now;
+          // the leader always answers: its own waits are bounded by the same
+          // deadline, so allow it twice the time before giving up here.
+          else if (now - t0 > 2 * gb.timeout_ns + 1000000ull) {
+            detail::record_error(gb, GSRB_DEV_TIMEOUT, episode);
+            ok = false;
+            break;
+          }
+        }
+      }
+    }
+    sh->ok = ok ? 1u : 0u;
+    epoch = next;
+    ++episode;
+  }
+  __syncthreads();
+  return sh->ok != 0u;
+}
+
+// V_SOFT2: the reference GSRB two-level structure with software groups
+// (group g = participant % ngroups, ngroups = min(participants, #SMs) by
+// default).  The last arriver of a group arrives at the root; all CTAs poll.
+template <>
+__device__ __forceinline__ bool GridSync<V_SOFT2>::sync() {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    bool ok = true;
+    if (!detail::global_arrive_atom(gb, my_index(), gb.nparticipants, epoch))
+      ok = detail::wait_ne(&gb.slot->epoch, epoch, gb, episode);
+    sh->ok = ok ? 1u : 0u;
+    ++epoch;
+    ++episode;
+  }
+  __syncthreads();
+  return sh->ok != 0u;
+}
+
+// V_FLAT: the reference GCPUSRB: one counter, every CTA arrives and polls.
+template <>
+__device__ __forceinline__ bool GridSync<V_FLAT>::sync() {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    bool ok = true;
+    GridBarrier flat = gb;
+    flat.ngroups = 0;
+    if (!detail::global_arrive_atom(flat, my_index(), gb.nparticipants, epoch))
+      ok = detail::wait_ne(&gb.slot->epoch, epoch, gb, episode);
+    sh->ok = ok ? 1u : 0u;
+    ++epoch;
+    ++episode;
+  }
+  __syncthreads();
+  return sh->ok != 0u;
+}
+
+namespace detail {
+// One sub-barrier of the HeteroSync atomic tree barrier
+// (Heterosync/cudaLocksBarrierAtomic.cu:6-57): arrive with an increment, then
+// try compare-and-swap(count: n -> 0); the barrier is passed once the counter is
+// seen at zero.  Bounded.
+__device__ __forceinline__ bool tree_sub(uint32_t* cnt, uint32_t n, const GridBarrier& gb,
+                                         uint32_t episode) {
+  ptx::atom_add_acq_rel_gpu(cnt, 1u);
+  uint64_t t0 = 0;
+  for (uint32_t it = 0;; ++it) {
+    if (ptx::atom_cas_acq_rel_gpu(cnt, n, 0u) == 0u) return true;
+    if ((it & 31u) == 31u) {
+      if (ptx::ld_relaxed_gpu(&gb.slot->status) != 0u) return false;
+      const uint64_t now = ptx::globaltimer_ns();
+      if (t0 == 0) t0 = now;
+      else if (now - t0 > gb.timeout_ns) {
+        record_error(gb, GSRB_DEV_TIMEOUT, episode);
+        return false;
+      }
+    }
+    if (gb.spin_ns) __nanosleep(gb.spin_ns);
+  }
+}
+}  // namespace detail
+
+// V_TREE: HeteroSync atomic tree barrier (joinBarrier_helper,
+// Heterosync/cudaLocksBarrierAtomic.cu:145-170): when a group holds more than
+// one CTA, a local two-counter barrier, then group member 0 does the global
+// two-counter barrier, then the local barrier again.
+template <>
+__device__ __forceinline__ bool GridSync<V_TREE>::sync() {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const uint32_t idx = my_index();
+    const uint32_t G = gb.ngroups ? gb.ngroups : 1u;
+    const uint32_t g = idx % G;
+    const uint32_t member = idx / G;
+    const uint32_t gsz = detail::group_size(gb.nparticipants, G, g);
+    bool ok = true;
+    if (gsz > 1) {
+      ok = detail::tree_sub(&gb.groups[g].count, gsz, gb, episode) &&
+           detail::tree_sub(&gb.groups[g].count2, gsz, gb, episode);
+      if (ok && member == 0)
+        ok = detail::tree_sub(&gb.slot->count, G, gb, episode) &&
+             detail::tree_sub(&gb.slot->count2, G, gb, episode);
+      if (ok)
+        ok = detail::tree_sub(&gb.groups[g].count, gsz, gb, episode) &&
+             detail::tree_sub(&gb.groups[g].count2, gsz, gb, episode);
+    } else {
+      ok = detail::tree_sub(&gb.slot->count, gb.nparticipants < G ? gb.nparticipants : G, gb, episode) &&
+           detail::tree_sub(&gb.slot->count2, gb.nparticipants < G ? gb.nparticipants : G, gb, episode);
+    }
+    sh->ok = ok ? 1u : 0u;
+    ++episode;
+  }
+  __syncthreads();
+  return sh->ok != 0u;
+}
+
+// V_CCG: the library barrier.  Only valid under a cooperative launch, which the
+// host side always uses for this variant (it refuses a grid that is not
+// co-resident instead of hanging).
+template <>
+__device__ __forceinline__ bool GridSync<V_CCG>::sync() {
+  cooperative_groups::this_grid().sync();
+  return true;
+}
+
+}  // namespace gsrb

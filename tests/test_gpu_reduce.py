@@ -1,0 +1,62 @@
+"""Persistent reduce: bit-exact against the serial int64 oracle."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+VARIANTS = [0, 2, 3, 4, 5, 6, 7]
+
+
+def _reduce(gsrb, ctx, a, cfg=None, offset=0):
+    d = ctx.array(a.size + offset, np.int32)
+    if a.size:
+        buf = np.zeros(a.size + offset, np.int32)
+        buf[offset:] = a
+        d.upload(buf)
+    out = ctx.array(1, np.int64).zero()
+    import ctypes
+    view = type("V", (), {})()
+    view.ptr = d.ptr + 4 * offset
+    gsrb.check(ctx.reduce_i32(view, a.size, out, cfg), "reduce")
+    ctx.check_status("reduce")
+    return int(out.download()[0])
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_reduce_seeded_uniform(gsrb, ctx, orc, variant):
+    a = gsrb.uniform_i32(0x5EED2022, 1_000_003, 0, 127)
+    c = gsrb.cfg(variant=variant, ctas_per_sm=2, threads=256, cluster=2)
+    assert _reduce(gsrb, ctx, a, c) == orc.sum_i32(a)
+
+
+def test_reduce_full_config(gsrb, ctx, orc):
+    # 2^24 int32 U[0,127], grid 148 x 2 x 256 (configuration 1)
+    a = gsrb.uniform_i32(0x5EED2022, 1 << 24, 0, 127)
+    assert _reduce(gsrb, ctx, a) == orc.sum_i32(a)
+
+
+@pytest.mark.parametrize("n", [0, 1, 3, 4, 5, 255, 256, 257, 4096 + 7, 303_104])
+@pytest.mark.parametrize("offset", [0, 1, 3])
+def test_reduce_edge_sizes_and_alignment(gsrb, ctx, orc, n, offset):
+    a = gsrb.uniform_i32(n + 17, n, -1000, 1000)
+    assert _reduce(gsrb, ctx, a, offset=offset) == orc.sum_i32(a)
+
+
+def test_reduce_all_ones_reference_golden(gsrb, ctx):
+    # Reduce/test_reduce.cu:14-17
+    for n in (1, 1000, 303_104, 1 << 22):
+        assert _reduce(gsrb, ctx, np.ones(n, np.int32)) == n
+
+
+def test_reduce_int64_no_overflow(gsrb, ctx, orc):
+    a = np.full(1 << 21, 2**31 - 1, dtype=np.int32)
+    assert _reduce(gsrb, ctx, a) == (2**31 - 1) * (1 << 21)
+    b = np.full(1 << 20, -2**31, dtype=np.int32)
+    assert _reduce(gsrb, ctx, b) == -(2**31) * (1 << 20)
+
+
+@pytest.mark.parametrize("k,threads", [(1, 1024), (4, 128), (4, 256)])
+def test_reduce_other_shapes(gsrb, ctx, orc, k, threads):
+    a = gsrb.uniform_i32(99, 777_777, 0, 127)
+    c = gsrb.cfg(ctas_per_sm=k, threads=threads, cluster=2)
+    assert _reduce(gsrb, ctx, a, c) == orc.sum_i32(a)

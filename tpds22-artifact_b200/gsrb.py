@@ -1,0 +1,396 @@
+"""ctypes binding of libgsrb (the C ABI declared in include/gsrb.h).
+
+This is the Python face of the library used by the tests and by bench.py.  It
+loads the in-tree ``lib/libgsrb.so`` and fails loudly when it is missing: there
+is no CPU fallback for any operation.
+
+The Python names mirror the reference entry points where one exists:
+``reduce`` (Reduce/reduce.cuh:47), ``sum_scan_blelloch``
+(scan/scan.h:16-18), ``cudaLocksInit`` / ``cudaLocksDestroy``
+(Heterosync/cudaLocks.h:24-27) and the Lonestar ``gg_main`` applications
+(LONESTAR/apps/{bfs,sssp,pr}/kernel_gsrb.cu).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import pathlib
+
+import numpy as np
+
+PKG_DIR = pathlib.Path(__file__).resolve().parent
+LIB_PATH = PKG_DIR / "lib" / "libgsrb.so"
+
+# status codes (include/gsrb.h)
+OK = 0
+ERR_ARG = -1
+ERR_CUDA = -2
+ERR_NOT_CORESIDENT = -3
+ERR_TIMEOUT = -4
+ERR_NOMEM = -5
+ERR_STATE = -6
+ERR_UNSUPPORTED = -7
+ERR_OVERFLOW = -8
+ERR_LOCK_TIMEOUT = -9
+ERR_INVARIANT = -10
+
+# barrier variants
+BAR_CLUSTER = 0
+BAR_CLUSTER_ALLPOLL = 1
+BAR_DSMEM = 2
+BAR_SOFT2 = 3
+BAR_FLAT = 4
+BAR_TREE = 5
+BAR_CCG = 6
+BAR_CLUSTER_RED = 7
+BAR_NONE = 99
+VARIANT_NAMES = {
+    BAR_CLUSTER: "gsrb_cluster",
+    BAR_CLUSTER_ALLPOLL: "gsrb_cluster_allpoll",
+    BAR_DSMEM: "gsrb_dsmem",
+    BAR_SOFT2: "gsrb_soft2",
+    BAR_FLAT: "gcpusrb_flat",
+    BAR_TREE: "atomic_tree",
+    BAR_CCG: "ccg_grid_sync",
+    BAR_CLUSTER_RED: "gsrb_cluster_red",
+    BAR_NONE: "none",
+}
+
+
+class GsrbError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        msg = _lib().gsrb_status_string(status).decode() if _LIB is not None else str(status)
+        super().__init__(f"{what}: {msg} ({status})" if what else f"{msg} ({status})")
+
+
+class Cfg(C.Structure):
+    _fields_ = [
+        ("variant", C.c_int32),
+        ("cluster", C.c_int32),
+        ("ctas_per_sm", C.c_int32),
+        ("threads", C.c_int32),
+        ("fanin_groups", C.c_int32),
+        ("spin_ns", C.c_int32),
+        ("timeout_ms", C.c_uint32),
+        ("tile", C.c_int32),
+        ("grid_override", C.c_int32),
+        ("reserved", C.c_int32 * 7),
+    ]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
+
+
+class HostCSR(C.Structure):
+    _fields_ = [
+        ("nnodes", C.c_uint32),
+        ("_pad", C.c_uint32),
+        ("nedges", C.c_uint64),
+        ("row_start", C.POINTER(C.c_uint32)),
+        ("edge_dst", C.POINTER(C.c_uint32)),
+        ("edge_data", C.POINTER(C.c_int32)),
+    ]
+
+
+_LIB = None
+
+_P = C.c_void_p
+_SIGS = {
+    "gsrb_cfg_default": (None, [C.POINTER(Cfg)]),
+    "gsrb_status_string": (C.c_char_p, [C.c_int32]),
+    "gsrb_ctx_create": (C.c_int32, [C.c_int, C.POINTER(_P)]),
+    "gsrb_ctx_destroy": (C.c_int32, [_P]),
+    "gsrb_ctx_set_stream": (C.c_int32, [_P, _P]),
+    "gsrb_ctx_info": (C.c_int32, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
+    "gsrb_ctx_status": (C.c_int32, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "gsrb_ctx_synchronize": (C.c_int32, [_P]),
+    "gsrb_max_coresident": (C.c_int32, [_P, C.POINTER(Cfg), C.c_int32, C.POINTER(C.c_int32)]),
+    "gsrb_malloc": (C.c_int32, [C.POINTER(_P), C.c_size_t]),
+    "gsrb_free": (C.c_int32, [_P]),
+    "gsrb_host_alloc": (C.c_int32, [C.POINTER(_P), C.c_size_t]),
+    "gsrb_host_free": (C.c_int32, [_P]),
+    "gsrb_memcpy_h2d": (C.c_int32, [_P, _P, _P, C.c_size_t]),
+    "gsrb_memcpy_d2h": (C.c_int32, [_P, _P, _P, C.c_size_t]),
+    "gsrb_memset": (C.c_int32, [_P, _P, C.c_int, C.c_size_t]),
+    "gsrb_event_record": (C.c_int32, [_P, C.c_int32]),
+    "gsrb_event_elapsed_ms": (C.c_int32, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_float)]),
+    "gsrb_l2_flush": (C.c_int32, [_P]),
+    "gsrb_launch_count": (C.c_uint64, []),
+    "gsrb_barrier_bench": (C.c_int32, [_P, C.POINTER(Cfg), C.c_int32, C.c_int32, _P, _P]),
+    "gsrb_barrier_litmus": (C.c_int32, [_P, C.POINTER(Cfg), C.c_int32, _P, _P]),
+    "gsrb_barrier_fault_short_grid": (C.c_int32, [_P, C.POINTER(Cfg)]),
+    "gsrb_reduce_i32": (C.c_int32, [_P, _P, C.c_size_t, _P, C.POINTER(Cfg)]),
+    "gsrb_probe_l2_atomics": (C.c_int32, [_P, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_float)]),
+    "gsrb_host_csr_free": (None, [C.POINTER(HostCSR)]),
+    "gsrb_gen_uniform_i32": (C.c_int32, [C.c_uint64, C.c_size_t, C.c_int32, C.c_int32, _P]),
+    "gsrb_gen_uniform_f32": (C.c_int32, [C.c_uint64, C.c_size_t, _P]),
+    "gsrb_edge_weight": (C.c_uint32, [C.c_uint32, C.c_uint32, C.c_uint64, C.c_int32, C.c_int32]),
+    "gsrb_csr_from_edges": (C.c_int32, [C.c_uint32, C.c_uint64, _P, _P, C.c_int, C.c_uint64, C.c_int32,
+                                        C.c_int32, C.POINTER(HostCSR)]),
+    "gsrb_gen_rmat": (C.c_int32, [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_uint64,
+                                  C.c_int32, C.c_int32, C.POINTER(HostCSR)]),
+    "gsrb_gen_grid2d": (C.c_int32, [C.c_int32, C.c_int32, C.c_uint64, C.c_int32, C.c_int32,
+                                    C.POINTER(HostCSR)]),
+    "gsrb_gr_read": (C.c_int32, [C.c_char_p, C.POINTER(HostCSR)]),
+    "gsrb_gr_write": (C.c_int32, [C.c_char_p, C.POINTER(HostCSR), C.c_int32]),
+}
+
+
+def _lib():
+    global _LIB
+    if _LIB is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(
+                f"libgsrb.so not built ({LIB_PATH}); run `make -C tpds22-artifact_b200` "
+                "or __graft_entry__.build() -- there is no CPU fallback")
+        lib = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = lib
+    return _LIB
+
+
+def register(name, restype, argtypes):
+    """Declare an additional entry point's signature (used by later modules)."""
+    _SIGS[name] = (restype, argtypes)
+    if _LIB is not None:
+        fn = getattr(_LIB, name)
+        fn.restype = restype
+        fn.argtypes = argtypes
+
+
+def lib():
+    return _lib()
+
+
+def check(st: int, what: str = ""):
+    if st != OK:
+        raise GsrbError(st, what)
+
+
+def cfg(**kw) -> Cfg:
+    c = Cfg()
+    _lib().gsrb_cfg_default(C.byref(c))
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+class DeviceArray:
+    """A device allocation with a numpy dtype and shape (plumbing only)."""
+
+    def __init__(self, ctx: "Context", shape, dtype):
+        self.ctx = ctx
+        self.dtype = np.dtype(dtype)
+        self.shape = (shape,) if np.isscalar(shape) else tuple(shape)
+        self.size = int(np.prod(self.shape)) if self.shape else 1
+        self.nbytes = self.size * self.dtype.itemsize
+        p = C.c_void_p()
+        check(_lib().gsrb_malloc(C.byref(p), max(self.nbytes, 1)), "gsrb_malloc")
+        self.ptr = p.value
+
+    def upload(self, a: np.ndarray):
+        a = np.ascontiguousarray(a, dtype=self.dtype)
+        assert a.nbytes <= self.nbytes
+        check(_lib().gsrb_memcpy_h2d(self.ctx.h, self.ptr, _ptr(a), a.nbytes), "h2d")
+        self.ctx.sync()
+        return self
+
+    def download(self, n=None) -> np.ndarray:
+        n = self.size if n is None else n
+        out = np.empty(n, dtype=self.dtype)
+        check(_lib().gsrb_memcpy_d2h(self.ctx.h, _ptr(out), self.ptr, out.nbytes), "d2h")
+        self.ctx.sync()
+        return out
+
+    def zero(self):
+        check(_lib().gsrb_memset(self.ctx.h, self.ptr, 0, self.nbytes), "memset")
+        return self
+
+    def free(self):
+        if self.ptr:
+            _lib().gsrb_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Context:
+    """One device context (stream, barrier state, scratch)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(_lib().gsrb_ctx_create(device, C.byref(h)), "gsrb_ctx_create")
+        self.h = h.value
+        n = C.c_int32()
+        l2 = C.c_int64()
+        d = C.c_int32()
+        check(_lib().gsrb_ctx_info(self.h, C.byref(n), C.byref(l2), C.byref(d)))
+        self.num_sms = n.value
+        self.l2_bytes = l2.value
+        self.device = d.value
+
+    def close(self):
+        if self.h:
+            _lib().gsrb_ctx_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- plumbing ---------------------------------------------------------
+    def array(self, shape, dtype) -> DeviceArray:
+        return DeviceArray(self, shape, dtype)
+
+    def to_device(self, a: np.ndarray) -> DeviceArray:
+        d = DeviceArray(self, a.shape, a.dtype)
+        return d.upload(a)
+
+    def sync(self):
+        check(_lib().gsrb_ctx_synchronize(self.h), "synchronize")
+
+    def status(self):
+        code = C.c_uint32()
+        where = C.c_uint32()
+        who = C.c_uint32()
+        st = _lib().gsrb_ctx_status(self.h, C.byref(code), C.byref(where), C.byref(who))
+        return st, code.value, where.value, who.value
+
+    def check_status(self, what=""):
+        st, code, where, who = self.status()
+        if st != OK:
+            raise GsrbError(st, f"{what} (device code {code}, episode {where}, block {who})")
+
+    def record(self, slot: int):
+        check(_lib().gsrb_event_record(self.h, slot))
+
+    def elapsed_ms(self, a: int, b: int) -> float:
+        ms = C.c_float()
+        check(_lib().gsrb_event_elapsed_ms(self.h, a, b, C.byref(ms)))
+        return ms.value
+
+    def l2_flush(self):
+        check(_lib().gsrb_l2_flush(self.h), "l2_flush")
+
+    def max_coresident(self, c: Cfg, family: int) -> int:
+        n = C.c_int32()
+        st = _lib().gsrb_max_coresident(self.h, C.byref(c), family, C.byref(n))
+        check(st, "max_coresident")
+        return n.value
+
+    # -- barrier ------------------------------------------------------------
+    def barrier_bench(self, c: Cfg, episodes: int, fma: int, sink: DeviceArray, count: DeviceArray) -> int:
+        return _lib().gsrb_barrier_bench(self.h, C.byref(c), episodes, fma, sink.ptr, count.ptr)
+
+    def barrier_litmus(self, c: Cfg, episodes: int, buf: DeviceArray, stale: DeviceArray) -> int:
+        return _lib().gsrb_barrier_litmus(self.h, C.byref(c), episodes, buf.ptr, stale.ptr)
+
+    def barrier_fault_short_grid(self, c: Cfg) -> int:
+        return _lib().gsrb_barrier_fault_short_grid(self.h, C.byref(c))
+
+    def probe_l2_atomics(self, ctas: int, iters: int, mode: int) -> float:
+        ms = C.c_float()
+        check(_lib().gsrb_probe_l2_atomics(self.h, ctas, iters, mode, C.byref(ms)), "probe")
+        return ms.value
+
+    # -- reduce ----------------------------------------------------------------
+    def reduce_i32(self, d_in: DeviceArray, n: int, d_out: DeviceArray, c: Cfg | None = None) -> int:
+        return _lib().gsrb_reduce_i32(self.h, d_in.ptr, n, d_out.ptr, C.byref(c) if c is not None else None)
+
+
+def launch_count() -> int:
+    return int(_lib().gsrb_launch_count())
+
+
+# ---- host-side inputs -------------------------------------------------------
+def uniform_i32(seed: int, n: int, lo: int, hi: int) -> np.ndarray:
+    out = np.empty(n, dtype=np.int32)
+    check(_lib().gsrb_gen_uniform_i32(seed, n, lo, hi, _ptr(out)), "gen_uniform_i32")
+    return out
+
+
+def uniform_f32(seed: int, n: int) -> np.ndarray:
+    out = np.empty(n, dtype=np.float32)
+    check(_lib().gsrb_gen_uniform_f32(seed, n, _ptr(out)), "gen_uniform_f32")
+    return out
+
+
+class Graph:
+    """Host CSR graph (numpy copies of the library-owned arrays)."""
+
+    def __init__(self, row_start: np.ndarray, edge_dst: np.ndarray, edge_data: np.ndarray):
+        self.row_start = np.ascontiguousarray(row_start, dtype=np.uint32)
+        self.edge_dst = np.ascontiguousarray(edge_dst, dtype=np.uint32)
+        self.edge_data = np.ascontiguousarray(edge_data, dtype=np.int32)
+        self.nnodes = len(self.row_start) - 1
+        self.nedges = len(self.edge_dst)
+
+    @staticmethod
+    def _from_host(h: HostCSR) -> "Graph":
+        n, m = h.nnodes, h.nedges
+        row = np.ctypeslib.as_array(h.row_start, shape=(n + 1,)).copy()
+        dst = np.ctypeslib.as_array(h.edge_dst, shape=(max(m, 1),))[:m].copy()
+        w = np.ctypeslib.as_array(h.edge_data, shape=(max(m, 1),))[:m].copy()
+        _lib().gsrb_host_csr_free(C.byref(h))
+        return Graph(row, dst, w)
+
+    def _as_host(self) -> HostCSR:
+        h = HostCSR()
+        h.nnodes = self.nnodes
+        h.nedges = self.nedges
+        h.row_start = self.row_start.ctypes.data_as(C.POINTER(C.c_uint32))
+        h.edge_dst = self.edge_dst.ctypes.data_as(C.POINTER(C.c_uint32))
+        h.edge_data = self.edge_data.ctypes.data_as(C.POINTER(C.c_int32))
+        return h
+
+    def degrees(self) -> np.ndarray:
+        return np.diff(self.row_start.astype(np.int64))
+
+    def write_gr(self, path, with_weights=True):
+        h = self._as_host()
+        check(_lib().gsrb_gr_write(os.fsencode(str(path)), C.byref(h), 1 if with_weights else 0), "gr_write")
+
+    @staticmethod
+    def read_gr(path) -> "Graph":
+        h = HostCSR()
+        check(_lib().gsrb_gr_read(os.fsencode(str(path)), C.byref(h)), "gr_read")
+        return Graph._from_host(h)
+
+
+def rmat(scale: int, edgefactor: int = 16, a=0.57, b=0.19, c=0.19, seed=0x5EED2022, wlo=1, whi=255) -> Graph:
+    h = HostCSR()
+    check(_lib().gsrb_gen_rmat(scale, edgefactor, a, b, c, seed, wlo, whi, C.byref(h)), "gen_rmat")
+    return Graph._from_host(h)
+
+
+def grid2d(width: int, height: int, seed=0x5EED2022, wlo=1, whi=1000) -> Graph:
+    h = HostCSR()
+    check(_lib().gsrb_gen_grid2d(width, height, seed, wlo, whi, C.byref(h)), "gen_grid2d")
+    return Graph._from_host(h)
+
+
+def csr_from_edges(n: int, src, dst, symmetrize=True, weight_seed=1, wlo=1, whi=255) -> Graph:
+    src = np.ascontiguousarray(src, dtype=np.uint32)
+    dst = np.ascontiguousarray(dst, dtype=np.uint32)
+    h = HostCSR()
+    check(_lib().gsrb_csr_from_edges(n, len(src), _ptr(src), _ptr(dst), 1 if symmetrize else 0, weight_seed,
+                                     wlo, whi, C.byref(h)), "csr_from_edges")
+    return Graph._from_host(h)
+
+
+def edge_weight(u: int, v: int, seed: int, lo: int, hi: int) -> int:
+    return int(_lib().gsrb_edge_weight(u, v, seed, lo, hi))
