@@ -51,7 +51,8 @@ enum {
   GSRB_BAR_FLAT = 4,             /* reference GCPUSRB: one counter for all CTAs */
   GSRB_BAR_TREE = 5,             /* HeteroSync atomic tree barrier (paper baseline) */
   GSRB_BAR_CCG = 6,              /* cooperative_groups grid.sync() (library baseline) */
-  GSRB_BAR_CLUSTER_RED = 7,      /* 3-level with red.release arrivals and a polling master */
+  GSRB_BAR_CLUSTER_RED = 7,      /* 3-level, completer-publishes protocol (red.release arrivals, polling master) */
+  GSRB_BAR_FLIP = 8,             /* 2-level: every CTA arrives on the split sum-to-flip words */
   GSRB_BAR_NONE = 99             /* no barrier (phase-only timing baseline) */
 };
 
@@ -66,7 +67,9 @@ typedef struct gsrb_cfg {
   uint32_t timeout_ms;   /* per-wait device deadline */
   int32_t tile;          /* elements per tile / segment hint (0 = auto) */
   int32_t grid_override; /* exact grid size (0 = ctas_per_sm * #SMs) */
-  int32_t reserved[7];
+  int32_t launch_mode;   /* 0 = cooperative launch when the driver accepts it, 1 = plain launch (default)
+                            (both only after the co-residency check; CCG is always cooperative) */
+  int32_t reserved[6];
 } gsrb_cfg_t;
 
 void gsrb_cfg_default(gsrb_cfg_t* cfg);
@@ -137,6 +140,120 @@ gsrb_status_t gsrb_probe_l2_atomics(gsrb_ctx_t ctx, int32_t ctas, int32_t iters,
  * (API Reduce/reduce.cuh:47).  Asynchronous. */
 gsrb_status_t gsrb_reduce_i32(gsrb_ctx_t ctx, const int32_t* d_in, size_t n, int64_t* d_out,
                               const gsrb_cfg_t* cfg);
+
+/* ---- scan --------------------------------------------
+ * Exclusive prefix sum, one persistent launch (default one 1024-thread CTA per
+ * SM, 96 KiB tiles double-buffered in shared memory, moved by cp.async.bulk),
+ * one grid barrier per segment of #CTAs tiles.  uint32 wraps around like the
+ * reference's cpu_sum_scan; the FP32 variant keeps tile offsets in FP64.
+ * In-place (d_in == d_out) is allowed.  Replaces gpu_prescan /
+ * sum_scan_blelloch of scan/scan_gsrb.cu:486-804 (API scan/scan.h:16-18).
+ * Asynchronous. */
+gsrb_status_t gsrb_scan_u32(gsrb_ctx_t ctx, const uint32_t* d_in, uint32_t* d_out, size_t n,
+                            const gsrb_cfg_t* cfg);
+gsrb_status_t gsrb_scan_f32(gsrb_ctx_t ctx, const float* d_in, float* d_out, size_t n, const gsrb_cfg_t* cfg);
+
+/* ---- lock state, mutexes and semaphores (the Heterosync cudaLocks layer) -------
+ * The reference-named host API (cudaLocksInit, cudaMutexCreate*, ...) is in
+ * gsrb/cudaLocks.h and the device API in gsrb/cudaLocks.cuh; these are the
+ * context-scoped equivalents (no global instance). */
+typedef struct gsrb_lock_data {  /* device pointers, layout of cudaLockData_t (Heterosync/cudaLocks.h:4-17) */
+  int32_t maxBufferSize;
+  int32_t arrayStride;
+  int32_t mutexCount;
+  int32_t semaphoreCount;
+  uint32_t* barrierBuffers;
+  int32_t* mutexBuffers;
+  uint32_t* mutexBufferHeads;
+  uint32_t* mutexBufferTails;
+  uint32_t* semaphoreBuffers;
+} gsrb_lock_data_t;
+typedef struct gsrb_locks* gsrb_locks_t;
+
+/* Allocates and initialises lock state like cudaLocksInit (Heterosync/cudaLocks.cu:3-87). */
+gsrb_status_t gsrb_locks_create(gsrb_ctx_t ctx, int32_t maxBlocks, int32_t numMutexes, int32_t numSemaphores,
+                                int32_t numSM, gsrb_locks_t* out);
+gsrb_status_t gsrb_locks_destroy(gsrb_locks_t locks);
+gsrb_status_t gsrb_locks_data(gsrb_locks_t locks, gsrb_lock_data_t* out);
+/* Semaphore record of cudaSemaphoreCreateSpin (Heterosync/cudaLocksSemaphoreSpin.cu:6-29). */
+gsrb_status_t gsrb_semaphore_init(gsrb_locks_t locks, int32_t semNum, uint32_t count, int32_t numSM);
+/* Synchronous: first status code recorded by a bounded lock wait (cleared). */
+gsrb_status_t gsrb_locks_status(gsrb_locks_t locks, uint32_t* code);
+
+/* Semaphore kinds for gsrb_semaphore_bench. */
+enum {
+  GSRB_SEM_REF_SPIN = 0,          /* reference spin semaphore protocol (lock word + count) */
+  GSRB_SEM_REF_EBO = 1,           /* ... with exponential backoff */
+  GSRB_SEM_REF_PRIORITY = 2,      /* reference TPDS'22 priority semaphore protocol */
+  GSRB_SEM_REF_PRIORITY_EBO = 3,  /* ... with exponential backoff */
+  GSRB_SEM_PRIORITY = 4           /* B200-native priority semaphore (wait-free posts, writer queue) */
+};
+/* Mutex kinds for gsrb_mutex_bench. */
+enum { GSRB_MUTEX_SPIN = 0, GSRB_MUTEX_EBO = 1, GSRB_MUTEX_FA = 2, GSRB_MUTEX_SLEEP = 3 };
+
+/* Semaphore microbenchmark: grid = cfg CTAs; CTA b is a
+ * writer when b % writer_every == 0; each CTA acquires `iters` times and adds 1
+ * to a shared counter `incs` times per acquire (writers: plain read-modify-write
+ * of W; readers: atomic add to R).  d_counters: 8 uint32, zeroed by the caller:
+ * [W, R, inside, max_readers, violations, acquires, timeouts, 0].  Synchronous.
+ * Reference: kernelSpinLockSemaphorePriority, Heterosync/main.cu:962-1040. */
+gsrb_status_t gsrb_semaphore_bench(gsrb_ctx_t ctx, const gsrb_cfg_t* cfg, int32_t kind, uint32_t capacity,
+                                   int32_t writer_every, int32_t iters, int32_t incs, uint32_t* d_counters);
+/* Mutex microbenchmark: every CTA locks `iters` times and adds 1 to W `incs`
+ * times with a plain read-modify-write.  Same counter layout.  Synchronous.
+ * Reference: kernelSpinLockMutex / EBO / FA / Sleep, Heterosync/main.cu:574-700. */
+gsrb_status_t gsrb_mutex_bench(gsrb_ctx_t ctx, const gsrb_cfg_t* cfg, int32_t kind, int32_t iters, int32_t incs,
+                               uint32_t* d_counters);
+
+/* ---- graph traversals (BASELINE configurations 4 and 5) -------------------------
+ * A gsrb_graph_t is a device CSR (row_start[n+1], edge_dst[m], edge_data[m]:
+ * the reference CSRGraph layout) plus the traversal scratch (queues, marks,
+ * counters, per-level trace ring).  Traversals are synchronous and return
+ * statistics.  Replaces the gg_main of LONESTAR/apps/{bfs,sssp,pr}/kernel_gsrb.cu
+ * (bfs :712-730, sssp :791-820, pr :683-715). */
+typedef struct gsrb_graph* gsrb_graph_t;
+typedef struct gsrb_host_csr gsrb_host_csr_t;  /* defined with the host-side graph section below */
+typedef struct gsrb_traversal_stats {
+  uint32_t levels;        /* BFS levels / SSSP relax rounds / PR iterations */
+  uint32_t aux;           /* BFS (learned): first level that fell back to the heuristic (0 = none);
+                             SSSP: buckets */
+  uint32_t decisions;     /* BFS (learned): levels decided by the policy network */
+  uint32_t trace_records; /* per-level trace records available (gsrb_graph_trace) */
+  uint64_t edges;         /* BFS: out-edges of reached vertices (the TEPS numerator);
+                             SSSP: edges relaxed */
+  float kernel_ms;        /* CUDA-event time of the traversal launch */
+  uint32_t _pad;
+} gsrb_traversal_stats_t;
+
+/* BFS direction modes. */
+enum {
+  GSRB_BFS_PUSH = 0,      /* worklist push every level (the reference's data-driven BFS) */
+  GSRB_BFS_HEURISTIC = 1, /* direction-optimizing with the fixed Beamer thresholds (alpha 15, beta 18) */
+  GSRB_BFS_LEARNED = 2,   /* the policy network decides; falls back to the heuristic after a 2x miss */
+  GSRB_BFS_PULL = 3,      /* pull every level after the first (trace collection) */
+  GSRB_BFS_TOPO = 4       /* topology-driven push every level (trace collection) */
+};
+
+/* Copy a host CSR to the device (owned by the graph). */
+gsrb_status_t gsrb_graph_upload(gsrb_ctx_t ctx, const gsrb_host_csr_t* h, gsrb_graph_t* out);
+/* Wrap caller-owned device CSR arrays (not freed by gsrb_graph_free). */
+gsrb_status_t gsrb_graph_wrap(gsrb_ctx_t ctx, uint32_t n, uint64_t m, const uint32_t* d_row,
+                              const uint32_t* d_dst, const int32_t* d_w, gsrb_graph_t* out);
+gsrb_status_t gsrb_graph_free(gsrb_graph_t g);
+gsrb_status_t gsrb_graph_info(gsrb_graph_t g, uint32_t* n, uint64_t* m, uint32_t* nhubs);
+/* Policy network weights (gsrb_mlp_* layout, gsrb_mlp_param_count() floats). */
+gsrb_status_t gsrb_graph_set_policy(gsrb_graph_t g, const float* h_weights, size_t count);
+/* Copy up to max_records 48-byte per-level trace records of the last traversal. */
+gsrb_status_t gsrb_graph_trace(gsrb_graph_t g, void* h_out, uint32_t max_records, uint32_t* records);
+/* BFS levels from src into d_level (int32[n]; INT32_MAX = unreachable). */
+gsrb_status_t gsrb_bfs(gsrb_ctx_t ctx, gsrb_graph_t g, uint32_t src, int32_t* d_level, int32_t mode,
+                       const gsrb_cfg_t* cfg, gsrb_traversal_stats_t* stats);
+/* SSSP distances (near-far buckets of width delta) into d_dist (int32[n]). */
+gsrb_status_t gsrb_sssp(gsrb_ctx_t ctx, gsrb_graph_t g, uint32_t src, int32_t* d_dist, int32_t delta,
+                        const gsrb_cfg_t* cfg, gsrb_traversal_stats_t* stats);
+/* Pull PageRank: x0 = 1 - alpha, `iters` iterations of x = (1-alpha) + alpha * sum x_u/deg(u). */
+gsrb_status_t gsrb_pagerank(gsrb_ctx_t ctx, gsrb_graph_t g, float alpha, int32_t iters, float* d_rank,
+                            const gsrb_cfg_t* cfg, gsrb_traversal_stats_t* stats);
 
 /* ---- host-side graphs and synthetic inputs ----------------------------------------
  * CSR in the layout of the reference CSRGraph (row_start[n+1], edge_dst[m],

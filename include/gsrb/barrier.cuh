@@ -56,7 +56,8 @@ enum Variant : int {
   V_TREE = 5,            // HeteroSync atomic tree barrier (two counters per level)
   V_CCG = 6,             // cooperative_groups::this_grid().sync()
   V_CLUSTER_RED = 7,     // HW cluster barrier -> red.release arrivals, master polls count
-  V_COUNT = 8
+  V_FLIP = 8,            // no cluster level: every CTA arrives on the split flip words
+  V_COUNT = 9
 };
 
 // One global barrier slot: four 128-byte lines so that the arrival counter, the
@@ -94,6 +95,9 @@ struct GridBarrier {
   uint32_t ngroups;       // global fan-in groups (0 = arrive directly at the root)
   uint32_t spin_ns;       // __nanosleep between polls (0 = hot spin)
   uint64_t timeout_ns;    // per-wait deadline
+  uint32_t* flip;         // flip words of the native variants (word r at flip[32 r])
+  uint32_t nflip;         // number of flip words in use (0 or 1 = one word)
+  uint32_t _pad;
 };
 
 // Shared-memory words a CTA needs for the cluster / DSMEM levels.
@@ -180,6 +184,69 @@ __device__ __forceinline__ bool global_arrive_atom(const GridBarrier& gb, uint32
   return true;
 }
 
+// ---- split "sum-to-flip" global level (the native variants) -----------------
+// R flip words (R = max(1, nflip)), each on its own 128-byte line of the
+// slot's flip area (separate from the counters of the other protocols).
+// Arrival unit idx of n adds to word r = idx % R: the first unit of each word
+// adds 0x80000000 - (count_r - 1), every other unit adds 1, so the word's top
+// bit toggles exactly when its last arrival lands and its low bits return to
+// their old value -- no completer, no reset store, and the arrivals are
+// fire-and-forget `red.release.gpu.add`.  Splitting the arrivals over R words
+// divides the same-address serialisation at the L2 by R.  A waiter knows the
+// sense it waits for (it toggles once per episode) and polls every word that
+// has not flipped yet with `ld.acquire.gpu`.
+__device__ __forceinline__ uint32_t* flip_word(const GridBarrier& gb, uint32_t r) { return gb.flip + r * 32u; }
+__device__ __forceinline__ uint32_t flip_words(const GridBarrier& gb) { return gb.nflip ? gb.nflip : 1u; }
+
+__device__ __forceinline__ void flip_arrive(const GridBarrier& gb, uint32_t idx, uint32_t n) {
+  const uint32_t R = flip_words(gb) < n ? flip_words(gb) : n;
+  const uint32_t r = idx % R;
+  const uint32_t cnt = group_size(n, R, r);
+  const uint32_t inc = (idx == r) ? (0x80000000u - (cnt - 1u)) : 1u;
+  ptx::red_add_release_gpu(flip_word(gb, r), inc);
+}
+
+// Wait until every word in use has top bit == sense.  Bounded.
+__device__ __forceinline__ bool flip_wait(const GridBarrier& gb, uint32_t n, uint32_t sense, uint32_t episode) {
+  const uint32_t R = flip_words(gb) < n ? flip_words(gb) : n;
+  uint64_t t0 = 0;
+  if (R == 1) {
+    const uint32_t* w = flip_word(gb, 0);
+    for (uint32_t it = 0;; ++it) {
+      if ((ptx::ld_acquire_gpu(w) >> 31) == sense) return true;
+      if ((it & 31u) == 31u) {
+        if (ptx::ld_relaxed_gpu(&gb.slot->status) != 0u) return false;
+        const uint64_t now = ptx::globaltimer_ns();
+        if (t0 == 0) t0 = now;
+        else if (now - t0 > gb.timeout_ns) {
+          record_error(gb, GSRB_DEV_TIMEOUT, episode);
+          return false;
+        }
+      }
+      if (gb.spin_ns) __nanosleep(gb.spin_ns);
+    }
+  }
+  uint32_t next = 0;  // words below `next` have flipped
+  for (uint32_t it = 0;; ++it) {
+    while (next < R && (ptx::ld_acquire_gpu(flip_word(gb, next)) >> 31) == sense) ++next;
+    if (next == R) return true;
+    if ((it & 31u) == 31u) {
+      if (ptx::ld_relaxed_gpu(&gb.slot->status) != 0u) return false;
+      const uint64_t now = ptx::globaltimer_ns();
+      if (t0 == 0) t0 = now;
+      else if (now - t0 > gb.timeout_ns) {
+        record_error(gb, GSRB_DEV_TIMEOUT, episode);
+        return false;
+      }
+    }
+    if (gb.spin_ns) __nanosleep(gb.spin_ns);
+  }
+}
+
+__device__ __forceinline__ uint32_t flip_sense0(const GridBarrier& gb) {
+  return ptx::ld_acquire_gpu(flip_word(gb, 0)) >> 31;
+}
+
 // Global level, red flavour: arrivals are fire-and-forget `red.release.gpu.add`;
 // participant 0 polls the counter, resets it and bumps the epoch.
 __device__ __forceinline__ bool global_arrive_red(const GridBarrier& gb, uint32_t idx,
@@ -204,6 +271,7 @@ struct GridSync {
   BarrierShared* sh;
   uint32_t epoch;    // meaningful in thread 0
   uint32_t episode;  // meaningful in thread 0
+  uint32_t sense;    // flip variants: top bit the next episode waits for (thread 0)
 
   // Index of this CTA among the participants and of its arrival unit.
   __device__ __forceinline__ uint32_t my_index() const { return blockIdx.x - gb.first_cta; }
@@ -218,8 +286,10 @@ struct GridSync {
     episode = 0;
     if (threadIdx.x == 0) {
       epoch = ptx::ld_acquire_gpu(&gb.slot->epoch);
+      sense = (V == V_CLUSTER || V == V_CLUSTER_ALLPOLL || V == V_DSMEM || V == V_FLIP)
+                  ? (detail::flip_sense0(gb) ^ 1u) : 0u;
       sh->arrive = 0;
-      sh->release = epoch;
+      sh->release = 0;
       sh->ok = 0;
     }
     if (V == V_CLUSTER || V == V_CLUSTER_ALLPOLL || V == V_DSMEM || V == V_CLUSTER_RED) {
@@ -251,30 +321,29 @@ struct GridSync {
 
 // ---------------------------------------------------------------------------
 // V_CLUSTER: level 2 = hardware cluster barrier; level 3 = the cluster leader's
-// thread 0 arrives (optionally through fan-in groups) and waits for the epoch;
-// the cluster is released by a second hardware cluster barrier.  The leader
-// writes the verdict into every peer's shared memory before releasing them.
+// thread 0 arrives on the split flip words and waits for them; the cluster is
+// released by a second hardware cluster barrier.  The leader writes the verdict
+// into every peer's shared memory before releasing them.
 template <>
 __device__ __forceinline__ bool GridSync<V_CLUSTER>::sync() {
   ptx::cluster_sync();
-  const uint32_t crank = ptx::cluster_ctarank();
-  if (crank == 0 && threadIdx.x == 0) {
-    const uint32_t ncl = gb.nparticipants / ptx::cluster_nctarank();
-    const uint32_t cid = my_index() / ptx::cluster_nctarank();
-    bool ok = true;
-    if (!detail::global_arrive_atom(gb, cid, ncl, epoch))
-      ok = detail::wait_ne(&gb.slot->epoch, epoch, gb, episode);
+  if (ptx::cluster_ctarank() == 0 && threadIdx.x == 0) {
     const uint32_t n = ptx::cluster_nctarank();
+    const uint32_t ncl = gb.nparticipants / n;
+    detail::flip_arrive(gb, my_index() / n, ncl);
+    const bool ok = detail::flip_wait(gb, ncl, sense, episode);
     const uint32_t sa = ptx::smem_u32(&sh->ok);
     for (uint32_t r = 0; r < n; ++r) ptx::st_cluster_relaxed_u32(ptx::mapa_shared(sa, r), ok ? 1u : 0u);
   }
   ptx::cluster_sync();
-  if (threadIdx.x == 0) { ++epoch; ++episode; }
+  if (threadIdx.x == 0) { sense ^= 1u; ++episode; }
   return sh->ok != 0u;
 }
 
-// V_CLUSTER_RED: as V_CLUSTER but arrivals are `red.release.gpu.add` and the
-// leader of cluster 0 polls the counter and publishes the new epoch.
+// V_CLUSTER_RED: the completer-publishes protocol with clusters: hardware
+// cluster barrier, `red.release.gpu.add` arrivals on one counter, the leader of
+// cluster 0 polls the counter, resets it and bumps the epoch; a second hardware
+// cluster barrier releases the clusters.
 template <>
 __device__ __forceinline__ bool GridSync<V_CLUSTER_RED>::sync() {
   ptx::cluster_sync();
@@ -294,7 +363,7 @@ __device__ __forceinline__ bool GridSync<V_CLUSTER_RED>::sync() {
 }
 
 // V_CLUSTER_ALLPOLL: one hardware cluster barrier for arrival; the leader
-// arrives globally; every CTA's thread 0 then polls the epoch itself.  The
+// arrives on the flip words; every CTA's thread 0 then polls them itself.  The
 // verdict is per CTA (not cluster-uniform), so a kernel using this variant must
 // keep calling sync() the same number of times on every CTA even after a
 // failure (the library's kernels only use it in fixed-count loops).
@@ -302,38 +371,32 @@ template <>
 __device__ __forceinline__ bool GridSync<V_CLUSTER_ALLPOLL>::sync() {
   ptx::cluster_sync();
   if (threadIdx.x == 0) {
-    bool ok = true;
-    bool done = false;
-    if (ptx::cluster_ctarank() == 0) {
-      const uint32_t ncl = gb.nparticipants / ptx::cluster_nctarank();
-      const uint32_t cid = my_index() / ptx::cluster_nctarank();
-      done = detail::global_arrive_atom(gb, cid, ncl, epoch);
-    }
-    if (!done) ok = detail::wait_ne(&gb.slot->epoch, epoch, gb, episode);
-    sh->ok = ok ? 1u : 0u;
-    ++epoch;
+    const uint32_t n = ptx::cluster_nctarank();
+    const uint32_t ncl = gb.nparticipants / n;
+    if (ptx::cluster_ctarank() == 0) detail::flip_arrive(gb, my_index() / n, ncl);
+    sh->ok = detail::flip_wait(gb, ncl, sense, episode) ? 1u : 0u;
+    sense ^= 1u;
     ++episode;
   }
   __syncthreads();
   return sh->ok != 0u;
 }
 
-// V_DSMEM: every CTA's thread 0 adds one to the leader's shared-memory arrival
-// counter (red.release.cluster); the leader polls it, arrives globally, waits,
-// and writes the new epoch into every peer's release word; peers poll their own
-// shared memory.  No hardware cluster barrier per episode.
+// V_DSMEM: no hardware cluster barrier per episode.  Every non-leader CTA's
+// thread 0 adds one to the leader's shared-memory arrival counter
+// (red.release.cluster); the leader polls its own shared memory, arrives on the
+// flip words, waits, and stores (episode + 1, top bit = failure) into every
+// peer's release word (st.release.cluster); peers poll their own shared memory.
 template <>
 __device__ __forceinline__ bool GridSync<V_DSMEM>::sync() {
   __syncthreads();
   if (threadIdx.x == 0) {
     const uint32_t n = ptx::cluster_nctarank();
-    const uint32_t crank = ptx::cluster_ctarank();
-    const uint32_t next = epoch + 1u;
+    const uint32_t msg_ok = (episode + 1u) & 0x7fffffffu;
     bool ok = true;
-    if (crank == 0) {
-      // wait for the n-1 peers (bounded; a shared-memory poll)
+    if (ptx::cluster_ctarank() == 0) {
       uint64_t t0 = 0;
-      for (uint32_t it = 0;; ++it) {
+      for (uint32_t it = 0;; ++it) {  // the n-1 peers (bounded shared-memory poll)
         if (ptx::ld_shared_acquire_cluster_u32(&sh->arrive) == n - 1u) break;
         if ((it & 255u) == 255u) {
           if (ptx::ld_relaxed_gpu(&gb.slot->status) != 0u) { ok = false; break; }
@@ -347,28 +410,25 @@ __device__ __forceinline__ bool GridSync<V_DSMEM>::sync() {
         }
       }
       sh->arrive = 0;
+      const uint32_t ncl = gb.nparticipants / n;
       if (ok) {
-        const uint32_t ncl = gb.nparticipants / n;
-        const uint32_t cid = my_index() / n;
-        if (!detail::global_arrive_atom(gb, cid, ncl, epoch))
-          ok = detail::wait_ne(&gb.slot->epoch, epoch, gb, episode);
+        detail::flip_arrive(gb, my_index() / n, ncl);
+        ok = detail::flip_wait(gb, ncl, sense, episode);
       }
-      // broadcast: ok -> next epoch; failure -> next epoch with the top bit set
-      const uint32_t msg = ok ? next : (next | 0x80000000u);
+      const uint32_t msg = ok ? msg_ok : (msg_ok | 0x80000000u);
       const uint32_t sa = ptx::smem_u32(&sh->release);
       for (uint32_t r = 1; r < n; ++r) ptx::st_cluster_release_u32(ptx::mapa_shared(sa, r), msg);
-      sh->release = msg;
     } else {
       ptx::red_cluster_release_add_u32(ptx::mapa_shared(ptx::smem_u32(&sh->arrive), 0), 1u);
       uint64_t t0 = 0;
       for (uint32_t it = 0;; ++it) {
         const uint32_t v = ptx::ld_shared_acquire_cluster_u32(&sh->release);
-        if ((v & 0x7fffffffu) == (next & 0x7fffffffu)) { ok = (v & 0x80000000u) == 0u; break; }
+        if ((v & 0x7fffffffu) == msg_ok) { ok = (v & 0x80000000u) == 0u; break; }
         if ((it & 255u) == 255u) {
           const uint64_t now = ptx::globaltimer_ns();
           if (t0 == 0) t0 = now;
-          // the leader always answers: its own waits are bounded by the same
-          // deadline, so allow it twice the time before giving up here.
+          // the leader always answers (its own waits are bounded by the same
+          // deadline), so allow it twice the time before giving up here
           else if (now - t0 > 2 * gb.timeout_ns + 1000000ull) {
             detail::record_error(gb, GSRB_DEV_TIMEOUT, episode);
             ok = false;
@@ -378,7 +438,22 @@ __device__ __forceinline__ bool GridSync<V_DSMEM>::sync() {
       }
     }
     sh->ok = ok ? 1u : 0u;
-    epoch = next;
+    sense ^= 1u;
+    ++episode;
+  }
+  __syncthreads();
+  return sh->ok != 0u;
+}
+
+// V_FLIP: two levels without clusters: __syncthreads, then every CTA's thread 0
+// arrives on the split flip words and polls them.
+template <>
+__device__ __forceinline__ bool GridSync<V_FLIP>::sync() {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    detail::flip_arrive(gb, my_index(), gb.nparticipants);
+    sh->ok = detail::flip_wait(gb, gb.nparticipants, sense, episode) ? 1u : 0u;
+    sense ^= 1u;
     ++episode;
   }
   __syncthreads();

@@ -21,16 +21,14 @@
 // holding only the reference's raw buffer pointer can find it at ptr - 32 words.
 //
 // The B200-native priority semaphore (PrioritySem below) keeps the reference
-// record size (5 words per semaphore, word 3 = capacity + 1 as the reference
-// harness reads it, Heterosync/main.cu:973) but changes the protocol:
-//   word 0  state: bits 0..15 readers inside, bit 16 writer inside,
-//           bits 17..31 writers queued
-//   word 1  writer ticket dispenser      word 2  writer now-serving
-//   word 3  capacity + 1 (compatibility)  word 4  capacity
-// Releases are a single `red.release.gpu` (posts never wait: the reference's
-// "priority to exiting blocks" idea, Heterosync/cudaLocksSemaphoreSpin.cu:569-575,
-// taken to its limit); queued writers block new readers (writer precedence, the
-// reference's writerWaiting flag, :489-492); writers are served in ticket order.
+// record (5 words per semaphore, word 3 = capacity + 1 as the reference harness
+// reads it, Heterosync/main.cu:973) but changes the protocol: no lock word, the
+// count is claimed with one compare-and-swap, releases are a single
+// `red.release.gpu` (posts never wait: the reference's "priority to exiting
+// blocks" idea, Heterosync/cudaLocksSemaphoreSpin.cu:569-575, taken to its
+// limit), queued writers hold new readers back (writer precedence, the
+// reference's writerWaiting flag, :489-492) and writers are served in ticket
+// order.
 #pragma once
 #include <stdint.h>
 #include "gsrb/ptx.cuh"
@@ -222,16 +220,24 @@ __device__ __forceinline__ bool refsem_post(RefSem s, bool is_writer, uint32_t m
   return cta_bcast(ok);
 }
 
-// B200-native priority semaphore (layout in the header comment).
+// B200-native priority semaphore on the reference's 5-word record
+// [count, ticket, queued, max, serving]: count starts at max = capacity + 1
+// (Heterosync/cudaLocksSemaphoreSpin.cu:14-27 writes count + 1 into words 0 and
+// 3, and words 1, 2, 4 as 0, which are valid initial values here too).
+//   reader enters : no writer queued and count > 1   -> CAS count, count - 1
+//   writer enters : its ticket is being served and count == max -> CAS count, 0
+//   reader leaves : red.release count += 1          (never waits)
+//   writer leaves : red.release count += max, serving += 1 (never waits)
+// Mutual exclusion and the capacity bound rest on the single CAS-ed count
+// word; the queue and ticket words only order writers and hold readers back
+// while a writer waits (writer precedence).
 struct PrioritySem {
   uint32_t* rec;
-  static constexpr uint32_t kReaderMask = 0xffffu;
-  static constexpr uint32_t kWriterIn = 1u << 16;
-  static constexpr uint32_t kWriterQ = 1u << 17;
-  __device__ __forceinline__ uint32_t* state() const { return rec; }
+  __device__ __forceinline__ uint32_t* count() const { return rec; }
   __device__ __forceinline__ uint32_t* ticket() const { return rec + 1; }
-  __device__ __forceinline__ uint32_t* serving() const { return rec + 2; }
-  __device__ __forceinline__ uint32_t capacity() const { return ptx::ld_relaxed_gpu(rec + 4); }
+  __device__ __forceinline__ uint32_t* queued() const { return rec + 2; }
+  __device__ __forceinline__ uint32_t max_count() const { return ptx::ld_relaxed_gpu(rec + 3); }
+  __device__ __forceinline__ uint32_t* serving() const { return rec + 4; }
 };
 
 __device__ __forceinline__ bool psem_wait(PrioritySem s, bool is_writer, const void* buf,
@@ -240,14 +246,13 @@ __device__ __forceinline__ bool psem_wait(PrioritySem s, bool is_writer, const v
   __syncthreads();
   if (threadIdx.x == 0) {
     LockWait w(to);
+    const uint32_t mx = s.max_count();
+    uint32_t b = spin_ns ? spin_ns : 32;
     if (!is_writer) {
-      const uint32_t cap = s.capacity();
-      uint32_t b = spin_ns ? spin_ns : 32;
       for (;;) {
-        const uint32_t v = ptx::ld_relaxed_gpu(s.state());
-        // no writer inside, none queued, room for one more reader
-        if ((v >> 16) == 0u && (v & PrioritySem::kReaderMask) < cap) {
-          if (ptx::atom_cas_acquire_gpu(s.state(), v, v + 1u) == v) break;
+        if (ptx::ld_relaxed_gpu(s.queued()) == 0u) {
+          const uint32_t c = ptx::ld_relaxed_gpu(s.count());
+          if (c > 1u && c <= mx && ptx::atom_cas_acquire_gpu(s.count(), c, c - 1u) == c) break;
         }
         if (!w.tick()) { ok = false; break; }
         __nanosleep(b);
@@ -255,22 +260,19 @@ __device__ __forceinline__ bool psem_wait(PrioritySem s, bool is_writer, const v
       }
     } else {
       const uint32_t my = ptx::atom_add_relaxed_gpu(s.ticket(), 1u);
-      ptx::red_add_relaxed_gpu(s.state(), PrioritySem::kWriterQ);  // block new readers
+      ptx::red_add_relaxed_gpu(s.queued(), 1u);  // hold new readers back
       while (ptx::ld_acquire_gpu(s.serving()) != my) {
         if (!w.tick()) { ok = false; break; }
         __nanosleep(spin_ns ? spin_ns : 64);
       }
       if (ok) {
         for (;;) {
-          const uint32_t v = ptx::ld_relaxed_gpu(s.state());
-          if ((v & (PrioritySem::kReaderMask | PrioritySem::kWriterIn)) == 0u) {
-            const uint32_t nv = v - PrioritySem::kWriterQ + PrioritySem::kWriterIn;
-            if (ptx::atom_cas_acquire_gpu(s.state(), v, nv) == v) break;
-          }
+          if (ptx::ld_relaxed_gpu(s.count()) == mx && ptx::atom_cas_acquire_gpu(s.count(), mx, 0u) == mx) break;
           if (!w.tick()) { ok = false; break; }
           if (spin_ns) __nanosleep(spin_ns);
         }
       }
+      ptx::red_add_relaxed_gpu(s.queued(), 0xffffffffu);
     }
     if (!ok) lock_record_timeout(buf);
   }
@@ -281,10 +283,10 @@ __device__ __forceinline__ void psem_post(PrioritySem s, bool is_writer) {
   __syncthreads();
   if (threadIdx.x == 0) {
     if (is_writer) {
-      ptx::red_add_release_gpu(s.state(), 0u - PrioritySem::kWriterIn);
+      ptx::red_add_release_gpu(s.count(), s.max_count());
       ptx::red_add_release_gpu(s.serving(), 1u);
     } else {
-      ptx::red_add_release_gpu(s.state(), 0xffffffffu);
+      ptx::red_add_release_gpu(s.count(), 1u);
     }
   }
   __syncthreads();

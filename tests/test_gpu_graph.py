@@ -1,0 +1,92 @@
+"""Persistent BFS / SSSP / PageRank vs the CPU oracle (levels and distances
+bit-exact; PageRank within 1e-6 normalized L1 of FP64)."""
+import pathlib
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+GOLD = pathlib.Path(__file__).resolve().parent / "golden"
+PR_L1_TOL = 1e-6
+
+
+def _graphs(gsrb):
+    return {
+        "tiny": gsrb.Graph.read_gr(GOLD / "tiny.gr"),
+        "rmat12": gsrb.rmat(12, 16, seed=7),
+        "rmat16": gsrb.rmat(16, 16, seed=11),
+        "grid64": gsrb.grid2d(64, 48, seed=3),
+        "path": gsrb.csr_from_edges(3000, np.arange(2999), np.arange(1, 3000)),
+        "isolated": gsrb.csr_from_edges(100, [0, 1, 50], [1, 2, 51]),
+    }
+
+
+@pytest.fixture(scope="module")
+def graphs(gsrb):
+    return _graphs(gsrb)
+
+
+@pytest.mark.parametrize("name", ["tiny", "rmat12", "rmat16", "grid64", "path", "isolated"])
+@pytest.mark.parametrize("mode", [0, 1, 3, 4])
+def test_bfs_levels_exact(gsrb, ctx, orc, graphs, name, mode):
+    g = graphs[name]
+    dg = ctx.graph(g)
+    out = ctx.array(g.nnodes, np.int32)
+    rc, st = dg.bfs(0, out, mode)
+    gsrb.check(rc, "bfs")
+    ctx.check_status("bfs")
+    want = orc.bfs(g, 0)
+    assert np.array_equal(out.download(), want)
+    assert st.edges == orc.traversed_edges(g, want)
+
+
+@pytest.mark.parametrize("variant", [0, 2, 3, 4, 5, 6, 7, 8])
+def test_bfs_barrier_variants(gsrb, ctx, orc, graphs, variant):
+    g = graphs["rmat16"]
+    dg = ctx.graph(g)
+    out = ctx.array(g.nnodes, np.int32)
+    c = gsrb.cfg(variant=variant, ctas_per_sm=2, threads=256, cluster=2)
+    rc, st = dg.bfs(5, out, gsrb.BFS_HEURISTIC, c)
+    gsrb.check(rc)
+    assert np.array_equal(out.download(), orc.bfs(g, 5))
+
+
+@pytest.mark.parametrize("name,delta", [("tiny", 5), ("rmat12", 64), ("rmat16", 300), ("grid64", 2000),
+                                        ("path", 100), ("isolated", 10), ("rmat16", 1 << 30)])
+def test_sssp_distances_exact(gsrb, ctx, orc, graphs, name, delta):
+    g = graphs[name]
+    dg = ctx.graph(g)
+    out = ctx.array(g.nnodes, np.int32)
+    rc, st = dg.sssp(0, out, delta)
+    gsrb.check(rc, "sssp")
+    ctx.check_status("sssp")
+    assert np.array_equal(out.download(), orc.dijkstra(g, 0))
+
+
+@pytest.mark.parametrize("name", ["tiny", "rmat12", "rmat16", "grid64", "isolated"])
+def test_pagerank_l1(gsrb, ctx, orc, graphs, name):
+    g = graphs[name]
+    dg = ctx.graph(g)
+    out = ctx.array(g.nnodes, np.float32)
+    rc, st = dg.pagerank(out, 0.85, 50)
+    gsrb.check(rc, "pagerank")
+    assert st.levels == 50
+    ref = orc.pagerank(g, 0.85, 50)
+    got = out.download()
+    assert orc.normalized_l1(got, ref) <= PR_L1_TOL
+    assert np.max(np.abs(got - ref) / ref) < 1e-5
+
+
+def test_bfs_trace_records(gsrb, ctx, orc, graphs):
+    g = graphs["rmat16"]
+    dg = ctx.graph(g)
+    out = ctx.array(g.nnodes, np.int32)
+    rc, st = dg.bfs(0, out, gsrb.BFS_HEURISTIC)
+    gsrb.check(rc)
+    tr = dg.trace()
+    lv = orc.bfs(g, 0)
+    sizes = np.bincount(lv[lv != 2**31 - 1])
+    assert len(tr) == st.levels
+    # the frontier of level L holds the vertices at level L - 1
+    assert tr["nf"].tolist() == sizes[:len(tr)].tolist()
+    assert set(tr["dir"].tolist()) <= {0, 1}

@@ -1,0 +1,50 @@
+"""Mutexes and semaphores on the GPU: exact final counters, exclusion and capacity."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _counters(ctx):
+    return ctx.array(8, np.uint32).zero()
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("cap", [1, 2, 10, 120])
+def test_semaphore_counts_exact(gsrb, ctx, kind, cap):
+    k, iters, incs, every = 2, 4, 100, 11
+    c = gsrb.cfg(ctas_per_sm=k, threads=256, timeout_ms=3000)
+    cnt = _counters(ctx)
+    st = ctx.semaphore_bench(c, kind, cap, every, iters, incs, cnt)
+    gsrb.check(st, "semaphore_bench")
+    W, R, inside, maxr, viol, acq, tmo, _ = cnt.download().tolist()
+    grid = k * ctx.num_sms
+    writers = len([b for b in range(grid) if b % every == 0])
+    assert tmo == 0 and viol == 0 and inside == 0
+    assert acq == grid * iters
+    assert W == writers * iters * incs          # plain RMW: any writer overlap would lose updates
+    assert R == (grid - writers) * iters * incs
+    assert 1 <= maxr <= cap
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2, 3])
+def test_mutex_counts_exact(gsrb, ctx, kind):
+    k, iters, incs = 1, 3, 50
+    c = gsrb.cfg(ctas_per_sm=k, threads=128, timeout_ms=3000)
+    cnt = _counters(ctx)
+    gsrb.check(ctx.mutex_bench(c, kind, iters, incs, cnt), "mutex_bench")
+    W, R, inside, maxr, viol, acq, tmo, _ = cnt.download().tolist()
+    grid = k * ctx.num_sms
+    assert tmo == 0 and viol == 0
+    assert acq == grid * iters and W == grid * iters * incs
+
+
+def test_semaphore_full_residency(gsrb, ctx):
+    # 148 x 8 CTAs of 256 threads contend on one priority semaphore
+    c = gsrb.cfg(ctas_per_sm=8, threads=256, timeout_ms=5000)
+    cnt = _counters(ctx)
+    gsrb.check(ctx.semaphore_bench(c, gsrb.SEM_PRIORITY, 10, 11, 2, 100, cnt))
+    W, R, inside, maxr, viol, acq, tmo, _ = cnt.download().tolist()
+    grid = 8 * ctx.num_sms
+    writers = len([b for b in range(grid) if b % 11 == 0])
+    assert viol == 0 and tmo == 0 and W == writers * 200 and R == (grid - writers) * 200

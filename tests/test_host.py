@@ -11,10 +11,11 @@ GOLD = ROOT / "tests" / "golden"
 def test_library_exports_every_declared_symbol(gsrb):
     import ctypes
     decls = set()
-    for h in (ROOT / "include").glob("*.h"):
+    for h in (ROOT / "include").rglob("*.h"):
         text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
         decls |= set(re.findall(r"\b(gsrb_[a-z0-9_]+)\s*\(", text))
-        decls |= set(re.findall(r"\b(cuda[A-Za-z]+)\s*\(", text)) if h.name != "gsrb.h" else set()
+        if h.name != "gsrb.h":  # the drop-in cudaLocks host API
+            decls |= set(re.findall(r"\b(cuda[A-Z][A-Za-z]+)\s*\(", text))
     assert decls, "no declarations found"
     lib = ctypes.CDLL(str(gsrb.LIB_PATH))
     missing = [d for d in sorted(decls) if not hasattr(lib, d)]

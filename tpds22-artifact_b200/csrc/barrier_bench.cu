@@ -90,6 +90,7 @@ const void* bench_fn(int variant) {
     case gsrb::V_TREE: return (const void*)barrier_bench_kernel<gsrb::V_TREE>;
     case gsrb::V_CCG: return (const void*)barrier_bench_kernel<gsrb::V_CCG>;
     case gsrb::V_CLUSTER_RED: return (const void*)barrier_bench_kernel<gsrb::V_CLUSTER_RED>;
+    case gsrb::V_FLIP: return (const void*)barrier_bench_kernel<gsrb::V_FLIP>;
     case kNoBarrier: return (const void*)barrier_bench_kernel<kNoBarrier>;
     default: return nullptr;
   }
@@ -105,6 +106,7 @@ const void* litmus_fn(int variant) {
     case gsrb::V_TREE: return (const void*)barrier_litmus_kernel<gsrb::V_TREE>;
     case gsrb::V_CCG: return (const void*)barrier_litmus_kernel<gsrb::V_CCG>;
     case gsrb::V_CLUSTER_RED: return (const void*)barrier_litmus_kernel<gsrb::V_CLUSTER_RED>;
+    case gsrb::V_FLIP: return (const void*)barrier_litmus_kernel<gsrb::V_FLIP>;
     default: return nullptr;
   }
 }
@@ -153,7 +155,7 @@ gsrb_status_t gsrb_barrier_bench(gsrb_ctx_t ctx, const gsrb_cfg_t* cfgin, int32_
   gsrb::GridBarrier gb = make_barrier(ctx, c, 0, (uint32_t)grid, 0, 0);
   float a = 0.999999f, b = 1e-7f;
   void* args[] = {&gb, &episodes, &fma, &a, &b, &d_sink, &d_count};
-  return launch_persistent(ctx, fn, grid, c.threads, 0, c.cluster, c.variant == gsrb::V_CCG, args);
+  return launch_persistent(ctx, fn, grid, c.threads, 0, c.cluster, coop_of(c), args);
 }
 
 gsrb_status_t gsrb_barrier_litmus(gsrb_ctx_t ctx, const gsrb_cfg_t* cfgin, int32_t episodes,
@@ -168,7 +170,7 @@ gsrb_status_t gsrb_barrier_litmus(gsrb_ctx_t ctx, const gsrb_cfg_t* cfgin, int32
   if (grid % c.cluster) return GSRB_ERR_ARG;
   gsrb::GridBarrier gb = make_barrier(ctx, c, 0, (uint32_t)grid, 0, 0);
   void* args[] = {&gb, &episodes, &d_buf, &d_stale};
-  return launch_persistent(ctx, fn, grid, c.threads, 0, c.cluster, c.variant == gsrb::V_CCG, args);
+  return launch_persistent(ctx, fn, grid, c.threads, 0, c.cluster, coop_of(c), args);
 }
 
 gsrb_status_t gsrb_barrier_fault_short_grid(gsrb_ctx_t ctx, const gsrb_cfg_t* cfgin) {

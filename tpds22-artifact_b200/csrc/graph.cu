@@ -1,0 +1,901 @@
+// Persistent Lonestar-style graph traversals on the grid barrier: BFS (push
+// worklist, pull, topology push; direction chosen per level by a fixed
+// heuristic or by the learned policy), SSSP (near-far buckets with atomicMin)
+// and pull PageRank (FP32 state, FP64 per-vertex accumulation, fixed
+// iteration count).  One kernel launch per traversal; one grid barrier per
+// level / bucket step / iteration.
+//
+// Reference: the GGC "outlined iterate" kernels gg_main_pipe_1_gpu_gb of
+// LONESTAR/apps/bfs/kernel_gsrb.cu:591-626 (BFS), apps/sssp/kernel_gsrb.cu:637-687
+// (SSSP, DELTA default 10000, apps/sssp/support.cu:10), apps/pr/kernel_gsrb.cu:543-587
+// (push-residual PR), all launched as one persistent kernel that hits
+// kernelAtomicTreeBarrierUniqSRB once per level.  Level and distance
+// conventions: source 0, unreachable INT_MAX, BFS level L for vertices first
+// reached in round L (bfs/kernel_gsrb.cu:299-311, :473-479, :724).
+#include "internal.h"
+#include "graph_common.cuh"
+
+using namespace gsrbrt;
+using namespace gsrbg;
+
+namespace {
+
+enum BfsDir : uint32_t { DIR_PUSH = 0, DIR_PULL = 1, DIR_TOPO = 2 };
+
+struct BfsArgs {
+  DevCSR g;
+  uint32_t src;
+  int32_t* level;
+  uint32_t* q[2];
+  uint32_t* hq[2];
+  LevelCounters* cnt;  // [3]
+  uint32_t* overflow;
+  LevelTrace* trace;
+  uint32_t trace_cap;
+  const MLPWeights* mlp;
+  int32_t mode;        // GSRB_BFS_* (include/gsrb.h)
+  float alpha, beta;   // direction-optimizing thresholds (Beamer, Asanovic, Patterson, SC'12)
+  uint32_t* out;       // [0] levels, [1] fallback level (0 = none), [2] policy decisions, [3] overflow
+  unsigned long long* out_edges;
+};
+
+template <int V>
+__global__ void __launch_bounds__(1024)
+bfs_kernel(gsrb::GridBarrier gb, BfsArgs a) {
+  __shared__ gsrb::BarrierShared bsh;
+  __shared__ uint32_t s_dir;
+  __shared__ float s_pred;
+  gsrb::GridSync<V> bar;
+  bool ok = bar.init(gb, &bsh);
+  const DevCSR& g = a.g;
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+
+  // init (bfs_init, bfs/kernel_gsrb.cu:299-311) fused into the persistent kernel
+  for (uint32_t v = tid; v < g.n; v += nthreads) a.level[v] = (v == a.src) ? 0 : kInf;
+  const uint32_t dsrc = g.row[a.src + 1] - g.row[a.src];
+  if (tid == 0) {
+    const bool hub = dsrc > kBigDegree;
+    if (hub) a.hq[0][0] = a.src;
+    else a.q[0][0] = a.src;
+    a.cnt[0].n_reg = hub ? 0 : 1;
+    a.cnt[0].n_big = hub ? 1 : 0;
+    a.cnt[0].m_next = dsrc;
+    a.cnt[1].n_reg = a.cnt[1].n_big = a.cnt[1].m_next = 0;
+    a.cnt[2].n_reg = a.cnt[2].n_big = a.cnt[2].m_next = 0;
+  }
+  ok = bar.sync() && ok;
+
+  uint32_t nu = g.n - 1;
+  unsigned long long mu = (unsigned long long)g.m - dsrc;
+  unsigned long long edges = dsrc;
+  uint32_t dir = DIR_PUSH, prev_nf = 1;
+  bool fallback = a.mode != GSRB_BFS_LEARNED;
+  float pred = __int_as_float(0x7fc00000);
+  uint32_t L = 1;
+  uint32_t decisions = 0;
+  for (; ok; ++L) {
+    const LevelCounters cur = {__ldcg(&a.cnt[(L - 1) % 3].n_reg), __ldcg(&a.cnt[(L - 1) % 3].n_big),
+                               __ldcg(&a.cnt[(L - 1) % 3].m_next), 0};
+    const uint32_t nreg = (uint32_t)cur.n_reg, nbig = (uint32_t)cur.n_big;
+    const uint32_t nf = nreg + nbig;
+    if (nf == 0) break;
+    const unsigned long long mf = cur.m_next;
+    if (L > 1) {
+      nu -= nf;
+      mu -= mf;
+      edges += mf;
+    }
+    // ---- choose the level's direction (identical in every CTA)
+    if (!fallback && L > 1 && pred == pred) {
+      const float actual = log2f(1.f + (float)nf);
+      if (fabsf(actual - pred) > 1.f) fallback = true;  // missed by more than 2x
+    }
+    uint32_t nd = DIR_PUSH;
+    if (a.mode == GSRB_BFS_PULL) {
+      nd = L == 1 ? DIR_PUSH : DIR_PULL;
+    } else if (a.mode == GSRB_BFS_TOPO) {
+      nd = DIR_TOPO;
+    } else if (a.mode == GSRB_BFS_HEURISTIC || (a.mode == GSRB_BFS_LEARNED && fallback)) {
+      nd = dir;
+      if (dir != DIR_PULL && (double)mf > (double)mu / a.alpha) nd = DIR_PULL;
+      else if (dir == DIR_PULL && (double)nf < (double)g.n / a.beta) nd = DIR_PUSH;
+    } else if (a.mode == GSRB_BFS_LEARNED) {
+      if (threadIdx.x < 32) {
+        float feat[kFeat], out[kOut];
+        level_features(feat, g.n, g.m, L, nf, mf, nu, mu, prev_nf, dir);
+        mlp_forward_warp(a.mlp, feat, out);
+        if (threadIdx.x == 0) {
+          s_dir = out[0] > 0.f ? DIR_PULL : (out[1] > 0.f ? DIR_TOPO : DIR_PUSH);
+          s_pred = out[2];
+        }
+      }
+      __syncthreads();
+      nd = s_dir;
+      pred = s_pred;
+      ++decisions;
+    }
+    dir = nd;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      // the counter set of level L + 1 was last read before barrier L - 1
+      a.cnt[(L + 1) % 3].n_reg = 0;
+      a.cnt[(L + 1) % 3].n_big = 0;
+      a.cnt[(L + 1) % 3].m_next = 0;
+      if (L - 1 < a.trace_cap) {
+        LevelTrace t;
+        t.level = L;
+        t.dir = dir;
+        t.nf = nf;
+        t.nu = nu;
+        t.mf = mf;
+        t.mu = mu;
+        t.t_ns = gsrb::ptx::globaltimer_ns();
+        t.pred = (a.mode == GSRB_BFS_LEARNED && !fallback) ? pred : __int_as_float(0x7fc00000);
+        t.fallback = fallback ? 1u : 0u;
+        a.trace[L - 1] = t;
+      }
+    }
+    prev_nf = nf;
+
+    const uint32_t* qin = a.q[(L - 1) & 1];
+    const uint32_t* hin = a.hq[(L - 1) & 1];
+    uint32_t* qout = a.q[L & 1];
+    uint32_t* hout = a.hq[L & 1];
+    LevelCounters* c = &a.cnt[L % 3];
+    unsigned long long m_acc = 0;
+    const int32_t Li = (int32_t)L;
+
+    auto discover = [&](bool disc, uint32_t v) {
+      uint32_t d = 0;
+      if (disc) d = __ldg(g.row + v + 1) - __ldg(g.row + v);
+      warp_append(disc && d <= kBigDegree, v, qout, &c->n_reg, g.n, a.overflow);
+      warp_append(disc && d > kBigDegree, v, hout, &c->n_big, g.n, a.overflow);
+      m_acc += d;
+    };
+    auto push_edge = [&](uint32_t, uint32_t j, bool active) {
+      uint32_t v = 0;
+      bool disc = false;
+      if (active) {
+        v = __ldg(g.dst + j);
+        if (__ldcg(a.level + v) == kInf) disc = atomicCAS(a.level + v, kInf, Li) == kInf;
+      }
+      discover(disc, v);
+    };
+
+    if (dir == DIR_PUSH) {
+      expand_hubs(g, hin, nbig, push_edge);
+      expand_queue(g, qin, nreg, push_edge);
+    } else if (dir == DIR_TOPO) {
+      // topology-driven push: scan every vertex, expand those at level L - 1
+      expand_hubs(g, hin, nbig, push_edge);
+      const uint32_t lane = lane_id();
+      const uint32_t gw = tid >> 5, nw = nthreads >> 5;
+      for (uint32_t base = gw * 32u; base < g.n; base += nw * 32u) {
+        const uint32_t u = base + lane;
+        uint32_t b = 0, e = 0;
+        if (u < g.n && __ldcg(a.level + u) == Li - 1) {
+          b = __ldg(g.row + u);
+          e = __ldg(g.row + u + 1);
+          if (e - b > kBigDegree) e = b;  // hubs were expanded above
+        }
+        const uint32_t deg = e - b;
+        uint32_t coop = __ballot_sync(0xffffffffu, deg > kWarpDegree);
+        while (coop) {
+          const int s = __ffs(coop) - 1;
+          coop &= coop - 1;
+          const uint32_t bb = __shfl_sync(0xffffffffu, b, s), ee = __shfl_sync(0xffffffffu, e, s);
+          for (uint32_t j0 = bb; j0 < ee; j0 += 32) push_edge(0, j0 + lane, j0 + lane < ee);
+        }
+        const uint32_t mine = deg <= kWarpDegree ? deg : 0u;
+        const uint32_t kmax = warp_max_u32(mine);
+        for (uint32_t k = 0; k < kmax; ++k) push_edge(u, b + k, k < mine);
+      }
+    } else {
+      // pull: every unvisited vertex looks for a neighbour at level L - 1
+      const uint32_t lane = lane_id();
+      const uint32_t gw = tid >> 5, nw = nthreads >> 5;
+      for (uint32_t base = gw * 32u; base < g.n; base += nw * 32u) {
+        const uint32_t v = base + lane;
+        bool unv = false;
+        uint32_t b = 0, e = 0;
+        if (v < g.n && __ldcg(a.level + v) == kInf) {
+          unv = true;
+          b = __ldg(g.row + v);
+          e = __ldg(g.row + v + 1);
+        }
+        const uint32_t deg = e - b;
+        bool found = false;
+        if (unv && deg <= kWarpDegree) {
+          for (uint32_t j = b; j < e; ++j)
+            if (__ldcg(a.level + __ldg(g.dst + j)) == Li - 1) { found = true; break; }
+        }
+        uint32_t coop = __ballot_sync(0xffffffffu, unv && deg > kWarpDegree);
+        while (coop) {
+          const int s = __ffs(coop) - 1;
+          coop &= coop - 1;
+          const uint32_t bb = __shfl_sync(0xffffffffu, b, s), ee = __shfl_sync(0xffffffffu, e, s);
+          bool hit = false;
+          for (uint32_t j0 = bb; j0 < ee && !hit; j0 += 32) {
+            const uint32_t j = j0 + lane;
+            const bool h = j < ee && __ldcg(a.level + __ldg(g.dst + j)) == Li - 1;
+            hit = __ballot_sync(0xffffffffu, h) != 0u;
+          }
+          if ((int)lane == s) found = hit;
+        }
+        if (found) gsrb::ptx::st_relaxed_gpu_s32(a.level + v, Li);
+        discover(found, v);
+      }
+    }
+    // per-warp edge sums of the new frontier
+    const unsigned long long ws = warp_sum_u64(m_acc);
+    if (lane_id() == 0 && ws) atomicAdd(&c->m_next, ws);
+    ok = bar.sync();
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.out[0] = L - 1;  // levels with a non-empty frontier beyond the source
+    a.out[2] = decisions;
+    a.out[3] = ok ? 0u : 1u;
+    *a.out_edges = edges;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && a.mode == GSRB_BFS_LEARNED) {
+    // first level at which the policy fell back (0 = never); recomputed from the trace
+    uint32_t fb = 0;
+    for (uint32_t i = 0; i + 1 < L && i < a.trace_cap; ++i)
+      if (a.trace[i].fallback) { fb = a.trace[i].level; break; }
+    a.out[1] = fb;
+  }
+  bar.finish();
+}
+
+// ------------------------------------------------------------------- SSSP ---
+struct SsspArgs {
+  DevCSR g;
+  uint32_t src;
+  int32_t* dist;
+  uint32_t* q[2];
+  uint32_t* hq[2];
+  uint32_t* far[2];
+  uint32_t* mark;       // near-queue stamps
+  uint32_t* fmark;      // far-pile stamps
+  LevelCounters* cnt;   // [3] near counters
+  unsigned long long* fcnt;  // [2] far counters
+  uint32_t* overflow;
+  LevelTrace* trace;
+  uint32_t trace_cap;
+  int32_t delta;
+  uint32_t* out;        // [0] relax rounds, [1] buckets, [3] failure
+  unsigned long long* out_edges;
+};
+
+template <int V>
+__global__ void __launch_bounds__(1024)
+sssp_kernel(gsrb::GridBarrier gb, SsspArgs a) {
+  __shared__ gsrb::BarrierShared bsh;
+  gsrb::GridSync<V> bar;
+  bool ok = bar.init(gb, &bsh);
+  const DevCSR& g = a.g;
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+  for (uint32_t v = tid; v < g.n; v += nthreads) {
+    a.dist[v] = (v == a.src) ? 0 : kInf;
+    a.mark[v] = 0;
+    a.fmark[v] = 0;
+  }
+  const uint32_t dsrc = g.row[a.src + 1] - g.row[a.src];
+  if (tid == 0) {
+    const bool hub = dsrc > kBigDegree;
+    if (hub) a.hq[0][0] = a.src;
+    else a.q[0][0] = a.src;
+    for (int k = 0; k < 3; ++k) a.cnt[k].n_reg = a.cnt[k].n_big = a.cnt[k].m_next = 0;
+    a.cnt[0].n_reg = hub ? 0 : 1;
+    a.cnt[0].n_big = hub ? 1 : 0;
+    a.fcnt[0] = a.fcnt[1] = 0;
+  }
+  ok = bar.sync() && ok;
+
+  // near threshold: vertices with dist < T are relaxed in the current bucket
+  long long T = a.delta;
+  uint32_t step = 1;       // index of the near counter set in use (rotating by 3)
+  uint32_t fpar = 0;       // far pile parity
+  uint32_t fgen = 1;       // generation of the current far pile (fmark stamps: a vertex enters a pile once)
+  uint32_t rounds = 0, buckets = 1;
+  unsigned long long relaxed_edges = 0;
+  while (ok) {
+    const LevelCounters cur = {__ldcg(&a.cnt[(step - 1) % 3].n_reg), __ldcg(&a.cnt[(step - 1) % 3].n_big), 0, 0};
+    const uint32_t nreg = (uint32_t)cur.n_reg, nbig = (uint32_t)cur.n_big;
+    const uint32_t nf = nreg + nbig;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      a.cnt[(step + 1) % 3].n_reg = 0;
+      a.cnt[(step + 1) % 3].n_big = 0;
+      a.cnt[(step + 1) % 3].m_next = 0;
+    }
+    if (nf == 0) {
+      // ---- near bucket empty: advance the threshold and refill from the far pile
+      const uint32_t nfar = (uint32_t)__ldcg(&a.fcnt[fpar]);
+      if (nfar == 0) break;
+      T += a.delta;
+      ++buckets;
+      const uint32_t* fin = a.far[fpar];
+      uint32_t* fout = a.far[fpar ^ 1];
+      unsigned long long* fc_out = &a.fcnt[fpar ^ 1];
+      uint32_t* qout = a.q[step & 1];
+      uint32_t* hout = a.hq[step & 1];
+      LevelCounters* c = &a.cnt[step % 3];
+      const uint32_t stamp = step;
+      const uint32_t next_gen = fgen + 1;
+      if (blockIdx.x == 0 && threadIdx.x == 0) *fc_out = 0;  // last read before the previous barrier
+      // fc_out must be zero before anyone appends: appends happen below, after
+      // this CTA's store, so publish it through the barrier first
+      ok = bar.sync();
+      if (!ok) break;
+      const uint32_t lane = lane_id();
+      const uint32_t gw = tid >> 5, nw = nthreads >> 5;
+      for (uint32_t base = gw * 32u; base < nfar; base += nw * 32u) {
+        const uint32_t i = base + lane;
+        uint32_t v = 0;
+        bool near = false, keep = false;
+        if (i < nfar) {
+          v = __ldcg(fin + i);
+          const int32_t dv = __ldcg(a.dist + v);
+          if ((long long)dv < T) near = atomicExch(a.mark + v, stamp) != stamp;
+          else keep = atomicExch(a.fmark + v, next_gen) != next_gen;
+        }
+        uint32_t d = 0;
+        if (near) d = __ldg(g.row + v + 1) - __ldg(g.row + v);
+        warp_append(near && d <= kBigDegree, v, qout, &c->n_reg, g.n, a.overflow);
+        warp_append(near && d > kBigDegree, v, hout, &c->n_big, g.n, a.overflow);
+        warp_append(keep, v, fout, fc_out, g.n, a.overflow);
+      }
+      fpar ^= 1;
+      fgen = next_gen;
+      ++step;
+      ok = bar.sync();
+      continue;
+    }
+    // ---- relax the near frontier
+    ++rounds;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && rounds - 1 < a.trace_cap) {
+      LevelTrace t;
+      t.level = rounds;
+      t.dir = 0;
+      t.nf = nf;
+      t.nu = buckets;
+      t.mf = 0;
+      t.mu = (unsigned long long)T;
+      t.t_ns = gsrb::ptx::globaltimer_ns();
+      t.pred = __int_as_float(0x7fc00000);
+      t.fallback = 0;
+      a.trace[rounds - 1] = t;
+    }
+    const uint32_t* qin = a.q[(step - 1) & 1];
+    const uint32_t* hin = a.hq[(step - 1) & 1];
+    uint32_t* qout = a.q[step & 1];
+    uint32_t* hout = a.hq[step & 1];
+    LevelCounters* c = &a.cnt[step % 3];
+    uint32_t* fout = a.far[fpar];
+    unsigned long long* fc = &a.fcnt[fpar];
+    const uint32_t stamp = step + 1;  // stamps of vertices queued for the next round
+    unsigned long long my_edges = 0;
+    auto relax = [&](uint32_t u, uint32_t j, bool active) {
+      uint32_t v = 0;
+      bool to_near = false, to_far = false;
+      if (active) {
+        ++my_edges;
+        v = __ldg(g.dst + j);
+        const long long nd = (long long)__ldcg(a.dist + u) + (long long)__ldg(g.w + j);
+        if (nd < (long long)__ldcg(a.dist + v)) {
+          const int32_t old = atomicMin(a.dist + v, (int32_t)nd);
+          if (nd < (long long)old) {
+            if (nd < T) to_near = atomicExch(a.mark + v, stamp) != stamp;
+            else to_far = atomicExch(a.fmark + v, fgen) != fgen;
+          }
+        }
+      }
+      uint32_t d = 0;
+      if (to_near) d = __ldg(g.row + v + 1) - __ldg(g.row + v);
+      warp_append(to_near && d <= kBigDegree, v, qout, &c->n_reg, g.n, a.overflow);
+      warp_append(to_near && d > kBigDegree, v, hout, &c->n_big, g.n, a.overflow);
+      warp_append(to_far, v, fout, fc, g.n, a.overflow);
+    };
+    expand_hubs(g, hin, nbig, relax);
+    expand_queue(g, qin, nreg, relax);
+    relaxed_edges += my_edges;
+    ++step;
+    ok = bar.sync();
+  }
+  // per-thread relaxed-edge counts -> one total
+  const unsigned long long ws = warp_sum_u64(relaxed_edges);
+  if (lane_id() == 0 && ws) atomicAdd(a.out_edges, ws);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.out[0] = rounds;
+    a.out[1] = buckets;
+    a.out[3] = ok ? 0u : 1u;
+  }
+  bar.finish();
+}
+
+// --------------------------------------------------------------- PageRank ---
+struct PrArgs {
+  DevCSR g;
+  float alpha;
+  int32_t iters;
+  float* rank;          // output x (FP32)
+  float* contrib[2];    // x / deg, double-buffered by iteration parity
+  const uint32_t* hubs; // vertices of degree > kBigDegree
+  uint32_t nhubs;
+  double* hub_part;     // [nhubs * gridDim] partial sums of hub rows
+  uint32_t* out;
+};
+
+// Gathers sum_{u in N(v)} c[u] for every non-hub vertex with a warp per 32
+// vertices (lane per vertex for low degree, warp-cooperative above), FP64
+// accumulation in a fixed order.
+template <int V>
+__global__ void __launch_bounds__(1024)
+pagerank_kernel(gsrb::GridBarrier gb, PrArgs a) {
+  __shared__ gsrb::BarrierShared bsh;
+  __shared__ double s_red[32];
+  gsrb::GridSync<V> bar;
+  bool ok = bar.init(gb, &bsh);
+  const DevCSR& g = a.g;
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+  const float base = 1.f - a.alpha;
+  // x0 = 1 - alpha (apps/pr/kernel_gsrb.cu:311)
+  for (uint32_t v = tid; v < g.n; v += nthreads) {
+    const uint32_t d = __ldg(g.row + v + 1) - __ldg(g.row + v);
+    a.rank[v] = base;
+    a.contrib[0][v] = d ? base / (float)d : 0.f;
+  }
+  ok = bar.sync() && ok;
+  const uint32_t lane = lane_id();
+  const uint32_t gw = tid >> 5, nw = nthreads >> 5;
+  int32_t it = 0;
+  for (; ok && it < a.iters; ++it) {
+    const float* cin = a.contrib[it & 1];
+    float* cout = a.contrib[(it + 1) & 1];
+    // hub rows: every CTA reduces its slice of every hub's edges
+    for (uint32_t k = 0; k < a.nhubs; ++k) {
+      const uint32_t u = __ldg(a.hubs + k);
+      const uint32_t b = __ldg(g.row + u), e = __ldg(g.row + u + 1);
+      const uint64_t len = e - b;
+      const uint32_t s0 = b + (uint32_t)(len * blockIdx.x / gridDim.x);
+      const uint32_t s1 = b + (uint32_t)(len * (blockIdx.x + 1) / gridDim.x);
+      double s = 0.0;
+      for (uint32_t j = s0 + threadIdx.x; j < s1; j += blockDim.x) s += (double)__ldcg(cin + __ldg(g.dst + j));
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+      if (lane == 0) s_red[threadIdx.x >> 5] = s;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (uint32_t i = 0; i < (blockDim.x >> 5); ++i) t += s_red[i];
+        a.hub_part[(size_t)k * gridDim.x + blockIdx.x] = t;
+      }
+      __syncthreads();
+    }
+    for (uint32_t vb = gw * 32u; vb < g.n; vb += nw * 32u) {
+      const uint32_t v = vb + lane;
+      uint32_t b = 0, e = 0;
+      if (v < g.n) {
+        b = __ldg(g.row + v);
+        e = __ldg(g.row + v + 1);
+      }
+      const uint32_t deg = e - b;
+      double s = 0.0;
+      if (deg <= kWarpDegree)
+        for (uint32_t j = b; j < e; ++j) s += (double)__ldcg(cin + __ldg(g.dst + j));
+      uint32_t coop = __ballot_sync(0xffffffffu, deg > kWarpDegree && deg <= kBigDegree);
+      while (coop) {
+        const int src = __ffs(coop) - 1;
+        coop &= coop - 1;
+        const uint32_t bb = __shfl_sync(0xffffffffu, b, src), ee = __shfl_sync(0xffffffffu, e, src);
+        double t = 0.0;
+        for (uint32_t j = bb + lane; j < ee; j += 32) t += (double)__ldcg(cin + __ldg(g.dst + j));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        if ((int)lane == src) s = t;
+      }
+      if (v < g.n && deg <= kBigDegree) {
+        const float x = (float)((double)base + (double)a.alpha * s);
+        a.rank[v] = x;
+        cout[v] = deg ? x / (float)deg : 0.f;
+      }
+    }
+    ok = bar.sync();
+    if (!ok) break;
+    // hub rows: combine the per-CTA partials in CTA order (deterministic)
+    for (uint32_t k = blockIdx.x; k < a.nhubs; k += gridDim.x) {
+      double s = 0.0;
+      for (uint32_t i = threadIdx.x; i < gridDim.x; i += blockDim.x) s += __ldcg(a.hub_part + (size_t)k * gridDim.x + i);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+      if (lane == 0) s_red[threadIdx.x >> 5] = s;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (uint32_t i = 0; i < (blockDim.x >> 5); ++i) t += s_red[i];
+        const uint32_t u = __ldg(a.hubs + k);
+        const uint32_t d = __ldg(g.row + u + 1) - __ldg(g.row + u);
+        const float x = (float)((double)base + (double)a.alpha * t);
+        a.rank[u] = x;
+        cout[u] = x / (float)d;
+      }
+      __syncthreads();
+    }
+    if (a.nhubs) {
+      ok = bar.sync();
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.out[0] = (uint32_t)it;
+    a.out[3] = ok ? 0u : 1u;
+  }
+  bar.finish();
+}
+
+template <template <int> class K>
+struct Dummy {};
+
+#define GSRB_GRAPH_FN(KERNEL)                                                    \
+  [](int variant) -> const void* {                                              \
+    switch (variant) {                                                          \
+      case gsrb::V_CLUSTER: return (const void*)KERNEL<gsrb::V_CLUSTER>;         \
+      case gsrb::V_DSMEM: return (const void*)KERNEL<gsrb::V_DSMEM>;             \
+      case gsrb::V_SOFT2: return (const void*)KERNEL<gsrb::V_SOFT2>;             \
+      case gsrb::V_FLAT: return (const void*)KERNEL<gsrb::V_FLAT>;               \
+      case gsrb::V_TREE: return (const void*)KERNEL<gsrb::V_TREE>;               \
+      case gsrb::V_CCG: return (const void*)KERNEL<gsrb::V_CCG>;                 \
+      case gsrb::V_CLUSTER_RED: return (const void*)KERNEL<gsrb::V_CLUSTER_RED>; \
+      case gsrb::V_FLIP: return (const void*)KERNEL<gsrb::V_FLIP>;               \
+      default: return nullptr;                                                  \
+    }                                                                           \
+  }
+
+const void* bfs_fn(int v) { return GSRB_GRAPH_FN(bfs_kernel)(v); }
+const void* sssp_fn(int v) { return GSRB_GRAPH_FN(sssp_kernel)(v); }
+const void* pr_fn(int v) { return GSRB_GRAPH_FN(pagerank_kernel)(v); }
+
+}  // namespace
+
+const void* gsrb_graph_kernel_for(int variant) { return bfs_fn(variant); }
+
+// ------------------------------------------------------------ host side ----
+struct gsrb_graph {
+  gsrb_ctx* ctx = nullptr;
+  uint32_t n = 0;
+  uint32_t m = 0;
+  bool owns = false;
+  uint32_t* row = nullptr;
+  uint32_t* dst = nullptr;
+  int32_t* w = nullptr;
+  // scratch
+  uint32_t* q[2] = {};
+  uint32_t* hq[2] = {};
+  uint32_t* far[2] = {};
+  uint32_t* mark = nullptr;
+  uint32_t* fmark = nullptr;
+  LevelCounters* cnt = nullptr;
+  unsigned long long* fcnt = nullptr;
+  uint32_t* flags = nullptr;  // [0] overflow, [4..8) out, edges at byte 64
+  LevelTrace* trace = nullptr;
+  uint32_t trace_cap = 0;
+  float* contrib[2] = {};
+  uint32_t* hubs = nullptr;
+  uint32_t nhubs = 0;
+  double* hub_part = nullptr;
+  MLPWeights* mlp = nullptr;
+  bool mlp_set = false;
+};
+
+namespace {
+
+template <class T>
+cudaError_t dalloc(T** p, size_t count) {
+  return cudaMalloc((void**)p, sizeof(T) * (count ? count : 1));
+}
+
+gsrb_status_t graph_scratch(gsrb_graph* G) {
+  const size_t n = G->n;
+  cudaError_t e = cudaSuccess;
+  for (int k = 0; k < 2 && !e; ++k) {
+    e = dalloc(&G->q[k], n);
+    if (!e) e = dalloc(&G->hq[k], n);
+    if (!e) e = dalloc(&G->far[k], n);
+    if (!e) e = dalloc(&G->contrib[k], n);
+  }
+  if (!e) e = dalloc(&G->mark, n);
+  if (!e) e = dalloc(&G->fmark, n);
+  if (!e) e = dalloc(&G->cnt, 3);
+  if (!e) e = dalloc(&G->fcnt, 2);
+  if (!e) e = dalloc(&G->flags, 32);
+  G->trace_cap = 1u << 16;
+  if (!e) e = dalloc(&G->trace, G->trace_cap);
+  if (!e) e = dalloc(&G->mlp, 1);
+  if (!e) e = cudaMemset(G->mlp, 0, sizeof(MLPWeights));
+  // hub list for PageRank (degree > kBigDegree), built on the host from row_start
+  if (!e) {
+    uint32_t* hrow = (uint32_t*)malloc(sizeof(uint32_t) * (n + 1));
+    if (!hrow) return GSRB_ERR_NOMEM;
+    e = cudaMemcpy(hrow, G->row, sizeof(uint32_t) * (n + 1), cudaMemcpyDeviceToHost);
+    uint32_t* hl = (uint32_t*)malloc(sizeof(uint32_t) * (n ? n : 1));
+    uint32_t nh = 0;
+    for (size_t v = 0; !e && v < n; ++v)
+      if (hrow[v + 1] - hrow[v] > kBigDegree) hl[nh++] = (uint32_t)v;
+    G->nhubs = nh;
+    if (!e) e = dalloc(&G->hubs, nh);
+    if (!e && nh) e = cudaMemcpy(G->hubs, hl, sizeof(uint32_t) * nh, cudaMemcpyHostToDevice);
+    if (!e) e = dalloc(&G->hub_part, (size_t)(nh ? nh : 1) * 148 * 32);
+    free(hrow);
+    free(hl);
+  }
+  if (!e) e = cudaDeviceSynchronize();
+  if (e) return cuda_err(e, "graph scratch");
+  return GSRB_OK;
+}
+
+void graph_free(gsrb_graph* G) {
+  if (G->owns) {
+    cudaFree(G->row);
+    cudaFree(G->dst);
+    cudaFree(G->w);
+  }
+  for (int k = 0; k < 2; ++k) {
+    cudaFree(G->q[k]);
+    cudaFree(G->hq[k]);
+    cudaFree(G->far[k]);
+    cudaFree(G->contrib[k]);
+  }
+  cudaFree(G->mark);
+  cudaFree(G->fmark);
+  cudaFree(G->cnt);
+  cudaFree(G->fcnt);
+  cudaFree(G->flags);
+  cudaFree(G->trace);
+  cudaFree(G->hubs);
+  cudaFree(G->hub_part);
+  cudaFree(G->mlp);
+}
+
+DevCSR dev_csr(const gsrb_graph* G) {
+  DevCSR d;
+  d.n = G->n;
+  d.m = G->m;
+  d.row = G->row;
+  d.dst = G->dst;
+  d.w = G->w;
+  return d;
+}
+
+gsrb_cfg_t graph_cfg(gsrb_ctx* ctx, const gsrb_cfg_t* in) {
+  gsrb_cfg_t c = resolve_cfg(ctx, in);
+  if (!in) {
+    c.ctas_per_sm = 2;
+    c.threads = 512;
+    c.cluster = 2;
+  }
+  return c;
+}
+
+gsrb_status_t finish_stats(gsrb_graph* G, gsrb_traversal_stats_t* st, float ms) {
+  uint32_t h[32];
+  unsigned long long edges = 0;
+  GSRB_CUDA(cudaStreamSynchronize(G->ctx->stream));
+  GSRB_CUDA(cudaMemcpy(h, G->flags, sizeof(h), cudaMemcpyDeviceToHost));
+  GSRB_CUDA(cudaMemcpy(&edges, (char*)G->flags + 64, sizeof(edges), cudaMemcpyDeviceToHost));
+  if (st) {
+    st->levels = h[4];
+    st->aux = h[5];
+    st->decisions = h[6];
+    st->edges = edges;
+    st->kernel_ms = ms;
+    st->trace_records = h[4] < G->trace_cap ? h[4] : G->trace_cap;
+  }
+  if (h[0]) return GSRB_ERR_OVERFLOW;
+  if (h[7]) return GSRB_ERR_TIMEOUT;
+  return GSRB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+gsrb_status_t gsrb_graph_upload(gsrb_ctx_t ctx, const gsrb_host_csr_t* h, gsrb_graph_t* out) {
+  if (!ctx || !h || !out || !h->row_start || (h->nedges && !h->edge_dst) || h->nedges >= (1ull << 32))
+    return GSRB_ERR_ARG;
+  gsrb_graph* G = new gsrb_graph();
+  G->ctx = ctx;
+  G->n = h->nnodes;
+  G->m = (uint32_t)h->nedges;
+  G->owns = true;
+  cudaError_t e = dalloc(&G->row, (size_t)G->n + 1);
+  if (!e) e = dalloc(&G->dst, G->m);
+  if (!e) e = dalloc(&G->w, G->m);
+  if (!e) e = cudaMemcpy(G->row, h->row_start, sizeof(uint32_t) * ((size_t)G->n + 1), cudaMemcpyHostToDevice);
+  if (!e && G->m) e = cudaMemcpy(G->dst, h->edge_dst, sizeof(uint32_t) * G->m, cudaMemcpyHostToDevice);
+  if (!e && G->m && h->edge_data) e = cudaMemcpy(G->w, h->edge_data, sizeof(int32_t) * G->m, cudaMemcpyHostToDevice);
+  gsrb_status_t st = e ? cuda_err(e, "graph upload") : graph_scratch(G);
+  if (st) {
+    graph_free(G);
+    delete G;
+    return st;
+  }
+  *out = G;
+  return GSRB_OK;
+}
+
+gsrb_status_t gsrb_graph_wrap(gsrb_ctx_t ctx, uint32_t n, uint64_t m, const uint32_t* d_row, const uint32_t* d_dst,
+                              const int32_t* d_w, gsrb_graph_t* out) {
+  if (!ctx || !out || !d_row || (m && !d_dst) || m >= (1ull << 32)) return GSRB_ERR_ARG;
+  gsrb_graph* G = new gsrb_graph();
+  G->ctx = ctx;
+  G->n = n;
+  G->m = (uint32_t)m;
+  G->owns = false;
+  G->row = const_cast<uint32_t*>(d_row);
+  G->dst = const_cast<uint32_t*>(d_dst);
+  G->w = const_cast<int32_t*>(d_w);
+  gsrb_status_t st = graph_scratch(G);
+  if (st) {
+    graph_free(G);
+    delete G;
+    return st;
+  }
+  *out = G;
+  return GSRB_OK;
+}
+
+gsrb_status_t gsrb_graph_free(gsrb_graph_t G) {
+  if (!G) return GSRB_ERR_ARG;
+  cudaStreamSynchronize(G->ctx->stream);
+  graph_free(G);
+  delete G;
+  return GSRB_OK;
+}
+
+gsrb_status_t gsrb_graph_info(gsrb_graph_t G, uint32_t* n, uint64_t* m, uint32_t* nhubs) {
+  if (!G) return GSRB_ERR_ARG;
+  if (n) *n = G->n;
+  if (m) *m = G->m;
+  if (nhubs) *nhubs = G->nhubs;
+  return GSRB_OK;
+}
+
+gsrb_status_t gsrb_graph_set_policy(gsrb_graph_t G, const float* h_weights, size_t count) {
+  if (!G || !h_weights || count != sizeof(MLPWeights) / sizeof(float)) return GSRB_ERR_ARG;
+  GSRB_CUDA(cudaMemcpy(G->mlp, h_weights, sizeof(MLPWeights), cudaMemcpyHostToDevice));
+  G->mlp_set = true;
+  return GSRB_OK;
+}
+
+gsrb_status_t gsrb_graph_trace(gsrb_graph_t G, void* h_out, uint32_t max_records, uint32_t* records) {
+  if (!G || !h_out) return GSRB_ERR_ARG;
+  uint32_t h[32];
+  GSRB_CUDA(cudaStreamSynchronize(G->ctx->stream));
+  GSRB_CUDA(cudaMemcpy(h, G->flags, sizeof(h), cudaMemcpyDeviceToHost));
+  uint32_t r = h[4] < G->trace_cap ? h[4] : G->trace_cap;
+  if (r > max_records) r = max_records;
+  if (r) GSRB_CUDA(cudaMemcpy(h_out, G->trace, sizeof(LevelTrace) * r, cudaMemcpyDeviceToHost));
+  if (records) *records = r;
+  return GSRB_OK;
+}
+
+gsrb_status_t gsrb_bfs(gsrb_ctx_t ctx, gsrb_graph_t G, uint32_t src, int32_t* d_level, int32_t mode,
+                       const gsrb_cfg_t* cfgin, gsrb_traversal_stats_t* stats) {
+  if (!ctx || !G || !d_level || src >= G->n || mode < 0 || mode > GSRB_BFS_TOPO) return GSRB_ERR_ARG;
+  if (mode == GSRB_BFS_LEARNED && !G->mlp_set) return GSRB_ERR_STATE;
+  gsrb_cfg_t c = graph_cfg(ctx, cfgin);
+  const void* fn = bfs_fn(c.variant);
+  if (!fn) return GSRB_ERR_UNSUPPORTED;
+  const int grid = grid_of(ctx, c);
+  if (grid % c.cluster || c.threads % 32) return GSRB_ERR_ARG;
+  BfsArgs a;
+  a.g = dev_csr(G);
+  a.src = src;
+  a.level = d_level;
+  a.q[0] = G->q[0];
+  a.q[1] = G->q[1];
+  a.hq[0] = G->hq[0];
+  a.hq[1] = G->hq[1];
+  a.cnt = G->cnt;
+  a.overflow = G->flags;
+  a.trace = G->trace;
+  a.trace_cap = G->trace_cap;
+  a.mlp = G->mlp;
+  a.mode = mode;
+  a.alpha = 15.f;
+  a.beta = 18.f;
+  a.out = G->flags + 4;
+  a.out_edges = (unsigned long long*)((char*)G->flags + 64);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  GSRB_CUDA(cudaMemsetAsync(G->flags, 0, 128, ctx->stream));
+  gsrb::GridBarrier gb = make_barrier(ctx, c, 0, (uint32_t)grid, 0, 0);
+  void* args[] = {&gb, &a};
+  if (!ctx->events[62]) GSRB_CUDA(cudaEventCreate(&ctx->events[62]));
+  if (!ctx->events[63]) GSRB_CUDA(cudaEventCreate(&ctx->events[63]));
+  GSRB_CUDA(cudaEventRecord(ctx->events[62], ctx->stream));
+  gsrb_status_t st = launch_persistent(ctx, fn, grid, c.threads, 0, c.cluster, coop_of(c), args);
+  if (st) return st;
+  GSRB_CUDA(cudaEventRecord(ctx->events[63], ctx->stream));
+  GSRB_CUDA(cudaEventSynchronize(ctx->events[63]));
+  float ms = 0;
+  GSRB_CUDA(cudaEventElapsedTime(&ms, ctx->events[62], ctx->events[63]));
+  return finish_stats(G, stats, ms);
+}
+
+gsrb_status_t gsrb_sssp(gsrb_ctx_t ctx, gsrb_graph_t G, uint32_t src, int32_t* d_dist, int32_t delta,
+                        const gsrb_cfg_t* cfgin, gsrb_traversal_stats_t* stats) {
+  if (!ctx || !G || !d_dist || src >= G->n || delta <= 0) return GSRB_ERR_ARG;
+  gsrb_cfg_t c = graph_cfg(ctx, cfgin);
+  const void* fn = sssp_fn(c.variant);
+  if (!fn) return GSRB_ERR_UNSUPPORTED;
+  const int grid = grid_of(ctx, c);
+  if (grid % c.cluster || c.threads % 32) return GSRB_ERR_ARG;
+  SsspArgs a;
+  a.g = dev_csr(G);
+  a.src = src;
+  a.dist = d_dist;
+  for (int k = 0; k < 2; ++k) {
+    a.q[k] = G->q[k];
+    a.hq[k] = G->hq[k];
+    a.far[k] = G->far[k];
+  }
+  a.mark = G->mark;
+  a.fmark = G->fmark;
+  a.cnt = G->cnt;
+  a.fcnt = G->fcnt;
+  a.overflow = G->flags;
+  a.trace = G->trace;
+  a.trace_cap = G->trace_cap;
+  a.delta = delta;
+  a.out = G->flags + 4;
+  a.out_edges = (unsigned long long*)((char*)G->flags + 64);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  GSRB_CUDA(cudaMemsetAsync(G->flags, 0, 128, ctx->stream));
+  gsrb::GridBarrier gb = make_barrier(ctx, c, 0, (uint32_t)grid, 0, 0);
+  void* args[] = {&gb, &a};
+  if (!ctx->events[62]) GSRB_CUDA(cudaEventCreate(&ctx->events[62]));
+  if (!ctx->events[63]) GSRB_CUDA(cudaEventCreate(&ctx->events[63]));
+  GSRB_CUDA(cudaEventRecord(ctx->events[62], ctx->stream));
+  gsrb_status_t st = launch_persistent(ctx, fn, grid, c.threads, 0, c.cluster, coop_of(c), args);
+  if (st) return st;
+  GSRB_CUDA(cudaEventRecord(ctx->events[63], ctx->stream));
+  GSRB_CUDA(cudaEventSynchronize(ctx->events[63]));
+  float ms = 0;
+  GSRB_CUDA(cudaEventElapsedTime(&ms, ctx->events[62], ctx->events[63]));
+  return finish_stats(G, stats, ms);
+}
+
+gsrb_status_t gsrb_pagerank(gsrb_ctx_t ctx, gsrb_graph_t G, float alpha, int32_t iters, float* d_rank,
+                            const gsrb_cfg_t* cfgin, gsrb_traversal_stats_t* stats) {
+  if (!ctx || !G || !d_rank || iters < 0 || !(alpha >= 0.f && alpha < 1.f)) return GSRB_ERR_ARG;
+  gsrb_cfg_t c = graph_cfg(ctx, cfgin);
+  const void* fn = pr_fn(c.variant);
+  if (!fn) return GSRB_ERR_UNSUPPORTED;
+  const int grid = grid_of(ctx, c);
+  if (grid % c.cluster || c.threads % 32 || grid > 148 * 32) return GSRB_ERR_ARG;
+  PrArgs a;
+  a.g = dev_csr(G);
+  a.alpha = alpha;
+  a.iters = iters;
+  a.rank = d_rank;
+  a.contrib[0] = G->contrib[0];
+  a.contrib[1] = G->contrib[1];
+  a.hubs = G->hubs;
+  a.nhubs = G->nhubs;
+  a.hub_part = G->hub_part;
+  a.out = G->flags + 4;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  GSRB_CUDA(cudaMemsetAsync(G->flags, 0, 128, ctx->stream));
+  gsrb::GridBarrier gb = make_barrier(ctx, c, 0, (uint32_t)grid, 0, 0);
+  void* args[] = {&gb, &a};
+  if (!ctx->events[62]) GSRB_CUDA(cudaEventCreate(&ctx->events[62]));
+  if (!ctx->events[63]) GSRB_CUDA(cudaEventCreate(&ctx->events[63]));
+  GSRB_CUDA(cudaEventRecord(ctx->events[62], ctx->stream));
+  gsrb_status_t st = launch_persistent(ctx, fn, grid, c.threads, 0, c.cluster, coop_of(c), args);
+  if (st) return st;
+  GSRB_CUDA(cudaEventRecord(ctx->events[63], ctx->stream));
+  GSRB_CUDA(cudaEventSynchronize(ctx->events[63]));
+  float ms = 0;
+  GSRB_CUDA(cudaEventElapsedTime(&ms, ctx->events[62], ctx->events[63]));
+  return finish_stats(G, stats, ms);
+}
+
+}  // extern "C"

@@ -1,0 +1,197 @@
+// Shared device pieces of the persistent graph traversals (BFS, SSSP, PR):
+// the device CSR view, warp-aggregated worklist appends, warp-synchronous
+// frontier expansion with hub vertices split across the whole grid, the
+// per-level trace record and the small MLP used by the learned policy.
+//
+// Reference structures restated: the CSRGraph layout
+// (LONESTAR/rt/include/csr_graph.h.prehip:20-103), the two-slot worklists with
+// warp-aggregated pushes (LONESTAR/rt/include/worklist.h.prehip:348-420,
+// cutil_subset.h.prehip:43-48) and the nested-parallel edge expansion with
+// thread / warp / thread-block granularity (internal.h.prehip:99-158,
+// apps/bfs/kernel_gsrb.cu:400-553).
+#pragma once
+#include <stdint.h>
+#include "gsrb/ptx.cuh"
+
+namespace gsrbg {
+
+constexpr int32_t kInf = 0x7fffffff;        // INF = INT_MAX (apps/bfs/kernel_gsrb.cu:295)
+constexpr uint32_t kBigDegree = 4096;       // vertices above this are expanded by the whole grid
+constexpr uint32_t kWarpDegree = 32;        // above this a warp expands the vertex cooperatively
+
+struct DevCSR {
+  uint32_t n;
+  uint32_t m;
+  const uint32_t* __restrict__ row;  // n + 1
+  const uint32_t* __restrict__ dst;  // m
+  const int32_t* __restrict__ w;     // m (may be null for BFS / PR)
+};
+
+// One record per level / bucket step, written by CTA 0 after the barrier.
+struct LevelTrace {
+  uint32_t level;
+  uint32_t dir;          // 0 push-worklist, 1 pull, 2 push-topology
+  uint32_t nf;           // frontier vertices entering this level
+  uint32_t nu;           // unvisited vertices before this level
+  unsigned long long mf; // frontier out-edges
+  unsigned long long mu; // out-edges of unvisited vertices
+  unsigned long long t_ns;  // %globaltimer when the level started
+  float pred;            // policy's predicted log2(1 + next nf) (NaN if none)
+  uint32_t fallback;     // 1 once the policy fell back to the heuristic
+};
+static_assert(sizeof(LevelTrace) == 48, "trace layout");
+
+// Per-level counters (three rotating sets; see the BFS kernel for the protocol).
+struct LevelCounters {
+  unsigned long long n_reg;   // regular-queue appends
+  unsigned long long n_big;   // hub-queue appends
+  unsigned long long m_next;  // out-edges of appended vertices
+  unsigned long long pad;
+};
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Warp-aggregated append of `v` (where `pred`) to queue q with counter *cnt.
+// Must be called by all 32 lanes (warp-synchronous).  Returns nothing; the
+// queue capacity is checked by the caller's sizing (<= n distinct vertices).
+__device__ __forceinline__ void warp_append(bool pred, uint32_t v, uint32_t* q, unsigned long long* cnt,
+                                            uint32_t cap, uint32_t* overflow) {
+  const uint32_t mask = __ballot_sync(0xffffffffu, pred);
+  if (!mask) return;
+  const uint32_t leader = __ffs(mask) - 1;
+  unsigned long long base = 0;
+  if (lane_id() == leader) base = atomicAdd(cnt, (unsigned long long)__popc(mask));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (pred) {
+    const unsigned long long pos = base + __popc(mask & lanemask_lt());
+    if (pos < cap) q[pos] = v;
+    else atomicExch(overflow, 1u);
+  }
+}
+
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return __shfl_sync(0xffffffffu, v, 0);
+}
+__device__ __forceinline__ uint32_t warp_max_u32(uint32_t v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Expand the regular queue q[0, nq): calls f(u, edge_index) warp-synchronously
+// (every lane calls f in every step, with `active` telling whether the lane has
+// an edge).  Vertices of degree <= kWarpDegree: one lane each; larger: the warp
+// strides over the edges together.  Warps take 32-vertex groups grid-stride.
+template <class F>
+__device__ __forceinline__ void expand_queue(const DevCSR& g, const uint32_t* __restrict__ q, uint32_t nq, F& f) {
+  const uint32_t lane = lane_id();
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t base = gw * 32u; base < nq; base += nwarps * 32u) {
+    const uint32_t i = base + lane;
+    uint32_t u = 0, b = 0, e = 0;
+    if (i < nq) {
+      u = __ldcg(q + i);
+      b = __ldg(g.row + u);
+      e = __ldg(g.row + u + 1);
+    }
+    const uint32_t deg = e - b;
+    // warp-cooperative vertices
+    uint32_t coop = __ballot_sync(0xffffffffu, deg > kWarpDegree);
+    while (coop) {
+      const int src = __ffs(coop) - 1;
+      coop &= coop - 1;
+      const uint32_t uu = __shfl_sync(0xffffffffu, u, src);
+      const uint32_t bb = __shfl_sync(0xffffffffu, b, src);
+      const uint32_t ee = __shfl_sync(0xffffffffu, e, src);
+      for (uint32_t j0 = bb; j0 < ee; j0 += 32) {
+        const uint32_t j = j0 + lane;
+        f(uu, j, j < ee);
+      }
+    }
+    // lane-per-vertex for the small ones
+    const uint32_t mine = deg <= kWarpDegree ? deg : 0u;
+    const uint32_t kmax = warp_max_u32(mine);
+    for (uint32_t k = 0; k < kmax; ++k) f(u, b + k, k < mine);
+  }
+}
+
+// Expand the hub queue: every CTA takes an equal slice of every hub's edges.
+template <class F>
+__device__ __forceinline__ void expand_hubs(const DevCSR& g, const uint32_t* __restrict__ hq, uint32_t nh, F& f) {
+  const uint32_t G = gridDim.x;
+  for (uint32_t k = 0; k < nh; ++k) {
+    const uint32_t u = __ldcg(hq + k);
+    const uint32_t b = __ldg(g.row + u), e = __ldg(g.row + u + 1);
+    const uint64_t len = e - b;
+    const uint32_t s0 = b + (uint32_t)(len * blockIdx.x / G);
+    const uint32_t s1 = b + (uint32_t)(len * (blockIdx.x + 1) / G);
+    // warp-synchronous strides of the CTA over its slice
+    for (uint32_t j0 = s0 + (threadIdx.x & ~31u); j0 < s1; j0 += blockDim.x) {
+      const uint32_t j = j0 + lane_id();
+      f(u, j, j < s1);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- MLP -------
+// 12 -> 32 -> 32 -> 4 fully connected, ReLU; outputs: [0] logit(pull), [1]
+// logit(topology push), [2] predicted log2(1 + next frontier size), [3] spare.
+constexpr int kFeat = 12, kHid = 32, kOut = 4;
+struct MLPWeights {
+  float w1[kHid][kFeat];
+  float b1[kHid];
+  float w2[kHid][kHid];
+  float b2[kHid];
+  float w3[kOut][kHid];
+  float b3[kOut];
+};
+
+// Warp-cooperative forward pass (lane j computes hidden unit j); every lane
+// returns the 4 outputs.  Deterministic: same inputs give the same outputs in
+// every CTA, so every CTA takes the same decision without communicating.
+__device__ __forceinline__ void mlp_forward_warp(const MLPWeights* __restrict__ W, const float* feat, float out[kOut]) {
+  const uint32_t j = lane_id();
+  float h1 = W->b1[j];
+#pragma unroll
+  for (int i = 0; i < kFeat; ++i) h1 = fmaf(W->w1[j][i], feat[i], h1);
+  h1 = fmaxf(h1, 0.f);
+  float h2 = W->b2[j];
+#pragma unroll
+  for (int i = 0; i < kHid; ++i) h2 = fmaf(W->w2[j][i], __shfl_sync(0xffffffffu, h1, i), h2);
+  h2 = fmaxf(h2, 0.f);
+#pragma unroll
+  for (int o = 0; o < kOut; ++o) {
+    float p = W->w3[o][j] * h2;
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) p += __shfl_xor_sync(0xffffffffu, p, s);
+    out[o] = p + W->b3[o];
+  }
+}
+
+// Feature vector of a level (all log-scaled or normalised to O(1)).
+__device__ __forceinline__ void level_features(float feat[kFeat], uint32_t n, uint32_t m, uint32_t level,
+                                               uint32_t nf, unsigned long long mf, uint32_t nu,
+                                               unsigned long long mu, uint32_t prev_nf, uint32_t prev_dir) {
+  feat[0] = log2f(1.f + (float)nf);
+  feat[1] = log2f(1.f + (float)mf);
+  feat[2] = log2f(1.f + (float)nu);
+  feat[3] = log2f(1.f + (float)mu);
+  feat[4] = (float)nf / (float)(n ? n : 1);
+  feat[5] = (float)((double)mf / (double)(mu + 1));
+  feat[6] = log2f(1.f + (float)((double)mf / (double)(nf ? nf : 1)));  // mean frontier degree
+  feat[7] = log2f(1.f + (float)level);
+  feat[8] = (float)prev_dir;
+  feat[9] = log2f((float)(n ? n : 1));
+  feat[10] = log2f(1.f + (float)m) - log2f((float)(n ? n : 1));  // log mean degree
+  feat[11] = log2f(1.f + (float)nf) - log2f(1.f + (float)prev_nf);  // growth
+}
+
+}  // namespace gsrbg

@@ -21,6 +21,7 @@ struct gsrb_ctx {
   // barrier state: kSlots slots + kGroups fan-in groups (device)
   gsrb::BarrierSlot* slots = nullptr;
   gsrb::GroupSlot* groups = nullptr;
+  uint32_t* flip = nullptr;  // kSlots * kMaxFlip lines of 32 words
   // general scratch (device), grown on demand
   void* scratch = nullptr;
   size_t scratch_bytes = 0;
@@ -34,6 +35,7 @@ namespace gsrbrt {
 
 constexpr int kSlots = 128;     // slot 0: whole-grid barrier; others: sub-grid barriers
 constexpr int kGroups = 8192;   // fan-in / per-group counters shared by all slots
+constexpr int kMaxFlip = 16;    // flip words per slot (native variants)
 
 extern std::atomic<uint64_t> g_launches;
 
@@ -55,10 +57,16 @@ gsrb::GridBarrier make_barrier(gsrb_ctx* ctx, const gsrb_cfg_t& c, int slot, uin
                                uint32_t first, uint32_t group_base);
 
 // Launch a persistent kernel.  Refuses (GSRB_ERR_NOT_CORESIDENT) a grid larger
-// than the co-resident capacity; uses a cooperative launch whenever the driver
-// accepts it (always for GSRB_BAR_CCG); attaches the cluster dimension.
+// than the co-resident capacity; attaches the cluster dimension.  coop:
+// 2 = cooperative launch required (GSRB_BAR_CCG), 1 = cooperative when the
+// driver accepts it, 0 = plain launch (safe: co-residency was checked and every
+// device wait is bounded).
 gsrb_status_t launch_persistent(gsrb_ctx* ctx, const void* fn, int grid, int block, size_t smem,
-                                int cluster, bool need_coop, void** args);
+                                int cluster, int coop, void** args);
+inline int coop_of(const gsrb_cfg_t& c) {
+  if (c.variant == gsrb::V_CCG) return 2;
+  return c.launch_mode == 1 ? 0 : 1;
+}
 // Plain (non-persistent) launch on the context stream.
 gsrb_status_t launch_plain(gsrb_ctx* ctx, const void* fn, dim3 grid, dim3 block, size_t smem, void** args);
 // Co-resident capacity (CTAs) of fn for the given shape.
@@ -72,17 +80,3 @@ gsrb_status_t map_dev(uint32_t code);
 
 }  // namespace gsrbrt
 
-// Dispatch a templated kernel over the barrier variant.  F is a functor
-// template with `template <int V> const void* get()`.
-#define GSRB_VARIANT_SWITCH(v, BODY)                               \
-  switch (v) {                                                     \
-    case gsrb::V_CLUSTER: { constexpr int V = gsrb::V_CLUSTER; BODY; break; } \
-    case gsrb::V_CLUSTER_ALLPOLL: { constexpr int V = gsrb::V_CLUSTER_ALLPOLL; BODY; break; } \
-    case gsrb::V_DSMEM: { constexpr int V = gsrb::V_DSMEM; BODY; break; } \
-    case gsrb::V_SOFT2: { constexpr int V = gsrb::V_SOFT2; BODY; break; } \
-    case gsrb::V_FLAT: { constexpr int V = gsrb::V_FLAT; BODY; break; } \
-    case gsrb::V_TREE: { constexpr int V = gsrb::V_TREE; BODY; break; } \
-    case gsrb::V_CCG: { constexpr int V = gsrb::V_CCG; BODY; break; } \
-    case gsrb::V_CLUSTER_RED: { constexpr int V = gsrb::V_CLUSTER_RED; BODY; break; } \
-    default: return GSRB_ERR_ARG;                                  \
-  }

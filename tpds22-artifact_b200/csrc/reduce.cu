@@ -114,6 +114,7 @@ const void* reduce_fn(int variant) {
     case gsrb::V_TREE: return (const void*)reduce_i32_kernel<gsrb::V_TREE>;
     case gsrb::V_CCG: return (const void*)reduce_i32_kernel<gsrb::V_CCG>;
     case gsrb::V_CLUSTER_RED: return (const void*)reduce_i32_kernel<gsrb::V_CLUSTER_RED>;
+    case gsrb::V_FLIP: return (const void*)reduce_i32_kernel<gsrb::V_FLIP>;
     default: return nullptr;  // V_CLUSTER_ALLPOLL is kept to fixed-count loops
   }
 }
@@ -140,5 +141,5 @@ extern "C" gsrb_status_t gsrb_reduce_i32(gsrb_ctx_t ctx, const int32_t* d_in, si
   long long* partials = (long long*)part;
   long long* out = (long long*)d_out;
   void* args[] = {&gb, &d_in, &n64, &partials, &out};
-  return launch_persistent(ctx, fn, grid, c.threads, 0, c.cluster, c.variant == gsrb::V_CCG, args);
+  return launch_persistent(ctx, fn, grid, c.threads, 0, c.cluster, coop_of(c), args);
 }

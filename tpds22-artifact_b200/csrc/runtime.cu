@@ -59,7 +59,7 @@ gsrb::GridBarrier make_barrier(gsrb_ctx* ctx, const gsrb_cfg_t& c, int slot, uin
   gb.groups = ctx->groups + group_base;
   gb.nparticipants = np;
   gb.first_cta = first;
-  uint32_t ng = 0;
+  uint32_t ng = 0, nflip = 0;
   switch (c.variant) {
     case gsrb::V_SOFT2:
     case gsrb::V_TREE:
@@ -68,17 +68,24 @@ gsrb::GridBarrier make_barrier(gsrb_ctx* ctx, const gsrb_cfg_t& c, int slot, uin
       ng = c.fanin_groups > 0 ? (uint32_t)c.fanin_groups
                               : (np < (uint32_t)ctx->num_sms ? np : (uint32_t)ctx->num_sms);
       break;
-    case gsrb::V_FLAT:
-    case gsrb::V_CCG:
-      ng = 0;
+    case gsrb::V_CLUSTER:
+    case gsrb::V_CLUSTER_ALLPOLL:
+    case gsrb::V_DSMEM:
+    case gsrb::V_FLIP:
+      // native variants: fanin_groups = number of split flip words
+      nflip = c.fanin_groups > 0 ? (uint32_t)c.fanin_groups : 1u;
+      if (nflip > (uint32_t)kMaxFlip) nflip = kMaxFlip;
       break;
     default:
-      ng = (uint32_t)c.fanin_groups;
+      ng = 0;
   }
   if (ng + group_base > (uint32_t)kGroups) ng = kGroups - group_base;
   gb.ngroups = ng;
   gb.spin_ns = (uint32_t)c.spin_ns;
   gb.timeout_ns = (uint64_t)c.timeout_ms * 1000000ull;
+  gb.flip = ctx->flip + (size_t)slot * kMaxFlip * 32;
+  gb.nflip = nflip;
+  gb._pad = 0;
   return gb;
 }
 
@@ -111,7 +118,7 @@ gsrb_status_t coresident_ctas(gsrb_ctx* ctx, const void* fn, int block, size_t s
 }
 
 gsrb_status_t launch_persistent(gsrb_ctx* ctx, const void* fn, int grid, int block, size_t smem,
-                                int cluster, bool need_coop, void** args) {
+                                int cluster, int coop, void** args) {
   if (grid <= 0 || block <= 0 || block > 1024) return GSRB_ERR_ARG;
   if (cluster < 1) cluster = 1;
   if (grid % cluster) return GSRB_ERR_ARG;
@@ -138,13 +145,15 @@ gsrb_status_t launch_persistent(gsrb_ctx* ctx, const void* fn, int grid, int blo
     attr[na].val.clusterDim.z = 1;
     ++na;
   }
-  attr[na].id = cudaLaunchAttributeCooperative;
-  attr[na].val.cooperative = 1;
-  ++na;
+  if (coop > 0) {
+    attr[na].id = cudaLaunchAttributeCooperative;
+    attr[na].val.cooperative = 1;
+    ++na;
+  }
   cfg.attrs = attr;
   cfg.numAttrs = na;
   cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
-  if (e != cudaSuccess && !need_coop && cluster > 1 && e != cudaErrorCooperativeLaunchTooLarge) {
+  if (e != cudaSuccess && coop == 1 && cluster > 1 && e != cudaErrorCooperativeLaunchTooLarge) {
     // Some drivers refuse cooperative + cluster; the occupancy check above
     // already guarantees the grid fits, and every device wait is bounded.
     (void)cudaGetLastError();
@@ -204,9 +213,15 @@ gsrb_status_t map_dev(uint32_t code) {
 using namespace gsrbrt;
 
 namespace {
-__global__ void l2_flush_kernel(uint4* buf, size_t n, uint32_t salt) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    buf[i] = make_uint4(salt, (uint32_t)i, salt ^ 0x9e3779b9u, (uint32_t)(i >> 32));
+// Reads (does not write) a buffer of twice the L2 size, so the next timed
+// kernel starts with clean, unrelated lines in L2 and pays no write-backs.
+__global__ void l2_flush_kernel(const uint4* buf, size_t n, uint32_t salt, uint32_t* sink) {
+  uint32_t acc = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const uint4 v = __ldcg(buf + i);
+    acc ^= v.x ^ v.y ^ v.z ^ v.w;
+  }
+  if (acc == salt) sink[0] = acc;  // practically never; keeps the loads alive
 }
 }  // namespace
 
@@ -224,6 +239,9 @@ void gsrb_cfg_default(gsrb_cfg_t* c) {
   c->timeout_ms = 2000;
   c->tile = 0;
   c->grid_override = 0;
+  // plain launches: a cooperative launch costs ~2 us more on B200 and buys
+  // nothing here (co-residency is checked first and every wait is bounded)
+  c->launch_mode = 1;
 }
 
 const char* gsrb_status_string(gsrb_status_t s) {
@@ -265,6 +283,9 @@ gsrb_status_t gsrb_ctx_create(int device, gsrb_ctx_t* out) {
   size_t gbytes = sizeof(gsrb::GroupSlot) * kGroups;
   e = cudaMalloc(&c->slots, sbytes);
   if (e == cudaSuccess) e = cudaMalloc(&c->groups, gbytes);
+  const size_t fbytes = sizeof(uint32_t) * 32 * (size_t)kSlots * kMaxFlip;
+  if (e == cudaSuccess) e = cudaMalloc(&c->flip, fbytes);
+  if (e == cudaSuccess) e = cudaMemset(c->flip, 0, fbytes);
   if (e == cudaSuccess) e = cudaMemset(c->slots, 0, sbytes);
   if (e == cudaSuccess) e = cudaMemset(c->groups, 0, gbytes);
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -284,6 +305,7 @@ gsrb_status_t gsrb_ctx_destroy(gsrb_ctx_t c) {
     if (ev) cudaEventDestroy(ev);
   if (c->slots) cudaFree(c->slots);
   if (c->groups) cudaFree(c->groups);
+  if (c->flip) cudaFree(c->flip);
   if (c->scratch) cudaFree(c->scratch);
   if (c->flush) cudaFree(c->flush);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -334,6 +356,7 @@ gsrb_status_t gsrb_ctx_status(gsrb_ctx_t c, uint32_t* code, uint32_t* where, uin
     // a failed episode leaves counters half-way: reset all barrier state
     GSRB_CUDA(cudaMemset(c->slots, 0, sizeof(gsrb::BarrierSlot) * kSlots));
     GSRB_CUDA(cudaMemset(c->groups, 0, sizeof(gsrb::GroupSlot) * kGroups));
+    GSRB_CUDA(cudaMemset(c->flip, 0, sizeof(uint32_t) * 32 * (size_t)kSlots * kMaxFlip));
     GSRB_CUDA(cudaDeviceSynchronize());
   }
   return map_dev(worst);
@@ -393,14 +416,16 @@ gsrb_status_t gsrb_l2_flush(gsrb_ctx_t c) {
   if (c->flush_bytes < want) {
     if (c->flush) GSRB_CUDA(cudaFree(c->flush));
     c->flush = nullptr;
-    GSRB_CUDA(cudaMalloc(&c->flush, want));
+    GSRB_CUDA(cudaMalloc(&c->flush, want + 256));
+    GSRB_CUDA(cudaMemsetAsync(c->flush, 0x5a, want + 256, c->stream));
     c->flush_bytes = want;
   }
   static uint32_t salt = 1;
-  uint4* buf = (uint4*)c->flush;
+  const uint4* buf = (const uint4*)c->flush;
   size_t n = c->flush_bytes / sizeof(uint4);
   uint32_t s = salt++;
-  void* args[] = {&buf, &n, &s};
+  uint32_t* sink = (uint32_t*)((char*)c->flush + c->flush_bytes);
+  void* args[] = {&buf, &n, &s, &sink};
   return launch_plain(c, (const void*)l2_flush_kernel, dim3(c->num_sms * 4), dim3(512), 0, args);
 }
 

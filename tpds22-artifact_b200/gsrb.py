@@ -43,6 +43,7 @@ BAR_FLAT = 4
 BAR_TREE = 5
 BAR_CCG = 6
 BAR_CLUSTER_RED = 7
+BAR_FLIP = 8
 BAR_NONE = 99
 VARIANT_NAMES = {
     BAR_CLUSTER: "gsrb_cluster",
@@ -53,6 +54,7 @@ VARIANT_NAMES = {
     BAR_TREE: "atomic_tree",
     BAR_CCG: "ccg_grid_sync",
     BAR_CLUSTER_RED: "gsrb_cluster_red",
+    BAR_FLIP: "gsrb_flip",
     BAR_NONE: "none",
 }
 
@@ -75,7 +77,8 @@ class Cfg(C.Structure):
         ("timeout_ms", C.c_uint32),
         ("tile", C.c_int32),
         ("grid_override", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("launch_mode", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
     def as_dict(self):
@@ -134,7 +137,36 @@ _SIGS = {
                                     C.POINTER(HostCSR)]),
     "gsrb_gr_read": (C.c_int32, [C.c_char_p, C.POINTER(HostCSR)]),
     "gsrb_gr_write": (C.c_int32, [C.c_char_p, C.POINTER(HostCSR), C.c_int32]),
+    "gsrb_scan_u32": (C.c_int32, [_P, _P, _P, C.c_size_t, C.POINTER(Cfg)]),
+    "gsrb_scan_f32": (C.c_int32, [_P, _P, _P, C.c_size_t, C.POINTER(Cfg)]),
+    "gsrb_semaphore_bench": (C.c_int32, [_P, C.POINTER(Cfg), C.c_int32, C.c_uint32, C.c_int32, C.c_int32,
+                                         C.c_int32, _P]),
+    "gsrb_mutex_bench": (C.c_int32, [_P, C.POINTER(Cfg), C.c_int32, C.c_int32, C.c_int32, _P]),
+    "gsrb_graph_upload": (C.c_int32, [_P, C.POINTER(HostCSR), C.POINTER(_P)]),
+    "gsrb_graph_free": (C.c_int32, [_P]),
+    "gsrb_graph_info": (C.c_int32, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
+    "gsrb_graph_set_policy": (C.c_int32, [_P, _P, C.c_size_t]),
+    "gsrb_graph_trace": (C.c_int32, [_P, _P, C.c_uint32, C.POINTER(C.c_uint32)]),
+    "gsrb_bfs": (C.c_int32, [_P, _P, C.c_uint32, _P, C.c_int32, C.POINTER(Cfg), C.c_void_p]),
+    "gsrb_sssp": (C.c_int32, [_P, _P, C.c_uint32, _P, C.c_int32, C.POINTER(Cfg), C.c_void_p]),
+    "gsrb_pagerank": (C.c_int32, [_P, _P, C.c_float, C.c_int32, _P, C.POINTER(Cfg), C.c_void_p]),
 }
+
+# semaphore / mutex kinds, BFS modes
+SEM_REF_SPIN, SEM_REF_EBO, SEM_REF_PRIORITY, SEM_REF_PRIORITY_EBO, SEM_PRIORITY = range(5)
+MUTEX_SPIN, MUTEX_EBO, MUTEX_FA, MUTEX_SLEEP = range(4)
+BFS_PUSH, BFS_HEURISTIC, BFS_LEARNED, BFS_PULL, BFS_TOPO = range(5)
+
+
+class TraversalStats(C.Structure):
+    _fields_ = [("levels", C.c_uint32), ("aux", C.c_uint32), ("decisions", C.c_uint32),
+                ("trace_records", C.c_uint32), ("edges", C.c_uint64), ("kernel_ms", C.c_float),
+                ("_pad", C.c_uint32)]
+
+
+TRACE_DTYPE = np.dtype([("level", "<u4"), ("dir", "<u4"), ("nf", "<u4"), ("nu", "<u4"), ("mf", "<u8"),
+                        ("mu", "<u8"), ("t_ns", "<u8"), ("pred", "<f4"), ("fallback", "<u4")])
+assert TRACE_DTYPE.itemsize == 48
 
 
 def _lib():
@@ -162,8 +194,21 @@ def register(name, restype, argtypes):
         fn.argtypes = argtypes
 
 
+class _Checked:
+    """Exposes only entry points with a declared signature: calling a C function
+    through ctypes without argtypes would silently truncate 64-bit pointers."""
+
+    def __init__(self, raw):
+        self._raw = raw
+
+    def __getattr__(self, name):
+        if name not in _SIGS:
+            raise AttributeError(f"{name}: no ctypes signature declared in gsrb.py")
+        return getattr(self._raw, name)
+
+
 def lib():
-    return _lib()
+    return _Checked(_lib())
 
 
 def check(st: int, what: str = ""):
@@ -310,6 +355,78 @@ class Context:
     # -- reduce ----------------------------------------------------------------
     def reduce_i32(self, d_in: DeviceArray, n: int, d_out: DeviceArray, c: Cfg | None = None) -> int:
         return _lib().gsrb_reduce_i32(self.h, d_in.ptr, n, d_out.ptr, C.byref(c) if c is not None else None)
+
+
+    # -- scan ------------------------------------------------------------------
+    def scan(self, d_in: DeviceArray, d_out: DeviceArray, n: int, c: Cfg | None = None) -> int:
+        fn = _lib().gsrb_scan_f32 if d_in.dtype == np.float32 else _lib().gsrb_scan_u32
+        return fn(self.h, d_in.ptr, d_out.ptr, n, C.byref(c) if c is not None else None)
+
+    # -- locks ------------------------------------------------------------------
+    def semaphore_bench(self, c: Cfg, kind: int, capacity: int, writer_every: int, iters: int, incs: int,
+                        counters: DeviceArray) -> int:
+        return _lib().gsrb_semaphore_bench(self.h, C.byref(c), kind, capacity, writer_every, iters, incs,
+                                           counters.ptr)
+
+    def mutex_bench(self, c: Cfg, kind: int, iters: int, incs: int, counters: DeviceArray) -> int:
+        return _lib().gsrb_mutex_bench(self.h, C.byref(c), kind, iters, incs, counters.ptr)
+
+    # -- graphs -----------------------------------------------------------------
+    def graph(self, g: "Graph") -> "DeviceGraph":
+        return DeviceGraph(self, g)
+
+
+class DeviceGraph:
+    """A graph resident on the device with its traversal scratch."""
+
+    def __init__(self, ctx: Context, g: "Graph"):
+        self.ctx = ctx
+        self.host = g
+        h = g._as_host()
+        p = C.c_void_p()
+        check(_lib().gsrb_graph_upload(ctx.h, C.byref(h), C.byref(p)), "graph_upload")
+        self.h = p.value
+        self.n = g.nnodes
+        self.m = g.nedges
+
+    def free(self):
+        if self.h:
+            _lib().gsrb_graph_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def set_policy(self, weights: np.ndarray):
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        check(_lib().gsrb_graph_set_policy(self.h, w.ctypes.data, w.size), "set_policy")
+
+    def trace(self, max_records=1 << 16) -> np.ndarray:
+        out = np.zeros(max_records, dtype=TRACE_DTYPE)
+        r = C.c_uint32()
+        check(_lib().gsrb_graph_trace(self.h, out.ctypes.data, max_records, C.byref(r)), "trace")
+        return out[:r.value]
+
+    def bfs(self, src: int, out: DeviceArray, mode: int = BFS_HEURISTIC, c: Cfg | None = None):
+        st = TraversalStats()
+        rc = _lib().gsrb_bfs(self.ctx.h, self.h, src, out.ptr, mode, C.byref(c) if c is not None else None,
+                             C.addressof(st))
+        return rc, st
+
+    def sssp(self, src: int, out: DeviceArray, delta: int, c: Cfg | None = None):
+        st = TraversalStats()
+        rc = _lib().gsrb_sssp(self.ctx.h, self.h, src, out.ptr, delta, C.byref(c) if c is not None else None,
+                              C.addressof(st))
+        return rc, st
+
+    def pagerank(self, out: DeviceArray, alpha: float = 0.85, iters: int = 50, c: Cfg | None = None):
+        st = TraversalStats()
+        rc = _lib().gsrb_pagerank(self.ctx.h, self.h, alpha, iters, out.ptr,
+                                  C.byref(c) if c is not None else None, C.addressof(st))
+        return rc, st
 
 
 def launch_count() -> int:
