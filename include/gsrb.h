@@ -53,6 +53,9 @@ enum {
   GSRB_BAR_CCG = 6,              /* cooperative_groups grid.sync() (library baseline) */
   GSRB_BAR_CLUSTER_RED = 7,      /* 3-level, completer-publishes protocol (red.release arrivals, polling master) */
   GSRB_BAR_FLIP = 8,             /* 2-level: every CTA arrives on the split sum-to-flip words */
+  GSRB_BAR_FANOUT = 9,           /* 2-level: counter + generation published to R wake-up lines */
+  GSRB_BAR_CLUSTER_FANOUT = 10,  /* 3-level: HW cluster arrival, leader on the counter, R wake-up lines */
+  GSRB_BAR_HIER = 11,            /* 3-level: group counters (fanin_groups) -> root counter -> R wake-up lines */
   GSRB_BAR_NONE = 99             /* no barrier (phase-only timing baseline) */
 };
 
@@ -69,7 +72,8 @@ typedef struct gsrb_cfg {
   int32_t grid_override; /* exact grid size (0 = ctas_per_sm * #SMs) */
   int32_t launch_mode;   /* 0 = cooperative launch when the driver accepts it, 1 = plain launch (default)
                             (both only after the co-residency check; CCG is always cooperative) */
-  int32_t reserved[6];
+  int32_t wake_lines;    /* FANOUT / CLUSTER_FANOUT / HIER: wake-up lines the generation is published to (0 = 8) */
+  int32_t reserved[5];
 } gsrb_cfg_t;
 
 void gsrb_cfg_default(gsrb_cfg_t* cfg);
@@ -254,6 +258,55 @@ gsrb_status_t gsrb_sssp(gsrb_ctx_t ctx, gsrb_graph_t g, uint32_t src, int32_t* d
 /* Pull PageRank: x0 = 1 - alpha, `iters` iterations of x = (1-alpha) + alpha * sum x_u/deg(u). */
 gsrb_status_t gsrb_pagerank(gsrb_ctx_t ctx, gsrb_graph_t g, float alpha, int32_t iters, float* d_rank,
                             const gsrb_cfg_t* cfg, gsrb_traversal_stats_t* stats);
+
+/* ---- batched traversals --------------------------------
+ * k graphs (k <= 127) traversed in ONE persistent launch: instance i owns a
+ * contiguous range of CTAs (in proportion to its edges, at least one) and a
+ * sub-grid barrier of its own carved from the context's barrier state, so
+ * instances never wait for each other.  cfg->variant must not use hardware
+ * cluster barriers (SOFT2, FLAT, TREE, FLIP, FANOUT; default FANOUT).
+ * The launches are asynchronous and can be captured in a CUDA graph. */
+typedef struct gsrb_batch* gsrb_batch_t;
+gsrb_status_t gsrb_batch_create(gsrb_ctx_t ctx, const gsrb_graph_t* graphs, int32_t k, const gsrb_cfg_t* cfg,
+                                gsrb_batch_t* out);
+gsrb_status_t gsrb_batch_free(gsrb_batch_t b);
+/* CTA range of every instance (arrays of k, may be NULL). */
+gsrb_status_t gsrb_batch_layout(gsrb_batch_t b, uint32_t* first, uint32_t* count);
+/* Asynchronous: BFS of every instance (d_levels[i] int32[n_i]) / SSSP (d_dists[i]). */
+gsrb_status_t gsrb_batch_bfs(gsrb_batch_t b, const uint32_t* srcs, int32_t* const* d_levels, int32_t mode);
+gsrb_status_t gsrb_batch_sssp(gsrb_batch_t b, const uint32_t* srcs, int32_t* const* d_dists, int32_t delta);
+/* Synchronous: per-instance statistics of the last batched launch (array of k). */
+gsrb_status_t gsrb_batch_stats(gsrb_batch_t b, gsrb_traversal_stats_t* stats);
+
+/* CUDA graphs over the context stream: capture asynchronous calls, replay them. */
+typedef struct gsrb_exec* gsrb_exec_t;
+gsrb_status_t gsrb_capture_begin(gsrb_ctx_t ctx);
+gsrb_status_t gsrb_capture_end(gsrb_ctx_t ctx, gsrb_exec_t* out);
+gsrb_status_t gsrb_exec_launch(gsrb_ctx_t ctx, gsrb_exec_t exec);
+gsrb_status_t gsrb_exec_free(gsrb_exec_t exec);
+
+/* ---- the learned policy: a 12 -> 32 -> 32 -> 4 FP32 MLP -----------------------------
+ * Parameter layout (floats): w1[32][12], b1[32], w2[32][32], b2[32], w3[4][32], b3[4].
+ * Heads: [0] logit(pull faster than push), [1] logit(topology push faster than
+ * worklist push), [2] log2(1 + next frontier size), [3] spare.  Loss: masked
+ * BCE-with-logits on heads 0-1, masked 0.5*(z-y)^2 on heads 2-3, batch mean.
+ * No counterpart in the reference (its traversals use fixed schedules). */
+size_t gsrb_mlp_param_count(void);
+/* He-uniform initialisation from a seed (host). */
+gsrb_status_t gsrb_mlp_init(uint64_t seed, float* h_params);
+/* The 12 features of a level, as the traversal computes them on the device. */
+void gsrb_level_features(uint32_t n, uint32_t m, uint32_t level, uint32_t nf, uint64_t mf, uint32_t nu, uint64_t mu,
+                         uint32_t prev_nf, uint32_t prev_dir, float* h_out12);
+/* Inference: d_out[B][4] from d_x[B][12].  Asynchronous. */
+gsrb_status_t gsrb_mlp_forward(gsrb_ctx_t ctx, const float* d_params, const float* d_x, int32_t B, float* d_out);
+/* One loss + gradient evaluation (d_grad: param_count floats, d_loss: 1 float).  Asynchronous. */
+gsrb_status_t gsrb_mlp_loss_grad(gsrb_ctx_t ctx, const float* d_params, const float* d_x, const float* d_y,
+                                 const float* d_mask, int32_t B, float* d_grad, float* d_loss);
+/* Full-batch Adam training, `steps` steps, in one persistent launch (grid barrier
+ * between the forward/backward and the update phases).  d_loss_hist: steps floats
+ * (may be NULL).  Asynchronous. */
+gsrb_status_t gsrb_mlp_train(gsrb_ctx_t ctx, float* d_params, const float* d_x, const float* d_y,
+                             const float* d_mask, int32_t B, int32_t steps, float lr, float* d_loss_hist);
 
 /* ---- host-side graphs and synthetic inputs ----------------------------------------
  * CSR in the layout of the reference CSRGraph (row_start[n+1], edge_dst[m],

@@ -57,7 +57,10 @@ enum Variant : int {
   V_CCG = 6,             // cooperative_groups::this_grid().sync()
   V_CLUSTER_RED = 7,     // HW cluster barrier -> red.release arrivals, master polls count
   V_FLIP = 8,            // no cluster level: every CTA arrives on the split flip words
-  V_COUNT = 9
+  V_FANOUT = 9,          // one arrival counter, generation published to R wake-up lines
+  V_CLUSTER_FANOUT = 10, // HW cluster arrival -> leader on the counter -> every CTA polls its wake-up line
+  V_HIER = 11,           // group counters on separate lines -> root counter -> wake-up lines
+  V_COUNT = 12
 };
 
 // One global barrier slot: four 128-byte lines so that the arrival counter, the
@@ -185,50 +188,55 @@ __device__ __forceinline__ bool global_arrive_atom(const GridBarrier& gb, uint32
 }
 
 // ---- split "sum-to-flip" global level (the native variants) -----------------
-// R flip words (R = max(1, nflip)), each on its own 128-byte line of the
-// slot's flip area (separate from the counters of the other protocols).
-// Arrival unit idx of n adds to word r = idx % R: the first unit of each word
-// adds 0x80000000 - (count_r - 1), every other unit adds 1, so the word's top
-// bit toggles exactly when its last arrival lands and its low bits return to
-// their old value -- no completer, no reset store, and the arrivals are
-// fire-and-forget `red.release.gpu.add`.  Splitting the arrivals over R words
-// divides the same-address serialisation at the L2 by R.  A waiter knows the
-// sense it waits for (it toggles once per episode) and polls every word that
-// has not flipped yet with `ld.acquire.gpu`.
+// R flip words (R = min(nflip, n), nflip <= kFlipLines), each on its own
+// 128-byte line in the first half of the slot's flip area (separate from the
+// counters of the other protocols).  Arrival unit idx of n adds to word
+// r = idx % R: the first unit of each word adds 0x80000000 - (count_r - 1),
+// every other unit adds 1, so the word's top bit toggles exactly when its last
+// arrival lands and its low bits return to their old value -- no completer, no
+// reset store, and the arrivals are fire-and-forget `red.release.gpu.add`.
+// Splitting the arrivals over R words divides the same-address serialisation
+// at the L2 by R.  Each waiter keeps the top bit it expects of every word (a
+// word's parity depends on how many episodes it has seen over earlier
+// launches, so the words are tracked separately) and polls the words that have
+// not flipped yet with `ld.acquire.gpu`.
+constexpr uint32_t kFlipLines = 8;    // lines 0..7: flip words
+constexpr uint32_t kFanoutBase = 8;   // lines 8..15: wake-up lines of the fan-out protocol
+constexpr uint32_t kFanoutLines = 8;
+
 __device__ __forceinline__ uint32_t* flip_word(const GridBarrier& gb, uint32_t r) { return gb.flip + r * 32u; }
-__device__ __forceinline__ uint32_t flip_words(const GridBarrier& gb) { return gb.nflip ? gb.nflip : 1u; }
+__device__ __forceinline__ uint32_t flip_count(const GridBarrier& gb, uint32_t n) {
+  uint32_t R = gb.nflip ? gb.nflip : 1u;
+  if (R > kFlipLines) R = kFlipLines;
+  return R < n ? R : n;
+}
 
 __device__ __forceinline__ void flip_arrive(const GridBarrier& gb, uint32_t idx, uint32_t n) {
-  const uint32_t R = flip_words(gb) < n ? flip_words(gb) : n;
+  const uint32_t R = flip_count(gb, n);
   const uint32_t r = idx % R;
   const uint32_t cnt = group_size(n, R, r);
   const uint32_t inc = (idx == r) ? (0x80000000u - (cnt - 1u)) : 1u;
   ptx::red_add_release_gpu(flip_word(gb, r), inc);
 }
 
-// Wait until every word in use has top bit == sense.  Bounded.
-__device__ __forceinline__ bool flip_wait(const GridBarrier& gb, uint32_t n, uint32_t sense, uint32_t episode) {
-  const uint32_t R = flip_words(gb) < n ? flip_words(gb) : n;
+// Bit r of the returned mask = the top bit word r will show after the next flip.
+__device__ __forceinline__ uint32_t flip_expect_init(const GridBarrier& gb, uint32_t n) {
+  const uint32_t R = flip_count(gb, n);
+  uint32_t m = 0;
+  for (uint32_t r = 0; r < R; ++r) m |= ((ptx::ld_acquire_gpu(flip_word(gb, r)) >> 31) ^ 1u) << r;
+  return m;
+}
+__device__ __forceinline__ uint32_t flip_all(const GridBarrier& gb, uint32_t n) {
+  return (1u << flip_count(gb, n)) - 1u;
+}
+
+// Wait until every word r in use shows top bit == bit r of `expect`.  Bounded.
+__device__ __forceinline__ bool flip_wait(const GridBarrier& gb, uint32_t n, uint32_t expect, uint32_t episode) {
+  const uint32_t R = flip_count(gb, n);
   uint64_t t0 = 0;
-  if (R == 1) {
-    const uint32_t* w = flip_word(gb, 0);
-    for (uint32_t it = 0;; ++it) {
-      if ((ptx::ld_acquire_gpu(w) >> 31) == sense) return true;
-      if ((it & 31u) == 31u) {
-        if (ptx::ld_relaxed_gpu(&gb.slot->status) != 0u) return false;
-        const uint64_t now = ptx::globaltimer_ns();
-        if (t0 == 0) t0 = now;
-        else if (now - t0 > gb.timeout_ns) {
-          record_error(gb, GSRB_DEV_TIMEOUT, episode);
-          return false;
-        }
-      }
-      if (gb.spin_ns) __nanosleep(gb.spin_ns);
-    }
-  }
   uint32_t next = 0;  // words below `next` have flipped
   for (uint32_t it = 0;; ++it) {
-    while (next < R && (ptx::ld_acquire_gpu(flip_word(gb, next)) >> 31) == sense) ++next;
+    while (next < R && (ptx::ld_acquire_gpu(flip_word(gb, next)) >> 31) == ((expect >> next) & 1u)) ++next;
     if (next == R) return true;
     if ((it & 31u) == 31u) {
       if (ptx::ld_relaxed_gpu(&gb.slot->status) != 0u) return false;
@@ -243,8 +251,58 @@ __device__ __forceinline__ bool flip_wait(const GridBarrier& gb, uint32_t n, uin
   }
 }
 
-__device__ __forceinline__ uint32_t flip_sense0(const GridBarrier& gb) {
-  return ptx::ld_acquire_gpu(flip_word(gb, 0)) >> 31;
+// ---- counter + fan-out wake-up lines (V_FANOUT, V_CLUSTER_FANOUT) -------------
+// Arrivals (one per unit) go to the counter line slot->count with a release
+// RMW (fence.acq_rel + relaxed atom); the unit whose arrival completes the
+// episode acquires (fence.acq_rel), resets the counter and writes the new
+// generation into all kFanoutLines wake-up lines (second half of the flip
+// area; all of them, so they always hold the same value whatever R a later
+// launch uses); unit u polls line u % R with ld.acquire.  Keeping the polled
+// lines apart from the counter line means the polling loads never queue in
+// front of the arrival atomics, and R lines divide the polling load per L2
+// slice by R.  Returns true when this unit completed the episode.
+__device__ __forceinline__ uint32_t* fanout_line(const GridBarrier& gb, uint32_t r) {
+  return gb.flip + (kFanoutBase + r) * 32u;
+}
+__device__ __forceinline__ uint32_t fanout_count(const GridBarrier& gb) {
+  uint32_t R = gb.nflip ? gb.nflip : 1u;
+  return R > kFanoutLines ? kFanoutLines : R;
+}
+__device__ __forceinline__ bool fanout_arrive(const GridBarrier& gb, uint32_t n, uint32_t epoch) {
+  ptx::fence_acq_rel_gpu();
+  if (ptx::atom_add_relaxed_gpu(&gb.slot->count, 1u) != n - 1u) return false;
+  ptx::fence_acq_rel_gpu();
+  ptx::st_relaxed_gpu(&gb.slot->count, 0u);
+  for (uint32_t r = 0; r < kFanoutLines; ++r) ptx::st_relaxed_gpu(fanout_line(gb, r), epoch + 1u);
+  return true;
+}
+__device__ __forceinline__ bool fanout_wait(const GridBarrier& gb, uint32_t unit, uint32_t epoch, uint32_t episode) {
+  return wait_ne(fanout_line(gb, unit % fanout_count(gb)), epoch, gb, episode);
+}
+
+// ---- two-level counters + wake-up lines (V_HIER) --------------------------------
+// Unit u arrives on group counter u % G (each group counter on its own 256-byte
+// line, so G groups spread the same-address serialisation over G L2 lines);
+// the group's last arrival acquires and arrives on the root counter for the
+// group; the root's last arrival resets the counters it completed and publishes
+// the generation to every wake-up line.  Every RMW is a release (fence.acq_rel
+// before a relaxed atom); a completer acquires with a second fence.
+__device__ __forceinline__ bool hier_arrive(const GridBarrier& gb, uint32_t idx, uint32_t n, uint32_t epoch) {
+  const uint32_t G = gb.ngroups;
+  ptx::fence_acq_rel_gpu();
+  if (G > 1 && n > G) {
+    const uint32_t g = idx % G;
+    uint32_t* gc = &gb.groups[g].count;
+    if (ptx::atom_add_relaxed_gpu(gc, 1u) != group_size(n, G, g) - 1u) return false;
+    ptx::fence_acq_rel_gpu();
+    ptx::st_relaxed_gpu(gc, 0u);
+    n = G;
+  }
+  if (ptx::atom_add_relaxed_gpu(&gb.slot->count, 1u) != n - 1u) return false;
+  ptx::fence_acq_rel_gpu();
+  ptx::st_relaxed_gpu(&gb.slot->count, 0u);
+  for (uint32_t r = 0; r < kFanoutLines; ++r) ptx::st_relaxed_gpu(fanout_line(gb, r), epoch + 1u);
+  return true;
 }
 
 // Global level, red flavour: arrivals are fire-and-forget `red.release.gpu.add`;
@@ -271,10 +329,19 @@ struct GridSync {
   BarrierShared* sh;
   uint32_t epoch;    // meaningful in thread 0
   uint32_t episode;  // meaningful in thread 0
-  uint32_t sense;    // flip variants: top bit the next episode waits for (thread 0)
+  uint32_t sense;    // flip variants: per-word top bits the next episode waits for (thread 0)
+
+  static constexpr bool kCluster = V == V_CLUSTER || V == V_CLUSTER_ALLPOLL || V == V_DSMEM ||
+                                   V == V_CLUSTER_RED || V == V_CLUSTER_FANOUT;
+  static constexpr bool kFlip = V == V_CLUSTER || V == V_CLUSTER_ALLPOLL || V == V_DSMEM || V == V_FLIP;
+  static constexpr bool kFanout = V == V_FANOUT || V == V_CLUSTER_FANOUT || V == V_HIER;
 
   // Index of this CTA among the participants and of its arrival unit.
   __device__ __forceinline__ uint32_t my_index() const { return blockIdx.x - gb.first_cta; }
+  // Arrival units at the global level (clusters for the cluster variants).
+  __device__ __forceinline__ uint32_t units() const {
+    return (V == V_FLIP || V == V_FANOUT) ? gb.nparticipants : gb.nparticipants / ptx::cluster_nctarank();
+  }
 
   // Reads the current generation and refuses to start after a recorded error.
   // For the cluster variants the verdict is taken by the cluster leader and
@@ -285,14 +352,15 @@ struct GridSync {
     sh = s;
     episode = 0;
     if (threadIdx.x == 0) {
-      epoch = ptx::ld_acquire_gpu(&gb.slot->epoch);
-      sense = (V == V_CLUSTER || V == V_CLUSTER_ALLPOLL || V == V_DSMEM || V == V_FLIP)
-                  ? (detail::flip_sense0(gb) ^ 1u) : 0u;
+      // the generation word each protocol waits on (read before this CTA
+      // arrives anywhere, so it cannot have moved past this launch's first episode)
+      epoch = kFanout ? ptx::ld_acquire_gpu(detail::fanout_line(gb, 0)) : ptx::ld_acquire_gpu(&gb.slot->epoch);
+      sense = kFlip ? detail::flip_expect_init(gb, units()) : 0u;
       sh->arrive = 0;
       sh->release = 0;
       sh->ok = 0;
     }
-    if (V == V_CLUSTER || V == V_CLUSTER_ALLPOLL || V == V_DSMEM || V == V_CLUSTER_RED) {
+    if (kCluster) {
       ptx::cluster_sync();  // peers' shared words are initialised
       if (threadIdx.x == 0 && ptx::cluster_ctarank() == 0) {
         const uint32_t ok = (ptx::ld_relaxed_gpu(&gb.slot->status) == 0u) ? 1u : 0u;
@@ -311,9 +379,7 @@ struct GridSync {
   // Cluster variants must not leave while a peer may still touch their shared
   // memory; every CTA calls finish() once, on every exit path.
   __device__ void finish() {
-    if (V == V_CLUSTER || V == V_CLUSTER_ALLPOLL || V == V_DSMEM || V == V_CLUSTER_RED) {
-      ptx::cluster_sync();
-    }
+    if (kCluster) ptx::cluster_sync();
   }
 
   __device__ bool sync();
@@ -336,7 +402,7 @@ __device__ __forceinline__ bool GridSync<V_CLUSTER>::sync() {
     for (uint32_t r = 0; r < n; ++r) ptx::st_cluster_relaxed_u32(ptx::mapa_shared(sa, r), ok ? 1u : 0u);
   }
   ptx::cluster_sync();
-  if (threadIdx.x == 0) { sense ^= 1u; ++episode; }
+  if (threadIdx.x == 0) { sense ^= detail::flip_all(gb, units()); ++episode; }
   return sh->ok != 0u;
 }
 
@@ -375,7 +441,7 @@ __device__ __forceinline__ bool GridSync<V_CLUSTER_ALLPOLL>::sync() {
     const uint32_t ncl = gb.nparticipants / n;
     if (ptx::cluster_ctarank() == 0) detail::flip_arrive(gb, my_index() / n, ncl);
     sh->ok = detail::flip_wait(gb, ncl, sense, episode) ? 1u : 0u;
-    sense ^= 1u;
+    sense ^= detail::flip_all(gb, ncl);
     ++episode;
   }
   __syncthreads();
@@ -438,7 +504,59 @@ __device__ __forceinline__ bool GridSync<V_DSMEM>::sync() {
       }
     }
     sh->ok = ok ? 1u : 0u;
-    sense ^= 1u;
+    sense ^= detail::flip_all(gb, gb.nparticipants / n);
+    ++episode;
+  }
+  __syncthreads();
+  return sh->ok != 0u;
+}
+
+// V_FANOUT: __syncthreads, every CTA's thread 0 arrives on the counter and the
+// completer publishes the generation to the wake-up lines; CTA b polls line b % R.
+template <>
+__device__ __forceinline__ bool GridSync<V_FANOUT>::sync() {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    bool ok = true;
+    if (!detail::fanout_arrive(gb, gb.nparticipants, epoch))
+      ok = detail::fanout_wait(gb, my_index(), epoch, episode);
+    sh->ok = ok ? 1u : 0u;
+    ++epoch;
+    ++episode;
+  }
+  __syncthreads();
+  return sh->ok != 0u;
+}
+
+// V_CLUSTER_FANOUT: one hardware cluster barrier for arrival; the cluster
+// leader arrives on the counter; every CTA's thread 0 polls its wake-up line.
+// Per-CTA verdict (see V_CLUSTER_ALLPOLL): fixed-count loops only.
+template <>
+__device__ __forceinline__ bool GridSync<V_CLUSTER_FANOUT>::sync() {
+  ptx::cluster_sync();
+  if (threadIdx.x == 0) {
+    bool done = false;
+    if (ptx::cluster_ctarank() == 0) done = detail::fanout_arrive(gb, gb.nparticipants / ptx::cluster_nctarank(), epoch);
+    sh->ok = (done || detail::fanout_wait(gb, my_index(), epoch, episode)) ? 1u : 0u;
+    ++epoch;
+    ++episode;
+  }
+  __syncthreads();
+  return sh->ok != 0u;
+}
+
+// V_HIER: __syncthreads; thread 0 arrives on its group counter (groups =
+// fanin_groups); group completers arrive on the root; the root completer
+// publishes to the wake-up lines (R = nflip, at most 8); CTA b polls line b % R.
+template <>
+__device__ __forceinline__ bool GridSync<V_HIER>::sync() {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    bool ok = true;
+    if (!detail::hier_arrive(gb, my_index(), gb.nparticipants, epoch))
+      ok = detail::fanout_wait(gb, my_index(), epoch, episode);
+    sh->ok = ok ? 1u : 0u;
+    ++epoch;
     ++episode;
   }
   __syncthreads();
@@ -453,7 +571,7 @@ __device__ __forceinline__ bool GridSync<V_FLIP>::sync() {
   if (threadIdx.x == 0) {
     detail::flip_arrive(gb, my_index(), gb.nparticipants);
     sh->ok = detail::flip_wait(gb, gb.nparticipants, sense, episode) ? 1u : 0u;
-    sense ^= 1u;
+    sense ^= detail::flip_all(gb, gb.nparticipants);
     ++episode;
   }
   __syncthreads();

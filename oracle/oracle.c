@@ -551,3 +551,97 @@ double orc_cpu_semaphore(int nthreads, int capacity, int writer_every, int iters
   free(s);
   return (double)nthreads * iters / (t1 - t0);
 }
+
+/* ---------------------------------------------- policy MLP (FP64 checker) */
+enum { MF = 12, MH = 32, MO = 4 };
+typedef struct {
+  const float *w1, *b1, *w2, *b2, *w3, *b3;
+} mlp_view;
+
+static mlp_view mlp_split(const float* p) {
+  mlp_view v;
+  v.w1 = p;
+  v.b1 = v.w1 + MH * MF;
+  v.w2 = v.b1 + MH;
+  v.b2 = v.w2 + MH * MH;
+  v.w3 = v.b2 + MH;
+  v.b3 = v.w3 + MO * MH;
+  return v;
+}
+
+static void mlp_fwd1(mlp_view v, const float* x, double* a1, double* a2, double* z3) {
+  for (int j = 0; j < MH; ++j) {
+    double s = v.b1[j];
+    for (int i = 0; i < MF; ++i) s += (double)v.w1[j * MF + i] * x[i];
+    a1[j] = s > 0 ? s : 0;
+  }
+  for (int j = 0; j < MH; ++j) {
+    double s = v.b2[j];
+    for (int k = 0; k < MH; ++k) s += (double)v.w2[j * MH + k] * a1[k];
+    a2[j] = s > 0 ? s : 0;
+  }
+  for (int o = 0; o < MO; ++o) {
+    double s = v.b3[o];
+    for (int k = 0; k < MH; ++k) s += (double)v.w3[o * MH + k] * a2[k];
+    z3[o] = s;
+  }
+}
+
+void orc_mlp_forward(const float* params, const float* X, int B, double* out) {
+  mlp_view v = mlp_split(params);
+  double a1[MH], a2[MH];
+  for (int b = 0; b < B; ++b) mlp_fwd1(v, X + b * MF, a1, a2, out + b * MO);
+}
+
+void orc_mlp_loss_grad(const float* params, const float* X, const float* Y, const float* M, int B, double* grad,
+                       double* loss) {
+  mlp_view v = mlp_split(params);
+  const int P = MH * MF + MH + MH * MH + MH + MO * MH + MO;
+  for (int p = 0; p < P; ++p) grad[p] = 0.0;
+  double* gw1 = grad;
+  double* gb1 = gw1 + MH * MF;
+  double* gw2 = gb1 + MH;
+  double* gb2 = gw2 + MH * MH;
+  double* gw3 = gb2 + MH;
+  double* gb3 = gw3 + MO * MH;
+  double L = 0.0;
+  for (int b = 0; b < B; ++b) {
+    const float* x = X + b * MF;
+    const float* y = Y + b * MO;
+    const float* m = M + b * MO;
+    double a1[MH], a2[MH], z[MO], g3[MO], g2[MH], g1[MH];
+    mlp_fwd1(v, x, a1, a2, z);
+    for (int o = 0; o < MO; ++o) {
+      if (o < 2) {
+        double sp = (z[o] > 0 ? z[o] : 0) + log1p(exp(-fabs(z[o])));
+        L += m[o] * (sp - y[o] * z[o]);
+        g3[o] = m[o] * (1.0 / (1.0 + exp(-z[o])) - y[o]) / B;
+      } else {
+        double e = z[o] - y[o];
+        L += m[o] * 0.5 * e * e;
+        g3[o] = m[o] * e / B;
+      }
+    }
+    for (int k = 0; k < MH; ++k) {
+      double s = 0;
+      for (int o = 0; o < MO; ++o) s += (double)v.w3[o * MH + k] * g3[o];
+      g2[k] = a2[k] > 0 ? s : 0;
+    }
+    for (int k = 0; k < MH; ++k) {
+      double s = 0;
+      for (int j = 0; j < MH; ++j) s += (double)v.w2[j * MH + k] * g2[j];
+      g1[k] = a1[k] > 0 ? s : 0;
+    }
+    for (int j = 0; j < MH; ++j) {
+      for (int i = 0; i < MF; ++i) gw1[j * MF + i] += g1[j] * x[i];
+      gb1[j] += g1[j];
+      for (int k = 0; k < MH; ++k) gw2[j * MH + k] += g2[j] * a1[k];
+      gb2[j] += g2[j];
+    }
+    for (int o = 0; o < MO; ++o) {
+      for (int k = 0; k < MH; ++k) gw3[o * MH + k] += g3[o] * a2[k];
+      gb3[o] += g3[o];
+    }
+  }
+  if (loss) *loss = L / B;
+}

@@ -83,6 +83,14 @@ double orc_cpu_srb_barrier(int nthreads, int ngroups, int episodes, uint64_t* st
 double orc_cpu_semaphore(int nthreads, int capacity, int writer_every, int iters, int incs,
                          uint64_t* W, uint64_t* R, uint32_t* max_readers, uint32_t* violations);
 
+/* FP64 forward + backward of the policy MLP (12 -> 32 -> 32 -> 4, ReLU; layout
+ * of gsrb_mlp_param_count()): masked BCE-with-logits on outputs 0-1, masked
+ * 0.5*(z-y)^2 on outputs 2-3, batch mean.  grad: 1604 doubles.  The checker of
+ * the GPU training kernels' gradients. */
+void orc_mlp_loss_grad(const float* params, const float* X, const float* Y, const float* M, int B, double* grad,
+                       double* loss);
+void orc_mlp_forward(const float* params, const float* X, int B, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -4,7 +4,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-ALL = [0, 1, 2, 3, 4, 5, 6, 7, 8]
+ALL = [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10]
 
 
 def _run_bench(gsrb, ctx, variant, k, cluster=2, episodes=2000, fma=0, threads=256, fanin=0):
@@ -59,7 +59,7 @@ def test_refuses_non_coresident_grid(gsrb, ctx):
     assert ctx.barrier_bench(c, 10, 0, sink, cnt) == gsrb.ERR_NOT_CORESIDENT
 
 
-@pytest.mark.parametrize("variant", [0, 2, 3, 4, 5, 8])
+@pytest.mark.parametrize("variant", [0, 2, 3, 4, 5, 8, 9])
 def test_short_grid_times_out_and_context_survives(gsrb, ctx, variant):
     # the expected arrival count is one participant higher than the launch:
     # every wait must run out (bounded) and report a timeout, not hang

@@ -57,14 +57,14 @@ def test_scan_u32_inplace_and_wraparound(gsrb, ctx, orc):
     assert np.array_equal(_scan(gsrb, ctx, a, inplace=True), orc.scan_u32(a))
 
 
-@pytest.mark.parametrize("variant", [0, 2, 3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("variant", [0, 2, 3, 4, 5, 6, 7, 8, 9])
 def test_scan_u32_barrier_variants(gsrb, ctx, orc, variant):
     a = gsrb.uniform_i32(11, 5_000_001, 0, 15).astype(np.uint32)
     c = gsrb.cfg(variant=variant, ctas_per_sm=1, threads=1024, cluster=2, tile=8192)
     assert np.array_equal(_scan(gsrb, ctx, a, cfg=c), orc.scan_u32(a))
 
 
-@pytest.mark.parametrize("k,threads,tile", [(2, 512, 12288), (1, 256, 4096), (2, 1024, 16384)])
+@pytest.mark.parametrize("k,threads,tile", [(2, 512, 12288), (1, 256, 4096), (1, 1024, 16384)])
 def test_scan_u32_shapes(gsrb, ctx, orc, k, threads, tile):
     a = gsrb.uniform_i32(k, 3_333_333, 0, 15).astype(np.uint32)
     c = gsrb.cfg(ctas_per_sm=k, threads=threads, cluster=2, tile=tile)

@@ -91,6 +91,9 @@ const void* bench_fn(int variant) {
     case gsrb::V_CCG: return (const void*)barrier_bench_kernel<gsrb::V_CCG>;
     case gsrb::V_CLUSTER_RED: return (const void*)barrier_bench_kernel<gsrb::V_CLUSTER_RED>;
     case gsrb::V_FLIP: return (const void*)barrier_bench_kernel<gsrb::V_FLIP>;
+    case gsrb::V_FANOUT: return (const void*)barrier_bench_kernel<gsrb::V_FANOUT>;
+    case gsrb::V_CLUSTER_FANOUT: return (const void*)barrier_bench_kernel<gsrb::V_CLUSTER_FANOUT>;
+    case gsrb::V_HIER: return (const void*)barrier_bench_kernel<gsrb::V_HIER>;
     case kNoBarrier: return (const void*)barrier_bench_kernel<kNoBarrier>;
     default: return nullptr;
   }
@@ -107,6 +110,9 @@ const void* litmus_fn(int variant) {
     case gsrb::V_CCG: return (const void*)barrier_litmus_kernel<gsrb::V_CCG>;
     case gsrb::V_CLUSTER_RED: return (const void*)barrier_litmus_kernel<gsrb::V_CLUSTER_RED>;
     case gsrb::V_FLIP: return (const void*)barrier_litmus_kernel<gsrb::V_FLIP>;
+    case gsrb::V_FANOUT: return (const void*)barrier_litmus_kernel<gsrb::V_FANOUT>;
+    case gsrb::V_CLUSTER_FANOUT: return (const void*)barrier_litmus_kernel<gsrb::V_CLUSTER_FANOUT>;
+    case gsrb::V_HIER: return (const void*)barrier_litmus_kernel<gsrb::V_HIER>;
     default: return nullptr;
   }
 }
@@ -176,7 +182,8 @@ gsrb_status_t gsrb_barrier_litmus(gsrb_ctx_t ctx, const gsrb_cfg_t* cfgin, int32
 gsrb_status_t gsrb_barrier_fault_short_grid(gsrb_ctx_t ctx, const gsrb_cfg_t* cfgin) {
   if (!ctx) return GSRB_ERR_ARG;
   gsrb_cfg_t c = resolve_cfg(ctx, cfgin);
-  if (c.variant == gsrb::V_CCG || c.variant == gsrb::V_CLUSTER_ALLPOLL) return GSRB_ERR_UNSUPPORTED;
+  if (c.variant == gsrb::V_CCG || c.variant == gsrb::V_CLUSTER_ALLPOLL || c.variant == gsrb::V_CLUSTER_FANOUT)
+    return GSRB_ERR_UNSUPPORTED;
   if (c.threads > 256 || c.threads % 32) return GSRB_ERR_ARG;
   const void* fn = bench_fn(c.variant);
   const int grid = grid_of(ctx, c);

@@ -15,6 +15,11 @@
 #include "internal.h"
 #include "graph_common.cuh"
 
+#include <algorithm>
+#include <string.h>
+#include <utility>
+#include <vector>
+
 using namespace gsrbrt;
 using namespace gsrbg;
 
@@ -39,16 +44,14 @@ struct BfsArgs {
   unsigned long long* out_edges;
 };
 
+// The traversal body, relative to a team (the whole grid, or one instance's
+// CTA range in a batch, synchronised by `bar`).
 template <int V>
-__global__ void __launch_bounds__(1024)
-bfs_kernel(gsrb::GridBarrier gb, BfsArgs a) {
-  __shared__ gsrb::BarrierShared bsh;
+__device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const BfsArgs& a, const Team team) {
   __shared__ uint32_t s_dir;
   __shared__ float s_pred;
-  gsrb::GridSync<V> bar;
-  bool ok = bar.init(gb, &bsh);
   const DevCSR& g = a.g;
-  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+  const uint32_t tid = team.tid(), nthreads = team.nthreads();
 
   // init (bfs_init, bfs/kernel_gsrb.cu:299-311) fused into the persistent kernel
   for (uint32_t v = tid; v < g.n; v += nthreads) a.level[v] = (v == a.src) ? 0 : kInf;
@@ -115,7 +118,7 @@ bfs_kernel(gsrb::GridBarrier gb, BfsArgs a) {
       ++decisions;
     }
     dir = nd;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (team.cta == 0 && threadIdx.x == 0) {
       // the counter set of level L + 1 was last read before barrier L - 1
       a.cnt[(L + 1) % 3].n_reg = 0;
       a.cnt[(L + 1) % 3].n_big = 0;
@@ -162,11 +165,11 @@ bfs_kernel(gsrb::GridBarrier gb, BfsArgs a) {
     };
 
     if (dir == DIR_PUSH) {
-      expand_hubs(g, hin, nbig, push_edge);
-      expand_queue(g, qin, nreg, push_edge);
+      expand_hubs(team, g, hin, nbig, push_edge);
+      expand_queue(team, g, qin, nreg, push_edge);
     } else if (dir == DIR_TOPO) {
       // topology-driven push: scan every vertex, expand those at level L - 1
-      expand_hubs(g, hin, nbig, push_edge);
+      expand_hubs(team, g, hin, nbig, push_edge);
       const uint32_t lane = lane_id();
       const uint32_t gw = tid >> 5, nw = nthreads >> 5;
       for (uint32_t base = gw * 32u; base < g.n; base += nw * 32u) {
@@ -230,19 +233,28 @@ bfs_kernel(gsrb::GridBarrier gb, BfsArgs a) {
     if (lane_id() == 0 && ws) atomicAdd(&c->m_next, ws);
     ok = bar.sync();
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (team.cta == 0 && threadIdx.x == 0) {
     a.out[0] = L - 1;  // levels with a non-empty frontier beyond the source
     a.out[2] = decisions;
     a.out[3] = ok ? 0u : 1u;
     *a.out_edges = edges;
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0 && a.mode == GSRB_BFS_LEARNED) {
+  if (team.cta == 0 && threadIdx.x == 0 && a.mode == GSRB_BFS_LEARNED) {
     // first level at which the policy fell back (0 = never); recomputed from the trace
     uint32_t fb = 0;
     for (uint32_t i = 0; i + 1 < L && i < a.trace_cap; ++i)
       if (a.trace[i].fallback) { fb = a.trace[i].level; break; }
     a.out[1] = fb;
   }
+}
+
+template <int V>
+__global__ void __launch_bounds__(1024)
+bfs_kernel(gsrb::GridBarrier gb, BfsArgs a) {
+  __shared__ gsrb::BarrierShared bsh;
+  gsrb::GridSync<V> bar;
+  const bool ok = bar.init(gb, &bsh);
+  bfs_run<V>(bar, ok, a, Team{blockIdx.x, gridDim.x});
   bar.finish();
 }
 
@@ -267,13 +279,9 @@ struct SsspArgs {
 };
 
 template <int V>
-__global__ void __launch_bounds__(1024)
-sssp_kernel(gsrb::GridBarrier gb, SsspArgs a) {
-  __shared__ gsrb::BarrierShared bsh;
-  gsrb::GridSync<V> bar;
-  bool ok = bar.init(gb, &bsh);
+__device__ __forceinline__ void sssp_run(gsrb::GridSync<V>& bar, bool ok, const SsspArgs& a, const Team team) {
   const DevCSR& g = a.g;
-  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+  const uint32_t tid = team.tid(), nthreads = team.nthreads();
   for (uint32_t v = tid; v < g.n; v += nthreads) {
     a.dist[v] = (v == a.src) ? 0 : kInf;
     a.mark[v] = 0;
@@ -302,7 +310,7 @@ sssp_kernel(gsrb::GridBarrier gb, SsspArgs a) {
     const LevelCounters cur = {__ldcg(&a.cnt[(step - 1) % 3].n_reg), __ldcg(&a.cnt[(step - 1) % 3].n_big), 0, 0};
     const uint32_t nreg = (uint32_t)cur.n_reg, nbig = (uint32_t)cur.n_big;
     const uint32_t nf = nreg + nbig;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (team.cta == 0 && threadIdx.x == 0) {
       a.cnt[(step + 1) % 3].n_reg = 0;
       a.cnt[(step + 1) % 3].n_big = 0;
       a.cnt[(step + 1) % 3].m_next = 0;
@@ -321,7 +329,7 @@ sssp_kernel(gsrb::GridBarrier gb, SsspArgs a) {
       LevelCounters* c = &a.cnt[step % 3];
       const uint32_t stamp = step;
       const uint32_t next_gen = fgen + 1;
-      if (blockIdx.x == 0 && threadIdx.x == 0) *fc_out = 0;  // last read before the previous barrier
+      if (team.cta == 0 && threadIdx.x == 0) *fc_out = 0;  // last read before the previous barrier
       // fc_out must be zero before anyone appends: appends happen below, after
       // this CTA's store, so publish it through the barrier first
       ok = bar.sync();
@@ -352,7 +360,7 @@ sssp_kernel(gsrb::GridBarrier gb, SsspArgs a) {
     }
     // ---- relax the near frontier
     ++rounds;
-    if (blockIdx.x == 0 && threadIdx.x == 0 && rounds - 1 < a.trace_cap) {
+    if (team.cta == 0 && threadIdx.x == 0 && rounds - 1 < a.trace_cap) {
       LevelTrace t;
       t.level = rounds;
       t.dir = 0;
@@ -395,8 +403,8 @@ sssp_kernel(gsrb::GridBarrier gb, SsspArgs a) {
       warp_append(to_near && d > kBigDegree, v, hout, &c->n_big, g.n, a.overflow);
       warp_append(to_far, v, fout, fc, g.n, a.overflow);
     };
-    expand_hubs(g, hin, nbig, relax);
-    expand_queue(g, qin, nreg, relax);
+    expand_hubs(team, g, hin, nbig, relax);
+    expand_queue(team, g, qin, nreg, relax);
     relaxed_edges += my_edges;
     ++step;
     ok = bar.sync();
@@ -404,11 +412,51 @@ sssp_kernel(gsrb::GridBarrier gb, SsspArgs a) {
   // per-thread relaxed-edge counts -> one total
   const unsigned long long ws = warp_sum_u64(relaxed_edges);
   if (lane_id() == 0 && ws) atomicAdd(a.out_edges, ws);
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (team.cta == 0 && threadIdx.x == 0) {
     a.out[0] = rounds;
     a.out[1] = buckets;
     a.out[3] = ok ? 0u : 1u;
   }
+}
+
+template <int V>
+__global__ void __launch_bounds__(1024)
+sssp_kernel(gsrb::GridBarrier gb, SsspArgs a) {
+  __shared__ gsrb::BarrierShared bsh;
+  gsrb::GridSync<V> bar;
+  const bool ok = bar.init(gb, &bsh);
+  sssp_run<V>(bar, ok, a, Team{blockIdx.x, gridDim.x});
+  bar.finish();
+}
+
+// ------------------------------------------------------------------ batches ---
+// Many traversals in one persistent launch: instance i owns CTAs
+// [first_i, first_i + count_i) and a barrier slot of its own (sub-grid
+// barriers carved from the same state block).  A CTA finds its instance in a
+// table, copies the instance's descriptor and runs the same traversal body as
+// the single-instance kernels.  Only barrier variants whose verdict does not
+// involve hardware cluster barriers are used (instances of one CTA are allowed).
+struct BatchDesc {
+  gsrb::GridBarrier gb;
+  uint32_t first;
+  uint32_t count;
+  uint32_t kind;  // 0 BFS, 1 SSSP
+  uint32_t pad;
+  BfsArgs bfs;
+  SsspArgs sssp;
+};
+
+template <int V>
+__global__ void __launch_bounds__(1024)
+batch_kernel(const BatchDesc* __restrict__ descs, const uint16_t* __restrict__ cta_inst) {
+  __shared__ gsrb::BarrierShared bsh;
+  const uint32_t i = cta_inst[blockIdx.x];
+  const BatchDesc& d = descs[i];
+  const Team team{blockIdx.x - d.first, d.count};
+  gsrb::GridSync<V> bar;
+  const bool ok = bar.init(d.gb, &bsh);
+  if (d.kind == 0) bfs_run<V>(bar, ok, d.bfs, team);
+  else sssp_run<V>(bar, ok, d.sssp, team);
   bar.finish();
 }
 
@@ -545,6 +593,8 @@ struct Dummy {};
       case gsrb::V_CCG: return (const void*)KERNEL<gsrb::V_CCG>;                 \
       case gsrb::V_CLUSTER_RED: return (const void*)KERNEL<gsrb::V_CLUSTER_RED>; \
       case gsrb::V_FLIP: return (const void*)KERNEL<gsrb::V_FLIP>;               \
+      case gsrb::V_FANOUT: return (const void*)KERNEL<gsrb::V_FANOUT>;           \
+      case gsrb::V_HIER: return (const void*)KERNEL<gsrb::V_HIER>;               \
       default: return nullptr;                                                  \
     }                                                                           \
   }
@@ -552,6 +602,17 @@ struct Dummy {};
 const void* bfs_fn(int v) { return GSRB_GRAPH_FN(bfs_kernel)(v); }
 const void* sssp_fn(int v) { return GSRB_GRAPH_FN(sssp_kernel)(v); }
 const void* pr_fn(int v) { return GSRB_GRAPH_FN(pagerank_kernel)(v); }
+const void* batch_fn(int v) {
+  switch (v) {  // variants without hardware cluster barriers (teams may be single CTAs)
+    case gsrb::V_SOFT2: return (const void*)batch_kernel<gsrb::V_SOFT2>;
+    case gsrb::V_FLAT: return (const void*)batch_kernel<gsrb::V_FLAT>;
+    case gsrb::V_TREE: return (const void*)batch_kernel<gsrb::V_TREE>;
+    case gsrb::V_FLIP: return (const void*)batch_kernel<gsrb::V_FLIP>;
+    case gsrb::V_FANOUT: return (const void*)batch_kernel<gsrb::V_FANOUT>;
+    case gsrb::V_HIER: return (const void*)batch_kernel<gsrb::V_HIER>;
+    default: return nullptr;
+  }
+}
 
 }  // namespace
 
@@ -896,6 +957,240 @@ gsrb_status_t gsrb_pagerank(gsrb_ctx_t ctx, gsrb_graph_t G, float alpha, int32_t
   float ms = 0;
   GSRB_CUDA(cudaEventElapsedTime(&ms, ctx->events[62], ctx->events[63]));
   return finish_stats(G, stats, ms);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- batches ----
+struct gsrb_batch {
+  gsrb_ctx* ctx = nullptr;
+  std::vector<gsrb_graph*> graphs;
+  gsrb_cfg_t cfg;
+  int grid = 0;
+  std::vector<uint32_t> first, count;
+  BatchDesc* h_desc = nullptr;  // pinned
+  BatchDesc* d_desc = nullptr;
+  uint16_t* d_cta_inst = nullptr;
+};
+
+namespace {
+
+BfsArgs bfs_args(gsrb_graph* G, uint32_t src, int32_t* level, int32_t mode) {
+  BfsArgs a;
+  a.g = dev_csr(G);
+  a.src = src;
+  a.level = level;
+  a.q[0] = G->q[0];
+  a.q[1] = G->q[1];
+  a.hq[0] = G->hq[0];
+  a.hq[1] = G->hq[1];
+  a.cnt = G->cnt;
+  a.overflow = G->flags;
+  a.trace = G->trace;
+  a.trace_cap = G->trace_cap;
+  a.mlp = G->mlp;
+  a.mode = mode;
+  a.alpha = 15.f;
+  a.beta = 18.f;
+  a.out = G->flags + 4;
+  a.out_edges = (unsigned long long*)((char*)G->flags + 64);
+  return a;
+}
+
+SsspArgs sssp_args(gsrb_graph* G, uint32_t src, int32_t* dist, int32_t delta) {
+  SsspArgs a;
+  a.g = dev_csr(G);
+  a.src = src;
+  a.dist = dist;
+  for (int k = 0; k < 2; ++k) {
+    a.q[k] = G->q[k];
+    a.hq[k] = G->hq[k];
+    a.far[k] = G->far[k];
+  }
+  a.mark = G->mark;
+  a.fmark = G->fmark;
+  a.cnt = G->cnt;
+  a.fcnt = G->fcnt;
+  a.overflow = G->flags;
+  a.trace = G->trace;
+  a.trace_cap = G->trace_cap;
+  a.delta = delta;
+  a.out = G->flags + 4;
+  a.out_edges = (unsigned long long*)((char*)G->flags + 64);
+  return a;
+}
+
+gsrb_status_t batch_launch(gsrb_batch* B, const uint32_t* srcs, int32_t* const* outs, int kind, int32_t param) {
+  if (!B || !srcs || !outs) return GSRB_ERR_ARG;
+  const int k = (int)B->graphs.size();
+  for (int i = 0; i < k; ++i)
+    if (!outs[i] || srcs[i] >= B->graphs[i]->n) return GSRB_ERR_ARG;
+  if (kind == 0 && param == GSRB_BFS_LEARNED)
+    for (int i = 0; i < k; ++i)
+      if (!B->graphs[i]->mlp_set) return GSRB_ERR_STATE;
+  gsrb_ctx* ctx = B->ctx;
+  const void* fn = batch_fn(B->cfg.variant);
+  if (!fn) return GSRB_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  for (int i = 0; i < k; ++i) {
+    BatchDesc& d = B->h_desc[i];
+    memset(&d, 0, sizeof(d));
+    // slot 1 + i and, for the group-counter variants, groups starting at the
+    // instance's first CTA (an instance never has more groups than CTAs)
+    d.gb = make_barrier(ctx, B->cfg, 1 + i, B->count[i], B->first[i], B->first[i]);
+    d.first = B->first[i];
+    d.count = B->count[i];
+    d.kind = (uint32_t)kind;
+    if (kind == 0) d.bfs = bfs_args(B->graphs[i], srcs[i], outs[i], param);
+    else d.sssp = sssp_args(B->graphs[i], srcs[i], outs[i], param);
+    GSRB_CUDA(cudaMemsetAsync(B->graphs[i]->flags, 0, 128, ctx->stream));
+  }
+  GSRB_CUDA(cudaMemcpyAsync(B->d_desc, B->h_desc, sizeof(BatchDesc) * k, cudaMemcpyHostToDevice, ctx->stream));
+  const BatchDesc* dd = B->d_desc;
+  const uint16_t* ci = B->d_cta_inst;
+  void* args[] = {(void*)&dd, (void*)&ci};
+  return launch_persistent(ctx, fn, B->grid, B->cfg.threads, 0, 1, coop_of(B->cfg), args);
+}
+
+}  // namespace
+
+extern "C" {
+
+gsrb_status_t gsrb_batch_create(gsrb_ctx_t ctx, const gsrb_graph_t* graphs, int32_t k, const gsrb_cfg_t* cfgin,
+                                gsrb_batch_t* out) {
+  if (!ctx || !graphs || !out || k <= 0 || k > kSlots - 1) return GSRB_ERR_ARG;
+  gsrb_cfg_t c = resolve_cfg(ctx, cfgin);
+  if (!cfgin) {
+    c.variant = gsrb::V_FANOUT;
+    c.ctas_per_sm = 2;
+    c.threads = 512;
+  }
+  c.cluster = 1;
+  if (!batch_fn(c.variant)) return GSRB_ERR_UNSUPPORTED;
+  const int grid = grid_of(ctx, c);
+  if (grid < k || grid > 65535) return GSRB_ERR_ARG;
+  gsrb_batch* B = new gsrb_batch();
+  B->ctx = ctx;
+  B->cfg = c;
+  B->grid = grid;
+  for (int i = 0; i < k; ++i) {
+    if (!graphs[i]) {
+      delete B;
+      return GSRB_ERR_ARG;
+    }
+    B->graphs.push_back(graphs[i]);
+  }
+  // CTAs in proportion to each instance's edges (+ vertices), at least one each
+  std::vector<double> w(k);
+  double W = 0;
+  for (int i = 0; i < k; ++i) {
+    w[i] = (double)graphs[i]->m + (double)graphs[i]->n;
+    W += w[i];
+  }
+  std::vector<uint32_t> cnt(k, 1);
+  int left = grid - k;
+  std::vector<std::pair<double, int>> rem;
+  for (int i = 0; i < k; ++i) {
+    const double share = W > 0 ? left * w[i] / W : 0.0;
+    const uint32_t extra = (uint32_t)share;
+    cnt[i] += extra;
+    rem.push_back({share - extra, i});
+  }
+  int used = 0;
+  for (int i = 0; i < k; ++i) used += (int)cnt[i];
+  std::sort(rem.begin(), rem.end(), [](const std::pair<double, int>& a, const std::pair<double, int>& b) {
+    return a.first > b.first || (a.first == b.first && a.second < b.second);
+  });
+  for (size_t j = 0; used < grid && j < rem.size(); ++j, ++used) cnt[rem[j].second] += 1;
+  std::vector<uint16_t> inst(grid);
+  uint32_t f = 0;
+  for (int i = 0; i < k; ++i) {
+    B->first.push_back(f);
+    B->count.push_back(cnt[i]);
+    for (uint32_t j = 0; j < cnt[i]; ++j) inst[f + j] = (uint16_t)i;
+    f += cnt[i];
+  }
+  cudaError_t e = cudaMallocHost(&B->h_desc, sizeof(BatchDesc) * k);
+  if (!e) e = cudaMalloc(&B->d_desc, sizeof(BatchDesc) * k);
+  if (!e) e = cudaMalloc(&B->d_cta_inst, sizeof(uint16_t) * grid);
+  if (!e) e = cudaMemcpy(B->d_cta_inst, inst.data(), sizeof(uint16_t) * grid, cudaMemcpyHostToDevice);
+  if (e) {
+    gsrb_batch_free(B);
+    return cuda_err(e, "batch_create");
+  }
+  *out = B;
+  return GSRB_OK;
+}
+
+gsrb_status_t gsrb_batch_free(gsrb_batch_t B) {
+  if (!B) return GSRB_ERR_ARG;
+  if (B->ctx) cudaStreamSynchronize(B->ctx->stream);
+  if (B->h_desc) cudaFreeHost(B->h_desc);
+  if (B->d_desc) cudaFree(B->d_desc);
+  if (B->d_cta_inst) cudaFree(B->d_cta_inst);
+  delete B;
+  return GSRB_OK;
+}
+
+gsrb_status_t gsrb_batch_layout(gsrb_batch_t B, uint32_t* first, uint32_t* count) {
+  if (!B) return GSRB_ERR_ARG;
+  for (size_t i = 0; i < B->graphs.size(); ++i) {
+    if (first) first[i] = B->first[i];
+    if (count) count[i] = B->count[i];
+  }
+  return GSRB_OK;
+}
+
+gsrb_status_t gsrb_batch_bfs(gsrb_batch_t B, const uint32_t* srcs, int32_t* const* d_levels, int32_t mode) {
+  if (mode < 0 || mode > GSRB_BFS_TOPO) return GSRB_ERR_ARG;
+  return batch_launch(B, srcs, d_levels, 0, mode);
+}
+
+gsrb_status_t gsrb_batch_sssp(gsrb_batch_t B, const uint32_t* srcs, int32_t* const* d_dists, int32_t delta) {
+  if (delta <= 0) return GSRB_ERR_ARG;
+  return batch_launch(B, srcs, d_dists, 1, delta);
+}
+
+gsrb_status_t gsrb_batch_stats(gsrb_batch_t B, gsrb_traversal_stats_t* stats) {
+  if (!B) return GSRB_ERR_ARG;
+  GSRB_CUDA(cudaStreamSynchronize(B->ctx->stream));
+  gsrb_status_t worst = GSRB_OK;
+  for (size_t i = 0; i < B->graphs.size(); ++i) {
+    gsrb_status_t st = finish_stats(B->graphs[i], stats ? &stats[i] : nullptr, 0.f);
+    if (st && !worst) worst = st;
+  }
+  return worst;
+}
+
+// ---- CUDA graphs: capture the context stream's work once, replay it ----------
+gsrb_status_t gsrb_capture_begin(gsrb_ctx_t ctx) {
+  if (!ctx) return GSRB_ERR_ARG;
+  GSRB_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  return GSRB_OK;
+}
+
+gsrb_status_t gsrb_capture_end(gsrb_ctx_t ctx, gsrb_exec_t* out) {
+  if (!ctx || !out) return GSRB_ERR_ARG;
+  cudaGraph_t graph = nullptr;
+  GSRB_CUDA(cudaStreamEndCapture(ctx->stream, &graph));
+  cudaGraphExec_t exec = nullptr;
+  cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e) return cuda_err(e, "cudaGraphInstantiate");
+  *out = (gsrb_exec_t)exec;
+  return GSRB_OK;
+}
+
+gsrb_status_t gsrb_exec_launch(gsrb_ctx_t ctx, gsrb_exec_t exec) {
+  if (!ctx || !exec) return GSRB_ERR_ARG;
+  GSRB_CUDA(cudaGraphLaunch((cudaGraphExec_t)exec, ctx->stream));
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return GSRB_OK;
+}
+
+gsrb_status_t gsrb_exec_free(gsrb_exec_t exec) {
+  if (exec) GSRB_CUDA(cudaGraphExecDestroy((cudaGraphExec_t)exec));
+  return GSRB_OK;
 }
 
 }  // extern "C"

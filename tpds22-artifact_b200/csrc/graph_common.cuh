@@ -49,6 +49,18 @@ struct LevelCounters {
   unsigned long long pad;
 };
 
+// The CTAs working on one traversal: the whole grid for a single traversal, a
+// contiguous CTA range (with its own sub-grid barrier) for one instance of a
+// batch.  All work distribution is relative to the team.
+struct Team {
+  uint32_t cta;   // this CTA's index in the team
+  uint32_t ncta;  // CTAs in the team
+  __device__ __forceinline__ uint32_t tid() const { return cta * blockDim.x + threadIdx.x; }
+  __device__ __forceinline__ uint32_t nthreads() const { return ncta * blockDim.x; }
+  __device__ __forceinline__ uint32_t warp() const { return tid() >> 5; }
+  __device__ __forceinline__ uint32_t nwarps() const { return nthreads() >> 5; }
+};
+
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 __device__ __forceinline__ uint32_t lanemask_lt() {
   uint32_t m;
@@ -90,10 +102,11 @@ __device__ __forceinline__ uint32_t warp_max_u32(uint32_t v) {
 // an edge).  Vertices of degree <= kWarpDegree: one lane each; larger: the warp
 // strides over the edges together.  Warps take 32-vertex groups grid-stride.
 template <class F>
-__device__ __forceinline__ void expand_queue(const DevCSR& g, const uint32_t* __restrict__ q, uint32_t nq, F& f) {
+__device__ __forceinline__ void expand_queue(const Team& t, const DevCSR& g, const uint32_t* __restrict__ q,
+                                             uint32_t nq, F& f) {
   const uint32_t lane = lane_id();
-  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t gw = t.warp();
+  const uint32_t nwarps = t.nwarps();
   for (uint32_t base = gw * 32u; base < nq; base += nwarps * 32u) {
     const uint32_t i = base + lane;
     uint32_t u = 0, b = 0, e = 0;
@@ -125,14 +138,15 @@ __device__ __forceinline__ void expand_queue(const DevCSR& g, const uint32_t* __
 
 // Expand the hub queue: every CTA takes an equal slice of every hub's edges.
 template <class F>
-__device__ __forceinline__ void expand_hubs(const DevCSR& g, const uint32_t* __restrict__ hq, uint32_t nh, F& f) {
-  const uint32_t G = gridDim.x;
+__device__ __forceinline__ void expand_hubs(const Team& t, const DevCSR& g, const uint32_t* __restrict__ hq,
+                                            uint32_t nh, F& f) {
+  const uint32_t G = t.ncta;
   for (uint32_t k = 0; k < nh; ++k) {
     const uint32_t u = __ldcg(hq + k);
     const uint32_t b = __ldg(g.row + u), e = __ldg(g.row + u + 1);
     const uint64_t len = e - b;
-    const uint32_t s0 = b + (uint32_t)(len * blockIdx.x / G);
-    const uint32_t s1 = b + (uint32_t)(len * (blockIdx.x + 1) / G);
+    const uint32_t s0 = b + (uint32_t)(len * t.cta / G);
+    const uint32_t s1 = b + (uint32_t)(len * (t.cta + 1) / G);
     // warp-synchronous strides of the CTA over its slice
     for (uint32_t j0 = s0 + (threadIdx.x & ~31u); j0 < s1; j0 += blockDim.x) {
       const uint32_t j = j0 + lane_id();
@@ -176,8 +190,9 @@ __device__ __forceinline__ void mlp_forward_warp(const MLPWeights* __restrict__ 
   }
 }
 
-// Feature vector of a level (all log-scaled or normalised to O(1)).
-__device__ __forceinline__ void level_features(float feat[kFeat], uint32_t n, uint32_t m, uint32_t level,
+// Feature vector of a level (all log-scaled or normalised to O(1)).  The same
+// function builds training rows on the host from trace records.
+__host__ __device__ __forceinline__ void level_features(float feat[kFeat], uint32_t n, uint32_t m, uint32_t level,
                                                uint32_t nf, unsigned long long mf, uint32_t nu,
                                                unsigned long long mu, uint32_t prev_nf, uint32_t prev_dir) {
   feat[0] = log2f(1.f + (float)nf);

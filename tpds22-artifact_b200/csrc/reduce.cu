@@ -115,6 +115,8 @@ const void* reduce_fn(int variant) {
     case gsrb::V_CCG: return (const void*)reduce_i32_kernel<gsrb::V_CCG>;
     case gsrb::V_CLUSTER_RED: return (const void*)reduce_i32_kernel<gsrb::V_CLUSTER_RED>;
     case gsrb::V_FLIP: return (const void*)reduce_i32_kernel<gsrb::V_FLIP>;
+    case gsrb::V_FANOUT: return (const void*)reduce_i32_kernel<gsrb::V_FANOUT>;
+    case gsrb::V_HIER: return (const void*)reduce_i32_kernel<gsrb::V_HIER>;
     default: return nullptr;  // V_CLUSTER_ALLPOLL is kept to fixed-count loops
   }
 }

@@ -25,7 +25,7 @@ gsrb_status_t cuda_err(cudaError_t e, const char* what) {
 
 bool is_cluster_variant(int v) {
   return v == gsrb::V_CLUSTER || v == gsrb::V_CLUSTER_ALLPOLL || v == gsrb::V_DSMEM ||
-         v == gsrb::V_CLUSTER_RED;
+         v == gsrb::V_CLUSTER_RED || v == gsrb::V_CLUSTER_FANOUT;
 }
 
 gsrb_cfg_t resolve_cfg(const gsrb_ctx* ctx, const gsrb_cfg_t* in) {
@@ -72,9 +72,18 @@ gsrb::GridBarrier make_barrier(gsrb_ctx* ctx, const gsrb_cfg_t& c, int slot, uin
     case gsrb::V_CLUSTER_ALLPOLL:
     case gsrb::V_DSMEM:
     case gsrb::V_FLIP:
-      // native variants: fanin_groups = number of split flip words
+      // split sum-to-flip words: fanin_groups of them (at most 8)
       nflip = c.fanin_groups > 0 ? (uint32_t)c.fanin_groups : 1u;
-      if (nflip > (uint32_t)kMaxFlip) nflip = kMaxFlip;
+      if (nflip > 8u) nflip = 8u;
+      break;
+    case gsrb::V_HIER:
+      // group counters: fanin_groups (the arrivals are spread over them)
+      ng = c.fanin_groups > 0 ? (uint32_t)c.fanin_groups : 0u;
+      // fall through: wake-up lines
+    case gsrb::V_FANOUT:
+    case gsrb::V_CLUSTER_FANOUT:
+      nflip = c.wake_lines > 0 ? (uint32_t)c.wake_lines : 8u;
+      if (nflip > 8u) nflip = 8u;
       break;
     default:
       ng = 0;

@@ -306,6 +306,8 @@ const void* scan_fn_t(int variant) {
     case gsrb::V_CCG: return (const void*)scan_kernel<gsrb::V_CCG, F32>;
     case gsrb::V_CLUSTER_RED: return (const void*)scan_kernel<gsrb::V_CLUSTER_RED, F32>;
     case gsrb::V_FLIP: return (const void*)scan_kernel<gsrb::V_FLIP, F32>;
+    case gsrb::V_FANOUT: return (const void*)scan_kernel<gsrb::V_FANOUT, F32>;
+    case gsrb::V_HIER: return (const void*)scan_kernel<gsrb::V_HIER, F32>;
     default: return nullptr;
   }
 }

@@ -44,6 +44,9 @@ BAR_TREE = 5
 BAR_CCG = 6
 BAR_CLUSTER_RED = 7
 BAR_FLIP = 8
+BAR_FANOUT = 9
+BAR_CLUSTER_FANOUT = 10
+BAR_HIER = 11
 BAR_NONE = 99
 VARIANT_NAMES = {
     BAR_CLUSTER: "gsrb_cluster",
@@ -55,6 +58,9 @@ VARIANT_NAMES = {
     BAR_CCG: "ccg_grid_sync",
     BAR_CLUSTER_RED: "gsrb_cluster_red",
     BAR_FLIP: "gsrb_flip",
+    BAR_FANOUT: "gsrb_fanout",
+    BAR_CLUSTER_FANOUT: "gsrb_cluster_fanout",
+    BAR_HIER: "gsrb_hier",
     BAR_NONE: "none",
 }
 
@@ -78,7 +84,8 @@ class Cfg(C.Structure):
         ("tile", C.c_int32),
         ("grid_override", C.c_int32),
         ("launch_mode", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("wake_lines", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
     def as_dict(self):
@@ -150,6 +157,23 @@ _SIGS = {
     "gsrb_bfs": (C.c_int32, [_P, _P, C.c_uint32, _P, C.c_int32, C.POINTER(Cfg), C.c_void_p]),
     "gsrb_sssp": (C.c_int32, [_P, _P, C.c_uint32, _P, C.c_int32, C.POINTER(Cfg), C.c_void_p]),
     "gsrb_pagerank": (C.c_int32, [_P, _P, C.c_float, C.c_int32, _P, C.POINTER(Cfg), C.c_void_p]),
+    "gsrb_batch_create": (C.c_int32, [_P, _P, C.c_int32, C.POINTER(Cfg), C.POINTER(_P)]),
+    "gsrb_batch_free": (C.c_int32, [_P]),
+    "gsrb_batch_layout": (C.c_int32, [_P, _P, _P]),
+    "gsrb_batch_bfs": (C.c_int32, [_P, _P, _P, C.c_int32]),
+    "gsrb_batch_sssp": (C.c_int32, [_P, _P, _P, C.c_int32]),
+    "gsrb_batch_stats": (C.c_int32, [_P, _P]),
+    "gsrb_capture_begin": (C.c_int32, [_P]),
+    "gsrb_capture_end": (C.c_int32, [_P, C.POINTER(_P)]),
+    "gsrb_exec_launch": (C.c_int32, [_P, _P]),
+    "gsrb_exec_free": (C.c_int32, [_P]),
+    "gsrb_mlp_param_count": (C.c_size_t, []),
+    "gsrb_mlp_init": (C.c_int32, [C.c_uint64, _P]),
+    "gsrb_level_features": (None, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32,
+                                   C.c_uint64, C.c_uint32, C.c_uint32, _P]),
+    "gsrb_mlp_forward": (C.c_int32, [_P, _P, _P, C.c_int32, _P]),
+    "gsrb_mlp_loss_grad": (C.c_int32, [_P, _P, _P, _P, _P, C.c_int32, _P, _P]),
+    "gsrb_mlp_train": (C.c_int32, [_P, _P, _P, _P, _P, C.c_int32, C.c_int32, C.c_float, _P]),
 }
 
 # semaphore / mutex kinds, BFS modes
@@ -431,6 +455,130 @@ class DeviceGraph:
 
 def launch_count() -> int:
     return int(_lib().gsrb_launch_count())
+
+
+# ---- batches and CUDA graphs -----------------------------------------------------
+class Batch:
+    """Many device graphs traversed in one persistent launch (sub-grid barriers)."""
+
+    def __init__(self, ctx: Context, graphs, c: Cfg | None = None):
+        self.ctx = ctx
+        self.graphs = list(graphs)
+        hs = (C.c_void_p * len(self.graphs))(*[g.h for g in self.graphs])
+        self._hs = hs
+        p = C.c_void_p()
+        check(_lib().gsrb_batch_create(ctx.h, hs, len(self.graphs), C.byref(c) if c is not None else None,
+                                       C.byref(p)), "batch_create")
+        self.h = p.value
+        self.k = len(self.graphs)
+
+    def free(self):
+        if self.h:
+            _lib().gsrb_batch_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def layout(self):
+        f = np.zeros(self.k, np.uint32)
+        n = np.zeros(self.k, np.uint32)
+        check(_lib().gsrb_batch_layout(self.h, f.ctypes.data, n.ctypes.data))
+        return f, n
+
+    def _ptrs(self, srcs, outs):
+        s = np.ascontiguousarray(srcs, dtype=np.uint32)
+        o = (C.c_void_p * self.k)(*[a.ptr for a in outs])
+        self._keep = (s, o)
+        return s, o
+
+    def bfs(self, srcs, outs, mode=BFS_HEURISTIC) -> int:
+        s, o = self._ptrs(srcs, outs)
+        return _lib().gsrb_batch_bfs(self.h, s.ctypes.data, o, mode)
+
+    def sssp(self, srcs, outs, delta) -> int:
+        s, o = self._ptrs(srcs, outs)
+        return _lib().gsrb_batch_sssp(self.h, s.ctypes.data, o, delta)
+
+    def stats(self):
+        st = (TraversalStats * self.k)()
+        rc = _lib().gsrb_batch_stats(self.h, st)
+        return rc, list(st)
+
+
+class CudaGraph:
+    """Capture asynchronous library calls on the context stream; replay them."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        self.h = None
+
+    def __enter__(self):
+        check(_lib().gsrb_capture_begin(self.ctx.h), "capture_begin")
+        return self
+
+    def __exit__(self, et, ev, tb):
+        p = C.c_void_p()
+        rc = _lib().gsrb_capture_end(self.ctx.h, C.byref(p))
+        if et is None:
+            check(rc, "capture_end")
+            self.h = p.value
+
+    def launch(self):
+        check(_lib().gsrb_exec_launch(self.ctx.h, self.h), "exec_launch")
+
+    def free(self):
+        if self.h:
+            _lib().gsrb_exec_free(self.h)
+            self.h = None
+
+
+# ---- the learned policy --------------------------------------------------------
+def mlp_param_count() -> int:
+    return int(_lib().gsrb_mlp_param_count())
+
+
+def mlp_init(seed: int) -> np.ndarray:
+    p = np.zeros(mlp_param_count(), dtype=np.float32)
+    check(_lib().gsrb_mlp_init(seed, p.ctypes.data), "mlp_init")
+    return p
+
+
+def level_features(n, m, level, nf, mf, nu, mu, prev_nf, prev_dir) -> np.ndarray:
+    out = np.zeros(12, dtype=np.float32)
+    _lib().gsrb_level_features(n, m, level, nf, mf, nu, mu, prev_nf, prev_dir, out.ctypes.data)
+    return out
+
+
+def mlp_forward(ctx: Context, params: np.ndarray, X: np.ndarray) -> np.ndarray:
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    B = X.shape[0]
+    dp, dx, do = ctx.to_device(params), ctx.to_device(X), ctx.array(B * 4, np.float32)
+    check(_lib().gsrb_mlp_forward(ctx.h, dp.ptr, dx.ptr, B, do.ptr), "mlp_forward")
+    return do.download().reshape(B, 4)
+
+
+def mlp_loss_grad(ctx: Context, params, X, Y, M):
+    X, Y, M = (np.ascontiguousarray(a, dtype=np.float32) for a in (X, Y, M))
+    B = X.shape[0]
+    dp, dx, dy, dm = (ctx.to_device(a) for a in (params, X, Y, M))
+    dg, dl = ctx.array(mlp_param_count(), np.float32), ctx.array(1, np.float32)
+    check(_lib().gsrb_mlp_loss_grad(ctx.h, dp.ptr, dx.ptr, dy.ptr, dm.ptr, B, dg.ptr, dl.ptr), "mlp_loss_grad")
+    return dg.download(), float(dl.download()[0])
+
+
+def mlp_train(ctx: Context, params, X, Y, M, steps=2000, lr=3e-3):
+    X, Y, M = (np.ascontiguousarray(a, dtype=np.float32) for a in (X, Y, M))
+    B = X.shape[0]
+    dp = ctx.to_device(np.ascontiguousarray(params, dtype=np.float32))
+    dx, dy, dm = (ctx.to_device(a) for a in (X, Y, M))
+    dh = ctx.array(max(steps, 1), np.float32)
+    check(_lib().gsrb_mlp_train(ctx.h, dp.ptr, dx.ptr, dy.ptr, dm.ptr, B, steps, lr, dh.ptr), "mlp_train")
+    ctx.check_status("mlp_train")
+    return dp.download(), dh.download()[:steps]
 
 
 # ---- host-side inputs -------------------------------------------------------

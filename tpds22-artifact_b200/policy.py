@@ -1,0 +1,113 @@
+"""The learned per-level policy of the BFS level loop: trace collection, labels,
+training on the GPU (gsrb_mlp_train) and evaluation helpers.
+
+The plain traversals emit one 48-byte record per level (gsrb_graph_trace):
+frontier size and out-edges, unvisited vertices and their edges, and the
+%globaltimer stamp at the start of the level.  Running the same BFS with the
+worklist push, the pull and the topology push gives, for every level, the time
+each direction took on the same frontier (the level sets do not depend on the
+direction).  Those times label each level:
+
+    head 0: pull faster than worklist push     (BCE)
+    head 1: topology push faster than worklist push (BCE)
+    head 2: log2(1 + size of the next frontier) (squared error)
+
+Features are computed by gsrb_level_features, the host twin of the function the
+traversal kernel evaluates on the device.  The policy changes only which
+direction a level runs in, never the levels; it falls back to the fixed
+heuristic for the rest of a traversal once its next-frontier prediction misses
+by more than 2x.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+INF = 2**31 - 1
+
+
+def _g():
+    import sys
+    return sys.modules["gsrb_b200"]
+
+
+def level_times(trace: np.ndarray, total_ms: float | None = None) -> np.ndarray:
+    """Duration of each level (ns) from consecutive start stamps; the last
+    level has no successor stamp and gets NaN."""
+    t = trace["t_ns"].astype(np.float64)
+    d = np.full(len(t), np.nan)
+    if len(t) > 1:
+        d[:-1] = np.diff(t)
+    return d
+
+
+def collect(ctx, dgraph, src: int = 0, reps: int = 1):
+    """Per-level features, labels and masks of one graph from three traversals."""
+    g = _g()
+    n, m = dgraph.n, dgraph.m
+    out = ctx.array(n, np.int32)
+    traces = {}
+    for mode in (g.BFS_PUSH, g.BFS_PULL, g.BFS_TOPO):
+        best = None
+        for _ in range(reps):
+            rc, st = dgraph.bfs(src, out, mode)
+            g.check(rc, "bfs (trace collection)")
+            tr = dgraph.trace()
+            d = level_times(tr)
+            best = d if best is None else np.fmin(best, d)
+        traces[mode] = (tr, best)
+    tr, t_push = traces[g.BFS_PUSH]
+    _, t_pull = traces[g.BFS_PULL]
+    _, t_topo = traces[g.BFS_TOPO]
+    L = len(tr)
+    X = np.zeros((L, 12), np.float32)
+    Y = np.zeros((L, 4), np.float32)
+    M = np.zeros((L, 4), np.float32)
+    prev_nf, prev_dir = 1, 0
+    for i in range(L):
+        r = tr[i]
+        X[i] = g.level_features(n, m, int(r["level"]), int(r["nf"]), int(r["mf"]), int(r["nu"]), int(r["mu"]),
+                                prev_nf, prev_dir)
+        prev_nf = int(r["nf"])
+        if np.isfinite(t_push[i]) and np.isfinite(t_pull[i]) and i > 0:
+            Y[i, 0] = 1.0 if t_pull[i] < t_push[i] else 0.0
+            M[i, 0] = 1.0
+        if np.isfinite(t_push[i]) and np.isfinite(t_topo[i]):
+            Y[i, 1] = 1.0 if t_topo[i] < t_push[i] else 0.0
+            M[i, 1] = 1.0
+        nxt = int(tr[i + 1]["nf"]) if i + 1 < L else 0
+        Y[i, 2] = np.log2(1.0 + nxt)
+        M[i, 2] = 1.0
+        prev_dir = 1 if Y[i, 0] > 0.5 and M[i, 0] > 0 else 0
+    return X, Y, M, {"push": t_push, "pull": t_pull, "topo": t_topo}
+
+
+def train(ctx, X, Y, M, steps: int = 3000, lr: float = 3e-3, seed: int = 2022):
+    """Adam on the GPU (one persistent launch); returns (params, loss history)."""
+    g = _g()
+    # normalise the regression target's weight so it does not dominate the loss
+    M = M.copy()
+    M[:, 2] *= 0.05
+    p0 = g.mlp_init(seed)
+    return g.mlp_train(ctx, p0, X, Y, M, steps=steps, lr=lr)
+
+
+def accuracy(ctx, params, X, Y, M):
+    g = _g()
+    out = g.mlp_forward(ctx, params, X)
+    res = {}
+    for h in (0, 1):
+        sel = M[:, h] > 0
+        if sel.any():
+            res[f"head{h}_acc"] = float(np.mean((out[sel, h] > 0) == (Y[sel, h] > 0.5)))
+    sel = M[:, 2] > 0
+    if sel.any():
+        res["head2_within_2x"] = float(np.mean(np.abs(out[sel, 2] - Y[sel, 2]) <= 1.0))
+    return res
+
+
+def save(path, params: np.ndarray):
+    np.save(path, np.asarray(params, dtype=np.float32))
+
+
+def load(path) -> np.ndarray:
+    return np.load(path).astype(np.float32)
