@@ -4,7 +4,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-ALL = [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10]
+ALL = [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11]
 
 
 def _run_bench(gsrb, ctx, variant, k, cluster=2, episodes=2000, fma=0, threads=256, fanin=0):
@@ -38,6 +38,19 @@ def test_cluster_sizes_and_fanin(gsrb, ctx, cluster, fanin):
     assert int(cnt.download()[0]) == 1000 * grid
 
 
+@pytest.mark.parametrize("groups", [0, 8, 37, 148])
+@pytest.mark.parametrize("wake", [1, 8])
+@pytest.mark.parametrize("k", [1, 8])
+def test_hier_groups_and_wake_lines(gsrb, ctx, groups, wake, k):
+    c = gsrb.cfg(variant=gsrb.BAR_HIER, ctas_per_sm=k, threads=256, fanin_groups=groups, wake_lines=wake)
+    grid = k * ctx.num_sms
+    sink = ctx.array(grid * 256, np.float32).zero()
+    cnt = ctx.array(1, np.uint32).zero()
+    gsrb.check(ctx.barrier_bench(c, 1500, 4, sink, cnt))
+    ctx.check_status()
+    assert int(cnt.download()[0]) == 1500 * grid
+
+
 @pytest.mark.parametrize("variant", ALL)
 def test_barrier_message_passing_litmus(gsrb, ctx, variant):
     c = gsrb.cfg(variant=variant, ctas_per_sm=4, threads=128, cluster=4)
@@ -59,7 +72,7 @@ def test_refuses_non_coresident_grid(gsrb, ctx):
     assert ctx.barrier_bench(c, 10, 0, sink, cnt) == gsrb.ERR_NOT_CORESIDENT
 
 
-@pytest.mark.parametrize("variant", [0, 2, 3, 4, 5, 8, 9])
+@pytest.mark.parametrize("variant", [0, 2, 3, 4, 5, 8, 9, 11])
 def test_short_grid_times_out_and_context_survives(gsrb, ctx, variant):
     # the expected arrival count is one participant higher than the launch:
     # every wait must run out (bounded) and report a timeout, not hang

@@ -26,7 +26,7 @@ def batch_graphs(gsrb):
     return gs
 
 
-@pytest.mark.parametrize("variant", [3, 4, 5, 8, 9])
+@pytest.mark.parametrize("variant", [3, 4, 5, 8, 9, 11])
 def test_batch_bfs_exact(gsrb, ctx, orc, batch_graphs, variant):
     dgs = [ctx.graph(g) for g in batch_graphs]
     outs = [ctx.array(g.nnodes, np.int32) for g in batch_graphs]

@@ -40,7 +40,7 @@ def test_bfs_levels_exact(gsrb, ctx, orc, graphs, name, mode):
     assert st.edges == orc.traversed_edges(g, want)
 
 
-@pytest.mark.parametrize("variant", [0, 2, 3, 4, 5, 6, 7, 8, 9])
+@pytest.mark.parametrize("variant", [0, 2, 3, 4, 5, 6, 7, 8, 9, 11])
 def test_bfs_barrier_variants(gsrb, ctx, orc, graphs, variant):
     g = graphs["rmat16"]
     dg = ctx.graph(g)

@@ -4,7 +4,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-VARIANTS = [0, 2, 3, 4, 5, 6, 7, 8, 9]
+VARIANTS = [0, 2, 3, 4, 5, 6, 7, 8, 9, 11]
 
 
 def _reduce(gsrb, ctx, a, cfg=None, offset=0):

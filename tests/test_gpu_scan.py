@@ -57,7 +57,7 @@ def test_scan_u32_inplace_and_wraparound(gsrb, ctx, orc):
     assert np.array_equal(_scan(gsrb, ctx, a, inplace=True), orc.scan_u32(a))
 
 
-@pytest.mark.parametrize("variant", [0, 2, 3, 4, 5, 6, 7, 8, 9])
+@pytest.mark.parametrize("variant", [0, 2, 3, 4, 5, 6, 7, 8, 9, 11])
 def test_scan_u32_barrier_variants(gsrb, ctx, orc, variant):
     a = gsrb.uniform_i32(11, 5_000_001, 0, 15).astype(np.uint32)
     c = gsrb.cfg(variant=variant, ctas_per_sm=1, threads=1024, cluster=2, tile=8192)

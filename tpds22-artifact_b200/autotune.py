@@ -1,0 +1,150 @@
+"""Autotuner: picks barrier variant, cluster size, fan-in, wake-up lines, CTAs
+per SM, threads and tile size per workload by measuring candidates on the
+device, and caches the winners in a JSON file (tuned.json next to this file by
+default).
+
+Families (the same split as gsrb_max_coresident):
+  barrier   -- the grid-barrier microbenchmark at a fixed CTAs/SM
+  reduce    -- gsrb_reduce_i32 on a given device array
+  scan      -- gsrb_scan_u32 on a given device array
+  bfs       -- gsrb_bfs on a given device graph
+Every candidate is timed with CUDA events on the context stream (median of
+`reps` launches after one warm-up); candidates the device cannot co-schedule
+are skipped (the library refuses them).
+"""
+from __future__ import annotations
+
+import json
+import pathlib
+import statistics
+import sys
+
+import numpy as np
+
+CACHE = pathlib.Path(__file__).resolve().parent / "tuned.json"
+
+
+def _g():
+    return sys.modules["gsrb_b200"]
+
+
+def barrier_candidates(k: int):
+    g = _g()
+    c = [dict(variant=g.BAR_CCG), dict(variant=g.BAR_FLAT), dict(variant=g.BAR_FLIP, fanin_groups=1)]
+    for R in (2, 4, 8):
+        for s in (0, 64):
+            c.append(dict(variant=g.BAR_FANOUT, wake_lines=R, spin_ns=s))
+    for G in (8, 16, 37, 74):
+        for R in (4, 8):
+            c.append(dict(variant=g.BAR_HIER, fanin_groups=G, wake_lines=R))
+    for cl in (2, 4, 8):
+        c.append(dict(variant=g.BAR_CLUSTER_FANOUT, cluster=cl, wake_lines=8))
+        c.append(dict(variant=g.BAR_CLUSTER, cluster=cl, fanin_groups=1))
+    return c
+
+
+def _median_ms(ctx, fn, reps):
+    ts = []
+    for i in range(reps + 1):
+        ctx.record(40)
+        st = fn()
+        if st:
+            return None
+        ctx.record(41)
+        t = ctx.elapsed_ms(40, 41)
+        if i:
+            ts.append(t)
+    if ctx.status()[0] != 0:
+        return None
+    return statistics.median(ts)
+
+
+def tune_barrier(ctx, k: int, threads: int = 256, episodes: int = 4000, reps: int = 3):
+    """Best barrier configuration for k CTAs per SM; returns (cfg dict, ns/episode, table)."""
+    g = _g()
+    grid = k * ctx.num_sms
+    sink = ctx.array(grid * threads, np.float32).zero()
+    cnt = ctx.array(1, np.uint32).zero()
+    base = _median_ms(ctx, lambda: ctx.barrier_bench(g.cfg(variant=g.BAR_NONE, ctas_per_sm=k, threads=threads),
+                                                     episodes, 0, sink, cnt), reps)
+    table = []
+    for cand in barrier_candidates(k):
+        c = g.cfg(ctas_per_sm=k, threads=threads, **cand)
+        t = _median_ms(ctx, lambda: ctx.barrier_bench(c, episodes, 0, sink, cnt), reps)
+        if t is not None and base is not None:
+            table.append((round((t - base) * 1e6 / episodes, 1), cand))
+    table.sort(key=lambda x: x[0])
+    best = dict(table[0][1], ctas_per_sm=k, threads=threads)
+    return best, table[0][0], table
+
+
+def tune_scan(ctx, d_in, d_out, n: int, reps: int = 3):
+    g = _g()
+    table = []
+    for tile in (8192, 16384, 24576):
+        for threads in (512, 1024):
+            for cand in (dict(variant=g.BAR_FANOUT, wake_lines=4), dict(variant=g.BAR_FLIP, fanin_groups=1),
+                         dict(variant=g.BAR_CCG), dict(variant=g.BAR_CLUSTER, cluster=2)):
+                c = g.cfg(ctas_per_sm=1, threads=threads, tile=tile, **cand)
+                t = _median_ms(ctx, lambda: ctx.scan(d_in, d_out, n, c), reps)
+                if t is not None:
+                    table.append((t, dict(cand, ctas_per_sm=1, threads=threads, tile=tile)))
+    table.sort(key=lambda x: x[0])
+    return table[0][1], table[0][0], table
+
+
+def tune_reduce(ctx, d_in, n: int, reps: int = 5):
+    g = _g()
+    out = ctx.array(1, np.int64)
+    table = []
+    for k, threads in ((1, 1024), (2, 256), (2, 512), (4, 256)):
+        for cand in (dict(variant=g.BAR_FANOUT, wake_lines=4), dict(variant=g.BAR_FLIP, fanin_groups=1),
+                     dict(variant=g.BAR_CCG)):
+            c = g.cfg(ctas_per_sm=k, threads=threads, **cand)
+
+            def run():
+                ctx.l2_flush()
+                return ctx.reduce_i32(d_in, n, out, c)
+            t = _median_ms(ctx, run, reps)
+            if t is not None:
+                table.append((t, dict(cand, ctas_per_sm=k, threads=threads)))
+    table.sort(key=lambda x: x[0])
+    return table[0][1], table[0][0], table
+
+
+def tune_bfs(ctx, dgraph, src: int, mode: int, reps: int = 2):
+    g = _g()
+    out = ctx.array(dgraph.n, np.int32)
+    table = []
+    for k, threads in ((1, 512), (2, 256), (2, 512), (4, 256)):
+        for cand in (dict(variant=g.BAR_FANOUT, wake_lines=4), dict(variant=g.BAR_FLIP, fanin_groups=1),
+                     dict(variant=g.BAR_HIER, fanin_groups=16, wake_lines=8), dict(variant=g.BAR_CCG)):
+            c = g.cfg(ctas_per_sm=k, threads=threads, **cand)
+            ts = []
+            for _ in range(reps):
+                rc, st = dgraph.bfs(src, out, mode, c)
+                if rc:
+                    ts = None
+                    break
+                ts.append(st.kernel_ms)
+            if ts:
+                table.append((statistics.median(ts), dict(cand, ctas_per_sm=k, threads=threads)))
+    table.sort(key=lambda x: x[0])
+    return table[0][1], table[0][0], table
+
+
+def load_cache(path=CACHE) -> dict:
+    try:
+        return json.loads(pathlib.Path(path).read_text())
+    except Exception:
+        return {}
+
+
+def save_cache(data: dict, path=CACHE):
+    pathlib.Path(path).write_text(json.dumps(data, indent=1, sort_keys=True))
+
+
+def cfg_from(entry: dict):
+    g = _g()
+    keys = {k: v for k, v in entry.items() if k in dict(g.Cfg._fields_)}
+    return g.cfg(**keys)
