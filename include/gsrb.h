@@ -145,6 +145,21 @@ gsrb_status_t gsrb_probe_l2_atomics(gsrb_ctx_t ctx, int32_t ctas, int32_t iters,
 gsrb_status_t gsrb_reduce_i32(gsrb_ctx_t ctx, const int32_t* d_in, size_t n, int64_t* d_out,
                               const gsrb_cfg_t* cfg);
 
+/* Allocation-free variant of gsrb_reduce_i32 (no counterpart in the reference).
+ * For callers that must not allocate device memory -- code running inside a
+ * host framework's fixed memory budget, or a plugin that may not grow the
+ * device footprint or call cudaMalloc -- and therefore cannot create a context.
+ * The barrier state and the per-CTA partials live in one fixed static device
+ * array of 17 KiB, which every GPU that loads the library holds until exit; the
+ * call needs only d_in, d_out and a stream (NULL = legacy default stream) and
+ * calls no cudaMalloc / cudaFree.  Limits: n <= 2^32 elements (larger n returns
+ * GSRB_ERR_ARG), grid = 2 CTAs per SM (at most 2048 CTAs).  The first call on a
+ * device looks up the array's device address with that device current; make it
+ * before any stream capture.  Every call clears the array's barrier words and
+ * reuses it, so calls whose kernels overlap on the GPU race.  Synchronous with
+ * respect to `stream`; returns GSRB_ERR_TIMEOUT if a bounded wait ran out. */
+gsrb_status_t gsrb_reduce_i32_noalloc(const int32_t* d_in, size_t n, int64_t* d_out, void* stream);
+
 /* ---- scan --------------------------------------------
  * Exclusive prefix sum, one persistent launch (default one 1024-thread CTA per
  * SM, 96 KiB tiles double-buffered in shared memory, moved by cp.async.bulk),
