@@ -1,24 +1,34 @@
 #!/usr/bin/env python
 """Benchmark driver: one JSON line on rank 0.
 
-Headline workload (the configuration the metric is quoted on): the grid-barrier
-microbenchmark -- one persistent launch of 148*k CTAs x 256 threads running
-10,000 barrier episodes (k = 8: full residency, 2048 threads per SM), each
-episode preceded by F dependent FP32 FMAs per thread (F = 0 for the headline).
-value = ns per grid barrier = (t_launch - t_phase_only) / episodes, lower is
-better.  The line also carries the data-phase kernels measured on the same
-device: reduce (2^24 int32) and scan (2^28 u32 / f32) GB/s against the measured
-HBM peak, and the comparison barriers (cooperative-groups grid.sync, the
-reference GSRB/GCPUSRB/atomic-tree algorithms) on the same shape.
+Headline workload (the configuration the metric's first clause is quoted on):
+the grid-barrier microbenchmark -- one persistent launch of 148*k CTAs x 256
+threads running 10,000 barrier episodes, k = 8 (full residency: 2048 threads
+per SM), each episode preceded by F = 0 dependent FP32 FMAs per thread.
+value = ns per grid barrier = (t_launch - t_phase_only) / episodes (lower is
+better), with the barrier configuration chosen by the autotuner at run time.
+
+The same line carries every other configuration of the benchmark plan,
+measured on the same device in the same run (disable with --no-extras):
+  barrier_table     ns/episode for k in {1,2,4,8} x F in {0,64,1024}: tuned
+                    native barrier vs cooperative-groups grid.sync and the
+                    reference algorithms (GSRB, GCPUSRB, atomic tree)
+  semaphore         acquires/s, capacity S in {1,2,10,120}, 1 writer per 10 readers
+  reduce_2e24       GB/s and fraction of measured HBM (cold L2), bit-exact check
+  scan_2e28         u32 (bit-exact) and f32 (1e-5 relative), GB/s, HBM fraction
+  graphs            RMAT-22 and the 2048^2 grid: BFS (plain push / heuristic /
+                    learned), SSSP, PageRank; GTEPS; levels/distances checked
+  batch             64 RMAT graphs (scales 14..20): plain one-by-one push BFS vs
+                    batched + learned in one CUDA-graph launch; aggregate GTEPS
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload barrier|reduce|scan] [--k 8] [--fma 0]
+                  [--workload barrier|reduce|scan|bfs] [--k 8] [--fma 0] [--no-extras]
 
 --impl reference times the reference's CPU implementation of the path on the
-host cores (the reference has no CPU barrier, so this is the oracle port of
-its sense-reversing barrier run by host threads), same metric and unit.
-Multi-GPU: the barrier does not shard (replicas only): every rank runs the same
-workload on its own GPU and the reported time is the max over ranks.
+host cores: the reference has no CPU barrier, so this is the oracle's port of
+its sense-reversing barrier run by host threads (same metric and unit).
+Multi-GPU: the barrier does not shard (replicas only): every rank runs the
+same workload on its own GPU and the reported time is the max over ranks.
 """
 from __future__ import annotations
 
@@ -36,21 +46,29 @@ import time
 import numpy as np
 
 ROOT = pathlib.Path(__file__).resolve().parent
+PKG = ROOT / "tpds22-artifact_b200"
 PEAKS = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
+SEED = 0x5EED2022
 
 
-def load_binding():
-    spec = importlib.util.spec_from_file_location("gsrb_b200", ROOT / "tpds22-artifact_b200" / "gsrb.py")
+def _load(name, path):
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, path)
     mod = importlib.util.module_from_spec(spec)
-    sys.modules["gsrb_b200"] = mod
+    sys.modules[name] = mod
     spec.loader.exec_module(mod)
     return mod
 
 
+def load_binding():
+    return _load("gsrb_b200", PKG / "gsrb.py")
+
+
 def load_oracle():
     sys.path.insert(0, str(ROOT / "tests"))
-    import oracle_binding  # noqa: E402  (CPU baseline leg only)
+    import oracle_binding  # the checker / CPU-baseline leg only
     return oracle_binding
 
 
@@ -72,7 +90,7 @@ class Dist:
             import datetime
 
             import torch.distributed as dist
-            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
             self.pg = dist
 
     def barrier(self):
@@ -143,23 +161,7 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-# ------------------------------------------------------------------ workloads
-def best_native_cfg(gsrb, ctx, k, threads=256):
-    """The native three-level barrier configuration used for the headline.
-
-    Cluster 8 with a fan-in layer keeps the global counter at <= 37 arrivals;
-    falls back to smaller clusters when the device cannot co-schedule it."""
-    for cl, fan in ((8, 0), (4, 0), (2, 0), (1, 0)):
-        c = gsrb.cfg(variant=gsrb.BAR_CLUSTER if cl > 1 else gsrb.BAR_SOFT2, ctas_per_sm=k, threads=threads,
-                     cluster=cl, fanin_groups=fan)
-        try:
-            if ctx.max_coresident(c, 0) >= k * ctx.num_sms:
-                return c
-        except gsrb.GsrbError:
-            continue
-    return gsrb.cfg(variant=gsrb.BAR_FLAT, ctas_per_sm=k, threads=threads)
-
-
+# ------------------------------------------------------------------- barrier
 def time_barrier(gsrb, ctx, c, episodes, fma, steps, warmup, flush=True):
     """Per-launch CUDA-event times (ms) of `steps` launches after `warmup`."""
     grid = c.ctas_per_sm * ctx.num_sms if c.grid_override <= 0 else c.grid_override
@@ -184,14 +186,13 @@ def time_barrier(gsrb, ctx, c, episodes, fma, steps, warmup, flush=True):
 
 
 def barrier_e2e(gsrb, ctx, c, episodes, fma, steps, warmup):
-    """Same launch through the public C ABI with host buffers: H2D of the
-    per-thread FMA state (pinned), the persistent launch, D2H of the results."""
+    """The same launch through the public C ABI with host buffers: H2D of the
+    per-thread FMA seeds from pinned memory, the launch, D2H of the results."""
     import ctypes as C
     lib = gsrb.lib()
     grid = c.ctas_per_sm * ctx.num_sms
     n = grid * c.threads
-    h_in = C.c_void_p()
-    h_out = C.c_void_p()
+    h_in, h_out = C.c_void_p(), C.c_void_p()
     gsrb.check(lib.gsrb_host_alloc(C.byref(h_in), n * 4))
     gsrb.check(lib.gsrb_host_alloc(C.byref(h_out), n * 4 + 4))
     C.memset(h_in, 0, n * 4)
@@ -215,7 +216,7 @@ def barrier_e2e(gsrb, ctx, c, episodes, fma, steps, warmup):
     return times, n * 4, n * 4 + 4
 
 
-def l2_atomic_peak(gsrb, ctx):
+def l2_atomic_peak(ctx):
     """Same-address red.add throughput (atomics/s) and atom round trip (ns)."""
     ctas, iters = 4 * ctx.num_sms, 2000
     ctx.probe_l2_atomics(ctas, 200, 0)
@@ -223,16 +224,75 @@ def l2_atomic_peak(gsrb, ctx):
     rate = ctas * iters / (ms * 1e-3)
     ctx.probe_l2_atomics(1, 1000, 1)
     ms1 = min(ctx.probe_l2_atomics(1, 20000, 1) for _ in range(3))
-    rtt_ns = ms1 * 1e6 / 20000
-    return rate, rtt_ns
+    return rate, ms1 * 1e6 / 20000
 
 
-def reduce_numbers(gsrb, ctx, orc, reps=10):
+def arrivals_per_episode(gsrb, c, grid):
+    if c.variant in (gsrb.BAR_CLUSTER, gsrb.BAR_CLUSTER_ALLPOLL, gsrb.BAR_DSMEM, gsrb.BAR_CLUSTER_RED,
+                     gsrb.BAR_CLUSTER_FANOUT):
+        return grid // max(1, c.cluster)
+    return grid
+
+
+def barrier_table(gsrb, ctx, tune, tuned_cache):
+    rows = []
+    for k in (1, 2, 4, 8):
+        best, _, _ = tune.tune_barrier(ctx, k, episodes=2000, reps=2)
+        tuned_cache[f"barrier_k{k}"] = best
+        bc = tune.cfg_from(best)
+        for F in (0, 64, 1024):
+            eps = 2000 if F < 1024 else 500
+            base = statistics.median(time_barrier(gsrb, ctx, gsrb.cfg(variant=gsrb.BAR_NONE, ctas_per_sm=k,
+                                                                     threads=256), eps, F, 3, 1))
+            row = {"k": k, "F": F, "tuned": gsrb.VARIANT_NAMES[best["variant"]]}
+            for name, c in (("native", bc), ("ccg", gsrb.cfg(variant=gsrb.BAR_CCG, ctas_per_sm=k, threads=256)),
+                            ("ref_gsrb", gsrb.cfg(variant=gsrb.BAR_SOFT2, ctas_per_sm=k, threads=256)),
+                            ("ref_gcpusrb", gsrb.cfg(variant=gsrb.BAR_FLAT, ctas_per_sm=k, threads=256)),
+                            ("atomic_tree", gsrb.cfg(variant=gsrb.BAR_TREE, ctas_per_sm=k, threads=256))):
+                try:
+                    t = statistics.median(time_barrier(gsrb, ctx, c, eps, F, 3, 1))
+                    row[name] = round((t - base) * 1e6 / eps, 1)
+                except (gsrb.GsrbError, AssertionError) as e:
+                    row[name] = f"failed: {e}"
+            if isinstance(row.get("ccg"), float) and isinstance(row.get("native"), float):
+                row["speedup_vs_ccg"] = round(row["ccg"] / max(row["native"], 1e-9), 3)
+            rows.append(row)
+    return rows
+
+
+def semaphore_numbers(gsrb, ctx):
+    out = []
+    for S in (1, 2, 10, 120):
+        row = {"S": S}
+        for name, kind, k in (("native_priority", gsrb.SEM_PRIORITY, 8), ("ref_priority", gsrb.SEM_REF_PRIORITY, 8),
+                              ("ref_spin_k2", gsrb.SEM_REF_SPIN, 2)):
+            c = gsrb.cfg(ctas_per_sm=k, threads=256, timeout_ms=5000)
+            cnt = ctx.array(8, np.uint32).zero()
+            iters = 2
+            ctx.record(6)
+            st = ctx.semaphore_bench(c, kind, S, 11, iters, 100, cnt)
+            ctx.record(7)
+            ms = ctx.elapsed_ms(6, 7)
+            W, R, inside, maxr, viol, acq, tmo, _ = cnt.download().tolist()
+            grid = k * ctx.num_sms
+            writers = len([b for b in range(grid) if b % 11 == 0])
+            exact = (st == 0 and W == writers * iters * 100 and R == (grid - writers) * iters * 100 and viol == 0
+                     and maxr <= S)
+            row[name] = {"acquires_per_s": round(acq / (ms * 1e-3), 1), "ms": round(ms, 3), "exact": exact,
+                         "ctas": grid}
+        out.append(row)
+    return out
+
+
+# --------------------------------------------------------------- data kernels
+def reduce_numbers(gsrb, ctx, orc, tune, cache, reps=10, fixed=None):
     n = 1 << 24
-    a = gsrb.uniform_i32(0x5EED2022, n, 0, 127)
+    a = gsrb.uniform_i32(SEED, n, 0, 127)
     d = ctx.to_device(a)
     out = ctx.array(1, np.int64).zero()
-    c = gsrb.cfg(ctas_per_sm=2, threads=256, cluster=2)
+    best = fixed or tune.tune_reduce(ctx, d, n, reps=3)[0]
+    cache["reduce"] = best
+    c = tune.cfg_from(best)
     times = []
     for i in range(3 + reps):
         ctx.l2_flush()  # 64 MiB fits in L2: time it cold
@@ -244,9 +304,232 @@ def reduce_numbers(gsrb, ctx, orc, reps=10):
     ctx.check_status("reduce")
     ok = int(out.download()[0]) == orc.sum_i32(a)
     t = statistics.median(times)
+    peak, src = hbm_peak()
     gbs = 4 * n / (t * 1e-3) / 1e9
     d.free()
-    return {"n": n, "ms": round(t, 5), "GB_s": round(gbs, 1), "bit_exact": ok, "cold_l2": True}
+    return {"n": n, "ms": round(t, 5), "GB_s": round(gbs, 1), "hbm_frac": round(gbs / peak, 4),
+            "peak_source": src, "bit_exact": ok, "cold_l2": True, "cfg": best}
+
+
+def scan_numbers(gsrb, ctx, orc, tune, cache, n=1 << 28, reps=5, fixed=None):
+    peak, src = hbm_peak()
+    res = {"n": n, "peak_source": src}
+    a = gsrb.uniform_i32(SEED, n, 0, 15).astype(np.uint32)
+    din = ctx.to_device(a)
+    dout = ctx.array(n, np.uint32)
+    best = fixed or tune.tune_scan(ctx, din, dout, n, reps=2)[0]
+    cache["scan"] = best
+    c = tune.cfg_from(best)
+    for kind in ("u32", "f32"):
+        if kind == "f32":
+            din.free()
+            dout.free()
+            a = gsrb.uniform_f32(SEED, n)
+            din = ctx.to_device(a)
+            dout = ctx.array(n, np.float32)
+        times = []
+        for i in range(1 + reps):
+            ctx.record(4)
+            gsrb.check(ctx.scan(din, dout, n, c))
+            ctx.record(5)
+            if i:
+                times.append(ctx.elapsed_ms(4, 5))
+        ctx.check_status("scan")
+        got = dout.download()
+        if kind == "u32":
+            ok = bool(np.array_equal(got, orc.scan_u32(a, threads=os.cpu_count() or 1)))
+            check = {"bit_exact": ok}
+        else:
+            ref = orc.scan_f32_f64(a)
+            err = orc.max_rel_err(got[1:], ref[1:])
+            check = {"max_rel_err": err, "within_1e-5": bool(err <= 1e-5)}
+            del ref
+        del got
+        t = statistics.median(times)
+        gbs = 8 * n / (t * 1e-3) / 1e9
+        res[kind] = dict({"ms": round(t, 4), "GB_s": round(gbs, 1), "hbm_frac": round(gbs / peak, 4)}, **check)
+    res["cfg"] = best
+    din.free()
+    dout.free()
+    return res
+
+
+# --------------------------------------------------------------------- graphs
+def train_policy(gsrb, ctx, pol):
+    """Per-level traces of training graphs (not the evaluation graphs) -> MLP."""
+    graphs = [gsrb.rmat(s, 16, seed=SEED + 1000 + s) for s in (14, 16, 18, 20)]
+    graphs += [gsrb.grid2d(256, 256, seed=SEED + 7), gsrb.grid2d(1024, 64, seed=SEED + 8)]
+    X, Y, M = [], [], []
+    for g in graphs:
+        dg = ctx.graph(g)
+        x, y, m, _ = pol.collect(ctx, dg, 0, reps=2)
+        X.append(x)
+        Y.append(y)
+        M.append(m)
+        dg.free()
+    X, Y, M = np.concatenate(X), np.concatenate(Y), np.concatenate(M)
+    t0 = time.time()
+    params, hist = pol.train(ctx, X, Y, M, steps=3000)
+    acc = pol.accuracy(ctx, params, X, Y, M)
+    return params, {"levels": int(len(X)), "train_s": round(time.time() - t0, 2), "loss_first": float(hist[0]),
+                    "loss_last": float(hist[-1]), **acc}
+
+
+def bfs_runs(gsrb, ctx, orc, dg, g, params, cfg, reps=3):
+    out = ctx.array(g.nnodes, np.int32)
+    want = orc.bfs(g, 0)
+    m_trav = orc.traversed_edges(g, want)
+    res = {"m_traversed": m_trav}
+    dg.set_policy(params)
+    for name, mode in (("plain_push", gsrb.BFS_PUSH), ("heuristic", gsrb.BFS_HEURISTIC),
+                       ("learned", gsrb.BFS_LEARNED)):
+        ts = []
+        for _ in range(reps):
+            rc, st = dg.bfs(0, out, mode, cfg)
+            gsrb.check(rc, f"bfs {name}")
+            ts.append(st.kernel_ms)
+        ok = bool(np.array_equal(out.download(), want))
+        t = statistics.median(ts)
+        res[name] = {"ms": round(t, 3), "GTEPS": round(m_trav / (t * 1e-3) / 1e9, 3), "levels": int(st.levels),
+                     "bit_exact": ok}
+        if mode == gsrb.BFS_LEARNED:
+            res[name]["policy_decisions"] = int(st.decisions)
+            res[name]["fallback_level"] = int(st.aux)
+    res["learned_vs_plain"] = round(res["plain_push"]["ms"] / res["learned"]["ms"], 3)
+    return res
+
+
+def sssp_runs(gsrb, ctx, orc, dg, g, deltas, cfg, verify=True):
+    out = ctx.array(g.nnodes, np.int32)
+    want = orc.dijkstra(g, 0) if verify else None
+    m_trav = orc.traversed_edges(g, want) if verify else g.nedges
+    res = {}
+    for name, delta in deltas:
+        rc, st = dg.sssp(0, out, delta, cfg)
+        gsrb.check(rc, "sssp")
+        rc, st = dg.sssp(0, out, delta, cfg)
+        gsrb.check(rc, "sssp")
+        ok = bool(np.array_equal(out.download(), want)) if verify else None
+        res[name] = {"delta": delta, "ms": round(st.kernel_ms, 3),
+                     "GTEPS": round(m_trav / (st.kernel_ms * 1e-3) / 1e9, 3), "rounds": int(st.levels),
+                     "buckets": int(st.aux), "edges_relaxed": int(st.edges), "bit_exact": ok}
+    return res
+
+
+def graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, verify_pr=True):
+    res = {}
+    t0 = time.time()
+    rm = gsrb.rmat(22, 16, a=0.57, b=0.19, c=0.19, seed=SEED, wlo=1, whi=255)
+    res["rmat22"] = {"n": rm.nnodes, "m": rm.nedges, "max_degree": int(rm.degrees().max()),
+                     "gen_s": round(time.time() - t0, 1)}
+    dg = ctx.graph(rm)
+    best, _, _ = tune.tune_bfs(ctx, dg, 0, gsrb.BFS_HEURISTIC, reps=1)
+    cache["bfs_rmat"] = best
+    cfg = tune.cfg_from(best)
+    res["rmat22"]["bfs"] = bfs_runs(gsrb, ctx, orc, dg, rm, params, cfg)
+    res["rmat22"]["sssp"] = sssp_runs(gsrb, ctx, orc, dg, rm, [("reference_delta", 10000), ("delta_256", 256)], cfg)
+    out = ctx.array(rm.nnodes, np.float32)
+    rc, st = dg.pagerank(out, 0.85, 50, cfg)
+    gsrb.check(rc, "pagerank")
+    rc, st = dg.pagerank(out, 0.85, 50, cfg)
+    gsrb.check(rc, "pagerank")
+    per_iter_bytes = 4 * (rm.nnodes + 1) + 4 * rm.nedges + 8 * rm.nnodes
+    l1 = orc.normalized_l1(out.download(), orc.pagerank(rm, 0.85, 50)) if verify_pr else None
+    res["rmat22"]["pagerank"] = {"iters": 50, "ms": round(st.kernel_ms, 3),
+                                 "edges_per_s": round(50 * rm.nedges / (st.kernel_ms * 1e-3), 1),
+                                 "GB_s_algorithmic": round(50 * per_iter_bytes / (st.kernel_ms * 1e-3) / 1e9, 1),
+                                 "l1_vs_fp64": l1, "within_1e-6": (l1 <= 1e-6) if l1 is not None else None}
+    dg.free()
+    del rm
+    gr = gsrb.grid2d(2048, 2048, seed=SEED, wlo=1, whi=1000)
+    dg = ctx.graph(gr)
+    best, _, _ = tune.tune_bfs(ctx, dg, 0, gsrb.BFS_PUSH, reps=1)
+    cache["bfs_grid"] = best
+    cfg = tune.cfg_from(best)
+    res["grid2048"] = {"n": gr.nnodes, "m": gr.nedges, "bfs": bfs_runs(gsrb, ctx, orc, dg, gr, params, cfg, reps=2)}
+    res["grid2048"]["sssp"] = sssp_runs(gsrb, ctx, orc, dg, gr, [("reference_delta", 10000), ("delta_4096", 4096)],
+                                        cfg)
+    dg.free()
+    return res
+
+
+def batch_numbers(gsrb, ctx, orc, params):
+    rng = np.random.default_rng(SEED)
+    scales = rng.integers(14, 21, 64)
+    t0 = time.time()
+    graphs = [gsrb.rmat(int(s), 16, seed=SEED + i, wlo=1, whi=255) for i, s in enumerate(scales)]
+    gen_s = time.time() - t0
+    dgs = [ctx.graph(g) for g in graphs]
+    for dg in dgs:
+        dg.set_policy(params)
+    outs = [ctx.array(g.nnodes, np.int32) for g in graphs]
+    wants = [orc.bfs(g, 0) for g in graphs]
+    m_total = sum(orc.traversed_edges(g, w) for g, w in zip(graphs, wants))
+    res = {"graphs": 64, "scales": [int(s) for s in scales], "m_total": int(sum(g.nedges for g in graphs)),
+           "m_traversed": int(m_total), "gen_s": round(gen_s, 1)}
+    # plain: the reference algorithm (worklist push), one whole-grid launch per graph
+    plain_cfg = gsrb.cfg(variant=gsrb.BAR_SOFT2, ctas_per_sm=2, threads=256)
+    for rep in range(2):
+        ctx.record(8)
+        for dg, o in zip(dgs, outs):
+            rc, _ = dg.bfs(0, o, gsrb.BFS_PUSH, plain_cfg)
+            gsrb.check(rc, "plain bfs")
+        ctx.record(9)
+        t_plain = ctx.elapsed_ms(8, 9)
+    ok_plain = all(np.array_equal(o.download(), w) for o, w in zip(outs, wants))
+    # batched + learned: one persistent launch, sub-grid barriers, CUDA graph replay
+    b = gsrb.Batch(ctx, dgs, gsrb.cfg(variant=gsrb.BAR_FANOUT, ctas_per_sm=2, threads=512, wake_lines=4))
+    cg = gsrb.CudaGraph(ctx)
+    with cg:
+        gsrb.check(b.bfs([0] * 64, outs, gsrb.BFS_LEARNED), "batch bfs")
+    for o in outs:
+        o.zero()
+    ts = []
+    for rep in range(3):
+        ctx.record(10)
+        cg.launch()
+        ctx.record(11)
+        ts.append(ctx.elapsed_ms(10, 11))
+    rc, st = b.stats()
+    gsrb.check(rc, "batch stats")
+    ok_batch = all(np.array_equal(o.download(), w) for o, w in zip(outs, wants))
+    t_batch = statistics.median(ts)
+    res["bfs"] = {"plain_ms": round(t_plain, 3), "plain_GTEPS": round(m_total / (t_plain * 1e-3) / 1e9, 3),
+                  "plain_bit_exact": ok_plain, "batched_learned_ms": round(t_batch, 3),
+                  "batched_learned_GTEPS": round(m_total / (t_batch * 1e-3) / 1e9, 3),
+                  "batched_learned_bit_exact": ok_batch, "speedup": round(t_plain / t_batch, 3),
+                  "policy_decisions": int(sum(s.decisions for s in st)),
+                  "fallbacks": int(sum(1 for s in st if s.aux))}
+    cg.free()
+    # SSSP: plain = one launch per graph with the reference's DELTA (10000);
+    # batched = one launch with a tuned bucket width
+    wants_d = [orc.dijkstra(g, 0) for g in graphs]
+    for rep in range(2):
+        ctx.record(8)
+        for dg, o in zip(dgs, outs):
+            rc, _ = dg.sssp(0, o, 10000, plain_cfg)
+            gsrb.check(rc, "plain sssp")
+        ctx.record(9)
+        t_plain = ctx.elapsed_ms(8, 9)
+    ok_plain = all(np.array_equal(o.download(), w) for o, w in zip(outs, wants_d))
+    ts = []
+    for rep in range(3):
+        ctx.record(10)
+        gsrb.check(b.sssp([0] * 64, outs, 256), "batch sssp")
+        ctx.record(11)
+        ts.append(ctx.elapsed_ms(10, 11))
+    rc, _ = b.stats()
+    gsrb.check(rc, "batch sssp stats")
+    ok_batch = all(np.array_equal(o.download(), w) for o, w in zip(outs, wants_d))
+    t_batch = statistics.median(ts)
+    res["sssp"] = {"plain_ms": round(t_plain, 3), "plain_GTEPS": round(m_total / (t_plain * 1e-3) / 1e9, 3),
+                   "plain_bit_exact": ok_plain, "batched_ms": round(t_batch, 3),
+                   "batched_GTEPS": round(m_total / (t_batch * 1e-3) / 1e9, 3), "batched_bit_exact": ok_batch,
+                   "speedup": round(t_plain / t_batch, 3)}
+    b.free()
+    for dg in dgs:
+        dg.free()
+    return res
 
 
 def cpu_barrier_baseline(orc, seconds=8.0):
@@ -256,8 +539,8 @@ def cpu_barrier_baseline(orc, seconds=8.0):
     episodes = int(max(2000, min(5_000_000, seconds * 1e9 / max(ns, 1.0) / 2)))
     ns, stale = orc.cpu_srb_barrier(threads, groups, episodes)
     return {"value": round(ns, 2), "unit": "ns per barrier", "cores": threads, "kind": "port",
-            "sample": f"{threads} host threads (one per core standing in for the 1184 CTAs), "
-                      f"{groups} groups, {2 * episodes} barrier episodes, stale reads {stale}"}
+            "sample": f"{threads} host threads (one per core, standing in for the 1184 CTAs), {groups} groups, "
+                      f"{2 * episodes} barrier episodes, stale reads {stale}"}
 
 
 # ----------------------------------------------------------------------- main
@@ -267,11 +550,15 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="barrier", choices=["barrier"])
+    ap.add_argument("--workload", default="barrier", choices=["barrier", "reduce", "scan", "bfs"])
     ap.add_argument("--k", type=int, default=8)
     ap.add_argument("--fma", type=int, default=0)
+    ap.add_argument("--cfg", type=json.loads, default=None,
+                    help="fixed configuration as JSON (skips the autotuner), e.g. '{\"variant\": 9}'")
     ap.add_argument("--episodes", type=int, default=10_000)
+    ap.add_argument("--scan-n", type=int, default=1 << 28)
     ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--skip-pr-check", action="store_true", help="skip the FP64 CPU PageRank (about 25 s)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -280,14 +567,11 @@ def main():
                             f"{args.episodes} episodes per launch, F={args.fma} FMAs/thread/episode",
                 "ctas": 148 * args.k, "threads_per_cta": 256, "episodes_per_step": args.episodes,
                 "fma_per_episode": args.fma, "parallelism": f"replicas x{args.gpus}",
-                "l2": "flushed (write of 2x L2) before every timed launch"}
+                "l2": "read-flushed (2x L2) before every timed launch"}
 
     if args.impl == "reference":
         if dist.rank == 0:
             orc = load_oracle()
-            res = []
-            for _ in range(args.warmup):
-                pass
             t0 = time.time()
             samples = [cpu_barrier_baseline(orc, seconds=4.0) for _ in range(max(1, min(args.steps, 3)))]
             v = statistics.median(s["value"] for s in samples)
@@ -303,11 +587,36 @@ def main():
         return
 
     gsrb = load_binding()
+    tune = _load("gsrb_autotune", PKG / "autotune.py")
     ctx = gsrb.Context(dist.local if dist.world > 1 else 0)
-    c = best_native_cfg(gsrb, ctx, args.k)
-    none = gsrb.cfg(variant=gsrb.BAR_NONE, ctas_per_sm=args.k, threads=256)
+    cache = {}
 
-    # phase-only baseline (same launch, no barrier)
+    if args.workload != "barrier":
+        # single data-kernel workloads (profiling entry points)
+        orc = load_oracle()
+        if args.workload == "reduce":
+            r = reduce_numbers(gsrb, ctx, orc, tune, cache, reps=args.steps, fixed=args.cfg)
+        elif args.workload == "scan":
+            r = scan_numbers(gsrb, ctx, orc, tune, cache, n=args.scan_n, reps=args.steps, fixed=args.cfg)
+        else:
+            pol = _load("gsrb_policy", PKG / "policy.py")
+            params = gsrb.mlp_init(1)
+            g = gsrb.rmat(18, 16, seed=SEED)
+            dg = ctx.graph(g)
+            r = bfs_runs(gsrb, ctx, orc, dg, g, params, None, reps=args.steps)
+        if dist.rank == 0:
+            print(json.dumps({"workload": args.workload, "result": r}), flush=True)
+        ctx.close()
+        dist.close()
+        return
+
+    if args.cfg:
+        best, tune_table = dict(args.cfg, ctas_per_sm=args.k, threads=256), []
+    else:
+        best, _, tune_table = tune.tune_barrier(ctx, args.k, episodes=2000, reps=2)
+    cache[f"barrier_k{args.k}"] = best
+    c = tune.cfg_from(best)
+    none = gsrb.cfg(variant=gsrb.BAR_NONE, ctas_per_sm=args.k, threads=256)
     t_phase = statistics.median(time_barrier(gsrb, ctx, none, args.episodes, args.fma, 5, 3))
 
     clocks = Clocks(ctx.device)
@@ -322,54 +631,53 @@ def main():
     dist.barrier()
 
     t_step = statistics.median(times)
-    ns_local = (t_step - t_phase) * 1e6 / args.episodes
-    ns = dist.max(ns_local)
+    ns = dist.max((t_step - t_phase) * 1e6 / args.episodes)
     ms_per_step = dist.max(statistics.mean(times))
-
     e2e_times, bi, bo = barrier_e2e(gsrb, ctx, c, args.episodes, args.fma, 5, 3)
     e2e_ns = dist.max(statistics.median(e2e_times) * 1e6 / args.episodes)
+    t_ccg = statistics.median(time_barrier(gsrb, ctx, gsrb.cfg(variant=gsrb.BAR_CCG, ctas_per_sm=args.k,
+                                                              threads=256), args.episodes, args.fma, 5, 2))
+    ns_ccg = (t_ccg - t_phase) * 1e6 / args.episodes
 
-    rate, rtt = l2_atomic_peak(gsrb, ctx)
+    rate, rtt = l2_atomic_peak(ctx)
     grid = args.k * ctx.num_sms
-    arrivals = grid // max(1, c.cluster) if c.variant in (0, 1, 2, 7) else grid
-    achieved = arrivals / (ns * 1e-9)  # global-level atomics per second
+    arrivals = arrivals_per_episode(gsrb, c, grid)
+    achieved = arrivals / (ns * 1e-9)
     roofline = {"bound": "l2_atomic", "achieved": round(achieved / 1e9, 4), "peak": round(rate / 1e9, 4),
                 "unit": "G same-address atomics/s", "frac": round(achieved / rate, 4), "traffic": None,
-                "peak_source": "measured live: same-address red.add throughput probe",
+                "peak_source": "measured live: same-address red.add throughput probe (MEASURED_PEAKS.json has no "
+                               "L2-atomic entry)",
                 "arrivals_per_episode": arrivals, "l2_atomic_rtt_ns": round(rtt, 1),
-                "latency_floor_ns": round(arrivals / rate * 1e9 + 2 * rtt, 1)}
+                "latency_floor_ns": round(arrivals / rate * 1e9 + 2 * rtt, 1),
+                "latency_floor_frac": round((arrivals / rate * 1e9 + 2 * rtt) / ns, 4)}
 
     line = {"metric": "ns per grid barrier", "value": round(ns, 2), "unit": "ns", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-            "data": "synthetic", "config": dict(base_cfg, barrier=gsrb.VARIANT_NAMES[c.variant],
-                                                 cluster=c.cluster, fanin_groups=c.fanin_groups),
-            "phase_only_ms": round(t_phase, 5), "roofline": roofline, "clocks": clk,
+            "data": "synthetic", "config": dict(base_cfg, barrier=gsrb.VARIANT_NAMES[c.variant], tuned=best),
+            "phase_only_ms": round(t_phase, 5), "ccg_grid_sync_ns": round(ns_ccg, 2),
+            "speedup_vs_ccg": round(ns_ccg / ns, 3), "roofline": roofline, "clocks": clk,
             "gpu_launches": int(l1 - l0),
             "e2e": {"value": round(e2e_ns, 2), "unit": "ns", "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
-                    "note": "per-episode time of the whole step incl. H2D/D2H copies and the FMA phase"}}
+                    "note": "per-episode time of the whole step incl. pinned H2D/D2H copies and the FMA phase"},
+            "autotune_top5": [{"ns": t, "cfg": cand} for t, cand in tune_table[:5]]}
 
     if not args.no_extras:
-        extras = {}
-        for name, v in (("ccg_grid_sync", gsrb.BAR_CCG), ("reference_gsrb_soft2", gsrb.BAR_SOFT2),
-                        ("reference_gcpusrb_flat", gsrb.BAR_FLAT), ("atomic_tree", gsrb.BAR_TREE)):
-            cc = gsrb.cfg(variant=v, ctas_per_sm=args.k, threads=256)
-            try:
-                tt = statistics.median(time_barrier(gsrb, ctx, cc, args.episodes, args.fma, 3, 1))
-                extras[name] = round((tt - t_phase) * 1e6 / args.episodes, 2)
-            except (gsrb.GsrbError, AssertionError) as e:
-                extras[name] = f"failed: {e}"
-        line["comparison_ns_per_barrier"] = extras
-        if isinstance(extras.get("ccg_grid_sync"), float):
-            line["speedup_vs_ccg"] = round(extras["ccg_grid_sync"] / ns, 3)
         orc = load_oracle()
-        peak, src = hbm_peak()
-        red = reduce_numbers(gsrb, ctx, orc)
-        red["hbm_frac"] = round(red["GB_s"] / peak, 4)
-        red["peak_source"] = src
-        line["reduce_2e24"] = red
+        pol = _load("gsrb_policy", PKG / "policy.py")
+        extras_t0 = time.time()
+        line["barrier_table"] = barrier_table(gsrb, ctx, tune, cache)
+        line["semaphore"] = semaphore_numbers(gsrb, ctx)
+        line["reduce_2e24"] = reduce_numbers(gsrb, ctx, orc, tune, cache)
+        line["scan_2e28"] = scan_numbers(gsrb, ctx, orc, tune, cache, n=args.scan_n)
+        params, pinfo = train_policy(gsrb, ctx, pol)
+        line["policy"] = pinfo
+        line["graphs"] = graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, not args.skip_pr_check)
+        line["batch"] = batch_numbers(gsrb, ctx, orc, params)
+        line["extras_wall_s"] = round(time.time() - extras_t0, 1)
         if dist.rank == 0:
             line["cpu_baseline"] = cpu_barrier_baseline(orc)
+    line["autotuned"] = cache
 
     if dist.rank == 0:
         print(json.dumps(line), flush=True)

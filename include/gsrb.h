@@ -112,7 +112,7 @@ gsrb_status_t gsrb_l2_flush(gsrb_ctx_t ctx);
 /* Number of kernels this library has launched in this process (for launch accounting). */
 uint64_t gsrb_launch_count(void);
 
-/* ---- grid barrier microbenchmark -------------------
+/* ---- grid barrier microbenchmark (148*k CTAs, episodes of F FMAs + one barrier) 
  * One persistent launch of grid = cfg->ctas_per_sm * #SMs CTAs of cfg->threads
  * threads; each CTA runs `episodes` times: `fma_per_episode` dependent FP32 FMAs
  * per thread, then one grid barrier of cfg->variant.  d_episode_count (uint32,
@@ -137,7 +137,7 @@ gsrb_status_t gsrb_barrier_fault_short_grid(gsrb_ctx_t ctx, const gsrb_cfg_t* cf
  * mode 1 = one thread issues `iters` dependent atom.add (round-trip latency). */
 gsrb_status_t gsrb_probe_l2_atomics(gsrb_ctx_t ctx, int32_t ctas, int32_t iters, int32_t mode, float* ms);
 
-/* ---- reduce ----------------------------------------
+/* ---- reduce (2^24 int32, one barrier between partials and combine) ------------
  * Sum of n int32 into *d_out (int64), one persistent launch: each CTA reduces a
  * contiguous chunk with 128-bit loads, one grid barrier, CTA 0 combines the
  * partials.  Replaces reduce_kernel/reduce() of Reduce/reduce_gsrb.cu:289-404
@@ -160,7 +160,7 @@ gsrb_status_t gsrb_reduce_i32(gsrb_ctx_t ctx, const int32_t* d_in, size_t n, int
  * respect to `stream`; returns GSRB_ERR_TIMEOUT if a bounded wait ran out. */
 gsrb_status_t gsrb_reduce_i32_noalloc(const int32_t* d_in, size_t n, int64_t* d_out, void* stream);
 
-/* ---- scan --------------------------------------------
+/* ---- scan (three-phase persistent exclusive prefix sum) ---------------------------
  * Exclusive prefix sum, one persistent launch (default one 1024-thread CTA per
  * SM, 96 KiB tiles double-buffered in shared memory, moved by cp.async.bulk),
  * one grid barrier per segment of #CTAs tiles.  uint32 wraps around like the
@@ -210,7 +210,7 @@ enum {
 /* Mutex kinds for gsrb_mutex_bench. */
 enum { GSRB_MUTEX_SPIN = 0, GSRB_MUTEX_EBO = 1, GSRB_MUTEX_FA = 2, GSRB_MUTEX_SLEEP = 3 };
 
-/* Semaphore microbenchmark (BASELINE configuration 2): grid = cfg CTAs; CTA b is a
+/* Semaphore microbenchmark: grid = cfg CTAs; CTA b is a
  * writer when b % writer_every == 0; each CTA acquires `iters` times and adds 1
  * to a shared counter `incs` times per acquire (writers: plain read-modify-write
  * of W; readers: atomic add to R).  d_counters: 8 uint32, zeroed by the caller:
@@ -224,7 +224,7 @@ gsrb_status_t gsrb_semaphore_bench(gsrb_ctx_t ctx, const gsrb_cfg_t* cfg, int32_
 gsrb_status_t gsrb_mutex_bench(gsrb_ctx_t ctx, const gsrb_cfg_t* cfg, int32_t kind, int32_t iters, int32_t incs,
                                uint32_t* d_counters);
 
-/* ---- graph traversals (BASELINE configurations 4 and 5) -------------------------
+/* ---- graph traversals (BFS / SSSP / PageRank level loops) -------------------------
  * A gsrb_graph_t is a device CSR (row_start[n+1], edge_dst[m], edge_data[m]:
  * the reference CSRGraph layout) plus the traversal scratch (queues, marks,
  * counters, per-level trace ring).  Traversals are synchronous and return
@@ -274,7 +274,7 @@ gsrb_status_t gsrb_sssp(gsrb_ctx_t ctx, gsrb_graph_t g, uint32_t src, int32_t* d
 gsrb_status_t gsrb_pagerank(gsrb_ctx_t ctx, gsrb_graph_t g, float alpha, int32_t iters, float* d_rank,
                             const gsrb_cfg_t* cfg, gsrb_traversal_stats_t* stats);
 
-/* ---- batched traversals --------------------------------
+/* ---- batched traversals (many graphs, one persistent launch) ----------------------
  * k graphs (k <= 127) traversed in ONE persistent launch: instance i owns a
  * contiguous range of CTAs (in proportion to its edges, at least one) and a
  * sub-grid barrier of its own carved from the context's barrier state, so

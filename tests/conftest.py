@@ -28,7 +28,7 @@ def _load_binding():
 
 def _ensure_built():
     lib = PKG / "lib" / "libgsrb.so"
-    if not lib.exists():
+    if not lib.exists() or not (PKG / "bin" / "bfs_gsrb").exists():
         subprocess.run(["make", "-C", str(PKG), "-j8"], check=True, capture_output=True)
     olib = ROOT / "oracle" / "lib" / "liboracle.so"
     if not olib.exists():

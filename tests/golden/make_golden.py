@@ -29,7 +29,7 @@ def scan_golden():
     rng = np.random.default_rng(2022)
     cases = {
         "ones_1000": np.ones(1000, dtype=np.uint32),                       # scan/main.cu:37-41
-        "u15_4099": rng.integers(0, 16, 4099, dtype=np.uint32),            # BASELINE int run values
+        "u15_4099": rng.integers(0, 16, 4099, dtype=np.uint32),            # the int32 scan run draws values in [0, 15]
         "wrap_777": rng.integers(2**31, 2**32, 777, dtype=np.uint64).astype(np.uint32),  # uint32 wraparound
         "single": np.array([7], dtype=np.uint32),
     }
