@@ -22,7 +22,8 @@ measured on the same device in the same run (disable with --no-extras):
                     batched + learned in one CUDA-graph launch; aggregate GTEPS
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload barrier|reduce|scan|bfs] [--k 8] [--fma 0] [--no-extras]
+                  [--workload barrier|reduce|scan|bfs|sssp|pr] [--graph rmat|grid] [--scale 22]
+                  [--k 8] [--fma 0] [--cfg JSON] [--no-extras]
 
 --impl reference times the reference's CPU implementation of the path on the
 host cores: the reference has no CPU barrier, so this is the oracle's port of
@@ -285,8 +286,7 @@ def semaphore_numbers(gsrb, ctx):
 
 
 # --------------------------------------------------------------- data kernels
-def reduce_numbers(gsrb, ctx, orc, tune, cache, reps=10, fixed=None):
-    n = 1 << 24
+def reduce_numbers(gsrb, ctx, orc, tune, cache, reps=10, fixed=None, n=1 << 24):
     a = gsrb.uniform_i32(SEED, n, 0, 127)
     d = ctx.to_device(a)
     out = ctx.array(1, np.int64).zero()
@@ -357,8 +357,9 @@ def scan_numbers(gsrb, ctx, orc, tune, cache, n=1 << 28, reps=5, fixed=None):
 # --------------------------------------------------------------------- graphs
 def train_policy(gsrb, ctx, pol):
     """Per-level traces of training graphs (not the evaluation graphs) -> MLP."""
-    graphs = [gsrb.rmat(s, 16, seed=SEED + 1000 + s) for s in (14, 16, 18, 20)]
-    graphs += [gsrb.grid2d(256, 256, seed=SEED + 7), gsrb.grid2d(1024, 64, seed=SEED + 8)]
+    graphs = [gsrb.rmat(s, 16, seed=SEED + 1000 + s) for s in (14, 16, 18, 20, 21)]
+    graphs += [gsrb.grid2d(256, 256, seed=SEED + 7), gsrb.grid2d(1024, 64, seed=SEED + 8),
+               gsrb.grid2d(1024, 1024, seed=SEED + 9), gsrb.grid2d(2048, 512, seed=SEED + 10)]
     X, Y, M = [], [], []
     for g in graphs:
         dg = ctx.graph(g)
@@ -550,13 +551,18 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="barrier", choices=["barrier", "reduce", "scan", "bfs"])
+    ap.add_argument("--workload", default="barrier", choices=["barrier", "reduce", "scan", "bfs", "sssp", "pr"])
+    ap.add_argument("--graph", default="rmat", choices=["rmat", "grid"], help="graph of the bfs/sssp/pr workloads")
+    ap.add_argument("--scale", type=int, default=22, help="log2 vertices of the bfs/sssp/pr workload graph")
+    ap.add_argument("--iters", type=int, default=50, help="PageRank iterations (pr workload)")
+    ap.add_argument("--delta", type=int, default=10000, help="SSSP bucket width (sssp workload)")
     ap.add_argument("--k", type=int, default=8)
     ap.add_argument("--fma", type=int, default=0)
     ap.add_argument("--cfg", type=json.loads, default=None,
                     help="fixed configuration as JSON (skips the autotuner), e.g. '{\"variant\": 9}'")
     ap.add_argument("--episodes", type=int, default=10_000)
     ap.add_argument("--scan-n", type=int, default=1 << 28)
+    ap.add_argument("--reduce-n", type=int, default=1 << 24)
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--skip-pr-check", action="store_true", help="skip the FP64 CPU PageRank (about 25 s)")
     args = ap.parse_args()
@@ -595,15 +601,28 @@ def main():
         # single data-kernel workloads (profiling entry points)
         orc = load_oracle()
         if args.workload == "reduce":
-            r = reduce_numbers(gsrb, ctx, orc, tune, cache, reps=args.steps, fixed=args.cfg)
+            r = reduce_numbers(gsrb, ctx, orc, tune, cache, reps=args.steps, fixed=args.cfg, n=args.reduce_n)
         elif args.workload == "scan":
             r = scan_numbers(gsrb, ctx, orc, tune, cache, n=args.scan_n, reps=args.steps, fixed=args.cfg)
         else:
-            pol = _load("gsrb_policy", PKG / "policy.py")
-            params = gsrb.mlp_init(1)
-            g = gsrb.rmat(18, 16, seed=SEED)
+            g = (gsrb.grid2d(1 << (args.scale // 2), 1 << (args.scale - args.scale // 2), seed=SEED)
+                 if args.graph == "grid" else gsrb.rmat(args.scale, 16, seed=SEED))
             dg = ctx.graph(g)
-            r = bfs_runs(gsrb, ctx, orc, dg, g, params, None, reps=args.steps)
+            c = tune.cfg_from(args.cfg) if args.cfg else None
+            if args.workload == "bfs":
+                r = bfs_runs(gsrb, ctx, orc, dg, g, gsrb.mlp_init(1), c, reps=args.steps)
+            elif args.workload == "sssp":
+                r = sssp_runs(gsrb, ctx, orc, dg, g, [("delta", args.delta)], c)
+            else:
+                out = ctx.array(g.nnodes, np.float32)
+                ts = []
+                for _ in range(args.steps):
+                    rc, st = dg.pagerank(out, 0.85, args.iters, c)
+                    gsrb.check(rc, "pagerank")
+                    ts.append(st.kernel_ms)
+                l1 = orc.normalized_l1(out.download(), orc.pagerank(g, 0.85, args.iters))
+                r = {"n": g.nnodes, "m": g.nedges, "iters": args.iters, "ms": ts, "l1_vs_fp64": l1}
+            dg.free()
         if dist.rank == 0:
             print(json.dumps({"workload": args.workload, "result": r}), flush=True)
         ctx.close()

@@ -68,7 +68,7 @@ typedef struct gsrb_cfg {
   int32_t fanin_groups;  /* global fan-in groups (0 = arrive at the root directly) */
   int32_t spin_ns;       /* __nanosleep between polls (0 = hot spin) */
   uint32_t timeout_ms;   /* per-wait device deadline */
-  int32_t tile;          /* elements per tile / segment hint (0 = auto) */
+  int32_t tile;          /* scan: elements per CTA chunk; reduce: 32 KiB stages (0 = auto) */
   int32_t grid_override; /* exact grid size (0 = ctas_per_sm * #SMs) */
   int32_t launch_mode;   /* 0 = cooperative launch when the driver accepts it, 1 = plain launch (default)
                             (both only after the co-residency check; CCG is always cooperative) */
@@ -81,6 +81,8 @@ const char* gsrb_status_string(gsrb_status_t s);
 
 /* ---- context ---------------------------------------------------------------- */
 gsrb_status_t gsrb_ctx_create(int device, gsrb_ctx_t* out);
+/* Release every graph and batch created on the context first: their free
+ * functions synchronise the context stream. */
 gsrb_status_t gsrb_ctx_destroy(gsrb_ctx_t ctx);
 /* Use an existing cudaStream_t (passed as void*); NULL = the context's own stream. */
 gsrb_status_t gsrb_ctx_set_stream(gsrb_ctx_t ctx, void* stream);
@@ -138,10 +140,12 @@ gsrb_status_t gsrb_barrier_fault_short_grid(gsrb_ctx_t ctx, const gsrb_cfg_t* cf
 gsrb_status_t gsrb_probe_l2_atomics(gsrb_ctx_t ctx, int32_t ctas, int32_t iters, int32_t mode, float* ms);
 
 /* ---- reduce (2^24 int32, one barrier between partials and combine) ------------
- * Sum of n int32 into *d_out (int64), one persistent launch: each CTA reduces a
- * contiguous chunk with 128-bit loads, one grid barrier, CTA 0 combines the
- * partials.  Replaces reduce_kernel/reduce() of Reduce/reduce_gsrb.cu:289-404
- * (API Reduce/reduce.cuh:47).  Asynchronous. */
+ * Sum of n int32 into *d_out (int64), one persistent launch: each CTA streams a
+ * contiguous chunk through a ring of 32 KiB shared-memory stages filled by
+ * cp.async.bulk (cfg->tile = stages, 0 = as many as fit, at most 6), one grid
+ * barrier, CTA 0 combines the partials in a fixed order.  cfg == NULL: one
+ * 1024-thread CTA per SM.  Replaces reduce_kernel/reduce() of
+ * Reduce/reduce_gsrb.cu:289-404 (API Reduce/reduce.cuh:47).  Asynchronous. */
 gsrb_status_t gsrb_reduce_i32(gsrb_ctx_t ctx, const int32_t* d_in, size_t n, int64_t* d_out,
                               const gsrb_cfg_t* cfg);
 
@@ -162,9 +166,11 @@ gsrb_status_t gsrb_reduce_i32_noalloc(const int32_t* d_in, size_t n, int64_t* d_
 
 /* ---- scan (three-phase persistent exclusive prefix sum) ---------------------------
  * Exclusive prefix sum, one persistent launch (default one 1024-thread CTA per
- * SM, 96 KiB tiles double-buffered in shared memory, moved by cp.async.bulk),
- * one grid barrier per segment of #CTAs tiles.  uint32 wraps around like the
- * reference's cpu_sum_scan; the FP32 variant keeps tile offsets in FP64.
+ * SM).  The input is walked in segments of one chunk per CTA (cfg->tile
+ * elements, 0 = 32768); per segment: chunk sums, one split-phase grid barrier
+ * that overlaps the next segment's reads, then the chunk is re-read from L2,
+ * scanned and written.  uint32 wraps around like the reference's
+ * cpu_sum_scan; the FP32 variant keeps chunk offsets in FP64.
  * In-place (d_in == d_out) is allowed.  Replaces gpu_prescan /
  * sum_scan_blelloch of scan/scan_gsrb.cu:486-804 (API scan/scan.h:16-18).
  * Asynchronous. */
@@ -259,6 +265,7 @@ gsrb_status_t gsrb_graph_upload(gsrb_ctx_t ctx, const gsrb_host_csr_t* h, gsrb_g
 gsrb_status_t gsrb_graph_wrap(gsrb_ctx_t ctx, uint32_t n, uint64_t m, const uint32_t* d_row,
                               const uint32_t* d_dst, const int32_t* d_w, gsrb_graph_t* out);
 gsrb_status_t gsrb_graph_free(gsrb_graph_t g);
+/* nhubs: vertices of degree > 128, whose rows PageRank splits into 2048-edge chunks. */
 gsrb_status_t gsrb_graph_info(gsrb_graph_t g, uint32_t* n, uint64_t* m, uint32_t* nhubs);
 /* Policy network weights (gsrb_mlp_* layout, gsrb_mlp_param_count() floats). */
 gsrb_status_t gsrb_graph_set_policy(gsrb_graph_t g, const float* h_weights, size_t count);

@@ -335,6 +335,8 @@ struct GridSync {
                                    V == V_CLUSTER_RED || V == V_CLUSTER_FANOUT;
   static constexpr bool kFlip = V == V_CLUSTER || V == V_CLUSTER_ALLPOLL || V == V_DSMEM || V == V_FLIP;
   static constexpr bool kFanout = V == V_FANOUT || V == V_CLUSTER_FANOUT || V == V_HIER;
+  // arrive() and wait() are split (a CTA may arrive and leave without waiting)
+  static constexpr bool kSplit = V == V_FANOUT || V == V_HIER || V == V_FLIP;
 
   // Index of this CTA among the participants and of its arrival unit.
   __device__ __forceinline__ uint32_t my_index() const { return blockIdx.x - gb.first_cta; }
@@ -383,6 +385,16 @@ struct GridSync {
   }
 
   __device__ bool sync();
+
+  // Split phase: arrive() then, after work that neither depends on this
+  // episode nor changes what other CTAs read through it, wait().  Both are
+  // whole-CTA collectives; every arrive() is followed by exactly one wait()
+  // before the next arrive() or sync().  Variants without a split form arrive
+  // and wait inside wait() (correct, no overlap).
+  __device__ __forceinline__ void arrive() { arrived_done = 0u; }
+  __device__ __forceinline__ bool wait() { return sync(); }
+
+  uint32_t arrived_done;  // thread 0: this CTA's arrival completed the episode
 };
 
 // ---------------------------------------------------------------------------
@@ -563,6 +575,39 @@ __device__ __forceinline__ bool GridSync<V_HIER>::sync() {
   return sh->ok != 0u;
 }
 
+template <>
+__device__ __forceinline__ void GridSync<V_FANOUT>::arrive() {
+  __syncthreads();
+  if (threadIdx.x == 0) arrived_done = detail::fanout_arrive(gb, gb.nparticipants, epoch) ? 1u : 0u;
+}
+template <>
+__device__ __forceinline__ bool GridSync<V_FANOUT>::wait() {
+  if (threadIdx.x == 0) {
+    const bool ok = arrived_done || detail::fanout_wait(gb, my_index(), epoch, episode);
+    sh->ok = ok ? 1u : 0u;
+    ++epoch;
+    ++episode;
+  }
+  __syncthreads();
+  return sh->ok != 0u;
+}
+template <>
+__device__ __forceinline__ void GridSync<V_HIER>::arrive() {
+  __syncthreads();
+  if (threadIdx.x == 0) arrived_done = detail::hier_arrive(gb, my_index(), gb.nparticipants, epoch) ? 1u : 0u;
+}
+template <>
+__device__ __forceinline__ bool GridSync<V_HIER>::wait() {
+  if (threadIdx.x == 0) {
+    const bool ok = arrived_done || detail::fanout_wait(gb, my_index(), epoch, episode);
+    sh->ok = ok ? 1u : 0u;
+    ++epoch;
+    ++episode;
+  }
+  __syncthreads();
+  return sh->ok != 0u;
+}
+
 // V_FLIP: two levels without clusters: __syncthreads, then every CTA's thread 0
 // arrives on the split flip words and polls them.
 template <>
@@ -570,6 +615,21 @@ __device__ __forceinline__ bool GridSync<V_FLIP>::sync() {
   __syncthreads();
   if (threadIdx.x == 0) {
     detail::flip_arrive(gb, my_index(), gb.nparticipants);
+    sh->ok = detail::flip_wait(gb, gb.nparticipants, sense, episode) ? 1u : 0u;
+    sense ^= detail::flip_all(gb, gb.nparticipants);
+    ++episode;
+  }
+  __syncthreads();
+  return sh->ok != 0u;
+}
+template <>
+__device__ __forceinline__ void GridSync<V_FLIP>::arrive() {
+  __syncthreads();
+  if (threadIdx.x == 0) detail::flip_arrive(gb, my_index(), gb.nparticipants);
+}
+template <>
+__device__ __forceinline__ bool GridSync<V_FLIP>::wait() {
+  if (threadIdx.x == 0) {
     sh->ok = detail::flip_wait(gb, gb.nparticipants, sense, episode) ? 1u : 0u;
     sense ^= detail::flip_all(gb, gb.nparticipants);
     ++episode;

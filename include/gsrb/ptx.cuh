@@ -176,6 +176,9 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* mbar, uint32_t b
   asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;"
                ::"r"(smem_u32(mbar)), "r"(bytes) : "memory");
 }
+__device__ __forceinline__ void mbar_arrive(uint64_t* mbar) {
+  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(mbar)) : "memory");
+}
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* mbar, uint32_t parity) {
   uint32_t ok;
   asm volatile(

@@ -81,11 +81,25 @@ def test_bfs_app_matches_oracle(ctx, orc, gr_files, tmp_path, variant, name):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("mode", ["push", "pull", "topo", "learned"])
-def test_bfs_app_modes(ctx, orc, gr_files, tmp_path, mode):
+def test_bfs_app_modes(gsrb, ctx, orc, gr_files, tmp_path, mode):
     path, g = gr_files["rmat12"]
     out = tmp_path / "levels.txt"
-    _run("bfs_gsrb", ["-s", "3", "-m", mode, "-o", str(out), str(path)], block_factor="1")
+    extra = []
+    if mode == "learned":
+        # any weights: the policy changes the schedule, never the levels
+        wfile = tmp_path / "policy.f32"
+        gsrb.mlp_init(7).astype(np.float32).tofile(wfile)
+        extra = ["-P", str(wfile)]
+    _run("bfs_gsrb", ["-s", "3", "-m", mode] + extra + ["-o", str(out), str(path)], block_factor="1")
     assert np.array_equal(_read_levels(out, g.nnodes), orc.bfs(g, 3))
+
+
+@pytest.mark.gpu
+def test_bfs_app_learned_needs_policy(ctx, gr_files):
+    path, _ = gr_files["rmat12"]
+    p = subprocess.run([str(BIN / "bfs_gsrb"), "-m", "learned", str(path)], input="1\n", capture_output=True,
+                       text=True, timeout=120)
+    assert p.returncode != 0 and "gsrb_bfs" in p.stderr
 
 
 @pytest.mark.gpu

@@ -30,7 +30,7 @@ def test_reduce_seeded_uniform(gsrb, ctx, orc, variant):
 
 
 def test_reduce_full_config(gsrb, ctx, orc):
-    # 2^24 int32 U[0,127], grid 148 x 2 x 256 (configuration 1)
+    # 2^24 int32 U[0,127], the library's default grid (one 1024-thread CTA per SM)
     a = gsrb.uniform_i32(0x5EED2022, 1 << 24, 0, 127)
     assert _reduce(gsrb, ctx, a) == orc.sum_i32(a)
 
@@ -55,8 +55,9 @@ def test_reduce_int64_no_overflow(gsrb, ctx, orc):
     assert _reduce(gsrb, ctx, b) == -(2**31) * (1 << 20)
 
 
-@pytest.mark.parametrize("k,threads", [(1, 1024), (4, 128), (4, 256)])
-def test_reduce_other_shapes(gsrb, ctx, orc, k, threads):
-    a = gsrb.uniform_i32(99, 777_777, 0, 127)
-    c = gsrb.cfg(ctas_per_sm=k, threads=threads, cluster=2)
+@pytest.mark.parametrize("k,threads,stages", [(1, 1024, 0), (4, 128, 0), (4, 256, 0), (1, 512, 1), (1, 1024, 7),
+                                              (2, 256, 2), (1, 64, 6)])
+def test_reduce_other_shapes(gsrb, ctx, orc, k, threads, stages):
+    a = gsrb.uniform_i32(99, 7_777_777, 0, 127)
+    c = gsrb.cfg(ctas_per_sm=k, threads=threads, cluster=2, tile=stages)
     assert _reduce(gsrb, ctx, a, c) == orc.sum_i32(a)

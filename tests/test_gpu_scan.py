@@ -40,7 +40,8 @@ def test_scan_u32_reference_golden(gsrb, ctx):
         assert np.array_equal(_scan(gsrb, ctx, z[k + "_in"]), z[k + "_out"]), k
 
 
-@pytest.mark.parametrize("n", [1, 3, 4, 5, 127, 128, 129, 4096, 24576 * 148 - 1, 24576 * 148 + 5, 10_000_019])
+@pytest.mark.parametrize("n", [1, 3, 4, 5, 127, 128, 129, 4096, 24576 * 148 - 1, 32768 * 148, 32768 * 148 + 5,
+                               2 * 32768 * 148 - 3, 10_000_019])
 def test_scan_u32_sizes(gsrb, ctx, orc, n):
     a = gsrb.uniform_i32(n, n, 0, 15).astype(np.uint32)
     assert np.array_equal(_scan(gsrb, ctx, a), orc.scan_u32(a))
@@ -64,7 +65,8 @@ def test_scan_u32_barrier_variants(gsrb, ctx, orc, variant):
     assert np.array_equal(_scan(gsrb, ctx, a, cfg=c), orc.scan_u32(a))
 
 
-@pytest.mark.parametrize("k,threads,tile", [(2, 512, 12288), (1, 256, 4096), (1, 1024, 16384)])
+@pytest.mark.parametrize("k,threads,tile", [(2, 512, 12288), (1, 256, 4096), (1, 1024, 16384), (2, 512, 65536),
+                                            (1, 1024, 4), (4, 256, 1000)])
 def test_scan_u32_shapes(gsrb, ctx, orc, k, threads, tile):
     a = gsrb.uniform_i32(k, 3_333_333, 0, 15).astype(np.uint32)
     c = gsrb.cfg(ctas_per_sm=k, threads=threads, cluster=2, tile=tile)
@@ -82,7 +84,7 @@ def test_scan_f32_tolerance(gsrb, ctx, orc, n):
 
 @pytest.mark.slow
 def test_scan_full_size_2e28(gsrb, ctx, orc):
-    # configuration 3 sizes: 2^28 elements, u32 in [0,15] bit-exact, f32 in [0,1) 1e-5 relative
+    # full size: 2^28 elements, u32 in [0,15] bit-exact, f32 in [0,1) 1e-5 relative
     n = 1 << 28
     a = gsrb.uniform_i32(0x5EED2022, n, 0, 15).astype(np.uint32)
     got = _scan(gsrb, ctx, a)

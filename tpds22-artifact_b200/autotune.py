@@ -81,14 +81,14 @@ def tune_barrier(ctx, k: int, threads: int = 256, episodes: int = 4000, reps: in
 def tune_scan(ctx, d_in, d_out, n: int, reps: int = 3):
     g = _g()
     table = []
-    for tile in (8192, 16384, 24576):
-        for threads in (512, 1024):
+    for chunk in (16384, 32768, 65536):
+        for k, threads in ((1, 1024), (2, 512), (1, 512)):
             for cand in (dict(variant=g.BAR_FANOUT, wake_lines=4), dict(variant=g.BAR_FLIP, fanin_groups=1),
-                         dict(variant=g.BAR_CCG), dict(variant=g.BAR_CLUSTER, cluster=2)):
-                c = g.cfg(ctas_per_sm=1, threads=threads, tile=tile, **cand)
+                         dict(variant=g.BAR_HIER, fanin_groups=16, wake_lines=8), dict(variant=g.BAR_CCG)):
+                c = g.cfg(ctas_per_sm=k, threads=threads, tile=chunk, **cand)
                 t = _median_ms(ctx, lambda: ctx.scan(d_in, d_out, n, c), reps)
                 if t is not None:
-                    table.append((t, dict(cand, ctas_per_sm=1, threads=threads, tile=tile)))
+                    table.append((t, dict(cand, ctas_per_sm=k, threads=threads, tile=chunk)))
     table.sort(key=lambda x: x[0])
     return table[0][1], table[0][0], table
 
@@ -97,17 +97,17 @@ def tune_reduce(ctx, d_in, n: int, reps: int = 5):
     g = _g()
     out = ctx.array(1, np.int64)
     table = []
-    for k, threads in ((1, 1024), (2, 256), (2, 512), (4, 256)):
+    for k, threads, stages in ((1, 1024, 6), (1, 1024, 4), (1, 512, 6), (2, 512, 3), (2, 256, 3)):
         for cand in (dict(variant=g.BAR_FANOUT, wake_lines=4), dict(variant=g.BAR_FLIP, fanin_groups=1),
                      dict(variant=g.BAR_CCG)):
-            c = g.cfg(ctas_per_sm=k, threads=threads, **cand)
+            c = g.cfg(ctas_per_sm=k, threads=threads, tile=stages, **cand)
 
             def run():
                 ctx.l2_flush()
                 return ctx.reduce_i32(d_in, n, out, c)
             t = _median_ms(ctx, run, reps)
             if t is not None:
-                table.append((t, dict(cand, ctas_per_sm=k, threads=threads)))
+                table.append((t, dict(cand, ctas_per_sm=k, threads=threads, tile=stages)))
     table.sort(key=lambda x: x[0])
     return table[0][1], table[0][0], table
 

@@ -465,22 +465,53 @@ struct PrArgs {
   DevCSR g;
   float alpha;
   int32_t iters;
-  float* rank;          // output x (FP32)
-  float* contrib[2];    // x / deg, double-buffered by iteration parity
-  const uint32_t* hubs; // vertices of degree > kBigDegree
-  uint32_t nhubs;
-  double* hub_part;     // [nhubs * gridDim] partial sums of hub rows
+  float* rank;            // output x (FP32)
+  float* contrib[2];      // x / deg, double-buffered by iteration parity
+  const uint32_t* hubs;   // vertices of degree > kPrHubDegree, ascending
+  const uint32_t* hub_c0; // [nhubs + 1] first chunk of each hub
+  const uint32_t* chunk_hub;  // [nchunks] hub index of each chunk
+  uint32_t nhubs, nchunks;
+  double* part;           // [nchunks] chunk sums
+  uint32_t* hub_done;     // [nhubs] finished chunks (monotonic over iterations)
+  unsigned long long* ticket;  // block tickets (monotonic over iterations)
   uint32_t* out;
 };
 
-// Gathers sum_{u in N(v)} c[u] for every non-hub vertex with a warp per 32
-// vertices (lane per vertex for low degree, warp-cooperative above), FP64
-// accumulation in a fixed order.
+// Sum of cin[dst[j]] over j in [j0, j1) by one warp: lanes stride the range,
+// 4 independent gathers in flight per lane, FP64 per lane, fixed-order
+// butterfly at the end (the same bits on every run).
+__device__ __forceinline__ double warp_gather_sum(const uint32_t* __restrict__ dst, const float* cin, uint32_t j0,
+                                                  uint32_t j1, uint32_t lane) {
+  double s = 0.0;
+  uint32_t j = j0 + lane;
+  for (; j + 96 < j1; j += 128) {
+    const uint32_t d0 = __ldg(dst + j), d1 = __ldg(dst + j + 32), d2 = __ldg(dst + j + 64), d3 = __ldg(dst + j + 96);
+    const float c0 = __ldcg(cin + d0), c1 = __ldcg(cin + d1), c2 = __ldcg(cin + d2), c3 = __ldcg(cin + d3);
+    s += (double)c0;
+    s += (double)c1;
+    s += (double)c2;
+    s += (double)c3;
+  }
+  for (; j < j1; j += 32) s += (double)__ldcg(cin + __ldg(dst + j));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return s;
+}
+
+// Pull PageRank, one grid barrier per iteration.
+//  * Hubs (degree > kPrHubDegree) are cut into chunks of kPrChunk edges; a warp
+//    sums a chunk, stores it, and bumps the hub's counter (acq_rel); the warp
+//    that finishes a hub's last chunk adds the chunk sums in chunk order and
+//    writes the hub's rank and contribution.
+//  * Every other vertex: a warp takes 32 consecutive vertices and walks their
+//    concatenated edge lists 32 edges per round (coalesced dst loads); each
+//    lane finds the owner of its edge by a binary search over the lanes'
+//    exclusive degree prefix, and a segmented shuffle scan hands each owner its
+//    segment's sum.  Per-vertex FP64 sums in a fixed order.
 template <int V>
 __global__ void __launch_bounds__(1024)
 pagerank_kernel(gsrb::GridBarrier gb, PrArgs a) {
   __shared__ gsrb::BarrierShared bsh;
-  __shared__ double s_red[32];
   gsrb::GridSync<V> bar;
   bool ok = bar.init(gb, &bsh);
   const DevCSR& g = a.g;
@@ -499,78 +530,115 @@ pagerank_kernel(gsrb::GridBarrier gb, PrArgs a) {
   for (; ok && it < a.iters; ++it) {
     const float* cin = a.contrib[it & 1];
     float* cout = a.contrib[(it + 1) & 1];
-    // hub rows: every CTA reduces its slice of every hub's edges
-    for (uint32_t k = 0; k < a.nhubs; ++k) {
+    // ---- hub chunks
+    for (uint32_t c = gw; c < a.nchunks; c += nw) {
+      const uint32_t k = __ldg(a.chunk_hub + c);
       const uint32_t u = __ldg(a.hubs + k);
-      const uint32_t b = __ldg(g.row + u), e = __ldg(g.row + u + 1);
-      const uint64_t len = e - b;
-      const uint32_t s0 = b + (uint32_t)(len * blockIdx.x / gridDim.x);
-      const uint32_t s1 = b + (uint32_t)(len * (blockIdx.x + 1) / gridDim.x);
-      double s = 0.0;
-      for (uint32_t j = s0 + threadIdx.x; j < s1; j += blockDim.x) s += (double)__ldcg(cin + __ldg(g.dst + j));
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-      if (lane == 0) s_red[threadIdx.x >> 5] = s;
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (uint32_t i = 0; i < (blockDim.x >> 5); ++i) t += s_red[i];
-        a.hub_part[(size_t)k * gridDim.x + blockIdx.x] = t;
+      const uint32_t c0 = __ldg(a.hub_c0 + k), c1 = __ldg(a.hub_c0 + k + 1);
+      const uint32_t ub = __ldg(g.row + u), ue = __ldg(g.row + u + 1);
+      const uint32_t j0 = ub + (c - c0) * kPrChunk;
+      const uint32_t j1 = min(ue, j0 + kPrChunk);
+      const double t = warp_gather_sum(g.dst, cin, j0, j1, lane);
+      uint32_t last = 0;
+      if (lane == 0) {
+        a.part[c] = t;
+        const uint32_t target = (c1 - c0) * (uint32_t)(it + 1);
+        last = gsrb::ptx::atom_add_acq_rel_gpu(a.hub_done + k, 1u) + 1u == target;
       }
-      __syncthreads();
+      last = __shfl_sync(0xffffffffu, last, 0);
+      if (last) {
+        // fixed order: lane-strided chunk sums, then the same butterfly
+        double s = 0.0;
+        for (uint32_t i = c0 + lane; i < c1; i += 32) s += __ldcg(a.part + i);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) {
+          const float x = (float)((double)base + (double)a.alpha * s);
+          a.rank[u] = x;
+          cout[u] = x / (float)(ue - ub);
+        }
+      }
     }
-    for (uint32_t vb = gw * 32u; vb < g.n; vb += nw * 32u) {
-      const uint32_t v = vb + lane;
-      uint32_t b = 0, e = 0;
+    // ---- everything else: blocks of 32 consecutive vertices, taken by warps
+    // from a ticket counter (block sizes vary by orders of magnitude)
+    const uint32_t nblocks = (g.n + 31u) >> 5;
+    const unsigned long long tbase = (unsigned long long)it * (nblocks + nw);
+    for (;;) {
+      unsigned long long t = 0;
+      if (lane == 0) t = atomicAdd(a.ticket, 1ull);
+      t = __shfl_sync(0xffffffffu, t, 0);
+      const unsigned long long blk = t - tbase;
+      if (blk >= nblocks) break;  // every warp draws exactly one ticket past the end
+      const uint32_t v = (uint32_t)blk * 32u + lane;
+      uint32_t b = 0, d = 0;
+      bool mine = false;
       if (v < g.n) {
         b = __ldg(g.row + v);
-        e = __ldg(g.row + v + 1);
+        const uint32_t dd = __ldg(g.row + v + 1) - b;
+        mine = dd <= kPrHubDegree;
+        d = mine ? dd : 0u;
       }
-      const uint32_t deg = e - b;
-      double s = 0.0;
-      if (deg <= kWarpDegree)
-        for (uint32_t j = b; j < e; ++j) s += (double)__ldcg(cin + __ldg(g.dst + j));
-      uint32_t coop = __ballot_sync(0xffffffffu, deg > kWarpDegree && deg <= kBigDegree);
-      while (coop) {
-        const int src = __ffs(coop) - 1;
-        coop &= coop - 1;
-        const uint32_t bb = __shfl_sync(0xffffffffu, b, src), ee = __shfl_sync(0xffffffffu, e, src);
-        double t = 0.0;
-        for (uint32_t j = bb + lane; j < ee; j += 32) t += (double)__ldcg(cin + __ldg(g.dst + j));
+      uint32_t inc = d;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-        if ((int)lane == src) s = t;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if ((int)lane >= o) inc += y;
       }
-      if (v < g.n && deg <= kBigDegree) {
-        const float x = (float)((double)base + (double)a.alpha * s);
+      const uint32_t excl = inc - d;
+      const uint32_t E = __shfl_sync(0xffffffffu, inc, 31);
+      double acc = 0.0;
+      // kRounds rounds of 32 edges per step: all gathers of a step in flight together
+      constexpr int kRounds = 4;
+      for (uint32_t f0 = 0; f0 < E; f0 += 32u * kRounds) {
+        uint32_t own[kRounds], nbr[kRounds];
+        double val[kRounds];
+#pragma unroll
+        for (int r = 0; r < kRounds; ++r) {
+          const uint32_t f = f0 + 32u * r + lane;
+          // owner = the last lane whose exclusive prefix is <= f
+          uint32_t lo = 0;
+#pragma unroll
+          for (uint32_t step = 16; step > 0; step >>= 1) {
+            const uint32_t x = __shfl_sync(0xffffffffu, excl, lo + step);
+            if (x <= f) lo += step;
+          }
+          own[r] = lo;
+          const uint32_t ob = __shfl_sync(0xffffffffu, b, lo), oe = __shfl_sync(0xffffffffu, excl, lo);
+          nbr[r] = f < E ? __ldg(g.dst + ob + (f - oe)) : 0u;
+        }
+#pragma unroll
+        for (int r = 0; r < kRounds; ++r) {
+          const uint32_t f = f0 + 32u * r + lane;
+          val[r] = f < E ? (double)__ldcg(cin + nbr[r]) : 0.0;
+        }
+#pragma unroll
+        for (int r = 0; r < kRounds; ++r) {
+          const uint32_t rb = f0 + 32u * r;
+          if (rb >= E) break;  // warp-uniform
+          // segmented inclusive scan keyed by owner (owners ascend with the lane)
+          double x = val[r];
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const double y = __shfl_up_sync(0xffffffffu, x, o);
+            const uint32_t ko = __shfl_up_sync(0xffffffffu, own[r], o);
+            if ((int)lane >= o && ko == own[r]) x += y;
+          }
+          // this lane's vertex: its segment in this round ends at flat index
+          // min(excl + d, rb + 32, E) - 1
+          const uint32_t seg_b = excl > rb ? excl : rb;
+          const uint32_t seg_e = min(min(excl + d, rb + 32u), E);
+          const uint32_t endl = seg_e > seg_b ? seg_e - 1u - rb : 0u;
+          const double t2 = __shfl_sync(0xffffffffu, x, endl);
+          if (seg_e > seg_b) acc += t2;
+        }
+      }
+      if (mine) {
+        const float x = (float)((double)base + (double)a.alpha * acc);
         a.rank[v] = x;
-        cout[v] = deg ? x / (float)deg : 0.f;
+        cout[v] = d ? x / (float)d : 0.f;
       }
     }
     ok = bar.sync();
-    if (!ok) break;
-    // hub rows: combine the per-CTA partials in CTA order (deterministic)
-    for (uint32_t k = blockIdx.x; k < a.nhubs; k += gridDim.x) {
-      double s = 0.0;
-      for (uint32_t i = threadIdx.x; i < gridDim.x; i += blockDim.x) s += __ldcg(a.hub_part + (size_t)k * gridDim.x + i);
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-      if (lane == 0) s_red[threadIdx.x >> 5] = s;
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (uint32_t i = 0; i < (blockDim.x >> 5); ++i) t += s_red[i];
-        const uint32_t u = __ldg(a.hubs + k);
-        const uint32_t d = __ldg(g.row + u + 1) - __ldg(g.row + u);
-        const float x = (float)((double)base + (double)a.alpha * t);
-        a.rank[u] = x;
-        cout[u] = x / (float)d;
-      }
-      __syncthreads();
-    }
-    if (a.nhubs) {
-      ok = bar.sync();
-    }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.out[0] = (uint32_t)it;
@@ -635,13 +703,17 @@ struct gsrb_graph {
   uint32_t* fmark = nullptr;
   LevelCounters* cnt = nullptr;
   unsigned long long* fcnt = nullptr;
-  uint32_t* flags = nullptr;  // [0] overflow, [4..8) out, edges at byte 64
+  uint32_t* flags = nullptr;  // [0] overflow, [4..8) out, edges at byte 64, PageRank tickets at byte 96
   LevelTrace* trace = nullptr;
   uint32_t trace_cap = 0;
   float* contrib[2] = {};
-  uint32_t* hubs = nullptr;
+  uint32_t* hubs = nullptr;       // PageRank hubs (degree > kPrHubDegree)
   uint32_t nhubs = 0;
-  double* hub_part = nullptr;
+  uint32_t* hub_c0 = nullptr;     // [nhubs + 1] first chunk of each hub
+  uint32_t* chunk_hub = nullptr;  // [nchunks] hub of each chunk
+  uint32_t nchunks = 0;
+  double* hub_part = nullptr;     // [nchunks] chunk sums
+  uint32_t* hub_done = nullptr;   // [nhubs] chunk counters
   MLPWeights* mlp = nullptr;
   bool mlp_set = false;
 };
@@ -671,21 +743,30 @@ gsrb_status_t graph_scratch(gsrb_graph* G) {
   if (!e) e = dalloc(&G->trace, G->trace_cap);
   if (!e) e = dalloc(&G->mlp, 1);
   if (!e) e = cudaMemset(G->mlp, 0, sizeof(MLPWeights));
-  // hub list for PageRank (degree > kBigDegree), built on the host from row_start
+  // PageRank hub chunks (degree > kPrHubDegree), built on the host from row_start
   if (!e) {
-    uint32_t* hrow = (uint32_t*)malloc(sizeof(uint32_t) * (n + 1));
-    if (!hrow) return GSRB_ERR_NOMEM;
-    e = cudaMemcpy(hrow, G->row, sizeof(uint32_t) * (n + 1), cudaMemcpyDeviceToHost);
-    uint32_t* hl = (uint32_t*)malloc(sizeof(uint32_t) * (n ? n : 1));
-    uint32_t nh = 0;
-    for (size_t v = 0; !e && v < n; ++v)
-      if (hrow[v + 1] - hrow[v] > kBigDegree) hl[nh++] = (uint32_t)v;
-    G->nhubs = nh;
-    if (!e) e = dalloc(&G->hubs, nh);
-    if (!e && nh) e = cudaMemcpy(G->hubs, hl, sizeof(uint32_t) * nh, cudaMemcpyHostToDevice);
-    if (!e) e = dalloc(&G->hub_part, (size_t)(nh ? nh : 1) * 148 * 32);
-    free(hrow);
-    free(hl);
+    std::vector<uint32_t> hrow(n + 1);
+    e = cudaMemcpy(hrow.data(), G->row, sizeof(uint32_t) * (n + 1), cudaMemcpyDeviceToHost);
+    std::vector<uint32_t> hl, c0, ch;
+    for (size_t v = 0; !e && v < n; ++v) {
+      const uint32_t d = hrow[v + 1] - hrow[v];
+      if (d <= kPrHubDegree) continue;
+      c0.push_back((uint32_t)ch.size());
+      for (uint32_t j = 0; j < d; j += kPrChunk) ch.push_back((uint32_t)hl.size());
+      hl.push_back((uint32_t)v);
+    }
+    c0.push_back((uint32_t)ch.size());
+    G->nhubs = (uint32_t)hl.size();
+    G->nchunks = (uint32_t)ch.size();
+    if (!e) e = dalloc(&G->hubs, hl.size());
+    if (!e) e = dalloc(&G->hub_c0, c0.size());
+    if (!e) e = dalloc(&G->chunk_hub, ch.size());
+    if (!e) e = dalloc(&G->hub_part, ch.size());
+    if (!e) e = dalloc(&G->hub_done, hl.size());
+    if (!e && !hl.empty()) e = cudaMemcpy(G->hubs, hl.data(), sizeof(uint32_t) * hl.size(), cudaMemcpyHostToDevice);
+    if (!e) e = cudaMemcpy(G->hub_c0, c0.data(), sizeof(uint32_t) * c0.size(), cudaMemcpyHostToDevice);
+    if (!e && !ch.empty())
+      e = cudaMemcpy(G->chunk_hub, ch.data(), sizeof(uint32_t) * ch.size(), cudaMemcpyHostToDevice);
   }
   if (!e) e = cudaDeviceSynchronize();
   if (e) return cuda_err(e, "graph scratch");
@@ -711,7 +792,10 @@ void graph_free(gsrb_graph* G) {
   cudaFree(G->flags);
   cudaFree(G->trace);
   cudaFree(G->hubs);
+  cudaFree(G->hub_c0);
+  cudaFree(G->chunk_hub);
   cudaFree(G->hub_part);
+  cudaFree(G->hub_done);
   cudaFree(G->mlp);
 }
 
@@ -940,11 +1024,17 @@ gsrb_status_t gsrb_pagerank(gsrb_ctx_t ctx, gsrb_graph_t G, float alpha, int32_t
   a.contrib[0] = G->contrib[0];
   a.contrib[1] = G->contrib[1];
   a.hubs = G->hubs;
+  a.hub_c0 = G->hub_c0;
+  a.chunk_hub = G->chunk_hub;
   a.nhubs = G->nhubs;
-  a.hub_part = G->hub_part;
+  a.nchunks = G->nchunks;
+  a.part = G->hub_part;
+  a.hub_done = G->hub_done;
+  a.ticket = reinterpret_cast<unsigned long long*>(G->flags + 24);
   a.out = G->flags + 4;
   std::lock_guard<std::mutex> g(ctx->mu);
   GSRB_CUDA(cudaMemsetAsync(G->flags, 0, 128, ctx->stream));
+  if (G->nhubs) GSRB_CUDA(cudaMemsetAsync(G->hub_done, 0, sizeof(uint32_t) * G->nhubs, ctx->stream));
   gsrb::GridBarrier gb = make_barrier(ctx, c, 0, (uint32_t)grid, 0, 0);
   void* args[] = {&gb, &a};
   if (!ctx->events[62]) GSRB_CUDA(cudaEventCreate(&ctx->events[62]));

@@ -18,6 +18,8 @@ namespace gsrbg {
 constexpr int32_t kInf = 0x7fffffff;        // INF = INT_MAX (apps/bfs/kernel_gsrb.cu:295)
 constexpr uint32_t kBigDegree = 4096;       // vertices above this are expanded by the whole grid
 constexpr uint32_t kWarpDegree = 32;        // above this a warp expands the vertex cooperatively
+constexpr uint32_t kPrHubDegree = 128;      // PageRank: above this a vertex's edges are cut into chunks
+constexpr uint32_t kPrChunk = 2048;         // PageRank: edges per hub chunk (one warp each)
 
 struct DevCSR {
   uint32_t n;

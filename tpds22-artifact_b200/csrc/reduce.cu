@@ -5,25 +5,26 @@
 // N is limited to the co-resident thread count, 148*2048 on B200), a
 // shared-memory tree per level and one grid barrier per level, int accumulation.
 //
-// Here: a fixed co-resident grid (default 148 SMs x 2 CTAs x 256 threads) where
-// each CTA streams a contiguous chunk with 128-bit non-allocating loads and
-// eight independent loads in flight per thread, accumulates in int64, reduces
-// with warp shuffles, publishes one partial per CTA, crosses ONE grid barrier,
-// and CTA 0 combines the partials in a fixed order (so the result is
-// deterministic and bit-exact against a serial int64 sum).
+// Here: a fixed co-resident grid (default one 1024-thread CTA per SM).  Each
+// CTA streams a contiguous chunk through a ring of 32 KiB shared-memory stages
+// filled by bulk copies (cp.async.bulk global->shared, completion counted on a
+// "full" mbarrier per stage; no multicast).  Thread 0 keeps up to `nbuf`
+// stages in flight (192 KiB per SM by default, well above the bytes in flight
+// an SM needs to stream its share of HBM bandwidth); every warp sums its part
+// of a stage in int64 and frees the stage on an "empty" mbarrier, so warps
+// never wait for each other inside the stream.  Warp shuffles reduce the CTA's sum to one partial; the CTA
+// arrives at the grid barrier (split phase: only CTA 0, which combines, waits)
+// and CTA 0 adds the partials in a fixed order, so the result is deterministic
+// and bit-exact against a serial int64 sum.
 #include "internal.h"
 
 using namespace gsrbrt;
 
 namespace {
 
-__device__ __forceinline__ int4 ld_stream_v4(const int4* p) {
-  int4 v;
-  asm volatile("ld.global.nc.L1::no_allocate.L2::256B.v4.s32 {%0,%1,%2,%3}, [%4];"
-               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-               : "l"(p));
-  return v;
-}
+constexpr uint32_t kStageBytes = 32768;
+constexpr uint32_t kMaxStages = 7;
+constexpr uint32_t kDefaultStages = 6;
 
 __device__ __forceinline__ long long warp_sum_i64(long long v) {
 #pragma unroll
@@ -45,62 +46,108 @@ __device__ __forceinline__ long long block_sum_i64(long long v, long long* warp_
   return t;
 }
 
-// Sum of in[beg, end) by one CTA (every thread returns its share).
-__device__ __forceinline__ long long chunk_sum(const int32_t* __restrict__ in, uint64_t beg, uint64_t end) {
-  long long acc = 0;
-  const int32_t* p = in + beg;
-  uint64_t len = end - beg;
-  // scalar head until 16-byte alignment
-  uint64_t head = ((16u - ((uintptr_t)p & 15u)) & 15u) >> 2;
-  if (head > len) head = len;
-  if (threadIdx.x < head) acc += p[threadIdx.x];
-  p += head;
-  len -= head;
-  const int4* v = reinterpret_cast<const int4*>(p);
-  const uint64_t nv = len >> 2;
-  const uint64_t T = blockDim.x;
-  uint64_t i = threadIdx.x;
-  for (; i + 7 * T < nv; i += 8 * T) {
-    int4 x[8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) x[u] = ld_stream_v4(v + i + u * T);
-#pragma unroll
-    for (int u = 0; u < 8; ++u)
-      acc += (long long)x[u].x + (long long)x[u].y + (long long)x[u].z + (long long)x[u].w;
+// Bounded wait on an mbarrier phase.  On expiry records a timeout and keeps
+// waiting once more (bounded) so that no copy is in flight when the CTA leaves.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* mbar, uint32_t parity, const gsrb::GridBarrier& gb) {
+  uint64_t t0 = 0;
+  bool ok = true;
+  for (uint32_t it = 0;; ++it) {
+    if (gsrb::ptx::mbar_try_wait(mbar, parity)) return ok;
+    if ((it & 63u) == 63u) {
+      const uint64_t now = gsrb::ptx::globaltimer_ns();
+      if (t0 == 0) t0 = now;
+      else if (now - t0 > gb.timeout_ns) {
+        if (!ok) return false;  // second deadline: give up
+        gsrb::detail::record_error(gb, gsrb::GSRB_DEV_TIMEOUT, 0xfffffff1u);
+        ok = false;
+        t0 = now;
+      }
+    }
   }
-  for (; i < nv; i += T) {
-    const int4 x = ld_stream_v4(v + i);
-    acc += (long long)x.x + (long long)x.y + (long long)x.z + (long long)x.w;
-  }
-  const uint64_t tail = len & 3u;
-  if (threadIdx.x < tail) acc += p[(nv << 2) + threadIdx.x];
-  return acc;
 }
 
 template <int V>
 __global__ void __launch_bounds__(1024)
 reduce_i32_kernel(gsrb::GridBarrier gb, const int32_t* __restrict__ in, uint64_t n,
-                  long long* __restrict__ partials, long long* __restrict__ out) {
+                  long long* __restrict__ partials, long long* __restrict__ out, uint32_t nbuf) {
+  extern __shared__ __align__(128) unsigned char stage[];
   __shared__ gsrb::BarrierShared bsh;
   __shared__ long long warp_buf[32];
+  __shared__ uint64_t full[kMaxStages], empty[kMaxStages];
   gsrb::GridSync<V> bar;
   const bool ok0 = bar.init(gb, &bsh);
+  const uint32_t tid = threadIdx.x, T = blockDim.x, lane = tid & 31u, nwarps = T >> 5;
   const uint64_t G = gridDim.x;
   uint64_t chunk = (n + G - 1) / G;
-  chunk = (chunk + 3) & ~3ull;  // keeps every chunk start 16-byte aligned
+  chunk = (chunk + 3) & ~3ull;
   const uint64_t beg = min(n, (uint64_t)blockIdx.x * chunk);
   const uint64_t end = min(n, beg + chunk);
-  long long acc = ok0 ? chunk_sum(in, beg, end) : 0;
+  const int32_t* p = in + beg;
+  uint64_t len = end - beg;
+  long long acc = 0;
+  // scalar head up to 16-byte alignment, scalar tail past the last 16 bytes
+  uint64_t head = ((16u - ((uintptr_t)p & 15u)) & 15u) >> 2;
+  if (head > len) head = len;
+  if (tid < head) acc += p[tid];
+  p += head;
+  len -= head;
+  const uint64_t nbytes = (len * 4u) & ~15ull;
+  const uint64_t tail = len - (nbytes >> 2);
+  if (tid < tail) acc += p[(nbytes >> 2) + tid];
+  const uint32_t nst = (uint32_t)((nbytes + kStageBytes - 1) / kStageBytes);
+  const unsigned char* src = reinterpret_cast<const unsigned char*>(p);
+
+  if (tid == 0) {
+    for (uint32_t i = 0; i < nbuf; ++i) {
+      gsrb::ptx::mbar_init(&full[i], 1);
+      gsrb::ptx::mbar_init(&empty[i], nwarps);
+    }
+    gsrb::ptx::fence_mbar_init();
+  }
+  __syncthreads();
+  auto bytes_of = [&](uint32_t k) {
+    return (uint32_t)min((uint64_t)kStageBytes, nbytes - (uint64_t)k * kStageBytes);
+  };
+  auto issue = [&](uint32_t k) {
+    const uint32_t buf = k % nbuf;
+    gsrb::ptx::mbar_arrive_expect_tx(&full[buf], bytes_of(k));
+    gsrb::ptx::bulk_g2s(stage + (size_t)buf * kStageBytes, src + (size_t)k * kStageBytes, bytes_of(k), &full[buf]);
+  };
+  if (tid == 0 && ok0)
+    for (uint32_t k = 0; k < nst && k < nbuf; ++k) issue(k);
+  bool ok = ok0;
+  if (ok0) {
+    // No CTA-wide barrier per stage: each warp frees a stage on `empty` when
+    // it has read its part; thread 0 refills a stage once every warp has.
+    for (uint32_t k = 0; k < nst; ++k) {
+      const uint32_t buf = k % nbuf, ph = (k / nbuf) & 1u;
+      ok = mbar_wait_bounded(&full[buf], ph, gb) && ok;
+      const int4* v = reinterpret_cast<const int4*>(stage + (size_t)buf * kStageBytes);
+      const uint32_t nv = bytes_of(k) >> 4;
+      for (uint32_t i = tid; i < nv; i += T) {
+        const int4 x = v[i];
+        acc += (long long)x.x + (long long)x.y + (long long)x.z + (long long)x.w;
+      }
+      __syncwarp();
+      if (lane == 0) gsrb::ptx::mbar_arrive(&empty[buf]);
+      if (tid == 0 && k + nbuf < nst) {
+        ok = mbar_wait_bounded(&empty[buf], ph, gb) && ok;
+        issue(k + nbuf);
+      }
+    }
+  }
   const long long bsum = block_sum_i64(acc, warp_buf);
-  if (threadIdx.x == 0) partials[blockIdx.x] = bsum;
-  const bool ok = bar.sync() && ok0;
-  if (ok && blockIdx.x == 0) {
+  if (tid == 0) partials[blockIdx.x] = bsum;
+  bar.arrive();
+  bool done = true;
+  if (!gsrb::GridSync<V>::kSplit || blockIdx.x == 0) done = bar.wait();
+  if (done && ok && blockIdx.x == 0) {
     // fixed-order combine of the G partials (deterministic)
     long long s = 0;
-    for (uint64_t j = threadIdx.x; j < G; j += blockDim.x) s += partials[j];
+    for (uint64_t j = tid; j < G; j += T) s += __ldcg(partials + j);
     __syncthreads();
     s = block_sum_i64(s, warp_buf);
-    if (threadIdx.x == 0) *out = s;
+    if (tid == 0) *out = s;
   }
   bar.finish();
 }
@@ -125,11 +172,30 @@ const void* reduce_fn(int variant) {
 
 const void* gsrb_reduce_kernel_for(int variant) { return reduce_fn(variant); }
 
+// Dynamic shared memory of a reduce launch: cfg->tile stages of 32 KiB; 0 =
+// as many as fit 200 KiB per SM over cfg->ctas_per_sm CTAs (at most 6, at least 1).
+size_t gsrb_reduce_smem_for(const gsrb_cfg_t& c) {
+  uint32_t nb = (uint32_t)c.tile;
+  if (c.tile <= 0) {
+    const uint32_t k = c.ctas_per_sm > 0 ? (uint32_t)c.ctas_per_sm : 1u;
+    nb = (200u * 1024u / k) / kStageBytes;
+    if (nb > kDefaultStages) nb = kDefaultStages;
+  }
+  if (nb < 1) nb = 1;
+  if (nb > kMaxStages) nb = kMaxStages;
+  return (size_t)nb * kStageBytes;
+}
+
 extern "C" gsrb_status_t gsrb_reduce_i32(gsrb_ctx_t ctx, const int32_t* d_in, size_t n, int64_t* d_out,
                                          const gsrb_cfg_t* cfgin) {
   if (!ctx || !d_out || (n && !d_in)) return GSRB_ERR_ARG;
   std::lock_guard<std::mutex> g(ctx->mu);
   gsrb_cfg_t c = resolve_cfg(ctx, cfgin);
+  if (!cfgin) {
+    // default shape: one 1024-thread CTA per SM, 8 stages (128 KiB) in flight
+    c.ctas_per_sm = 1;
+    c.threads = 1024;
+  }
   if (c.threads % 32 || c.threads > 1024) return GSRB_ERR_ARG;
   const void* fn = reduce_fn(c.variant);
   if (!fn) return GSRB_ERR_UNSUPPORTED;
@@ -142,6 +208,8 @@ extern "C" gsrb_status_t gsrb_reduce_i32(gsrb_ctx_t ctx, const int32_t* d_in, si
   uint64_t n64 = n;
   long long* partials = (long long*)part;
   long long* out = (long long*)d_out;
-  void* args[] = {&gb, &d_in, &n64, &partials, &out};
-  return launch_persistent(ctx, fn, grid, c.threads, 0, c.cluster, coop_of(c), args);
+  const size_t smem = gsrb_reduce_smem_for(c);
+  uint32_t nbuf = (uint32_t)(smem / kStageBytes);
+  void* args[] = {&gb, &d_in, &n64, &partials, &out, &nbuf};
+  return launch_persistent(ctx, fn, grid, c.threads, smem, c.cluster, coop_of(c), args);
 }

@@ -7,23 +7,28 @@
 // :440-482, :798-799), grid = ceil(N / 64) CTAs that must all be co-resident
 // (N <= 148*32*64 on B200).
 //
-// Here: a fixed co-resident grid (default one 1024-thread CTA per SM).  The
-// input is cut into segments of G tiles (one tile per CTA).  Per segment a CTA
-//   1. has its tile in shared memory (moved by cp.async.bulk, prefetched one
-//      segment ahead into a second buffer, so HBM keeps streaming while the CTA
-//      waits at the barrier),
-//   2. reduces it (warp shuffles) and publishes one partial,
-//   3. crosses ONE grid barrier,
-//   4. reads the G partials of the segment: its offset is the running carry
-//      plus the partials of the CTAs before it (every CTA computes the same
-//      carry, so the reference's separate "scan of block sums" pass and its
-//      second barrier are not needed),
-//   5. rescans the tile in place from shared memory and writes it back with a
-//      bulk store.
-// Every element is read from HBM once and written once (8N bytes).  Partials
-// are double-buffered by segment parity: a CTA can only write the buffer of
-// segment s+2 after the barrier of s+1, which every CTA reaches only after it
-// has read the partials of segment s.
+// Here: a fixed co-resident grid (default one 1024-thread CTA per SM) walks the
+// input in segments of G chunks (one chunk of `chunk` elements per CTA).  The
+// three phases of the reference run per segment, software-pipelined so that
+// the grid barrier of segment s overlaps the HBM reads of segment s + 1:
+//
+//   R(s+1)  every warp sums its slice of the CTA's chunk of segment s+1
+//           (128-bit L2-only loads, 8 per lane in flight); warp totals go to
+//           shared memory (double-buffered by segment parity)
+//   wait(s) the split-phase grid barrier of segment s completes
+//   W(s)    offset = running carry + the partials of the CTAs before this one
+//           (every CTA reads the G partials of the segment, so the reference's
+//           separate scan of block sums and its second barrier are not
+//           needed); each warp re-reads its slice (an L2 hit: the segment was
+//           read one step earlier and is a few tens of MB), scans it with warp
+//           shuffles and writes it with streaming stores
+//   arrive(s+1) after publishing the CTA's partial of segment s+1
+//
+// HBM sees each element read once and written once (8N bytes); the re-read is
+// served by the 126 MB L2.  Partials are double-buffered by segment parity: a
+// CTA publishes the partial of s+1 only after it has read those of s, and the
+// buffer of s+2 is written only after every CTA's arrival at s+1, i.e. after
+// every CTA has finished reading the partials of s.
 #include "internal.h"
 
 using namespace gsrbrt;
@@ -36,11 +41,13 @@ template <>
 struct ScanT<false> {
   using Elem = uint32_t;
   using Acc = uint32_t;  // uint32 wraparound, like cpu_sum_scan (scan/main.cu:15-20)
+  using Vec = uint4;
 };
 template <>
 struct ScanT<true> {
   using Elem = float;
-  using Acc = double;    // tile offsets and carries in FP64
+  using Acc = double;    // chunk offsets and carries in FP64
+  using Vec = float4;
 };
 
 __device__ __forceinline__ uint32_t shfl_up(uint32_t v, int o) { return __shfl_up_sync(0xffffffffu, v, o); }
@@ -66,21 +73,30 @@ __device__ __forceinline__ Acc warp_sum(Acc v) {
 __device__ __forceinline__ uint32_t vsum(uint4 v) { return v.x + v.y + v.z + v.w; }
 __device__ __forceinline__ double vsum(float4 v) { return (double)((v.x + v.y) + (v.z + v.w)); }
 
-constexpr uint32_t kChunk = 16384;  // bytes per bulk copy instruction
+// 128-bit loads / stores with cache hints: first read L2-only (the line stays
+// in L2 for the re-read), re-read evict-first, output streaming.
+__device__ __forceinline__ uint4 ld_cg(const uint4* p) { return __ldcg(p); }
+__device__ __forceinline__ float4 ld_cg(const float4* p) { return __ldcg(p); }
+__device__ __forceinline__ uint4 ld_cs(const uint4* p) { return __ldcs(p); }
+__device__ __forceinline__ float4 ld_cs(const float4* p) { return __ldcs(p); }
+__device__ __forceinline__ void st_cs(uint4* p, uint4 v) { __stcs(p, v); }
+__device__ __forceinline__ void st_cs(float4* p, float4 v) { __stcs(p, v); }
 
 struct TileGeom {
-  uint64_t beg;   // first element of this CTA's tile
+  uint64_t beg;   // first element of this CTA's chunk
   uint32_t cnt;   // valid elements
-  uint32_t span;  // tile stride of the segment (multiple of 4)
+  uint32_t span;  // chunk stride of the segment (multiple of 4)
 };
 
-__device__ __forceinline__ TileGeom tile_of(uint64_t s, uint64_t n, uint32_t G, uint32_t tile, uint32_t b) {
-  const uint64_t seg = (uint64_t)G * tile;
+// Full segments use chunks of `chunk` elements; the last segment is split
+// evenly (span rounded up to a multiple of 4, trailing CTAs may get less).
+__device__ __forceinline__ TileGeom tile_of(uint64_t s, uint64_t n, uint32_t G, uint32_t chunk, uint32_t b) {
+  const uint64_t seg = (uint64_t)G * chunk;
   const uint64_t base = s * seg;
   const uint64_t rem = n - base;
   TileGeom t;
   if (rem >= seg) {
-    t.span = tile;
+    t.span = chunk;
   } else {
     uint64_t q = (rem + G - 1) / G;
     t.span = (uint32_t)((q + 3) & ~3ull);
@@ -91,128 +107,149 @@ __device__ __forceinline__ TileGeom tile_of(uint64_t s, uint64_t n, uint32_t G, 
   return t;
 }
 
-// Bounded wait on an mbarrier phase.  On expiry records a timeout and keeps
-// waiting (bounded once more) so that no copy is in flight when the CTA leaves.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* mbar, uint32_t parity, const gsrb::GridBarrier& gb) {
-  uint64_t t0 = 0;
-  bool ok = true;
-  for (uint32_t it = 0;; ++it) {
-    if (gsrb::ptx::mbar_try_wait(mbar, parity)) return ok;
-    if ((it & 63u) == 63u) {
-      const uint64_t now = gsrb::ptx::globaltimer_ns();
-      if (t0 == 0) t0 = now;
-      else if (now - t0 > gb.timeout_ns) {
-        if (!ok) return false;  // second deadline: give up
-        gsrb::detail::record_error(gb, gsrb::GSRB_DEV_TIMEOUT, 0xfffffff0u);
-        ok = false;
-        t0 = now;
-      }
-    }
+// Vector v (elements 4v..4v+3) of a chunk; elements past cnt read as zero.
+template <bool F32, bool CS>
+__device__ __forceinline__ typename ScanT<F32>::Vec load_vec(const typename ScanT<F32>::Elem* __restrict__ in,
+                                                             const TileGeom& t, uint32_t v, bool vec_ok) {
+  using Elem = typename ScanT<F32>::Elem;
+  using Vec = typename ScanT<F32>::Vec;
+  Vec x;
+  const uint32_t e = 4u * v;
+  if (vec_ok && e + 3u < t.cnt) {
+    const Vec* p = reinterpret_cast<const Vec*>(in + t.beg + e);
+    x = CS ? ld_cs(p) : ld_cg(p);
+  } else {
+    Elem y[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) y[k] = (e + k < t.cnt) ? in[t.beg + e + k] : Elem(0);
+    x.x = y[0];
+    x.y = y[1];
+    x.z = y[2];
+    x.w = y[3];
   }
+  return x;
 }
 
 template <int V, bool F32>
 __global__ void __launch_bounds__(1024, 1)
 scan_kernel(gsrb::GridBarrier gb, const typename ScanT<F32>::Elem* __restrict__ in,
-            typename ScanT<F32>::Elem* __restrict__ out, uint64_t n, uint32_t tile,
-            unsigned long long* __restrict__ partials, int in_bulk, int out_bulk) {
+            typename ScanT<F32>::Elem* __restrict__ out, uint64_t n, uint32_t chunk,
+            unsigned long long* __restrict__ partials, int vec_in, int vec_out) {
   using Elem = typename ScanT<F32>::Elem;
   using Acc = typename ScanT<F32>::Acc;
-  using Vec = typename std::conditional<F32, float4, uint4>::type;
-  extern __shared__ __align__(128) unsigned char smem[];
+  using Vec = typename ScanT<F32>::Vec;
+  constexpr uint32_t kInFlight = 8;  // 128-bit loads per lane in flight in the reduce phase
   __shared__ gsrb::BarrierShared bsh;
-  __shared__ uint64_t mbar[2];
-  __shared__ Acc s_warp[32];
+  __shared__ Acc s_wsum[2][32];  // warp totals -> exclusive warp offsets, by segment parity
   __shared__ Acc s_red[2][32];
   __shared__ Acc s_bcast[2];
 
-  Elem* buf[2] = {reinterpret_cast<Elem*>(smem), reinterpret_cast<Elem*>(smem + (size_t)tile * sizeof(Elem))};
   const uint32_t tid = threadIdx.x, lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
   const uint32_t G = gridDim.x, b = blockIdx.x;
-
   gsrb::GridSync<V> bar;
   bool ok = bar.init(gb, &bsh);
-  if (tid == 0) {
-    gsrb::ptx::mbar_init(&mbar[0], 1);
-    gsrb::ptx::mbar_init(&mbar[1], 1);
-    gsrb::ptx::fence_mbar_init();
-  }
-  __syncthreads();
 
-  const uint64_t seg = (uint64_t)G * tile;
+  const uint64_t seg = (uint64_t)G * chunk;
   const uint64_t nseg = (n + seg - 1) / seg;
-  uint32_t phase[2] = {0u, 0u};
-  bool pending[2] = {false, false};
 
-  // thread 0: start the bulk load of segment s into buffer `which`
-  auto issue = [&](uint64_t s, int which) {
-    const TileGeom t = tile_of(s, n, G, tile, b);
-    uint32_t bytes = in_bulk ? ((t.cnt * (uint32_t)sizeof(Elem)) & ~15u) : 0u;
-    gsrb::ptx::mbar_arrive_expect_tx(&mbar[which], bytes);
-    const unsigned char* src = reinterpret_cast<const unsigned char*>(in + t.beg);
-    unsigned char* dst = reinterpret_cast<unsigned char*>(buf[which]);
-    for (uint32_t off = 0; off < bytes; off += kChunk) {
-      const uint32_t sz = min(kChunk, bytes - off);
-      gsrb::ptx::bulk_g2s(dst + off, src + off, sz, &mbar[which]);
-    }
-  };
-
-  if (ok && nseg > 0 && tid == 0) issue(0, 0);
-  pending[0] = ok && nseg > 0;
-  Acc carry = Acc(0);
-
-  for (uint64_t s = 0; ok && s < nseg; ++s) {
-    const int which = (int)(s & 1);
-    const TileGeom t = tile_of(s, n, G, tile, b);
-    Elem* cur = buf[which];
-    // A copy that never lands is recorded in the status word by the wait; the
-    // loop is left only on the barrier's verdict, which is the same for every
-    // CTA of a cluster (hardware cluster barriers need matching arrivals).
-    mbar_wait_bounded(&mbar[which], phase[which], gb);
-    phase[which] ^= 1u;
-    pending[which] = false;
-    // elements the bulk copy did not cover: the ragged end (and everything when
-    // the input is not 16-byte aligned), then zeros up to the tile span
-    const uint32_t done = in_bulk ? (((t.cnt * (uint32_t)sizeof(Elem)) & ~15u) / (uint32_t)sizeof(Elem)) : 0u;
-    for (uint32_t i = done + tid; i < t.cnt; i += blockDim.x) cur[i] = in[t.beg + i];
-    for (uint32_t i = t.cnt + tid; i < t.span; i += blockDim.x) cur[i] = Elem(0);
-    __syncthreads();
-
-    // prefetch the next segment into the other buffer once its last store has
-    // finished reading it
-    if (s + 1 < nseg) {
-      if (tid == 0) {
-        gsrb::ptx::bulk_wait_read_all();
-        issue(s + 1, which ^ 1);
-      }
-      pending[which ^ 1] = true;
-    }
-
-    // ---- phase 1: per-warp totals, block total -> partial
+  // R(s): warp totals of this CTA's chunk of segment s into s_wsum[s & 1]
+  auto reduce_phase = [&](uint64_t s) {
+    const TileGeom t = tile_of(s, n, G, chunk, b);
     const uint32_t nvec = t.span >> 2;
     const uint32_t vpw = (nvec + nw - 1) / nw;
     const uint32_t v0 = w * vpw, v1 = min(nvec, v0 + vpw);
-    const Vec* cv = reinterpret_cast<const Vec*>(cur);
     Acc lsum = Acc(0);
-    for (uint32_t v = v0 + lane; v < v1; v += 32) lsum += vsum(cv[v]);
+    for (uint32_t v = v0 + lane; v < v1; v += 32u * kInFlight) {
+      Vec x[kInFlight];
+#pragma unroll
+      for (uint32_t k = 0; k < kInFlight; ++k) {
+        const uint32_t vk = v + 32u * k;
+        if (vk < v1) x[k] = load_vec<F32, false>(in, t, vk, vec_in != 0);
+        else memset(&x[k], 0, sizeof(Vec));
+      }
+#pragma unroll
+      for (uint32_t k = 0; k < kInFlight; ++k) lsum += vsum(x[k]);
+    }
     const Acc wt = warp_sum(lsum);
-    if (lane == 0) s_warp[w] = wt;
-    __syncthreads();
+    if (lane == 0) s_wsum[s & 1][w] = wt;
+  };
+  // after a __syncthreads: exclusive warp offsets, and the CTA's partial
+  auto publish = [&](uint64_t s) {
     if (tid == 0) {
       Acc run = Acc(0);
       for (uint32_t i = 0; i < nw; ++i) {
-        const Acc x = s_warp[i];
-        s_warp[i] = run;  // exclusive warp offsets within the tile
+        const Acc x = s_wsum[s & 1][i];
+        s_wsum[s & 1][i] = run;
         run += x;
       }
       __stcg(&partials[(s & 1) * G + b], (unsigned long long)acc_bits(run));
     }
+  };
+  // W(s): re-read, scan and write this CTA's chunk of segment s
+  auto write_phase = [&](uint64_t s, Acc base) {
+    const TileGeom t = tile_of(s, n, G, chunk, b);
+    const uint32_t nvec = t.span >> 2;
+    const uint32_t vpw = (nvec + nw - 1) / nw;
+    const uint32_t v0 = w * vpw, v1 = min(nvec, v0 + vpw);
+    Acc run = base + s_wsum[s & 1][w];
+    for (uint32_t r0 = v0; r0 < v1; r0 += 32u * kInFlight) {
+      // all re-reads of this step in flight together (L2 hits), then the rounds
+      Vec xs[kInFlight];
+#pragma unroll
+      for (uint32_t k = 0; k < kInFlight; ++k) {
+        const uint32_t v = r0 + 32u * k + lane;
+        if (v < v1) xs[k] = load_vec<F32, true>(in, t, v, vec_in != 0);
+        else memset(&xs[k], 0, sizeof(Vec));
+      }
+#pragma unroll
+      for (uint32_t k = 0; k < kInFlight; ++k) {
+        if (r0 + 32u * k >= v1) break;  // warp-uniform
+        const uint32_t v = r0 + 32u * k + lane;
+        const Vec x = xs[k];
+        // lane-local inclusive prefix of 4 elements
+        const Elem a0 = x.x, a1 = a0 + x.y, a2 = a1 + x.z, a3 = a2 + x.w;
+        const Acc lt = Acc(a3);
+        Acc incl = lt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const Acc y = shfl_up(incl, o);
+          if ((int)lane >= o) incl += y;
+        }
+        const Acc e0 = run + (incl - lt);
+        Vec y;
+        y.x = Elem(e0);
+        y.y = Elem(e0 + Acc(a0));
+        y.z = Elem(e0 + Acc(a1));
+        y.w = Elem(e0 + Acc(a2));
+        const uint32_t e = 4u * v;
+        if (v < v1) {
+          if (vec_out && e + 3u < t.cnt) {
+            st_cs(reinterpret_cast<Vec*>(out + t.beg + e), y);
+          } else {
+            const Elem ys[4] = {y.x, y.y, y.z, y.w};
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              if (e + q < t.cnt) out[t.beg + e + q] = ys[q];
+          }
+        }
+        run += shfl_idx(incl, 31);
+      }
+    }
+  };
 
-    // ---- the grid barrier of this segment
-    ok = bar.sync();
+  if (ok && nseg > 0) {
+    reduce_phase(0);
+    __syncthreads();
+    publish(0);
+    bar.arrive();
+  }
+  Acc carry = Acc(0);
+  for (uint64_t s = 0; ok && s < nseg; ++s) {
+    if (s + 1 < nseg) reduce_phase(s + 1);  // overlaps the barrier of segment s
+    ok = bar.wait();
     if (!ok) break;
 
-    // ---- phase 2: offset = carry + sum of the partials of the CTAs before b
+    // offset = carry + sum of the partials of the CTAs before b
     Acc pre = Acc(0), tot = Acc(0);
     for (uint32_t j = tid; j < G; j += blockDim.x) {
       Acc x;
@@ -239,59 +276,14 @@ scan_kernel(gsrb::GridBarrier gb, const typename ScanT<F32>::Elem* __restrict__ 
     __syncthreads();
     const Acc base = carry + s_bcast[0];
     carry += s_bcast[1];
+    write_phase(s, base);
 
-    // ---- phase 3: rescan the tile in place (exclusive)
-    Acc run = base + s_warp[w];
-    Vec* wv = reinterpret_cast<Vec*>(cur);
-    for (uint32_t r0 = v0; r0 < v1; r0 += 32) {
-      const uint32_t v = r0 + lane;
-      const bool valid = v < v1;
-      Vec x;
-      if (valid) x = wv[v];
-      else memset(&x, 0, sizeof(x));
-      // lane-local inclusive prefix of 4 elements
-      const Elem a0 = x.x, a1 = a0 + x.y, a2 = a1 + x.z, a3 = a2 + x.w;
-      const Acc lt = Acc(a3);
-      Acc incl = lt;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const Acc y = shfl_up(incl, o);
-        if ((int)lane >= o) incl += y;
-      }
-      const Acc e0 = run + (incl - lt);
-      if (valid) {
-        Vec y;
-        y.x = Elem(e0);
-        y.y = Elem(e0 + Acc(a0));
-        y.z = Elem(e0 + Acc(a1));
-        y.w = Elem(e0 + Acc(a2));
-        wv[v] = y;
-      }
-      run += shfl_idx(incl, 31);
+    if (s + 1 < nseg) {
+      __syncthreads();  // warp totals of s+1 are in shared memory; s_red/s_bcast reads are done
+      publish(s + 1);
+      bar.arrive();
     }
-    gsrb::ptx::fence_proxy_async_smem();
-    __syncthreads();
-
-    // ---- write back
-    const uint32_t sdone = out_bulk ? (((t.cnt * (uint32_t)sizeof(Elem)) & ~15u) / (uint32_t)sizeof(Elem)) : 0u;
-    if (tid == 0 && sdone) {
-      unsigned char* dst = reinterpret_cast<unsigned char*>(out + t.beg);
-      const unsigned char* src = reinterpret_cast<const unsigned char*>(cur);
-      const uint32_t bytes = sdone * (uint32_t)sizeof(Elem);
-      for (uint32_t off = 0; off < bytes; off += kChunk) gsrb::ptx::bulk_s2g(dst + off, src + off, min(kChunk, bytes - off));
-      gsrb::ptx::bulk_commit();
-    }
-    for (uint32_t i = sdone + tid; i < t.cnt; i += blockDim.x) out[t.beg + i] = cur[i];
-    // the generic stores above must finish reading `cur` before it is refilled
-    __syncthreads();
   }
-
-  // leave nothing in flight: a prefetch that was issued but not consumed, and
-  // every bulk store
-  for (int k = 0; k < 2; ++k)
-    if (pending[k]) mbar_wait_bounded(&mbar[k], phase[k], gb);
-  if (tid == 0) gsrb::ptx::bulk_wait_all();
-  __syncthreads();
   bar.finish();
 }
 
@@ -312,7 +304,7 @@ const void* scan_fn_t(int variant) {
   }
 }
 
-constexpr uint32_t kDefaultTile = 24576;  // elements per CTA tile (96 KiB), two buffers per CTA
+constexpr uint32_t kDefaultChunk = 32768;  // elements per CTA per segment (128 KiB; a segment of 148 is 19 MiB)
 
 gsrb_status_t scan_launch(gsrb_ctx_t ctx, const void* d_in, void* d_out, size_t n, const gsrb_cfg_t* cfgin,
                           bool f32) {
@@ -328,10 +320,9 @@ gsrb_status_t scan_launch(gsrb_ctx_t ctx, const void* d_in, void* d_out, size_t 
   }
   if (c.threads % 128 || c.threads > 1024) return GSRB_ERR_ARG;
   if (n == 0) return GSRB_OK;
-  uint32_t tile = c.tile > 0 ? (uint32_t)c.tile : kDefaultTile;
+  uint32_t tile = c.tile > 0 ? (uint32_t)c.tile : kDefaultChunk;
   tile = (tile + 3) & ~3u;
-  const size_t smem = 2 * (size_t)tile * 4;
-  if ((int)smem > ctx->max_smem_optin - 2048) return GSRB_ERR_ARG;
+  const size_t smem = 0;
   const void* fn = f32 ? scan_fn_t<true>(c.variant) : scan_fn_t<false>(c.variant);
   if (!fn) return GSRB_ERR_UNSUPPORTED;
   const int grid = grid_of(ctx, c);

@@ -13,6 +13,7 @@ The Python names mirror the reference entry points where one exists:
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 import os
 import pathlib
 
@@ -309,9 +310,16 @@ class Context:
         self.num_sms = n.value
         self.l2_bytes = l2.value
         self.device = d.value
+        # graphs and batches refer to the context's stream: they are released
+        # before the context (gsrb_graph_free / gsrb_batch_free need it alive)
+        self._owned = weakref.WeakSet()
 
     def close(self):
         if self.h:
+            for obj in [o for o in self._owned if isinstance(o, Batch)]:
+                obj.free()
+            for obj in list(self._owned):
+                obj.free()
             _lib().gsrb_ctx_destroy(self.h)
             self.h = None
 
@@ -410,6 +418,7 @@ class DeviceGraph:
         p = C.c_void_p()
         check(_lib().gsrb_graph_upload(ctx.h, C.byref(h), C.byref(p)), "graph_upload")
         self.h = p.value
+        ctx._owned.add(self)
         self.n = g.nnodes
         self.m = g.nedges
 
@@ -470,6 +479,7 @@ class Batch:
         check(_lib().gsrb_batch_create(ctx.h, hs, len(self.graphs), C.byref(c) if c is not None else None,
                                        C.byref(p)), "batch_create")
         self.h = p.value
+        ctx._owned.add(self)
         self.k = len(self.graphs)
 
     def free(self):

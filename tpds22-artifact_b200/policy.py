@@ -10,6 +10,8 @@ direction).  Those times label each level:
 
     head 0: pull faster than worklist push     (BCE)
     head 1: topology push faster than worklist push (BCE)
+    (both weighted by |log2 of the time ratio|: the loss follows the cost of a
+    wrong choice, not the count of levels)
     head 2: log2(1 + size of the next frontier) (squared error)
 
 Features are computed by gsrb_level_features, the host twin of the function the
@@ -38,6 +40,14 @@ def level_times(trace: np.ndarray, total_ms: float | None = None) -> np.ndarray:
     if len(t) > 1:
         d[:-1] = np.diff(t)
     return d
+
+
+def _weight(t_a: float, t_b: float) -> float:
+    """Cost-sensitive sample weight: |log2(t_a / t_b)| clipped to [0.05, 4].
+    A level where the two directions take about the same time hardly matters;
+    one where the wrong choice costs 10x dominates the loss."""
+    r = abs(np.log2(max(t_a, 1.0) / max(t_b, 1.0)))
+    return float(min(4.0, max(0.05, r)))
 
 
 def collect(ctx, dgraph, src: int = 0, reps: int = 1):
@@ -70,10 +80,10 @@ def collect(ctx, dgraph, src: int = 0, reps: int = 1):
         prev_nf = int(r["nf"])
         if np.isfinite(t_push[i]) and np.isfinite(t_pull[i]) and i > 0:
             Y[i, 0] = 1.0 if t_pull[i] < t_push[i] else 0.0
-            M[i, 0] = 1.0
+            M[i, 0] = _weight(t_push[i], t_pull[i])
         if np.isfinite(t_push[i]) and np.isfinite(t_topo[i]):
             Y[i, 1] = 1.0 if t_topo[i] < t_push[i] else 0.0
-            M[i, 1] = 1.0
+            M[i, 1] = _weight(t_push[i], t_topo[i])
         nxt = int(tr[i + 1]["nf"]) if i + 1 < L else 0
         Y[i, 2] = np.log2(1.0 + nxt)
         M[i, 2] = 1.0
