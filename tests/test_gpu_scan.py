@@ -73,6 +73,19 @@ def test_scan_u32_shapes(gsrb, ctx, orc, k, threads, tile):
     assert np.array_equal(_scan(gsrb, ctx, a, cfg=c), orc.scan_u32(a))
 
 
+@pytest.mark.parametrize("k,threads,tile,variant", [(1, 1024, 32768, 9), (2, 512, 16384, 9), (1, 128, 4096, 9),
+                                                    (4, 256, 1000, 9), (1, 1024, 65536, 11), (2, 512, 8, 11)])
+@pytest.mark.parametrize("n", [1, 4097, 3_333_333])
+def test_scan_warp_specialised_shapes(gsrb, ctx, orc, k, threads, tile, variant, n):
+    # FANOUT and HIER run the reader/writer warp-specialised kernel
+    a = gsrb.uniform_i32(n + k, n, 0, 15).astype(np.uint32)
+    c = gsrb.cfg(variant=variant, ctas_per_sm=k, threads=threads, tile=tile, wake_lines=4, fanin_groups=16)
+    assert np.array_equal(_scan(gsrb, ctx, a, cfg=c), orc.scan_u32(a))
+    f = gsrb.uniform_f32(n + 7, n)
+    got = _scan(gsrb, ctx, f, f32=True, cfg=c)
+    assert orc.max_rel_err(got[1:], orc.scan_f32_f64(f)[1:]) <= REL_TOL_F32
+
+
 @pytest.mark.parametrize("n", [1, 5, 1000, 24576 * 148 + 3, 8_000_001])
 def test_scan_f32_tolerance(gsrb, ctx, orc, n):
     a = gsrb.uniform_f32(n + 1, n)

@@ -79,12 +79,14 @@ def tune_barrier(ctx, k: int, threads: int = 256, episodes: int = 4000, reps: in
 
 
 def tune_scan(ctx, d_in, d_out, n: int, reps: int = 3):
+    """FANOUT and HIER run the warp-specialised scan (readers one segment ahead
+    of writers); FLIP and CCG the single-role pipelined one."""
     g = _g()
     table = []
-    for chunk in (16384, 32768, 65536):
-        for k, threads in ((1, 1024), (2, 512), (1, 512)):
-            for cand in (dict(variant=g.BAR_FANOUT, wake_lines=4), dict(variant=g.BAR_FLIP, fanin_groups=1),
-                         dict(variant=g.BAR_HIER, fanin_groups=16, wake_lines=8), dict(variant=g.BAR_CCG)):
+    for chunk in (24576, 32768, 49152):
+        for k, threads in ((1, 1024), (2, 512)):
+            for cand in (dict(variant=g.BAR_FANOUT, wake_lines=4), dict(variant=g.BAR_HIER, fanin_groups=16, wake_lines=8),
+                         dict(variant=g.BAR_FLIP, fanin_groups=1), dict(variant=g.BAR_CCG)):
                 c = g.cfg(ctas_per_sm=k, threads=threads, tile=chunk, **cand)
                 t = _median_ms(ctx, lambda: ctx.scan(d_in, d_out, n, c), reps)
                 if t is not None:

@@ -43,17 +43,21 @@ struct ScanT<false> {
   using Acc = uint32_t;  // uint32 wraparound, like cpu_sum_scan (scan/main.cu:15-20)
   using Vec = uint4;
 };
+// FP32: chunk offsets and carries in FP64; the scan inside one warp round (32
+// lanes x 4 elements, depth 7 additions of non-negative partial sums) in FP32,
+// which adds at most ~7 ulp relative to the round's partial sums before the
+// FP64 carry is added.
 template <>
 struct ScanT<true> {
   using Elem = float;
-  using Acc = double;    // chunk offsets and carries in FP64
+  using Acc = double;
   using Vec = float4;
 };
 
 __device__ __forceinline__ uint32_t shfl_up(uint32_t v, int o) { return __shfl_up_sync(0xffffffffu, v, o); }
-__device__ __forceinline__ double shfl_up(double v, int o) { return __shfl_up_sync(0xffffffffu, v, o); }
+__device__ __forceinline__ float shfl_up(float v, int o) { return __shfl_up_sync(0xffffffffu, v, o); }
+__device__ __forceinline__ float shfl_idx(float v, int l) { return __shfl_sync(0xffffffffu, v, l); }
 __device__ __forceinline__ uint32_t shfl_idx(uint32_t v, int l) { return __shfl_sync(0xffffffffu, v, l); }
-__device__ __forceinline__ double shfl_idx(double v, int l) { return __shfl_sync(0xffffffffu, v, l); }
 __device__ __forceinline__ uint32_t shfl_down(uint32_t v, int o) { return __shfl_down_sync(0xffffffffu, v, o); }
 __device__ __forceinline__ double shfl_down(double v, int o) { return __shfl_down_sync(0xffffffffu, v, o); }
 
@@ -73,14 +77,40 @@ __device__ __forceinline__ Acc warp_sum(Acc v) {
 __device__ __forceinline__ uint32_t vsum(uint4 v) { return v.x + v.y + v.z + v.w; }
 __device__ __forceinline__ double vsum(float4 v) { return (double)((v.x + v.y) + (v.z + v.w)); }
 
-// 128-bit loads / stores with cache hints: first read L2-only (the line stays
-// in L2 for the re-read), re-read evict-first, output streaming.
-__device__ __forceinline__ uint4 ld_cg(const uint4* p) { return __ldcg(p); }
-__device__ __forceinline__ float4 ld_cg(const float4* p) { return __ldcg(p); }
-__device__ __forceinline__ uint4 ld_cs(const uint4* p) { return __ldcs(p); }
-__device__ __forceinline__ float4 ld_cs(const float4* p) { return __ldcs(p); }
-__device__ __forceinline__ void st_cs(uint4* p, uint4 v) { __stcs(p, v); }
-__device__ __forceinline__ void st_cs(float4* p, float4 v) { __stcs(p, v); }
+// 128-bit loads / stores with L2 eviction-priority hints: the first read of a
+// chunk marks its lines evict-last (they are read again one step later), the
+// re-read marks them evict-first, the output is written evict-first.  The
+// policies come from createpolicy (fraction 1.0).
+__device__ __forceinline__ uint64_t l2_policy_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_policy_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint4 ld_hint(const uint4* ptr, uint64_t pol) {
+  uint4 v;
+  asm volatile("ld.global.L1::no_allocate.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(ptr), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ float4 ld_hint(const float4* ptr, uint64_t pol) {
+  float4 v;
+  asm volatile("ld.global.L1::no_allocate.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(ptr), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ void st_hint(uint4* ptr, uint4 v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v4.u32 [%0], {%1,%2,%3,%4}, %5;"
+               ::"l"(ptr), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void st_hint(float4* ptr, float4 v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1,%2,%3,%4}, %5;"
+               ::"l"(ptr), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w), "l"(pol) : "memory");
+}
 
 struct TileGeom {
   uint64_t beg;   // first element of this CTA's chunk
@@ -108,16 +138,16 @@ __device__ __forceinline__ TileGeom tile_of(uint64_t s, uint64_t n, uint32_t G, 
 }
 
 // Vector v (elements 4v..4v+3) of a chunk; elements past cnt read as zero.
-template <bool F32, bool CS>
+template <bool F32>
 __device__ __forceinline__ typename ScanT<F32>::Vec load_vec(const typename ScanT<F32>::Elem* __restrict__ in,
-                                                             const TileGeom& t, uint32_t v, bool vec_ok) {
+                                                             const TileGeom& t, uint32_t v, bool vec_ok,
+                                                             uint64_t pol) {
   using Elem = typename ScanT<F32>::Elem;
   using Vec = typename ScanT<F32>::Vec;
   Vec x;
   const uint32_t e = 4u * v;
   if (vec_ok && e + 3u < t.cnt) {
-    const Vec* p = reinterpret_cast<const Vec*>(in + t.beg + e);
-    x = CS ? ld_cs(p) : ld_cg(p);
+    x = ld_hint(reinterpret_cast<const Vec*>(in + t.beg + e), pol);
   } else {
     Elem y[4];
 #pragma unroll
@@ -146,6 +176,7 @@ scan_kernel(gsrb::GridBarrier gb, const typename ScanT<F32>::Elem* __restrict__ 
 
   const uint32_t tid = threadIdx.x, lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
   const uint32_t G = gridDim.x, b = blockIdx.x;
+  const uint64_t pol_keep = l2_policy_evict_last(), pol_drop = l2_policy_evict_first();
   gsrb::GridSync<V> bar;
   bool ok = bar.init(gb, &bsh);
 
@@ -164,7 +195,7 @@ scan_kernel(gsrb::GridBarrier gb, const typename ScanT<F32>::Elem* __restrict__ 
 #pragma unroll
       for (uint32_t k = 0; k < kInFlight; ++k) {
         const uint32_t vk = v + 32u * k;
-        if (vk < v1) x[k] = load_vec<F32, false>(in, t, vk, vec_in != 0);
+        if (vk < v1) x[k] = load_vec<F32>(in, t, vk, vec_in != 0, pol_keep);
         else memset(&x[k], 0, sizeof(Vec));
       }
 #pragma unroll
@@ -198,7 +229,7 @@ scan_kernel(gsrb::GridBarrier gb, const typename ScanT<F32>::Elem* __restrict__ 
 #pragma unroll
       for (uint32_t k = 0; k < kInFlight; ++k) {
         const uint32_t v = r0 + 32u * k + lane;
-        if (v < v1) xs[k] = load_vec<F32, true>(in, t, v, vec_in != 0);
+        if (v < v1) xs[k] = load_vec<F32>(in, t, v, vec_in != 0, pol_drop);
         else memset(&xs[k], 0, sizeof(Vec));
       }
 #pragma unroll
@@ -208,14 +239,14 @@ scan_kernel(gsrb::GridBarrier gb, const typename ScanT<F32>::Elem* __restrict__ 
         const Vec x = xs[k];
         // lane-local inclusive prefix of 4 elements
         const Elem a0 = x.x, a1 = a0 + x.y, a2 = a1 + x.z, a3 = a2 + x.w;
-        const Acc lt = Acc(a3);
-        Acc incl = lt;
+        const Elem lt = a3;
+        Elem incl = lt;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-          const Acc y = shfl_up(incl, o);
+          const Elem y = shfl_up(incl, o);
           if ((int)lane >= o) incl += y;
         }
-        const Acc e0 = run + (incl - lt);
+        const Acc e0 = run + Acc(incl - lt);
         Vec y;
         y.x = Elem(e0);
         y.y = Elem(e0 + Acc(a0));
@@ -224,7 +255,7 @@ scan_kernel(gsrb::GridBarrier gb, const typename ScanT<F32>::Elem* __restrict__ 
         const uint32_t e = 4u * v;
         if (v < v1) {
           if (vec_out && e + 3u < t.cnt) {
-            st_cs(reinterpret_cast<Vec*>(out + t.beg + e), y);
+            st_hint(reinterpret_cast<Vec*>(out + t.beg + e), y, pol_drop);
           } else {
             const Elem ys[4] = {y.x, y.y, y.z, y.w};
 #pragma unroll
@@ -232,7 +263,7 @@ scan_kernel(gsrb::GridBarrier gb, const typename ScanT<F32>::Elem* __restrict__ 
               if (e + q < t.cnt) out[t.beg + e + q] = ys[q];
           }
         }
-        run += shfl_idx(incl, 31);
+        run += Acc(shfl_idx(incl, 31));
       }
     }
   };
@@ -287,6 +318,247 @@ scan_kernel(gsrb::GridBarrier gb, const typename ScanT<F32>::Elem* __restrict__ 
   bar.finish();
 }
 
+// ---------------------------------------------------------------------------
+// Warp-specialised form (barriers with a thread-level split protocol: V_FANOUT
+// and V_HIER).  Readers (warps [0, NR)) run the chunk sums R(s) one segment
+// ahead; writers (warps [NR, 2 NR)) wait for the grid barrier of s, read the
+// partials and run W(s) (re-read from L2, scan, stream out).  The HBM reads of
+// s+1 then overlap the barrier latency, the partial reads and the re-read of s
+// instead of alternating with them.  Reader warp j and writer warp j own the
+// same slice of the chunk.
+//
+// Ordering (all waits bounded):
+//  * readers start R(s) only after the writers finished W(s-2), so at most two
+//    segments (the one being read, the one being written) are in L2 between
+//    their first read and their re-read;
+//  * the reader leader arrives for s only after the writer leader passed the
+//    barrier of s-1 (each episode's counter is reset by its completer);
+//  * slice offsets and partials rotate over kBufs = 4 buffers: partial(s) is
+//    written after this CTA's writer passed s-1, so every CTA arrived at s-1,
+//    so every writer passed s-2 and has finished reading the partials of s-3
+//    and older; offsets(s) are written after this CTA's writers finished
+//    W(s-2), the last user of buffer (s + 2) % 4 ... and of s % 4 (W(s-4)).
+__device__ __forceinline__ void named_sync(uint32_t id, uint32_t nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// Bounded wait for a shared counter written by another warp of the CTA.
+__device__ __forceinline__ bool smem_wait_ge(const volatile uint32_t* p, uint32_t target,
+                                             const gsrb::GridBarrier& gb) {
+  uint64_t t0 = 0;
+  for (uint32_t it = 0;; ++it) {
+    if ((int32_t)(*p - target) >= 0) {
+      __threadfence_block();
+      return true;
+    }
+    if ((it & 63u) == 63u) {
+      if (gsrb::ptx::ld_relaxed_gpu(&gb.slot->status) != 0u) return false;
+      const uint64_t now = gsrb::ptx::globaltimer_ns();
+      if (t0 == 0) t0 = now;
+      else if (now - t0 > gb.timeout_ns) {
+        gsrb::detail::record_error(gb, gsrb::GSRB_DEV_TIMEOUT, 0xfffffff2u);
+        return false;
+      }
+    }
+  }
+}
+
+template <int V>
+__device__ __forceinline__ void ws_arrive(const gsrb::GridBarrier& gb, uint32_t idx, uint32_t n, uint32_t epoch) {
+  if (V == gsrb::V_HIER) gsrb::detail::hier_arrive(gb, idx, n, epoch);
+  else gsrb::detail::fanout_arrive(gb, n, epoch);
+}
+
+template <int V, bool F32>
+__global__ void __launch_bounds__(1024, 1)
+scan_ws_kernel(gsrb::GridBarrier gb, const typename ScanT<F32>::Elem* __restrict__ in,
+               typename ScanT<F32>::Elem* __restrict__ out, uint64_t n, uint32_t chunk,
+               unsigned long long* __restrict__ partials, int vec_in, int vec_out) {
+  using Elem = typename ScanT<F32>::Elem;
+  using Acc = typename ScanT<F32>::Acc;
+  using Vec = typename ScanT<F32>::Vec;
+  constexpr uint32_t kInFlight = 8;
+  constexpr uint32_t kBufs = 4;
+  __shared__ gsrb::BarrierShared bsh;
+  __shared__ Acc s_rtmp[2][16];     // reader warp totals, by parity of s
+  __shared__ Acc s_off[kBufs][16];  // exclusive slice offsets, by s % kBufs
+  __shared__ Acc s_wred[2][16];
+  __shared__ Acc s_wb[2];
+  __shared__ volatile uint32_t s_wr_passed, s_wr_done, s_rfail, s_wfail;
+  __shared__ uint32_t s_epoch0;
+
+  const uint32_t tid = threadIdx.x, lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
+  const uint32_t NR = nw >> 1, rth = NR * 32u;  // readers: warps [0, NR); writers: [NR, 2 NR)
+  const uint32_t G = gridDim.x, b = blockIdx.x;
+  const uint64_t pol_keep = l2_policy_evict_last(), pol_drop = l2_policy_evict_first();
+  gsrb::GridSync<V> bar;
+  const bool ok0 = bar.init(gb, &bsh);
+  if (tid == 0) {
+    s_epoch0 = bar.epoch;
+    s_wr_passed = 0;
+    s_wr_done = 0;
+    s_rfail = ok0 ? 0u : 1u;
+    s_wfail = ok0 ? 0u : 1u;
+  }
+  __syncthreads();
+  const uint32_t epoch0 = s_epoch0;
+  const uint64_t seg = (uint64_t)G * chunk;
+  const uint64_t nseg = (n + seg - 1) / seg;
+
+  if (w < NR) {
+    // ------------------------------------------------------------ readers
+    for (uint64_t s = 0; s < nseg; ++s) {
+      if (s >= 1) {
+        if (tid == 0 && s >= 2 && !smem_wait_ge(&s_wr_done, (uint32_t)(s - 1), gb)) s_rfail = 1u;  // W(s-2) done
+        named_sync(1, rth);
+      }
+      // s_rfail is only written by the leader before a reader barrier (or
+      // before the block-wide one ahead of the loop): every reader sees the
+      // same value here
+      if (s_rfail) break;
+      const TileGeom t = tile_of(s, n, G, chunk, b);
+      const uint32_t nvec = t.span >> 2;
+      const uint32_t vps = (nvec + NR - 1) / NR;
+      const uint32_t v0 = w * vps, v1 = min(nvec, v0 + vps);
+      Acc lsum = Acc(0);
+      for (uint32_t v = v0 + lane; v < v1; v += 32u * kInFlight) {
+        Vec x[kInFlight];
+#pragma unroll
+        for (uint32_t k = 0; k < kInFlight; ++k) {
+          const uint32_t vk = v + 32u * k;
+          if (vk < v1) x[k] = load_vec<F32>(in, t, vk, vec_in != 0, pol_keep);
+          else memset(&x[k], 0, sizeof(Vec));
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < kInFlight; ++k) lsum += vsum(x[k]);
+      }
+      const Acc wt = warp_sum(lsum);
+      if (lane == 0) s_rtmp[s & 1][w] = wt;
+      named_sync(1, rth);
+      if (tid == 0) {
+        bool ok = s == 0 || smem_wait_ge(&s_wr_passed, (uint32_t)s, gb);  // writers passed s-1
+        if (ok) {
+          Acc run = Acc(0);
+          for (uint32_t i = 0; i < NR; ++i) {
+            const Acc x = s_rtmp[s & 1][i];
+            s_off[s % kBufs][i] = run;
+            run += x;
+          }
+          __stcg(&partials[(s % kBufs) * G + b], (unsigned long long)acc_bits(run));
+          ws_arrive<V>(gb, b - gb.first_cta, gb.nparticipants, epoch0 + (uint32_t)s);
+        } else {
+          s_rfail = 1u;
+        }
+      }
+    }
+  } else {
+    // ------------------------------------------------------------ writers
+    const uint32_t wt_id = tid - rth, ww = w - NR;
+    const bool leader = wt_id == 0;
+    Acc carry = Acc(0);
+    for (uint64_t s = 0; s < nseg; ++s) {
+      if (leader) {
+        const bool ok = gsrb::detail::fanout_wait(gb, b - gb.first_cta, epoch0 + (uint32_t)s, (uint32_t)s);
+        if (!ok) s_wfail = 1u;
+        __threadfence_block();
+        s_wr_passed = (uint32_t)s + 1u;
+      }
+      named_sync(2, rth);
+      if (s_wfail) break;  // uniform: written by the leader before this barrier
+      // offset = carry + partials of the CTAs before b
+      Acc pre = Acc(0), tot = Acc(0);
+      for (uint32_t j = wt_id; j < G; j += rth) {
+        Acc x;
+        acc_from(__ldcg(&partials[(s % kBufs) * G + j]), x);
+        tot += x;
+        if (j < b) pre += x;
+      }
+      pre = warp_sum(pre);
+      tot = warp_sum(tot);
+      if (lane == 0) {
+        s_wred[0][ww] = pre;
+        s_wred[1][ww] = tot;
+      }
+      named_sync(2, rth);
+      if (leader) {
+        Acc p = Acc(0), q = Acc(0);
+        for (uint32_t i = 0; i < NR; ++i) {
+          p += s_wred[0][i];
+          q += s_wred[1][i];
+        }
+        s_wb[0] = p;
+        s_wb[1] = q;
+      }
+      named_sync(2, rth);
+      const Acc base = carry + s_wb[0];
+      carry += s_wb[1];
+      // W(s): re-read the slice (L2), scan, stream out
+      const TileGeom t = tile_of(s, n, G, chunk, b);
+      const uint32_t nvec = t.span >> 2;
+      const uint32_t vps = (nvec + NR - 1) / NR;
+      const uint32_t v0 = ww * vps, v1 = min(nvec, v0 + vps);
+      Acc run = base + s_off[s % kBufs][ww];
+      for (uint32_t r0 = v0; r0 < v1; r0 += 32u * kInFlight) {
+        Vec xs[kInFlight];
+#pragma unroll
+        for (uint32_t k = 0; k < kInFlight; ++k) {
+          const uint32_t v = r0 + 32u * k + lane;
+          if (v < v1) xs[k] = load_vec<F32>(in, t, v, vec_in != 0, pol_drop);
+          else memset(&xs[k], 0, sizeof(Vec));
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < kInFlight; ++k) {
+          if (r0 + 32u * k >= v1) break;  // warp-uniform
+          const uint32_t v = r0 + 32u * k + lane;
+          const Vec x = xs[k];
+          const Elem a0 = x.x, a1 = a0 + x.y, a2 = a1 + x.z, a3 = a2 + x.w;
+          const Elem lt = a3;
+          Elem incl = lt;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const Elem y = shfl_up(incl, o);
+            if ((int)lane >= o) incl += y;
+          }
+          const Acc e0 = run + Acc(incl - lt);
+          Vec y;
+          y.x = Elem(e0);
+          y.y = Elem(e0 + Acc(a0));
+          y.z = Elem(e0 + Acc(a1));
+          y.w = Elem(e0 + Acc(a2));
+          const uint32_t e = 4u * v;
+          if (v < v1) {
+            if (vec_out && e + 3u < t.cnt) {
+              st_hint(reinterpret_cast<Vec*>(out + t.beg + e), y, pol_drop);
+            } else {
+              const Elem ys[4] = {y.x, y.y, y.z, y.w};
+#pragma unroll
+              for (int q = 0; q < 4; ++q)
+                if (e + q < t.cnt) out[t.beg + e + q] = ys[q];
+            }
+          }
+          run += Acc(shfl_idx(incl, 31));
+        }
+      }
+      named_sync(2, rth);
+      if (leader) {
+        __threadfence_block();
+        s_wr_done = (uint32_t)s + 1u;
+      }
+    }
+  }
+  __syncthreads();
+  bar.finish();
+}
+
+template <bool F32>
+const void* scan_ws_fn_t(int variant) {
+  switch (variant) {
+    case gsrb::V_FANOUT: return (const void*)scan_ws_kernel<gsrb::V_FANOUT, F32>;
+    case gsrb::V_HIER: return (const void*)scan_ws_kernel<gsrb::V_HIER, F32>;
+    default: return nullptr;
+  }
+}
+
 template <bool F32>
 const void* scan_fn_t(int variant) {
   switch (variant) {
@@ -320,15 +592,17 @@ gsrb_status_t scan_launch(gsrb_ctx_t ctx, const void* d_in, void* d_out, size_t 
   }
   if (c.threads % 128 || c.threads > 1024) return GSRB_ERR_ARG;
   if (n == 0) return GSRB_OK;
+  // barriers with a thread-level split protocol run the warp-specialised form
+  const void* fn = f32 ? scan_ws_fn_t<true>(c.variant) : scan_ws_fn_t<false>(c.variant);
+  if (!fn) fn = f32 ? scan_fn_t<true>(c.variant) : scan_fn_t<false>(c.variant);
+  if (!fn) return GSRB_ERR_UNSUPPORTED;
   uint32_t tile = c.tile > 0 ? (uint32_t)c.tile : kDefaultChunk;
   tile = (tile + 3) & ~3u;
   const size_t smem = 0;
-  const void* fn = f32 ? scan_fn_t<true>(c.variant) : scan_fn_t<false>(c.variant);
-  if (!fn) return GSRB_ERR_UNSUPPORTED;
   const int grid = grid_of(ctx, c);
   if (grid % c.cluster) return GSRB_ERR_ARG;
   void* part = nullptr;
-  gsrb_status_t st = scratch(ctx, sizeof(unsigned long long) * 2 * (size_t)grid, &part);
+  gsrb_status_t st = scratch(ctx, sizeof(unsigned long long) * 4 * (size_t)grid, &part);
   if (st) return st;
   gsrb::GridBarrier gb = make_barrier(ctx, c, 0, (uint32_t)grid, 0, 0);
   uint64_t n64 = n;
@@ -342,7 +616,8 @@ gsrb_status_t scan_launch(gsrb_ctx_t ctx, const void* d_in, void* d_out, size_t 
 }  // namespace
 
 const void* gsrb_scan_kernel_for(int variant, int f32) {
-  return f32 ? scan_fn_t<true>(variant) : scan_fn_t<false>(variant);
+  const void* fn = f32 ? scan_ws_fn_t<true>(variant) : scan_ws_fn_t<false>(variant);
+  return fn ? fn : (f32 ? scan_fn_t<true>(variant) : scan_fn_t<false>(variant));
 }
 
 extern "C" {
