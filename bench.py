@@ -236,13 +236,15 @@ def arrivals_per_episode(gsrb, c, grid):
 
 
 def barrier_table(gsrb, ctx, tune, tuned_cache):
+    """ns/episode for k in {1,2,4,8} x F in {0,64,1024}: the barrier tuned for
+    that (k, F) against cooperative groups and the reference algorithms."""
     rows = []
     for k in (1, 2, 4, 8):
-        best, _, _ = tune.tune_barrier(ctx, k, episodes=2000, reps=2)
-        tuned_cache[f"barrier_k{k}"] = best
-        bc = tune.cfg_from(best)
         for F in (0, 64, 1024):
             eps = 2000 if F < 1024 else 500
+            best, _, _ = tune.tune_barrier(ctx, k, episodes=eps, reps=2, fma=F)
+            tuned_cache[f"barrier_k{k}_F{F}"] = best
+            bc = tune.cfg_from(best)
             base = statistics.median(time_barrier(gsrb, ctx, gsrb.cfg(variant=gsrb.BAR_NONE, ctas_per_sm=k,
                                                                      threads=256), eps, F, 3, 1))
             row = {"k": k, "F": F, "tuned": gsrb.VARIANT_NAMES[best["variant"]]}

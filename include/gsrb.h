@@ -271,7 +271,8 @@ gsrb_status_t gsrb_graph_info(gsrb_graph_t g, uint32_t* n, uint64_t* m, uint32_t
 gsrb_status_t gsrb_graph_set_policy(gsrb_graph_t g, const float* h_weights, size_t count);
 /* Copy up to max_records 48-byte per-level trace records of the last traversal. */
 gsrb_status_t gsrb_graph_trace(gsrb_graph_t g, void* h_out, uint32_t max_records, uint32_t* records);
-/* BFS levels from src into d_level (int32[n]; INT32_MAX = unreachable). */
+/* BFS levels from src into d_level (int32[n]; INT32_MAX = unreachable).
+ * cfg == NULL: 2 CTAs x 512 threads per SM. */
 gsrb_status_t gsrb_bfs(gsrb_ctx_t ctx, gsrb_graph_t g, uint32_t src, int32_t* d_level, int32_t mode,
                        const gsrb_cfg_t* cfg, gsrb_traversal_stats_t* stats);
 /* SSSP distances (near-far buckets of width delta) into d_dist (int32[n]). */

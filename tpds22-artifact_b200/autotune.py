@@ -59,18 +59,19 @@ def _median_ms(ctx, fn, reps):
     return statistics.median(ts)
 
 
-def tune_barrier(ctx, k: int, threads: int = 256, episodes: int = 4000, reps: int = 3):
-    """Best barrier configuration for k CTAs per SM; returns (cfg dict, ns/episode, table)."""
+def tune_barrier(ctx, k: int, threads: int = 256, episodes: int = 4000, reps: int = 3, fma: int = 0):
+    """Best barrier configuration for k CTAs per SM with `fma` dependent FMAs per
+    thread before each episode; returns (cfg dict, ns/episode, table)."""
     g = _g()
     grid = k * ctx.num_sms
     sink = ctx.array(grid * threads, np.float32).zero()
     cnt = ctx.array(1, np.uint32).zero()
     base = _median_ms(ctx, lambda: ctx.barrier_bench(g.cfg(variant=g.BAR_NONE, ctas_per_sm=k, threads=threads),
-                                                     episodes, 0, sink, cnt), reps)
+                                                     episodes, fma, sink, cnt), reps)
     table = []
     for cand in barrier_candidates(k):
         c = g.cfg(ctas_per_sm=k, threads=threads, **cand)
-        t = _median_ms(ctx, lambda: ctx.barrier_bench(c, episodes, 0, sink, cnt), reps)
+        t = _median_ms(ctx, lambda: ctx.barrier_bench(c, episodes, fma, sink, cnt), reps)
         if t is not None and base is not None:
             table.append((round((t - base) * 1e6 / episodes, 1), cand))
     table.sort(key=lambda x: x[0])

@@ -42,7 +42,106 @@ struct BfsArgs {
   float alpha, beta;   // direction-optimizing thresholds (Beamer, Asanovic, Patterson, SC'12)
   uint32_t* out;       // [0] levels, [1] fallback level (0 = none), [2] policy decisions, [3] overflow
   unsigned long long* out_edges;
+  uint32_t* solo;      // [0] last level, [1] nu, [2] prev_nf, [3] solo levels, [4..5] mu, [6..7] edges
 };
+
+// Single-CTA phase: when a push level's frontier fits one pass of one CTA
+// (<= blockDim.x vertices and <= 4 blockDim.x out-edges) the heuristic and
+// learned schedules hand the following levels to the team's first CTA, which
+// runs them with __syncthreads and shared-memory queue counters while the
+// other CTAs wait at one grid barrier; it hands back when the frontier grows
+// past 2x the entry limits, after kSoloMaxLevels levels, or when the traversal
+// ends.  Small-frontier levels of high-diameter graphs (meshes, road
+// networks) then cost no grid barrier.
+constexpr uint32_t kSoloMaxLevels = 16384;
+
+// The single-CTA phase, run by every thread of the team's first CTA from level
+// L (whose frontier, nreg + nbig vertices of level L-1, is in the global
+// queues; the caller has already done level L's accounting).  Leaves the
+// frontier of the last level it ran in the global queues and counters, and
+// that level, nu, mu, edges and prev_nf (accounting not yet applied for the
+// last level's discoveries, as the level loop expects) in a.solo.
+__device__ __noinline__ void bfs_solo(const BfsArgs& a, uint32_t L, uint32_t nreg, uint32_t nbig, uint32_t nu,
+                                      unsigned long long mu, unsigned long long edges, uint32_t prev_nf) {
+  __shared__ LevelCounters s_c;
+  const DevCSR& g = a.g;
+  const Team one{0u, 1u};
+  uint32_t levels = 0;
+  for (;;) {
+    const uint32_t* qin = a.q[(L - 1) & 1];
+    const uint32_t* hin = a.hq[(L - 1) & 1];
+    uint32_t* qout = a.q[L & 1];
+    uint32_t* hout = a.hq[L & 1];
+    if (threadIdx.x == 0) {
+      s_c.n_reg = 0;
+      s_c.n_big = 0;
+      s_c.m_next = 0;
+    }
+    __syncthreads();
+    unsigned long long m_acc = 0;
+    const int32_t Li = (int32_t)L;
+    auto push_edge = [&](uint32_t, uint32_t j, bool active) {
+      uint32_t v = 0, d = 0;
+      bool disc = false;
+      if (active) {
+        v = __ldg(g.dst + j);
+        if (__ldcg(a.level + v) == kInf) disc = atomicCAS(a.level + v, kInf, Li) == kInf;
+        if (disc) d = __ldg(g.row + v + 1) - __ldg(g.row + v);
+      }
+      warp_append(disc && d <= kBigDegree, v, qout, &s_c.n_reg, g.n, a.overflow);
+      warp_append(disc && d > kBigDegree, v, hout, &s_c.n_big, g.n, a.overflow);
+      m_acc += d;
+    };
+    expand_hubs(one, g, hin, nbig, push_edge);
+    expand_queue(one, g, qin, nreg, push_edge);
+    const unsigned long long ws = warp_sum_u64(m_acc);
+    if (lane_id() == 0 && ws) atomicAdd(&s_c.m_next, ws);
+    __syncthreads();
+    ++levels;
+    const uint32_t nr = (uint32_t)s_c.n_reg, nb = (uint32_t)s_c.n_big;
+    const uint32_t nf = nr + nb;
+    const unsigned long long mf = s_c.m_next;
+    const bool stop = nf == 0 || nf > 2u * blockDim.x || mf > 8ull * blockDim.x || levels >= kSoloMaxLevels;
+    if (stop) {
+      if (threadIdx.x == 0) {
+        a.cnt[L % 3].n_reg = nr;
+        a.cnt[L % 3].n_big = nb;
+        a.cnt[L % 3].m_next = mf;
+        a.cnt[(L + 1) % 3].n_reg = 0;
+        a.cnt[(L + 1) % 3].n_big = 0;
+        a.cnt[(L + 1) % 3].m_next = 0;
+        a.solo[0] = L;
+        a.solo[1] = nu;
+        a.solo[2] = prev_nf;
+        a.solo[3] += levels;
+        *reinterpret_cast<unsigned long long*>(a.solo + 4) = mu;
+        *reinterpret_cast<unsigned long long*>(a.solo + 6) = edges;
+      }
+      return;  // the caller's grid barrier publishes all of it
+    }
+    // next level (the level loop's accounting, done here)
+    ++L;
+    nu -= nf;
+    mu -= mf;
+    edges += mf;
+    if (threadIdx.x == 0 && L - 1 < a.trace_cap) {
+      LevelTrace t;
+      t.level = L;
+      t.dir = 3u;  // single-CTA push
+      t.nf = nf;
+      t.nu = nu;
+      t.mf = mf;
+      t.mu = mu;
+      t.t_ns = gsrb::ptx::globaltimer_ns();
+      t.pred = __int_as_float(0x7fc00000);
+      t.fallback = 0u;
+      a.trace[L - 1] = t;
+    }
+    prev_nf = nf;
+    nreg = nr;
+    nbig = nb;
+  }
+}
 
 // The traversal body, relative to a team (the whole grid, or one instance's
 // CTA range in a batch, synchronised by `bar`).
@@ -50,8 +149,10 @@ template <int V>
 __device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const BfsArgs& a, const Team team) {
   __shared__ uint32_t s_dir;
   __shared__ float s_pred;
+  __shared__ MLPShared s_mlp;
   const DevCSR& g = a.g;
   const uint32_t tid = team.tid(), nthreads = team.nthreads();
+  if (a.mode == GSRB_BFS_LEARNED) mlp_stage(a.mlp, &s_mlp);  // visible after the barrier below
 
   // init (bfs_init, bfs/kernel_gsrb.cu:299-311) fused into the persistent kernel
   for (uint32_t v = tid; v < g.n; v += nthreads) a.level[v] = (v == a.src) ? 0 : kInf;
@@ -106,7 +207,7 @@ __device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const B
       if (threadIdx.x < 32) {
         float feat[kFeat], out[kOut];
         level_features(feat, g.n, g.m, L, nf, mf, nu, mu, prev_nf, dir);
-        mlp_forward_warp(a.mlp, feat, out);
+        mlp_forward_smem(&s_mlp, feat, out);
         if (threadIdx.x == 0) {
           s_dir = out[0] > 0.f ? DIR_PULL : (out[1] > 0.f ? DIR_TOPO : DIR_PUSH);
           s_pred = out[2];
@@ -138,6 +239,21 @@ __device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const B
       }
     }
     prev_nf = nf;
+
+    if (team.ncta > 1 && dir == DIR_PUSH && nf <= blockDim.x && mf <= 4ull * blockDim.x &&
+        (a.mode == GSRB_BFS_HEURISTIC || a.mode == GSRB_BFS_LEARNED)) {
+      if (team.cta == 0) bfs_solo(a, L, nreg, nbig, nu, mu, edges, prev_nf);
+      ok = bar.sync();
+      if (!ok) break;
+      L = __ldcg(a.solo + 0);
+      nu = __ldcg(a.solo + 1);
+      prev_nf = __ldcg(a.solo + 2);
+      mu = __ldcg(reinterpret_cast<const unsigned long long*>(a.solo + 4));
+      edges = __ldcg(reinterpret_cast<const unsigned long long*>(a.solo + 6));
+      dir = DIR_PUSH;
+      pred = __int_as_float(0x7fc00000);  // no prediction for the level after the phase
+      continue;
+    }
 
     const uint32_t* qin = a.q[(L - 1) & 1];
     const uint32_t* hin = a.hq[(L - 1) & 1];
@@ -248,8 +364,10 @@ __device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const B
   }
 }
 
+constexpr int kGraphMaxThreads = 1024;
+
 template <int V>
-__global__ void __launch_bounds__(1024)
+__global__ void __launch_bounds__(kGraphMaxThreads)
 bfs_kernel(gsrb::GridBarrier gb, BfsArgs a) {
   __shared__ gsrb::BarrierShared bsh;
   gsrb::GridSync<V> bar;
@@ -447,7 +565,7 @@ struct BatchDesc {
 };
 
 template <int V>
-__global__ void __launch_bounds__(1024)
+__global__ void __launch_bounds__(kGraphMaxThreads)
 batch_kernel(const BatchDesc* __restrict__ descs, const uint16_t* __restrict__ cta_inst) {
   __shared__ gsrb::BarrierShared bsh;
   const uint32_t i = cta_inst[blockIdx.x];
@@ -703,7 +821,7 @@ struct gsrb_graph {
   uint32_t* fmark = nullptr;
   LevelCounters* cnt = nullptr;
   unsigned long long* fcnt = nullptr;
-  uint32_t* flags = nullptr;  // [0] overflow, [4..8) out, edges at byte 64, PageRank tickets at byte 96
+  uint32_t* flags = nullptr;  // [0] overflow, [4..8) out, [8..16) BFS single-CTA state, edges at byte 64, PageRank tickets at byte 96
   LevelTrace* trace = nullptr;
   uint32_t trace_cap = 0;
   float* contrib[2] = {};
@@ -930,7 +1048,7 @@ gsrb_status_t gsrb_bfs(gsrb_ctx_t ctx, gsrb_graph_t G, uint32_t src, int32_t* d_
   const void* fn = bfs_fn(c.variant);
   if (!fn) return GSRB_ERR_UNSUPPORTED;
   const int grid = grid_of(ctx, c);
-  if (grid % c.cluster || c.threads % 32) return GSRB_ERR_ARG;
+  if (grid % c.cluster || c.threads % 32 || c.threads > kGraphMaxThreads) return GSRB_ERR_ARG;
   BfsArgs a;
   a.g = dev_csr(G);
   a.src = src;
@@ -949,6 +1067,7 @@ gsrb_status_t gsrb_bfs(gsrb_ctx_t ctx, gsrb_graph_t G, uint32_t src, int32_t* d_
   a.beta = 18.f;
   a.out = G->flags + 4;
   a.out_edges = (unsigned long long*)((char*)G->flags + 64);
+  a.solo = G->flags + 8;
   std::lock_guard<std::mutex> g(ctx->mu);
   GSRB_CUDA(cudaMemsetAsync(G->flags, 0, 128, ctx->stream));
   gsrb::GridBarrier gb = make_barrier(ctx, c, 0, (uint32_t)grid, 0, 0);
@@ -1084,6 +1203,7 @@ BfsArgs bfs_args(gsrb_graph* G, uint32_t src, int32_t* level, int32_t mode) {
   a.beta = 18.f;
   a.out = G->flags + 4;
   a.out_edges = (unsigned long long*)((char*)G->flags + 64);
+  a.solo = G->flags + 8;
   return a;
 }
 
@@ -1157,6 +1277,7 @@ gsrb_status_t gsrb_batch_create(gsrb_ctx_t ctx, const gsrb_graph_t* graphs, int3
   }
   c.cluster = 1;
   if (!batch_fn(c.variant)) return GSRB_ERR_UNSUPPORTED;
+  if (c.threads % 32 || c.threads > kGraphMaxThreads) return GSRB_ERR_ARG;
   const int grid = grid_of(ctx, c);
   if (grid < k || grid > 65535) return GSRB_ERR_ARG;
   gsrb_batch* B = new gsrb_batch();

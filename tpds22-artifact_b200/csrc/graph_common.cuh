@@ -32,7 +32,7 @@ struct DevCSR {
 // One record per level / bucket step, written by CTA 0 after the barrier.
 struct LevelTrace {
   uint32_t level;
-  uint32_t dir;          // 0 push-worklist, 1 pull, 2 push-topology
+  uint32_t dir;          // 0 push-worklist, 1 pull, 2 push-topology, 3 push by a single CTA
   uint32_t nf;           // frontier vertices entering this level
   uint32_t nu;           // unvisited vertices before this level
   unsigned long long mf; // frontier out-edges
@@ -190,6 +190,56 @@ __device__ __forceinline__ void mlp_forward_warp(const MLPWeights* __restrict__ 
     for (int s = 16; s > 0; s >>= 1) p += __shfl_xor_sync(0xffffffffu, p, s);
     out[o] = p + W->b3[o];
   }
+}
+
+// The same network staged in shared memory, weights transposed so that lane j
+// reads column j of every layer without bank conflicts.  Filled once per CTA
+// (mlp_stage) and evaluated by one warp per level (mlp_forward_smem), with the
+// additions in the same order as mlp_forward_warp.
+struct MLPShared {
+  float w1t[kFeat][kHid];
+  float b1[kHid];
+  float w2t[kHid][kHid];
+  float b2[kHid];
+  float w3[kOut][kHid];
+  float b3[kOut];
+  float h1[kHid];
+};
+
+__device__ __forceinline__ void mlp_stage(const MLPWeights* __restrict__ W, MLPShared* m) {
+  for (uint32_t i = threadIdx.x; i < kFeat * kHid; i += blockDim.x) m->w1t[i % kFeat][i / kFeat] = W->w1[i / kFeat][i % kFeat];
+  for (uint32_t i = threadIdx.x; i < kHid * kHid; i += blockDim.x) m->w2t[i % kHid][i / kHid] = W->w2[i / kHid][i % kHid];
+  for (uint32_t i = threadIdx.x; i < kOut * kHid; i += blockDim.x) m->w3[i / kHid][i % kHid] = W->w3[i / kHid][i % kHid];
+  for (uint32_t i = threadIdx.x; i < kHid; i += blockDim.x) {
+    m->b1[i] = W->b1[i];
+    m->b2[i] = W->b2[i];
+  }
+  for (uint32_t i = threadIdx.x; i < kOut; i += blockDim.x) m->b3[i] = W->b3[i];
+}
+
+// One warp; every lane returns the 4 outputs.
+__device__ __forceinline__ void mlp_forward_smem(MLPShared* m, const float* feat, float out[kOut]) {
+  const uint32_t j = lane_id();
+  float h1 = m->b1[j];
+#pragma unroll
+  for (int i = 0; i < kFeat; ++i) h1 = fmaf(m->w1t[i][j], feat[i], h1);
+  h1 = fmaxf(h1, 0.f);
+  m->h1[j] = h1;
+  __syncwarp();
+  float h2 = m->b2[j];
+#pragma unroll
+  for (int i = 0; i < kHid; ++i) h2 = fmaf(m->w2t[i][j], m->h1[i], h2);
+  h2 = fmaxf(h2, 0.f);
+  __syncwarp();  // h1 may be rewritten by the next call
+  float p[kOut];
+#pragma unroll
+  for (int o = 0; o < kOut; ++o) p[o] = m->w3[o][j] * h2;
+#pragma unroll
+  for (int sft = 16; sft > 0; sft >>= 1)
+#pragma unroll
+    for (int o = 0; o < kOut; ++o) p[o] += __shfl_xor_sync(0xffffffffu, p[o], sft);
+#pragma unroll
+  for (int o = 0; o < kOut; ++o) out[o] = p[o] + m->b3[o];
 }
 
 // Feature vector of a level (all log-scaled or normalised to O(1)).  The same
