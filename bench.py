@@ -664,8 +664,13 @@ def main():
     grid = args.k * ctx.num_sms
     arrivals = arrivals_per_episode(gsrb, c, grid)
     achieved = arrivals / (ns * 1e-9)
+    # DRAM bytes of one launch from an ncu capture of this kernel (1184 x 256,
+    # FANOUT): the per-thread FMA seeds, read once, independent of episodes
+    traffic = 1218560 if args.k == 8 and args.fma == 0 else None
     roofline = {"bound": "l2_atomic", "achieved": round(achieved / 1e9, 4), "peak": round(rate / 1e9, 4),
-                "unit": "G same-address atomics/s", "frac": round(achieved / rate, 4), "traffic": None,
+                "unit": "G same-address atomics/s", "frac": round(achieved / rate, 4), "traffic": traffic,
+                "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum per launch (ncu); the barrier is "
+                                "L2-latency bound, DRAM idle",
                 "peak_source": "measured live: same-address red.add throughput probe (MEASURED_PEAKS.json has no "
                                "L2-atomic entry)",
                 "arrivals_per_episode": arrivals, "l2_atomic_rtt_ns": round(rtt, 1),
