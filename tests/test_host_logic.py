@@ -1,0 +1,157 @@
+"""Host-side logic on CPU: configuration defaults, the policy's labels and
+features, the autotuner's candidate sets, and bench.py's reference arm and
+multi-process (gloo) path."""
+import ctypes as C
+import importlib.util
+import json
+import math
+import os
+import pathlib
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = pathlib.Path(__file__).resolve().parents[1]
+PKG = ROOT / "tpds22-artifact_b200"
+
+
+def _mod(name, path):
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, path)
+    m = importlib.util.module_from_spec(spec)
+    sys.modules[name] = m
+    spec.loader.exec_module(m)
+    return m
+
+
+@pytest.fixture(scope="module")
+def pol(gsrb):
+    return _mod("gsrb_policy", PKG / "policy.py")
+
+
+@pytest.fixture(scope="module")
+def tune(gsrb):
+    return _mod("gsrb_autotune", PKG / "autotune.py")
+
+
+def test_cfg_default_matches_header(gsrb):
+    c = gsrb.Cfg()
+    gsrb.lib().gsrb_cfg_default(C.byref(c))
+    assert c.variant == gsrb.BAR_CLUSTER and c.cluster == 2 and c.ctas_per_sm == 2 and c.threads == 256
+    assert c.timeout_ms == 2000 and c.launch_mode == 1 and c.tile == 0
+    # every variant has a name; the status strings are defined for every code
+    for v in range(12):
+        assert v in gsrb.VARIANT_NAMES
+    for st in range(0, -11, -1):
+        s = gsrb.lib().gsrb_status_string(st)
+        assert s and b"unknown" not in s.lower()
+
+
+def test_policy_weight_is_cost_sensitive(pol):
+    assert pol._weight(100.0, 100.0) == pytest.approx(0.05)        # a tie hardly counts
+    assert pol._weight(1000.0, 100.0) == pytest.approx(math.log2(10))
+    assert pol._weight(100.0, 1000.0) == pytest.approx(math.log2(10))
+    assert pol._weight(1e6, 1.0) == 4.0                              # clipped
+
+
+def test_policy_level_times(pol):
+    tr = np.zeros(4, dtype=[("t_ns", "<u8")])
+    tr["t_ns"] = [100, 250, 600, 700]
+    d = pol.level_times(tr)
+    assert d[:3].tolist() == [150.0, 350.0, 100.0] and math.isnan(d[3])
+
+
+def test_level_features_host_twin(gsrb):
+    # the device evaluates the same function; check it against a restatement
+    n, m, lvl, nf, mf, nu, mu, pnf, pdir = 4096, 65536, 3, 100, 1600, 3000, 40000, 10, 1
+    f = gsrb.level_features(n, m, lvl, nf, mf, nu, mu, pnf, pdir)
+    want = [math.log2(1 + nf), math.log2(1 + mf), math.log2(1 + nu), math.log2(1 + mu), nf / n, mf / (mu + 1),
+            math.log2(1 + mf / nf), math.log2(1 + lvl), pdir, math.log2(n), math.log2(1 + m) - math.log2(n),
+            math.log2(1 + nf) - math.log2(1 + pnf)]
+    assert np.allclose(f, want, rtol=1e-5, atol=1e-6)
+
+
+def test_mlp_init_layout(gsrb):
+    p = gsrb.mlp_init(3)
+    assert p.size == gsrb.mlp_param_count() == 32 * 12 + 32 + 32 * 32 + 32 + 4 * 32 + 4
+    assert np.array_equal(p, gsrb.mlp_init(3)) and not np.array_equal(p, gsrb.mlp_init(4))
+    assert np.all(np.isfinite(p))
+
+
+def test_autotune_candidates_and_cfg_roundtrip(gsrb, tune):
+    cands = tune.barrier_candidates(8)
+    variants = {c["variant"] for c in cands}
+    assert {gsrb.BAR_CCG, gsrb.BAR_FLAT, gsrb.BAR_FLIP, gsrb.BAR_FANOUT, gsrb.BAR_HIER} <= variants
+    e = dict(variant=gsrb.BAR_FANOUT, wake_lines=2, spin_ns=64, ctas_per_sm=8, threads=256, bogus=1)
+    c = tune.cfg_from(e)
+    assert (c.variant, c.wake_lines, c.spin_ns, c.ctas_per_sm, c.threads) == (9, 2, 64, 8, 256)
+    p = tune.CACHE.parent / "_tuned_test.json"
+    try:
+        tune.save_cache({"x": e}, p)
+        assert tune.load_cache(p)["x"]["wake_lines"] == 2
+    finally:
+        if p.exists():
+            p.unlink()
+    assert tune.load_cache(ROOT / "does-not-exist.json") == {}
+
+
+def _bench_env():
+    env = dict(os.environ)
+    env["MASTER_ADDR"] = "127.0.0.1"
+    return env
+
+
+def test_bench_reference_arm_line():
+    p = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "3"], capture_output=True, text=True, timeout=600, env=_bench_env())
+    assert p.returncode == 0, p.stderr[-2000:]
+    lines = [ln for ln in p.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+              "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["impl"] == "reference" and d["higher_is_better"] is False and d["value"] > 0
+    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
+
+
+def test_bench_two_ranks_gloo():
+    # torchrun with two CPU ranks: rank 0 alone prints the reference line, rank 1 exits cleanly
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", "29633", str(ROOT / "bench.py"), "--impl",
+           "reference", "--gpus", "2", "--steps", "1", "--warmup", "3"]
+    p = subprocess.run(cmd, capture_output=True, text=True, timeout=900, env=_bench_env())
+    assert p.returncode == 0, p.stderr[-3000:]
+    lines = [ln for ln in p.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    assert json.loads(lines[0])["n_gpus"] == 2
+
+
+def _max_worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    sys.path.insert(0, str(ROOT))
+    bench = _mod("bench_under_test", ROOT / "bench.py")
+    d = bench.Dist()
+    v = d.max(float(10 * (rank + 1)))
+    d.barrier()
+    d.close()
+    q.put((rank, v))
+
+
+def test_dist_max_over_ranks_gloo():
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    ps = [ctx.Process(target=_max_worker, args=(r, 2, 29655, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    got = dict(q.get(timeout=300) for _ in ps)
+    for p in ps:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert got == {0: 20.0, 1: 20.0}
