@@ -337,6 +337,9 @@ struct GridSync {
   static constexpr bool kFanout = V == V_FANOUT || V == V_CLUSTER_FANOUT || V == V_HIER;
   // arrive() and wait() are split (a CTA may arrive and leave without waiting)
   static constexpr bool kSplit = V == V_FANOUT || V == V_HIER || V == V_FLIP;
+  // arrive() tells thread 0 (arrived_done) whether its arrival completed the
+  // episode; the completer has then acquired every other CTA's arrival
+  static constexpr bool kCompleter = V == V_FANOUT || V == V_HIER;
 
   // Index of this CTA among the participants and of its arrival unit.
   __device__ __forceinline__ uint32_t my_index() const { return blockIdx.x - gb.first_cta; }

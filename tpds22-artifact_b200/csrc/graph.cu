@@ -177,6 +177,8 @@ __device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const B
   float pred = __int_as_float(0x7fc00000);
   uint32_t L = 1;
   uint32_t decisions = 0;
+  uint32_t last_dir = DIR_PUSH, last_nf = 0;  // the policy's last decision and the frontier it saw
+  unsigned long long last_mf = 0;
   for (; ok; ++L) {
     const LevelCounters cur = {__ldcg(&a.cnt[(L - 1) % 3].n_reg), __ldcg(&a.cnt[(L - 1) % 3].n_big),
                                __ldcg(&a.cnt[(L - 1) % 3].m_next), 0};
@@ -204,19 +206,33 @@ __device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const B
       if (dir != DIR_PULL && (double)mf > (double)mu / a.alpha) nd = DIR_PULL;
       else if (dir == DIR_PULL && (double)nf < (double)g.n / a.beta) nd = DIR_PUSH;
     } else if (a.mode == GSRB_BFS_LEARNED) {
-      if (threadIdx.x < 32) {
-        float feat[kFeat], out[kOut];
-        level_features(feat, g.n, g.m, L, nf, mf, nu, mu, prev_nf, dir);
-        mlp_forward_smem(&s_mlp, feat, out);
-        if (threadIdx.x == 0) {
-          s_dir = out[0] > 0.f ? DIR_PULL : (out[1] > 0.f ? DIR_TOPO : DIR_PUSH);
-          s_pred = out[2];
+      // the network is evaluated again only when the frontier's size or edge
+      // count has moved by more than 2x since its last decision (on meshes and
+      // road networks that skips most levels); a reused decision carries no
+      // prediction, so it cannot trigger the fallback
+      const bool reuse = decisions > 0 && nf <= 2u * last_nf && 2u * nf >= last_nf && mf <= 2ull * last_mf &&
+                         2ull * mf >= last_mf;
+      if (reuse) {
+        nd = last_dir;
+        pred = __int_as_float(0x7fc00000);
+      } else {
+        if (threadIdx.x < 32) {
+          float feat[kFeat], out[kOut];
+          level_features(feat, g.n, g.m, L, nf, mf, nu, mu, prev_nf, dir);
+          mlp_forward_smem(&s_mlp, feat, out);
+          if (threadIdx.x == 0) {
+            s_dir = out[0] > 0.f ? DIR_PULL : (out[1] > 0.f ? DIR_TOPO : DIR_PUSH);
+            s_pred = out[2];
+          }
         }
+        __syncthreads();
+        nd = s_dir;
+        pred = s_pred;
+        last_dir = nd;
+        last_nf = nf;
+        last_mf = mf;
+        ++decisions;
       }
-      __syncthreads();
-      nd = s_dir;
-      pred = s_pred;
-      ++decisions;
     }
     dir = nd;
     if (team.cta == 0 && threadIdx.x == 0) {
@@ -522,7 +538,69 @@ __device__ __forceinline__ void sssp_run(gsrb::GridSync<V>& bar, bool ok, const 
       warp_append(to_far, v, fout, fc, g.n, a.overflow);
     };
     expand_hubs(team, g, hin, nbig, relax);
-    expand_queue(team, g, qin, nreg, relax);
+    {
+      // regular queue: vertices of degree > kWarpDegree edge-parallel across the
+      // warp; smaller ones one lane each with 4 edges per lane in flight through
+      // every dependent step (ids and weights, distance probe, atomicMin, stamp)
+      const uint32_t lane = lane_id();
+      const uint32_t gw = team.warp(), nwarps = team.nwarps();
+      for (uint32_t base = gw * 32u; base < nreg; base += nwarps * 32u) {
+        const uint32_t i = base + lane;
+        uint32_t u = 0, b = 0, e = 0;
+        if (i < nreg) {
+          u = __ldcg(qin + i);
+          b = __ldg(g.row + u);
+          e = __ldg(g.row + u + 1);
+        }
+        const uint32_t deg = e - b;
+        uint32_t coop = __ballot_sync(0xffffffffu, deg > kWarpDegree);
+        while (coop) {
+          const int src = __ffs(coop) - 1;
+          coop &= coop - 1;
+          const uint32_t uu = __shfl_sync(0xffffffffu, u, src);
+          const uint32_t bb = __shfl_sync(0xffffffffu, b, src), ee = __shfl_sync(0xffffffffu, e, src);
+          for (uint32_t j0 = bb; j0 < ee; j0 += 32) relax(uu, j0 + lane, j0 + lane < ee);
+        }
+        const uint32_t mine = deg <= kWarpDegree ? deg : 0u;
+        const uint32_t kmax = warp_max_u32(mine);
+        const long long du = mine ? (long long)__ldcg(a.dist + u) : 0;
+        for (uint32_t k0 = 0; k0 < kmax; k0 += 4) {
+          uint32_t v[4];
+          long long nd[4];
+          bool to_near[4], to_far[4];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const bool act = k0 + r < mine;
+            v[r] = act ? __ldg(g.dst + b + k0 + r) : 0u;
+            nd[r] = act ? du + (long long)__ldg(g.w + b + k0 + r) : (long long)kInf;
+            my_edges += act ? 1u : 0u;
+          }
+          int32_t cur[4];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) cur[r] = (k0 + r < mine) ? __ldcg(a.dist + v[r]) : kInf;
+          bool imp[4];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) imp[r] = nd[r] < (long long)cur[r] && nd[r] < (long long)atomicMin(a.dist + v[r], (int32_t)nd[r]);
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            to_near[r] = imp[r] && nd[r] < T && atomicExch(a.mark + v[r], stamp) != stamp;
+            to_far[r] = imp[r] && nd[r] >= T && atomicExch(a.fmark + v[r], fgen) != fgen;
+          }
+          uint32_t d[4];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) d[r] = to_near[r] ? __ldg(g.row + v[r] + 1) - __ldg(g.row + v[r]) : 0u;
+          bool reg[4], big[4];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            reg[r] = to_near[r] && d[r] <= kBigDegree;
+            big[r] = to_near[r] && d[r] > kBigDegree;
+          }
+          warp_append_k<4>(reg, v, qout, &c->n_reg, g.n, a.overflow);
+          warp_append_k<4>(big, v, hout, &c->n_big, g.n, a.overflow);
+          warp_append_k<4>(to_far, v, fout, fc, g.n, a.overflow);
+        }
+      }
+    }
     relaxed_edges += my_edges;
     ++step;
     ok = bar.sync();

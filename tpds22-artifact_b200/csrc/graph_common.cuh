@@ -88,6 +88,35 @@ __device__ __forceinline__ void warp_append(bool pred, uint32_t v, uint32_t* q, 
   }
 }
 
+// Warp-aggregated append of up to K values per lane (v[r] where pred[r]) with
+// ONE reservation on the counter for the whole warp: the K appends of a lane
+// step cost one atomic round trip instead of K.  Warp-synchronous.
+template <int K>
+__device__ __forceinline__ void warp_append_k(const bool* pred, const uint32_t* v, uint32_t* q,
+                                              unsigned long long* cnt, uint32_t cap, uint32_t* overflow) {
+  uint32_t mask[K];
+  uint32_t tot = 0;
+#pragma unroll
+  for (int r = 0; r < K; ++r) {
+    mask[r] = __ballot_sync(0xffffffffu, pred[r]);
+    tot += __popc(mask[r]);
+  }
+  if (!tot) return;
+  unsigned long long base = 0;
+  if (lane_id() == 0) base = atomicAdd(cnt, (unsigned long long)tot);
+  base = __shfl_sync(0xffffffffu, base, 0);
+  const uint32_t lt = lanemask_lt();
+#pragma unroll
+  for (int r = 0; r < K; ++r) {
+    if (pred[r]) {
+      const unsigned long long pos = base + __popc(mask[r] & lt);
+      if (pos < cap) q[pos] = v[r];
+      else atomicExch(overflow, 1u);
+    }
+    base += __popc(mask[r]);
+  }
+}
+
 __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);

@@ -12,10 +12,12 @@
 // stages in flight (192 KiB per SM by default, well above the bytes in flight
 // an SM needs to stream its share of HBM bandwidth); every warp sums its part
 // of a stage in int64 and frees the stage on an "empty" mbarrier, so warps
-// never wait for each other inside the stream.  Warp shuffles reduce the CTA's sum to one partial; the CTA
-// arrives at the grid barrier (split phase: only CTA 0, which combines, waits)
-// and CTA 0 adds the partials in a fixed order, so the result is deterministic
-// and bit-exact against a serial int64 sum.
+// never wait for each other inside the stream.  Warp shuffles reduce the
+// CTA's sum to one partial; the CTA arrives at the grid barrier (split phase:
+// with the fan-out protocols the CTA whose arrival completes the barrier
+// combines and nobody waits; otherwise only CTA 0 waits) and the combiner adds
+// the partials in CTA order, so the result is deterministic and bit-exact
+// against a serial int64 sum.
 #include "internal.h"
 
 using namespace gsrbrt;
@@ -139,9 +141,19 @@ reduce_i32_kernel(gsrb::GridBarrier gb, const int32_t* __restrict__ in, uint64_t
   const long long bsum = block_sum_i64(acc, warp_buf);
   if (tid == 0) partials[blockIdx.x] = bsum;
   bar.arrive();
-  bool done = true;
-  if (!gsrb::GridSync<V>::kSplit || blockIdx.x == 0) done = bar.wait();
-  if (done && ok && blockIdx.x == 0) {
+  // the combiner: the CTA whose arrival completed the barrier when the protocol
+  // says so (it has acquired every partial; nobody waits), else CTA 0 after a wait
+  __shared__ uint32_t s_comb;
+  bool done = true, combiner;
+  if (gsrb::GridSync<V>::kCompleter) {
+    if (tid == 0) s_comb = bar.arrived_done;
+    __syncthreads();
+    combiner = s_comb != 0u;
+  } else {
+    combiner = blockIdx.x == 0;
+    if (!gsrb::GridSync<V>::kSplit || combiner) done = bar.wait();
+  }
+  if (done && ok && combiner) {
     // fixed-order combine of the G partials (deterministic)
     long long s = 0;
     for (uint64_t j = tid; j < G; j += T) s += __ldcg(partials + j);
