@@ -12,7 +12,7 @@ The same line carries every other configuration of the benchmark plan,
 measured on the same device in the same run (disable with --no-extras):
   barrier_table     ns/episode for k in {1,2,4,8} x F in {0,64,1024}: tuned
                     native barrier vs cooperative-groups grid.sync and the
-                    reference algorithms (GSRB, GCPUSRB, atomic tree)
+                    reference algorithms (GSRB, GCPUSRB, atomic tree, lock-free tree)
   semaphore         acquires/s, capacity S in {1,2,10,120}, 1 writer per 10 readers
   reduce_2e24       GB/s and fraction of measured HBM (cold L2), bit-exact check
   scan_2e28         u32 (bit-exact) and f32 (1e-5 relative), GB/s, HBM fraction
@@ -251,7 +251,8 @@ def barrier_table(gsrb, ctx, tune, tuned_cache):
             for name, c in (("native", bc), ("ccg", gsrb.cfg(variant=gsrb.BAR_CCG, ctas_per_sm=k, threads=256)),
                             ("ref_gsrb", gsrb.cfg(variant=gsrb.BAR_SOFT2, ctas_per_sm=k, threads=256)),
                             ("ref_gcpusrb", gsrb.cfg(variant=gsrb.BAR_FLAT, ctas_per_sm=k, threads=256)),
-                            ("atomic_tree", gsrb.cfg(variant=gsrb.BAR_TREE, ctas_per_sm=k, threads=256))):
+                            ("atomic_tree", gsrb.cfg(variant=gsrb.BAR_TREE, ctas_per_sm=k, threads=256)),
+                            ("ref_lockfree", gsrb.cfg(variant=gsrb.BAR_LOCKFREE, ctas_per_sm=k, threads=256))):
                 try:
                     t = statistics.median(time_barrier(gsrb, ctx, c, eps, F, 3, 1))
                     row[name] = round((t - base) * 1e6 / eps, 1)

@@ -56,6 +56,8 @@ enum {
   GSRB_BAR_FANOUT = 9,           /* 2-level: counter + generation published to R wake-up lines */
   GSRB_BAR_CLUSTER_FANOUT = 10,  /* 3-level: HW cluster arrival, leader on the counter, R wake-up lines */
   GSRB_BAR_HIER = 11,            /* 3-level: group counters (fanin_groups) -> root counter -> R wake-up lines */
+  GSRB_BAR_LOCKFREE = 12,        /* reference HeteroSync lock-free tree barrier (in/out flag arrays; per-SM
+                                    local level when there is more than one CTA per SM); barrier benchmark only */
   GSRB_BAR_NONE = 99             /* no barrier (phase-only timing baseline) */
 };
 

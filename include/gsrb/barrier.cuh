@@ -60,7 +60,8 @@ enum Variant : int {
   V_FANOUT = 9,          // one arrival counter, generation published to R wake-up lines
   V_CLUSTER_FANOUT = 10, // HW cluster arrival -> leader on the counter -> every CTA polls its wake-up line
   V_HIER = 11,           // group counters on separate lines -> root counter -> wake-up lines
-  V_COUNT = 12
+  V_LOCKFREE = 12,       // HeteroSync lock-free tree barrier: in/out flag arrays, master CTA scans
+  V_COUNT = 13
 };
 
 // One global barrier slot: four 128-byte lines so that the arrival counter, the
@@ -279,6 +280,62 @@ __device__ __forceinline__ bool fanout_arrive(const GridBarrier& gb, uint32_t n,
 __device__ __forceinline__ bool fanout_wait(const GridBarrier& gb, uint32_t unit, uint32_t epoch, uint32_t episode) {
   return wait_ne(fanout_line(gb, unit % fanout_count(gb)), epoch, gb, episode);
 }
+
+// ---- lock-free flag barrier (V_LOCKFREE) -------------------------------------
+// The HeteroSync "lock-free" tree barrier (Heterosync/cudaLocksBarrierFast.cu:
+// 182-330, after Xiao and Feng): member j sets in[j] = 1; the group's master
+// (member 0) has its threads scan all in flags, then resets in[i] = 0 and sets
+// out[i] = 1 (released); member j waits for out[j] = 1 and clears it.  Flags
+// return to 0 after every episode, so the protocol is stateless across
+// launches.  Restated with scoped ordering (the reference's plain volatile
+// stores in=0 / out=1 are not ordered against each other) and bounded waits.
+// `inner` runs in the whole master CTA after every member arrived and before
+// any is released (the global level of the two-level form).
+__device__ __forceinline__ bool lf_wait_eq(const uint32_t* word, uint32_t want, const GridBarrier& gb,
+                                           uint32_t episode) {
+  uint64_t t0 = 0;
+  for (uint32_t it = 0;; ++it) {
+    if (ptx::ld_acquire_gpu(word) == want) return true;
+    if ((it & 31u) == 31u) {
+      if (ptx::ld_relaxed_gpu(&gb.slot->status) != 0u) return false;
+      const uint64_t now = ptx::globaltimer_ns();
+      if (t0 == 0) {
+        t0 = now;
+      } else if (now - t0 > gb.timeout_ns) {
+        record_error(gb, GSRB_DEV_TIMEOUT, episode);
+        return false;
+      }
+    }
+  }
+}
+template <class Inner>
+__device__ __forceinline__ bool lf_episode(uint32_t* in, uint32_t* out, uint32_t members, uint32_t j,
+                                           const GridBarrier& gb, uint32_t episode, Inner inner) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ptx::fence_acq_rel_gpu();
+    ptx::st_relaxed_gpu(in + j, 1u);
+  }
+  bool ok = true;
+  if (j == 0) {
+    for (uint32_t i = threadIdx.x; i < members; i += blockDim.x) ok = lf_wait_eq(in + i, 1u, gb, episode) && ok;
+    ok = __syncthreads_and(ok) != 0;
+    if (ok) ok = inner();
+    for (uint32_t i = threadIdx.x; i < members; i += blockDim.x) {
+      ptx::st_relaxed_gpu(in + i, 0u);
+      ptx::st_release_gpu(out + i, 1u);
+    }
+  }
+  if (threadIdx.x == 0) {
+    ok = lf_wait_eq(out + j, 1u, gb, episode) && ok;
+    ptx::st_relaxed_gpu(out + j, 0u);
+  }
+  return __syncthreads_and(ok) != 0;
+}
+// Flag area layout (gb.flip points at it): global in / out arrays of
+// kLfGlobal words, then per-group local in / out arrays of kLfLocal words.
+constexpr uint32_t kLfGlobal = 8192, kLfGroups = 256, kLfLocal = 64;
+constexpr size_t kLfWords = 2 * (size_t)kLfGlobal + 2 * (size_t)kLfGroups * kLfLocal;
 
 // ---- two-level counters + wake-up lines (V_HIER) --------------------------------
 // Unit u arrives on group counter u % G (each group counter on its own 256-byte
@@ -639,6 +696,31 @@ __device__ __forceinline__ bool GridSync<V_FLIP>::wait() {
   }
   __syncthreads();
   return sh->ok != 0u;
+}
+
+// V_LOCKFREE: flat (ngroups <= 1: every CTA is a member of one flag barrier,
+// CTA 0 the master) or two-level (ngroups = G: group g = index % G with its
+// first member as local master, as the reference's per-SM local barrier;
+// the local masters form the global barrier, master = group 0's master).
+template <>
+__device__ __forceinline__ bool GridSync<V_LOCKFREE>::sync() {
+  uint32_t* gin = gb.flip;
+  uint32_t* gout = gb.flip + detail::kLfGlobal;
+  const uint32_t n = gb.nparticipants, p = my_index(), G = gb.ngroups;
+  const uint32_t ep = episode++;
+  bool ok;
+  if (G <= 1 || n <= G) {
+    ok = detail::lf_episode(gin, gout, n, p, gb, ep, [] { return true; });
+  } else {
+    const uint32_t g = p % G, j = p / G;
+    uint32_t* lin = gb.flip + 2 * detail::kLfGlobal + (size_t)g * 2 * detail::kLfLocal;
+    uint32_t* lout = lin + detail::kLfLocal;
+    const uint32_t m = detail::group_size(n, G, g);
+    ok = detail::lf_episode(lin, lout, m, j, gb, ep, [&] {
+      return detail::lf_episode(gin, gout, G, g, gb, ep, [] { return true; });
+    });
+  }
+  return ok;
 }
 
 // V_SOFT2: the reference GSRB two-level structure with software groups

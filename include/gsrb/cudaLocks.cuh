@@ -251,6 +251,29 @@ inline __device__ void joinBarrier_helperNaiveSRB(unsigned int* barrierBuffers, 
   const gsrb::GridBarrier gb = gsrb_compat_barrier(barrierBuffers, nullptr, 0, numBlocksAtBarr);
   if (b.init(gb, &s_bar)) b.sync();
 }
+// HeteroSync lock-free tree barrier (Heterosync/cudaLocksBarrierFast.cu:182-330):
+// the reference's flag layout -- global in/out flags at barrierBuffers and
+// barrierBuffers + arrayStride indexed by blockIdx (the per-SM masters are
+// CTAs 0 .. numBlocksAtBarr-1), per-SM in/out flags at perSMBarrierBuffers +
+// 2 * MAX_BLOCKS * smID indexed by perSM_blockID -- with scoped ordering and
+// bounded waits (gsrb::detail::lf_episode).
+inline __device__ void joinLFBarrier_helper(unsigned int* barrierBuffers, unsigned int* perSMBarrierBuffers,
+                                            const unsigned int numBlocksAtBarr, const int smID,
+                                            const int perSM_blockID, const int numTBs_perSM,
+                                            const int arrayStride, const int MAX_BLOCKS) {
+  const gsrb::GridBarrier gb = gsrb_compat_barrier(barrierBuffers + 2 * arrayStride, nullptr, 0, gridDim.x);
+  unsigned int* gin = barrierBuffers;
+  unsigned int* gout = barrierBuffers + arrayStride;
+  if (numTBs_perSM > 1) {
+    unsigned int* lin = perSMBarrierBuffers + (size_t)MAX_BLOCKS * smID * 2;
+    unsigned int* lout = lin + MAX_BLOCKS;
+    gsrb::detail::lf_episode(lin, lout, (uint32_t)numTBs_perSM, (uint32_t)perSM_blockID, gb, 0u, [&] {
+      return gsrb::detail::lf_episode(gin, gout, numBlocksAtBarr, (uint32_t)smID, gb, 0u, [] { return true; });
+    });
+  } else {
+    gsrb::detail::lf_episode(gin, gout, numBlocksAtBarr, blockIdx.x, gb, 0u, [] { return true; });
+  }
+}
 // HeteroSync atomic tree barrier (Heterosync/cudaLocksBarrierAtomic.cu:145-170).
 inline __device__ void joinBarrier_helper(unsigned int* barrierBuffers, unsigned int* perSMBarrierBuffers,
                                           const unsigned int numBlocksAtBarr, const int smID,

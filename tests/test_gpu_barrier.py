@@ -4,7 +4,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-ALL = [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11]
+ALL = [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12]
 
 
 def _run_bench(gsrb, ctx, variant, k, cluster=2, episodes=2000, fma=0, threads=256, fanin=0):
@@ -72,7 +72,7 @@ def test_refuses_non_coresident_grid(gsrb, ctx):
     assert ctx.barrier_bench(c, 10, 0, sink, cnt) == gsrb.ERR_NOT_CORESIDENT
 
 
-@pytest.mark.parametrize("variant", [0, 2, 3, 4, 5, 8, 9, 11])
+@pytest.mark.parametrize("variant", [0, 2, 3, 4, 5, 8, 9, 11, 12])
 def test_short_grid_times_out_and_context_survives(gsrb, ctx, variant):
     # the expected arrival count is one participant higher than the launch:
     # every wait must run out (bounded) and report a timeout, not hang
@@ -84,3 +84,14 @@ def test_short_grid_times_out_and_context_survives(gsrb, ctx, variant):
     gsrb.check(st)
     ctx.check_status()
     assert int(cnt.download()[0]) == 100 * grid
+
+
+@pytest.mark.parametrize("groups", [1, 16, 148])
+@pytest.mark.parametrize("k", [1, 4])
+def test_lockfree_flat_and_two_level(gsrb, ctx, groups, k):
+    # fanin_groups = 1: one flat flag barrier (CTA 0 scans every flag);
+    # > 1: per-group local barriers whose masters form the global one
+    st, grid, cnt = _run_bench(gsrb, ctx, gsrb.BAR_LOCKFREE, k, fanin=groups, episodes=500)
+    gsrb.check(st)
+    ctx.check_status()
+    assert int(cnt.download()[0]) == 500 * grid

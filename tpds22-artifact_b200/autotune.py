@@ -30,7 +30,8 @@ def _g():
 
 def barrier_candidates(k: int):
     g = _g()
-    c = [dict(variant=g.BAR_CCG), dict(variant=g.BAR_FLAT), dict(variant=g.BAR_FLIP, fanin_groups=1)]
+    c = [dict(variant=g.BAR_CCG), dict(variant=g.BAR_FLAT), dict(variant=g.BAR_FLIP, fanin_groups=1),
+         dict(variant=g.BAR_LOCKFREE)]
     for R in (2, 4, 8):
         for s in (0, 64):
             c.append(dict(variant=g.BAR_FANOUT, wake_lines=R, spin_ns=s))

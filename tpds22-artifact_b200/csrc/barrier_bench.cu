@@ -94,6 +94,7 @@ const void* bench_fn(int variant) {
     case gsrb::V_FANOUT: return (const void*)barrier_bench_kernel<gsrb::V_FANOUT>;
     case gsrb::V_CLUSTER_FANOUT: return (const void*)barrier_bench_kernel<gsrb::V_CLUSTER_FANOUT>;
     case gsrb::V_HIER: return (const void*)barrier_bench_kernel<gsrb::V_HIER>;
+    case gsrb::V_LOCKFREE: return (const void*)barrier_bench_kernel<gsrb::V_LOCKFREE>;
     case kNoBarrier: return (const void*)barrier_bench_kernel<kNoBarrier>;
     default: return nullptr;
   }
@@ -113,6 +114,7 @@ const void* litmus_fn(int variant) {
     case gsrb::V_FANOUT: return (const void*)barrier_litmus_kernel<gsrb::V_FANOUT>;
     case gsrb::V_CLUSTER_FANOUT: return (const void*)barrier_litmus_kernel<gsrb::V_CLUSTER_FANOUT>;
     case gsrb::V_HIER: return (const void*)barrier_litmus_kernel<gsrb::V_HIER>;
+    case gsrb::V_LOCKFREE: return (const void*)barrier_litmus_kernel<gsrb::V_LOCKFREE>;
     default: return nullptr;
   }
 }

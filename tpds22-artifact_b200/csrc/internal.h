@@ -22,6 +22,7 @@ struct gsrb_ctx {
   gsrb::BarrierSlot* slots = nullptr;
   gsrb::GroupSlot* groups = nullptr;
   uint32_t* flip = nullptr;  // kSlots * kMaxFlip lines of 32 words
+  uint32_t* lf = nullptr;    // lock-free flag barrier area (gsrb::detail::kLfWords words)
   // general scratch (device), grown on demand
   void* scratch = nullptr;
   size_t scratch_bytes = 0;

@@ -13,6 +13,7 @@
 // atomic add to R.  An occupancy gauge checks exclusion (a writer must be alone,
 // at most `capacity` readers at a time).  W and R are checked exactly.
 #include "internal.h"
+#include <stddef.h>
 #include "gsrb/locks.cuh"
 #include "gsrb/cudaLocks.h"
 
@@ -39,13 +40,27 @@ cudaError_t alloc_with_header(void** user, size_t bytes) {
 void free_with_header(void* user) {
   if (user) cudaFree((char*)user - 128);
 }
-uint32_t read_clear_status(void* user) {
-  if (!user) return 0;
+uint32_t read_clear_word(uint32_t* w) {
   uint32_t v = 0;
-  uint32_t* w = (uint32_t*)((char*)user - 128);
   cudaMemcpy(&v, w, 4, cudaMemcpyDeviceToHost);
   if (v) cudaMemset(w, 0, 4);
   return v;
+}
+
+uint32_t read_clear_status(void* user) {
+  if (!user) return 0;
+  return read_clear_word((uint32_t*)((char*)user - 128));
+}
+
+// Status words of the stateless barrier wrappers (gsrb/cudaLocks.cuh): the
+// native slot at the start of barrierBuffers, and the lock-free barrier's slot
+// after its 2 * arrayStride flag words.
+uint32_t read_clear_barrier_status(uint32_t* barrierBuffers, int arrayStride) {
+  if (!barrierBuffers) return 0;
+  const size_t status_word = offsetof(gsrb::BarrierSlot, status) / sizeof(uint32_t);
+  uint32_t v = read_clear_word(barrierBuffers + status_word);
+  const uint32_t v2 = read_clear_word(barrierBuffers + 2 * (size_t)arrayStride + status_word);
+  return v ? v : v2;
 }
 
 __global__ void ring_init_kernel(int32_t* ring, size_t n, int stride) {
@@ -64,9 +79,10 @@ cudaError_t locks_alloc(LockState* L, int maxBlocks, int numMutexes, int numSems
   if (L->d.arrayStride < 16) L->d.arrayStride = 16;
   L->d.mutexCount = numMutexes;
   L->d.semaphoreCount = numSems;
-  // barrierBuffers: the reference's 2*arrayStride words, and at least one
-  // native barrier slot plus per-group counters for the stateless device API
-  size_t bb = sizeof(uint32_t) * 2 * (size_t)L->d.arrayStride;
+  // barrierBuffers: the reference's 2*arrayStride words (lock-free barrier
+  // flags) followed by that barrier's status slot, and at least one native
+  // barrier slot plus per-group counters for the stateless device API
+  size_t bb = sizeof(uint32_t) * 2 * (size_t)L->d.arrayStride + sizeof(gsrb::BarrierSlot);
   const size_t native = sizeof(gsrb::BarrierSlot) + sizeof(gsrb::GroupSlot) * (size_t)(numSM > 0 ? numSM : 1);
   if (bb < native) bb = native;
   cudaError_t e = alloc_with_header((void**)&L->d.barrierBuffers, bb);
@@ -393,6 +409,8 @@ unsigned int gsrb_cudalocks_status(void) {
     uint32_t s = read_clear_status(b);
     if (!v) v = s;
   }
+  const uint32_t sb = read_clear_barrier_status(cpuLockData->barrierBuffers, cpuLockData->arrayStride);
+  if (!v) v = sb;
   return v;
 }
 

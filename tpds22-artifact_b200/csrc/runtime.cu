@@ -85,14 +85,21 @@ gsrb::GridBarrier make_barrier(gsrb_ctx* ctx, const gsrb_cfg_t& c, int slot, uin
       nflip = c.wake_lines > 0 ? (uint32_t)c.wake_lines : 8u;
       if (nflip > 8u) nflip = 8u;
       break;
+    case gsrb::V_LOCKFREE:
+      // the reference goes two-level (per-SM local barrier + global) when
+      // there is more than one CTA per SM (cudaLocksBarrierFast.cu:310-329)
+      ng = c.fanin_groups > 0 ? (uint32_t)c.fanin_groups
+                              : (np > (uint32_t)ctx->num_sms ? (uint32_t)ctx->num_sms : 0u);
+      if (ng > gsrb::detail::kLfGroups) ng = gsrb::detail::kLfGroups;
+      break;
     default:
       ng = 0;
   }
-  if (ng + group_base > (uint32_t)kGroups) ng = kGroups - group_base;
+  if (c.variant != gsrb::V_LOCKFREE && ng + group_base > (uint32_t)kGroups) ng = kGroups - group_base;
   gb.ngroups = ng;
   gb.spin_ns = (uint32_t)c.spin_ns;
   gb.timeout_ns = (uint64_t)c.timeout_ms * 1000000ull;
-  gb.flip = ctx->flip + (size_t)slot * kMaxFlip * 32;
+  gb.flip = c.variant == gsrb::V_LOCKFREE ? ctx->lf : ctx->flip + (size_t)slot * kMaxFlip * 32;
   gb.nflip = nflip;
   gb._pad = 0;
   return gb;
@@ -295,6 +302,8 @@ gsrb_status_t gsrb_ctx_create(int device, gsrb_ctx_t* out) {
   const size_t fbytes = sizeof(uint32_t) * 32 * (size_t)kSlots * kMaxFlip;
   if (e == cudaSuccess) e = cudaMalloc(&c->flip, fbytes);
   if (e == cudaSuccess) e = cudaMemset(c->flip, 0, fbytes);
+  if (e == cudaSuccess) e = cudaMalloc(&c->lf, sizeof(uint32_t) * gsrb::detail::kLfWords);
+  if (e == cudaSuccess) e = cudaMemset(c->lf, 0, sizeof(uint32_t) * gsrb::detail::kLfWords);
   if (e == cudaSuccess) e = cudaMemset(c->slots, 0, sbytes);
   if (e == cudaSuccess) e = cudaMemset(c->groups, 0, gbytes);
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -315,6 +324,7 @@ gsrb_status_t gsrb_ctx_destroy(gsrb_ctx_t c) {
   if (c->slots) cudaFree(c->slots);
   if (c->groups) cudaFree(c->groups);
   if (c->flip) cudaFree(c->flip);
+  if (c->lf) cudaFree(c->lf);
   if (c->scratch) cudaFree(c->scratch);
   if (c->flush) cudaFree(c->flush);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -366,6 +376,7 @@ gsrb_status_t gsrb_ctx_status(gsrb_ctx_t c, uint32_t* code, uint32_t* where, uin
     GSRB_CUDA(cudaMemset(c->slots, 0, sizeof(gsrb::BarrierSlot) * kSlots));
     GSRB_CUDA(cudaMemset(c->groups, 0, sizeof(gsrb::GroupSlot) * kGroups));
     GSRB_CUDA(cudaMemset(c->flip, 0, sizeof(uint32_t) * 32 * (size_t)kSlots * kMaxFlip));
+    GSRB_CUDA(cudaMemset(c->lf, 0, sizeof(uint32_t) * gsrb::detail::kLfWords));
     GSRB_CUDA(cudaDeviceSynchronize());
   }
   return map_dev(worst);

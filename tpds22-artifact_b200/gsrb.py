@@ -48,6 +48,7 @@ BAR_FLIP = 8
 BAR_FANOUT = 9
 BAR_CLUSTER_FANOUT = 10
 BAR_HIER = 11
+BAR_LOCKFREE = 12
 BAR_NONE = 99
 VARIANT_NAMES = {
     BAR_CLUSTER: "gsrb_cluster",
@@ -62,6 +63,7 @@ VARIANT_NAMES = {
     BAR_FANOUT: "gsrb_fanout",
     BAR_CLUSTER_FANOUT: "gsrb_cluster_fanout",
     BAR_HIER: "gsrb_hier",
+    BAR_LOCKFREE: "lockfree_tree",
     BAR_NONE: "none",
 }
 
