@@ -443,6 +443,18 @@ def graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, verify_pr=True):
                                  "edges_per_s": round(50 * rm.nedges / (st.kernel_ms * 1e-3), 1),
                                  "GB_s_algorithmic": round(50 * per_iter_bytes / (st.kernel_ms * 1e-3) / 1e9, 1),
                                  "l1_vs_fp64": l1, "within_1e-6": (l1 <= 1e-6) if l1 is not None else None}
+    # the reference's push-residual algorithm (epsilon 1e-6, run to empty
+    # worklist), checked against the pull form run to convergence (200 iterations)
+    conv = ctx.array(rm.nnodes, np.float32)
+    gsrb.check(dg.pagerank(conv, 0.85, 200, cfg)[0], "pagerank 200")
+    outr = ctx.array(rm.nnodes, np.float32)
+    gsrb.check(dg.pagerank_residual(outr, 0.85, 1e-6, 2**31 - 1, cfg)[0], "pagerank_residual")
+    rc, st = dg.pagerank_residual(outr, 0.85, 1e-6, 2**31 - 1, cfg)
+    gsrb.check(rc, "pagerank_residual")
+    res["rmat22"]["pagerank_residual"] = {"epsilon": 1e-6, "ms": round(st.kernel_ms, 3), "rounds": int(st.levels),
+                                          "pushes": int(st.edges),
+                                          "l1_vs_converged_pull": orc.normalized_l1(outr.download(),
+                                                                                    conv.download().astype(np.float64))}
     dg.free()
     del rm
     gr = gsrb.grid2d(2048, 2048, seed=SEED, wlo=1, whi=1000)

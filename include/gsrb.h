@@ -283,6 +283,15 @@ gsrb_status_t gsrb_sssp(gsrb_ctx_t ctx, gsrb_graph_t g, uint32_t src, int32_t* d
 /* Pull PageRank: x0 = 1 - alpha, `iters` iterations of x = (1-alpha) + alpha * sum x_u/deg(u). */
 gsrb_status_t gsrb_pagerank(gsrb_ctx_t ctx, gsrb_graph_t g, float alpha, int32_t iters, float* d_rank,
                             const gsrb_cfg_t* cfg, gsrb_traversal_stats_t* stats);
+/* The reference's push-residual PageRank (apps/pr/kernel_gsrb.cu:298-508):
+ * p = 1 - alpha, residuals seeded with (1 - alpha) * alpha * sum 1/outdeg, then
+ * rounds of "take the residual, add it to p, push alpha * res / outdeg along
+ * every out-edge" over a worklist of vertices whose residual crossed epsilon,
+ * until the worklist is empty or max_iters rounds ran.  FP32 atomics in a
+ * run-dependent order (as in the reference).  stats->levels = rounds,
+ * stats->edges = worklist pushes. */
+gsrb_status_t gsrb_pagerank_residual(gsrb_ctx_t ctx, gsrb_graph_t g, float alpha, float epsilon, int32_t max_iters,
+                                     float* d_rank, const gsrb_cfg_t* cfg, gsrb_traversal_stats_t* stats);
 
 /* ---- batched traversals (many graphs, one persistent launch) ----------------------
  * k graphs (k <= 127) traversed in ONE persistent launch: instance i owns a

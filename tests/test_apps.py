@@ -113,20 +113,38 @@ def test_sssp_app_matches_oracle(ctx, orc, gr_files, tmp_path, variant, name, de
     assert np.array_equal(_read_levels(out, g.nnodes), orc.dijkstra(g, 0))
 
 
-@pytest.mark.gpu
-@pytest.mark.parametrize("variant", ["gsrb", "ccg"])
-def test_pr_app_matches_oracle(ctx, orc, gr_files, tmp_path, variant):
-    path, g = gr_files["rmat12"]
-    out = tmp_path / "ranks.txt"
-    p = _run(f"pr_{variant}", ["-x", "50", "-o", str(out), str(path)])
-    assert "PR took 50 iterations" in p.stdout and "sum:" in p.stdout
-    r = np.zeros(g.nnodes, np.float64)
-    for line in out.read_text().splitlines():
+def _read_ranks(path, n):
+    r = np.zeros(n, np.float64)
+    for line in path.read_text().splitlines():
         i, v = line.split()
         r[int(i)] = float(v)
+    return r
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("variant", ["gsrb", "ccg"])
+def test_pr_app_pull_matches_oracle(ctx, orc, gr_files, tmp_path, variant):
+    path, g = gr_files["rmat12"]
+    out = tmp_path / "ranks.txt"
+    p = _run(f"pr_{variant}", ["-u", "-x", "50", "-o", str(out), str(path)])
+    assert "PR took 50 iterations" in p.stdout and "sum:" in p.stdout
+    r = _read_ranks(out, g.nnodes)
     ref = orc.pagerank(g, 0.85, 50)
     # "%f" keeps 6 decimals: allow the printing rounding on top of the 1e-6 bound
     tol = 1e-6 + 5e-7 * g.nnodes / ref.sum()
+    assert np.abs(r - ref).sum() / ref.sum() <= tol
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("variant", ["gsrb", "gcpusrb"])
+def test_pr_app_default_is_the_reference_residual_algorithm(ctx, orc, gr_files, tmp_path, variant):
+    path, g = gr_files["rmat12"]
+    out = tmp_path / "ranks.txt"
+    p = _run(f"pr_{variant}", ["-o", str(out), str(path)])
+    assert "PR took" in p.stdout and "sum:" in p.stdout
+    r = _read_ranks(out, g.nnodes)
+    ref = orc.pagerank(g, 0.85, 400)
+    tol = 2e-5 + 5e-7 * g.nnodes / ref.sum()
     assert np.abs(r - ref).sum() / ref.sum() <= tol
 
 

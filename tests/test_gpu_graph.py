@@ -77,6 +77,31 @@ def test_pagerank_l1(gsrb, ctx, orc, graphs, name):
     assert np.max(np.abs(got - ref) / ref) < 1e-5
 
 
+@pytest.mark.parametrize("name", ["tiny", "rmat12", "rmat16", "grid64", "isolated"])
+def test_pagerank_residual_converges_to_the_fixed_point(gsrb, ctx, orc, graphs, name):
+    # the reference's push-residual algorithm: every vertex's unpropagated
+    # residual ends below epsilon, so p is within about epsilon / (1 - alpha)
+    # (normalised) of the FP64 fixed point p = (1 - alpha) + alpha * A^T D^-1 p
+    g = graphs[name]
+    dg = ctx.graph(g)
+    out = ctx.array(g.nnodes, np.float32)
+    rc, st = dg.pagerank_residual(out, 0.85, 1e-6)
+    gsrb.check(rc, "pagerank_residual")
+    ctx.check_status("pagerank_residual")
+    ref = orc.pagerank(g, 0.85, 400)
+    assert orc.normalized_l1(out.download(), ref) <= 2e-5
+    assert st.levels >= 1
+
+
+def test_pagerank_residual_round_cap(gsrb, ctx, graphs):
+    g = graphs["rmat12"]
+    dg = ctx.graph(g)
+    out = ctx.array(g.nnodes, np.float32)
+    rc, st = dg.pagerank_residual(out, 0.85, 1e-6, max_iters=3)
+    gsrb.check(rc, "pagerank_residual")
+    assert st.levels == 3
+
+
 def test_bfs_trace_records(gsrb, ctx, orc, graphs):
     g = graphs["rmat16"]
     dg = ctx.graph(g)

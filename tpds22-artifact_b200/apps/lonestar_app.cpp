@@ -17,7 +17,10 @@
 // native grid barrier (library default), *_gcpusrb the flat CPU-style
 // sense-reversing barrier, *_ccg cooperative groups; -b <variant> overrides.
 // Extra options: -m <push|heuristic|learned|pull|topo> (BFS schedule),
-// -P <file> (policy weights, raw float32), -x <iterations> (PR, default 50).
+// -P <file> (policy weights, raw float32); PR runs the reference's
+// push-residual algorithm until no residual exceeds epsilon = 1e-6 (-x caps
+// the rounds, as in the reference), or with -u the pull form for -x
+// iterations (default 50).
 // -l is accepted for compatibility: hub vertices are always split across CTAs.
 #include <getopt.h>
 #include <stdint.h>
@@ -38,7 +41,7 @@
 
 namespace {
 
-int g_quiet = 0, g_device = 0, g_start = 0, g_delta = 10000, g_iters = 50, g_no_rank = 0, g_top = 0;
+int g_quiet = 0, g_device = 0, g_start = 0, g_delta = 10000, g_iters = -1, g_no_rank = 0, g_top = 0, g_pull = 0;
 int g_variant = -1, g_mode = GSRB_BFS_HEURISTIC;
 const char* g_output = nullptr;
 const char* g_policy = nullptr;
@@ -50,8 +53,8 @@ const char* kAppUsage = "[-l] [-s startNode] [-m push|heuristic|learned|pull|top
 const char* kAppOpts = "ls:d:";
 const char* kAppUsage = "[-l] [-d delta] [-s startNode]";
 #else
-const char* kAppOpts = "nt:x:";
-const char* kAppUsage = "[-n] [-t top_ranks] [-x max_iterations]";
+const char* kAppOpts = "nt:x:u";
+const char* kAppUsage = "[-n] [-t top_ranks] [-x max_iterations] [-u (pull form)]";
 #endif
 
 void usage(const char* argv0) {
@@ -115,6 +118,7 @@ void parse_args(int argc, char** argv) {
       case 'n': g_no_rank = 1; break;
       case 't': g_top = atoi(optarg); break;
       case 'x': g_iters = atoi(optarg); break;
+      case 'u': g_pull = 1; break;
       default: usage(argv[0]); exit(EXIT_FAILURE);
     }
   }
@@ -229,8 +233,15 @@ int main(int argc, char** argv) {
   if (GSRB_APP == 3) {
     float* d = nullptr;
     CHECK(gsrb_malloc((void**)&d, sizeof(float) * (n ? n : 1)));
-    rc = gsrb_pagerank(ctx, g, 0.85f, g_iters, d, &cfg, &st);
-    if (rc != GSRB_OK) die("gsrb_pagerank", rc);
+    if (g_pull) {
+      rc = gsrb_pagerank(ctx, g, 0.85f, g_iters >= 0 ? g_iters : 50, d, &cfg, &st);
+      if (rc != GSRB_OK) die("gsrb_pagerank", rc);
+    } else {
+      // ALPHA = 0.85, EPSILON = 1e-6 (apps/pr/kernel_gsrb.cu:291-292); MAX_ITERATIONS
+      // defaults to INT_MAX (apps/pr/support.cu:26)
+      rc = gsrb_pagerank_residual(ctx, g, 0.85f, 1e-6f, g_iters >= 0 ? g_iters : INT32_MAX, d, &cfg, &st);
+      if (rc != GSRB_OK) die("gsrb_pagerank_residual", rc);
+    }
     printf("Kernel time (ms) %f\n", st.kernel_ms);
     printf("PR took %u iterations\n", st.levels);
     std::vector<float> r(n);

@@ -843,6 +843,190 @@ pagerank_kernel(gsrb::GridBarrier gb, PrArgs a) {
   bar.finish();
 }
 
+// ------------------------------------------------------ push-residual PR ---
+// The reference's PageRank (apps/pr/kernel_gsrb.cu:298-508, restated):
+//   init_1  p[v] = 1 - alpha; r[w] += 1 / outdeg(u) over every edge u -> w
+//   init_2  r[v] *= (1 - alpha) * alpha; every vertex enters the worklist
+//   round   for every u in the worklist: res = exchange(r[u], 0); p[u] += res;
+//           for every edge u -> w: prev = r[w] += alpha * res / outdeg(u), and
+//           w enters the next worklist when r[w] crosses epsilon from below
+// until the worklist is empty or max_iters rounds ran; one grid barrier per
+// round (+1 when hub vertices, degree > kBigDegree, are in the worklist: their
+// residual is taken first and their edges are split across the grid).  FP32
+// atomics in an order that changes from run to run, as in the reference;
+// p[u] is updated atomically (the reference's plain += races when a vertex is
+// in a worklist twice).
+struct PrrArgs {
+  DevCSR g;
+  float alpha, eps;
+  int32_t max_iters;
+  float* p;             // output ranks
+  float* r;             // residuals
+  float* hub_upd;       // alpha * res / outdeg of the hubs of the current round, by vertex
+  uint32_t* mark;       // round stamps: a vertex enters a worklist at most once
+  uint32_t* q[2];
+  uint32_t* hq[2];
+  LevelCounters* cnt;   // [3]
+  uint32_t* overflow;
+  uint32_t* out;        // [0] rounds, [1] worklist pushes (low 32 bits), [3] failure
+  unsigned long long* out_edges;
+};
+
+template <int V>
+__global__ void __launch_bounds__(1024)
+pr_residual_kernel(gsrb::GridBarrier gb, PrrArgs a) {
+  __shared__ gsrb::BarrierShared bsh;
+  gsrb::GridSync<V> bar;
+  bool ok = bar.init(gb, &bsh);
+  const DevCSR& g = a.g;
+  const Team team{blockIdx.x, gridDim.x};
+  const uint32_t tid = team.tid(), nthreads = team.nthreads();
+  const uint32_t lane = lane_id();
+  // init_1
+  for (uint32_t v = tid; v < g.n; v += nthreads) {
+    a.p[v] = 1.f - a.alpha;
+    a.r[v] = 0.f;
+    a.mark[v] = 0;
+  }
+  if (tid == 0)
+    for (int k = 0; k < 3; ++k) a.cnt[k].n_reg = a.cnt[k].n_big = a.cnt[k].m_next = 0;
+  ok = bar.sync() && ok;
+  for (uint32_t gwarp = tid >> 5; gwarp * 32u < g.n; gwarp += nthreads >> 5) {
+    const uint32_t u = gwarp * 32u + lane;
+    uint32_t b = 0, e = 0;
+    if (u < g.n) {
+      b = __ldg(g.row + u);
+      e = __ldg(g.row + u + 1);
+    }
+    const float upd = e > b ? 1.f / (float)(e - b) : 0.f;
+    // warp-strided edges of the 32 vertices, one vertex at a time
+    for (int src = 0; src < 32; ++src) {
+      const uint32_t bb = __shfl_sync(0xffffffffu, b, src), ee = __shfl_sync(0xffffffffu, e, src);
+      const float uu = __shfl_sync(0xffffffffu, upd, src);
+      for (uint32_t j = bb + lane; j < ee; j += 32) atomicAdd(a.r + __ldg(g.dst + j), uu);
+    }
+  }
+  ok = bar.sync() && ok;
+  // init_2: scale, every vertex enters the worklist (hubs to the hub queue)
+  for (uint32_t base = (tid >> 5) * 32u; base < g.n; base += nthreads) {
+    const uint32_t v = base + lane;
+    bool reg = false, big = false;
+    if (v < g.n) {
+      a.r[v] *= (1.f - a.alpha) * a.alpha;
+      const uint32_t d = __ldg(g.row + v + 1) - __ldg(g.row + v);
+      big = d > kBigDegree;
+      reg = !big;
+    }
+    warp_append(reg, v, a.q[0], &a.cnt[0].n_reg, g.n, a.overflow);
+    warp_append(big, v, a.hq[0], &a.cnt[0].n_big, g.n, a.overflow);
+  }
+  ok = bar.sync() && ok;
+  uint32_t round = 0;
+  unsigned long long pushes = 0;
+  for (; ok && round < (uint32_t)a.max_iters; ++round) {
+    const uint32_t nreg = (uint32_t)__ldcg(&a.cnt[round % 3].n_reg);
+    const uint32_t nbig = (uint32_t)__ldcg(&a.cnt[round % 3].n_big);
+    if (nreg + nbig == 0) break;
+    if (tid == 0) {
+      a.cnt[(round + 2) % 3].n_reg = 0;
+      a.cnt[(round + 2) % 3].n_big = 0;
+    }
+    const uint32_t* qin = a.q[round & 1];
+    const uint32_t* hin = a.hq[round & 1];
+    uint32_t* qout = a.q[(round + 1) & 1];
+    uint32_t* hout = a.hq[(round + 1) & 1];
+    LevelCounters* c = &a.cnt[(round + 1) % 3];
+    // a vertex whose residual crosses epsilon twice in one round (its own
+    // exchange in this round restarted it from 0) enters the next list once
+    const uint32_t stamp = round + 2u;
+    auto push = [&](bool cross, uint32_t w) {
+      uint32_t d = 0;
+      if (cross) cross = atomicExch(a.mark + w, stamp) != stamp;
+      if (cross) d = __ldg(g.row + w + 1) - __ldg(g.row + w);
+      warp_append(cross && d <= kBigDegree, w, qout, &c->n_reg, g.n, a.overflow);
+      warp_append(cross && d > kBigDegree, w, hout, &c->n_big, g.n, a.overflow);
+      pushes += cross ? 1u : 0u;
+    };
+    if (nbig) {
+      // hubs: take the residual once, then split the edges across the grid
+      for (uint32_t k = tid; k < nbig; k += nthreads) {
+        const uint32_t u = __ldcg(hin + k);
+        const float res = atomicExch(a.r + u, 0.f);
+        atomicAdd(a.p + u, res);
+        a.hub_upd[u] = res * a.alpha / (float)(__ldg(g.row + u + 1) - __ldg(g.row + u));
+      }
+      ok = bar.sync();
+      if (!ok) break;
+      auto hub_edge = [&](uint32_t u, uint32_t j, bool active) {
+        bool cross = false;
+        uint32_t w = 0;
+        if (active) {
+          w = __ldg(g.dst + j);
+          const float upd = __ldcg(a.hub_upd + u);
+          const float prev = atomicAdd(a.r + w, upd);
+          cross = prev + upd > a.eps && prev < a.eps;
+        }
+        push(cross, w);
+      };
+      expand_hubs(team, g, hin, nbig, hub_edge);
+    }
+    // regular worklist: a lane per vertex (exchange once), edges per lane or
+    // per warp for degree > kWarpDegree
+    for (uint32_t base = (tid >> 5) * 32u; base < nreg; base += nthreads) {
+      const uint32_t i = base + lane;
+      uint32_t u = 0, b = 0, e = 0;
+      float upd = 0.f;
+      if (i < nreg) {
+        u = __ldcg(qin + i);
+        b = __ldg(g.row + u);
+        e = __ldg(g.row + u + 1);
+        const float res = atomicExch(a.r + u, 0.f);
+        atomicAdd(a.p + u, res);
+        upd = e > b ? res * a.alpha / (float)(e - b) : 0.f;
+      }
+      const uint32_t deg = e - b;
+      uint32_t coop = __ballot_sync(0xffffffffu, deg > kWarpDegree);
+      while (coop) {
+        const int src = __ffs(coop) - 1;
+        coop &= coop - 1;
+        const uint32_t bb = __shfl_sync(0xffffffffu, b, src), ee = __shfl_sync(0xffffffffu, e, src);
+        const float uu = __shfl_sync(0xffffffffu, upd, src);
+        for (uint32_t j0 = bb; j0 < ee; j0 += 32) {
+          const uint32_t j = j0 + lane;
+          bool cross = false;
+          uint32_t w = 0;
+          if (j < ee) {
+            w = __ldg(g.dst + j);
+            const float prev = atomicAdd(a.r + w, uu);
+            cross = prev + uu > a.eps && prev < a.eps;
+          }
+          push(cross, w);
+        }
+      }
+      const uint32_t mine = deg <= kWarpDegree ? deg : 0u;
+      const uint32_t kmax = warp_max_u32(mine);
+      for (uint32_t k = 0; k < kmax; ++k) {
+        bool cross = false;
+        uint32_t w = 0;
+        if (k < mine) {
+          w = __ldg(g.dst + b + k);
+          const float prev = atomicAdd(a.r + w, upd);
+          cross = prev + upd > a.eps && prev < a.eps;
+        }
+        push(cross, w);
+      }
+    }
+    ok = bar.sync();
+  }
+  const unsigned long long ws = warp_sum_u64(pushes);
+  if (lane == 0 && ws) atomicAdd(a.out_edges, ws);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.out[0] = round;
+    a.out[3] = ok ? 0u : 1u;
+  }
+  bar.finish();
+}
+
 template <template <int> class K>
 struct Dummy {};
 
@@ -866,6 +1050,7 @@ struct Dummy {};
 const void* bfs_fn(int v) { return GSRB_GRAPH_FN(bfs_kernel)(v); }
 const void* sssp_fn(int v) { return GSRB_GRAPH_FN(sssp_kernel)(v); }
 const void* pr_fn(int v) { return GSRB_GRAPH_FN(pagerank_kernel)(v); }
+const void* prr_fn(int v) { return GSRB_GRAPH_FN(pr_residual_kernel)(v); }
 const void* batch_fn(int v) {
   switch (v) {  // variants without hardware cluster barriers (teams may be single CTAs)
     case gsrb::V_SOFT2: return (const void*)batch_kernel<gsrb::V_SOFT2>;
@@ -1232,6 +1417,48 @@ gsrb_status_t gsrb_pagerank(gsrb_ctx_t ctx, gsrb_graph_t G, float alpha, int32_t
   std::lock_guard<std::mutex> g(ctx->mu);
   GSRB_CUDA(cudaMemsetAsync(G->flags, 0, 128, ctx->stream));
   if (G->nhubs) GSRB_CUDA(cudaMemsetAsync(G->hub_done, 0, sizeof(uint32_t) * G->nhubs, ctx->stream));
+  gsrb::GridBarrier gb = make_barrier(ctx, c, 0, (uint32_t)grid, 0, 0);
+  void* args[] = {&gb, &a};
+  if (!ctx->events[62]) GSRB_CUDA(cudaEventCreate(&ctx->events[62]));
+  if (!ctx->events[63]) GSRB_CUDA(cudaEventCreate(&ctx->events[63]));
+  GSRB_CUDA(cudaEventRecord(ctx->events[62], ctx->stream));
+  gsrb_status_t st = launch_persistent(ctx, fn, grid, c.threads, 0, c.cluster, coop_of(c), args);
+  if (st) return st;
+  GSRB_CUDA(cudaEventRecord(ctx->events[63], ctx->stream));
+  GSRB_CUDA(cudaEventSynchronize(ctx->events[63]));
+  float ms = 0;
+  GSRB_CUDA(cudaEventElapsedTime(&ms, ctx->events[62], ctx->events[63]));
+  return finish_stats(G, stats, ms);
+}
+
+gsrb_status_t gsrb_pagerank_residual(gsrb_ctx_t ctx, gsrb_graph_t G, float alpha, float epsilon, int32_t max_iters,
+                                     float* d_rank, const gsrb_cfg_t* cfgin, gsrb_traversal_stats_t* stats) {
+  if (!ctx || !G || !d_rank || max_iters < 0 || !(alpha >= 0.f && alpha < 1.f) || !(epsilon > 0.f))
+    return GSRB_ERR_ARG;
+  gsrb_cfg_t c = graph_cfg(ctx, cfgin);
+  const void* fn = prr_fn(c.variant);
+  if (!fn) return GSRB_ERR_UNSUPPORTED;
+  const int grid = grid_of(ctx, c);
+  if (grid % c.cluster || c.threads % 32) return GSRB_ERR_ARG;
+  PrrArgs a;
+  a.g = dev_csr(G);
+  a.alpha = alpha;
+  a.eps = epsilon;
+  a.max_iters = max_iters;
+  a.p = d_rank;
+  a.r = G->contrib[0];
+  a.hub_upd = G->contrib[1];
+  a.mark = G->mark;
+  a.q[0] = G->q[0];
+  a.q[1] = G->q[1];
+  a.hq[0] = G->hq[0];
+  a.hq[1] = G->hq[1];
+  a.cnt = G->cnt;
+  a.overflow = G->flags;
+  a.out = G->flags + 4;
+  a.out_edges = (unsigned long long*)((char*)G->flags + 64);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  GSRB_CUDA(cudaMemsetAsync(G->flags, 0, 128, ctx->stream));
   gsrb::GridBarrier gb = make_barrier(ctx, c, 0, (uint32_t)grid, 0, 0);
   void* args[] = {&gb, &a};
   if (!ctx->events[62]) GSRB_CUDA(cudaEventCreate(&ctx->events[62]));

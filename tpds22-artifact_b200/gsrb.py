@@ -160,6 +160,7 @@ _SIGS = {
     "gsrb_bfs": (C.c_int32, [_P, _P, C.c_uint32, _P, C.c_int32, C.POINTER(Cfg), C.c_void_p]),
     "gsrb_sssp": (C.c_int32, [_P, _P, C.c_uint32, _P, C.c_int32, C.POINTER(Cfg), C.c_void_p]),
     "gsrb_pagerank": (C.c_int32, [_P, _P, C.c_float, C.c_int32, _P, C.POINTER(Cfg), C.c_void_p]),
+    "gsrb_pagerank_residual": (C.c_int32, [_P, _P, C.c_float, C.c_float, C.c_int32, _P, C.POINTER(Cfg), C.c_void_p]),
     "gsrb_batch_create": (C.c_int32, [_P, _P, C.c_int32, C.POINTER(Cfg), C.POINTER(_P)]),
     "gsrb_batch_free": (C.c_int32, [_P]),
     "gsrb_batch_layout": (C.c_int32, [_P, _P, _P]),
@@ -461,6 +462,13 @@ class DeviceGraph:
         st = TraversalStats()
         rc = _lib().gsrb_pagerank(self.ctx.h, self.h, alpha, iters, out.ptr,
                                   C.byref(c) if c is not None else None, C.addressof(st))
+        return rc, st
+
+    def pagerank_residual(self, out: DeviceArray, alpha: float = 0.85, epsilon: float = 1e-6,
+                          max_iters: int = 2**31 - 1, c: Cfg | None = None):
+        st = TraversalStats()
+        rc = _lib().gsrb_pagerank_residual(self.ctx.h, self.h, alpha, epsilon, max_iters, out.ptr,
+                                           C.byref(c) if c is not None else None, C.addressof(st))
         return rc, st
 
 
