@@ -43,7 +43,7 @@ def test_cfg_default_matches_header(gsrb):
     assert c.variant == gsrb.BAR_CLUSTER and c.cluster == 2 and c.ctas_per_sm == 2 and c.threads == 256
     assert c.timeout_ms == 2000 and c.launch_mode == 1 and c.tile == 0
     # every variant has a name; the status strings are defined for every code
-    for v in range(12):
+    for v in range(13):
         assert v in gsrb.VARIANT_NAMES
     for st in range(0, -11, -1):
         s = gsrb.lib().gsrb_status_string(st)
@@ -155,3 +155,36 @@ def test_dist_max_over_ranks_gloo():
         p.join(timeout=120)
         assert p.exitcode == 0
     assert got == {0: 20.0, 1: 20.0}
+
+
+def _fake_trace(gsrb, nfs, mfs):
+    tr = np.zeros(len(nfs), dtype=gsrb.TRACE_DTYPE)
+    tr["level"] = np.arange(1, len(nfs) + 1)
+    tr["nf"] = nfs
+    tr["mf"] = mfs
+    tr["nu"] = 1000 - np.cumsum(nfs)
+    tr["mu"] = 16000 - np.cumsum(mfs)
+    tr["t_ns"] = np.cumsum([0] + [100] * (len(nfs) - 1))
+    return tr
+
+
+def test_trace_files_roundtrip_and_labels(gsrb, pol, tmp_path):
+    push = _fake_trace(gsrb, [1, 10, 300, 50], [16, 160, 4800, 800])
+    rec = {"n": 1000, "m": 16000, "src": 0, "push": push, "pull": push.copy(), "topo": push.copy(),
+           "push_ns": np.array([100.0, 900.0, 4000.0, np.nan]),
+           "pull_ns": np.array([5000.0, 1000.0, 400.0, np.nan]),
+           "topo_ns": np.array([300.0, 900.0, 8000.0, np.nan])}
+    path = tmp_path / "traces.npz"
+    pol.save_traces(path, [rec, rec])
+    back = pol.load_traces(path)
+    assert len(back) == 2 and back[1]["n"] == 1000 and np.array_equal(back[0]["push"], push)
+    X, Y, M = pol.dataset(back)
+    assert X.shape == (8, 12) and Y.shape == (8, 4)
+    # level 1 (index 0): no pull label (the first level is always a push)
+    assert M[0, 0] == 0.0
+    # level 3: pull 10x faster -> label 1, weight log2(10)
+    assert Y[2, 0] == 1.0 and M[2, 0] == pytest.approx(math.log2(10))
+    # level 2: pull 1.1x slower -> label 0, small weight
+    assert Y[1, 0] == 0.0 and M[1, 0] < 0.2
+    # next-frontier regression target
+    assert Y[0, 2] == pytest.approx(math.log2(11)) and Y[3, 2] == 0.0

@@ -50,13 +50,14 @@ def _weight(t_a: float, t_b: float) -> float:
     return float(min(4.0, max(0.05, r)))
 
 
-def collect(ctx, dgraph, src: int = 0, reps: int = 1):
-    """Per-level features, labels and masks of one graph from three traversals."""
+def collect_traces(ctx, dgraph, src: int = 0, reps: int = 1) -> dict:
+    """Raw material of one graph: the per-level trace of the worklist push, the
+    pull and the topology push traversals (the fastest of `reps` runs per
+    level) and the graph's size.  Storable with save_traces."""
     g = _g()
-    n, m = dgraph.n, dgraph.m
-    out = ctx.array(n, np.int32)
-    traces = {}
-    for mode in (g.BFS_PUSH, g.BFS_PULL, g.BFS_TOPO):
+    out = ctx.array(dgraph.n, np.int32)
+    rec = {"n": int(dgraph.n), "m": int(dgraph.m), "src": int(src)}
+    for name, mode in (("push", g.BFS_PUSH), ("pull", g.BFS_PULL), ("topo", g.BFS_TOPO)):
         best = None
         for _ in range(reps):
             rc, st = dgraph.bfs(src, out, mode)
@@ -64,10 +65,19 @@ def collect(ctx, dgraph, src: int = 0, reps: int = 1):
             tr = dgraph.trace()
             d = level_times(tr)
             best = d if best is None else np.fmin(best, d)
-        traces[mode] = (tr, best)
-    tr, t_push = traces[g.BFS_PUSH]
-    _, t_pull = traces[g.BFS_PULL]
-    _, t_topo = traces[g.BFS_TOPO]
+        rec[name] = tr
+        rec[name + "_ns"] = best
+    out.free()
+    return rec
+
+
+def features_labels(rec: dict):
+    """Per-level features, labels and cost-sensitive masks from one graph's
+    traces (collect_traces or load_traces)."""
+    g = _g()
+    n, m = rec["n"], rec["m"]
+    tr = rec["push"]
+    t_push, t_pull, t_topo = rec["push_ns"], rec["pull_ns"], rec["topo_ns"]
     L = len(tr)
     X = np.zeros((L, 12), np.float32)
     Y = np.zeros((L, 4), np.float32)
@@ -78,17 +88,56 @@ def collect(ctx, dgraph, src: int = 0, reps: int = 1):
         X[i] = g.level_features(n, m, int(r["level"]), int(r["nf"]), int(r["mf"]), int(r["nu"]), int(r["mu"]),
                                 prev_nf, prev_dir)
         prev_nf = int(r["nf"])
-        if np.isfinite(t_push[i]) and np.isfinite(t_pull[i]) and i > 0:
+        if i < len(t_pull) and np.isfinite(t_push[i]) and np.isfinite(t_pull[i]) and i > 0:
             Y[i, 0] = 1.0 if t_pull[i] < t_push[i] else 0.0
             M[i, 0] = _weight(t_push[i], t_pull[i])
-        if np.isfinite(t_push[i]) and np.isfinite(t_topo[i]):
+        if i < len(t_topo) and np.isfinite(t_push[i]) and np.isfinite(t_topo[i]):
             Y[i, 1] = 1.0 if t_topo[i] < t_push[i] else 0.0
             M[i, 1] = _weight(t_push[i], t_topo[i])
         nxt = int(tr[i + 1]["nf"]) if i + 1 < L else 0
         Y[i, 2] = np.log2(1.0 + nxt)
         M[i, 2] = 1.0
         prev_dir = 1 if Y[i, 0] > 0.5 and M[i, 0] > 0 else 0
-    return X, Y, M, {"push": t_push, "pull": t_pull, "topo": t_topo}
+    return X, Y, M
+
+
+def collect(ctx, dgraph, src: int = 0, reps: int = 1):
+    """Per-level features, labels and masks of one graph from three traversals."""
+    rec = collect_traces(ctx, dgraph, src, reps)
+    X, Y, M = features_labels(rec)
+    return X, Y, M, {"push": rec["push_ns"], "pull": rec["pull_ns"], "topo": rec["topo_ns"]}
+
+
+def save_traces(path, recs) -> None:
+    """Store the traces of several graphs in one .npz (offline training and
+    replay, in the spirit of the reference's Worklist::save/load,
+    LONESTAR/rt/include/worklist.h.prehip:183-220)."""
+    arrays = {"count": np.array([len(recs)], np.int64)}
+    for k, rec in enumerate(recs):
+        arrays[f"g{k}_meta"] = np.array([rec["n"], rec["m"], rec["src"]], np.int64)
+        for name in ("push", "pull", "topo"):
+            arrays[f"g{k}_{name}"] = rec[name]
+            arrays[f"g{k}_{name}_ns"] = np.asarray(rec[name + "_ns"], np.float64)
+    np.savez_compressed(path, **arrays)
+
+
+def load_traces(path) -> list:
+    z = np.load(path)
+    recs = []
+    for k in range(int(z["count"][0])):
+        n, m, src = (int(x) for x in z[f"g{k}_meta"])
+        rec = {"n": n, "m": m, "src": src}
+        for name in ("push", "pull", "topo"):
+            rec[name] = z[f"g{k}_{name}"]
+            rec[name + "_ns"] = z[f"g{k}_{name}_ns"]
+        recs.append(rec)
+    return recs
+
+
+def dataset(recs):
+    """Stacked (X, Y, M) of many graphs' traces."""
+    parts = [features_labels(r) for r in recs]
+    return tuple(np.concatenate([p[i] for p in parts]) for i in range(3))
 
 
 def train(ctx, X, Y, M, steps: int = 3000, lr: float = 3e-3, seed: int = 2022):
