@@ -21,6 +21,8 @@
 // Include in exactly the translation units that launch the kernels (like the
 // reference's #include "cudaLocks*.cu"), and link libgsrb.so for the host API.
 #pragma once
+#include <cstddef>
+
 #include "gsrb/barrier.cuh"
 #include "gsrb/cudaLocks.h"
 #include "gsrb/locks.cuh"
@@ -207,6 +209,19 @@ inline __device__ void cudaSemaphoreEBOPostPriority(const cudaSemaphore_t sem, c
   (void)maxSemCount;
   gsrb::psem_post(gsrb::PrioritySem{gsrb_sem_rec(sem, semaphoreBuffers, NUM_SM, 0)}, isWriter);
 }
+inline __device__ void cudaSemaphoreEBOWaitLocalPriority(const cudaSemaphore_t sem, const unsigned int smID,
+                                                         const bool isWriter, const unsigned int maxSemCount,
+                                                         unsigned int* semaphoreBuffers, const int NUM_SM) {
+  (void)maxSemCount;
+  gsrb::psem_wait(gsrb::PrioritySem{gsrb_sem_rec(sem, semaphoreBuffers, NUM_SM, smID)}, isWriter, semaphoreBuffers,
+                  GSRB_LOCKS_TIMEOUT_NS, 64);
+}
+inline __device__ void cudaSemaphoreEBOPostLocalPriority(const cudaSemaphore_t sem, const unsigned int smID,
+                                                         const bool isWriter, const unsigned int maxSemCount,
+                                                         unsigned int* semaphoreBuffers, const int NUM_SM) {
+  (void)maxSemCount;
+  gsrb::psem_post(gsrb::PrioritySem{gsrb_sem_rec(sem, semaphoreBuffers, NUM_SM, smID)}, isWriter);
+}
 
 // ------------------------------------------------------------------ barriers --
 // Stateless wrappers over the native barriers: `barrierBuffers` (allocated by
@@ -284,4 +299,118 @@ inline __device__ void joinBarrier_helper(unsigned int* barrierBuffers, unsigned
   gsrb::GridSync<gsrb::V_TREE> b;
   const gsrb::GridBarrier gb = gsrb_compat_barrier(barrierBuffers, perSMBarrierBuffers, numBlocksAtBarr, gridDim.x);
   if (b.init(gb, &s_bar)) b.sync();
+}
+
+// Flat lock-free flag barrier (Heterosync/cudaLocksBarrierFast.cu:182-224): CTA
+// 0 collects the in flags of CTAs 0 .. numBlocksAtBarr-1 and releases their out
+// flags; the global flags sit where joinLFBarrier_helper keeps them.
+inline __device__ void cudaBarrier(unsigned int* barrierBuffers, const int arrayStride,
+                                   const unsigned int numBlocksAtBarr) {
+  const gsrb::GridBarrier gb = gsrb_compat_barrier(barrierBuffers + 2 * arrayStride, nullptr, 0, gridDim.x);
+  gsrb::detail::lf_episode(barrierBuffers, barrierBuffers + arrayStride, numBlocksAtBarr, blockIdx.x, gb, 0u,
+                           [] { return true; });
+}
+// Per-SM lock-free flag barrier (Heterosync/cudaLocksBarrierFast.cu:226-293):
+// the numTBs_perSM CTAs of group smID meet on the group's in/out flags; with
+// isLocalGlobalBarr the group's first CTA joins the flat barrier in between.
+inline __device__ void cudaBarrierLocal(unsigned int* barrierBuffers, const unsigned int numBlocksAtBarr,
+                                        const int arrayStride, unsigned int* perSMBarrierBuffers,
+                                        const unsigned int smID, const unsigned int numTBs_perSM,
+                                        const unsigned int perSM_blockID, const bool isLocalGlobalBarr,
+                                        const int MAX_BLOCKS) {
+  const gsrb::GridBarrier gb = gsrb_compat_barrier(barrierBuffers + 2 * arrayStride, nullptr, 0, gridDim.x);
+  unsigned int* lin = perSMBarrierBuffers + (size_t)MAX_BLOCKS * smID * 2;
+  gsrb::detail::lf_episode(lin, lin + MAX_BLOCKS, numTBs_perSM, perSM_blockID, gb, 0u, [&] {
+    if (!isLocalGlobalBarr) return true;
+    return gsrb::detail::lf_episode(barrierBuffers, barrierBuffers + arrayStride, numBlocksAtBarr, smID, gb, 0u,
+                                    [] { return true; });
+  });
+}
+// Heterosync/cudaLocksBarrierFast.cu:295-313.
+inline __device__ void cudaBarrierLocalGlobal(unsigned int* barrierBuffers, const unsigned int numBlocksAtBarr,
+                                              const int arrayStride, unsigned int* perSMBarrierBuffers,
+                                              const unsigned int smID, const unsigned int numTBs_perSM,
+                                              const unsigned int perSM_blockID, const int MAX_BLOCKS) {
+  cudaBarrierLocal(barrierBuffers, numBlocksAtBarr, arrayStride, perSMBarrierBuffers, smID, numTBs_perSM,
+                   perSM_blockID, true, MAX_BLOCKS);
+}
+
+// Every thread of every CTA arrives (Heterosync/cudaLocksBarrierAtomicSRB.cu:242-256,
+// numThreadsAtBarr = gridDim.x * blockDim.x): each thread adds one to the global
+// counter; the last arrival resets it and bumps the generation word, which
+// every thread polls (bounded).
+inline __device__ void joinBarrier_helperNaiveAllSRB(unsigned int* barrierBuffers, unsigned int* perSMBarrierBuffers,
+                                                     const unsigned int numThreadsAtBarr, const int smID,
+                                                     const int MAX_BLOCKS) {
+  (void)perSMBarrierBuffers; (void)smID; (void)MAX_BLOCKS;
+  const gsrb::GridBarrier gb = gsrb_compat_barrier(barrierBuffers, nullptr, 0, gridDim.x);
+  __syncthreads();
+  const uint32_t gen = gsrb::ptx::ld_relaxed_gpu(&gb.slot->epoch);
+  gsrb::ptx::fence_acq_rel_gpu();
+  if (gsrb::ptx::atom_add_relaxed_gpu(&gb.slot->count, 1u) == numThreadsAtBarr - 1u) {
+    gsrb::ptx::fence_acq_rel_gpu();
+    gsrb::ptx::st_relaxed_gpu(&gb.slot->count, 0u);
+    gsrb::ptx::st_release_gpu(&gb.slot->epoch, gen + 1u);
+  } else {
+    gsrb::detail::wait_ne(&gb.slot->epoch, gen, gb, 0u);
+  }
+  __syncthreads();
+}
+
+// ------------------------------------------------------------ local barriers --
+// Status of the barriers that get no lock buffer (the per-SM local barriers
+// below): one slot per translation unit, read and cleared on the host with
+// gsrb_cudalocks_local_status().
+static __device__ gsrb::BarrierSlot gsrb_local_status_slot;
+
+// Per-group counter barrier of the local-exchange steps
+// (Heterosync/cudaLocksBarrierAtomic.cu:82-140, cudaLocksBarrierAtomicSRB.cu:133-190):
+// the numTBs_thisSM CTAs of group smID meet on a counter and a generation word
+// of their own.  Group smID's record is the gsrb::GroupSlot at index
+// MAX_BLOCKS + smID of the per-SM area (count = arrivals, count2 = generation):
+// past the group slots of the two-level grid barriers (fewer than NUM_SM <=
+// MAX_BLOCKS of them), and inside the harness's NUM_SM * MAX_BLOCKS * 2 words
+// whenever NUM_SM >= 64 and MAX_BLOCKS >= 64.
+inline __device__ void gsrb_compat_local_barrier(unsigned int* perSMBarrierBuffers, const unsigned int smID,
+                                                 const unsigned int numTBs_thisSM, const int MAX_BLOCKS) {
+  gsrb::GroupSlot* rec = reinterpret_cast<gsrb::GroupSlot*>(perSMBarrierBuffers) + (size_t)MAX_BLOCKS + smID;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const gsrb::GridBarrier gb =
+        gsrb_compat_barrier(reinterpret_cast<unsigned int*>(&gsrb_local_status_slot), nullptr, 0, numTBs_thisSM);
+    const uint32_t gen = gsrb::ptx::ld_relaxed_gpu(&rec->count2);
+    gsrb::ptx::fence_acq_rel_gpu();
+    if (gsrb::ptx::atom_add_relaxed_gpu(&rec->count, 1u) == numTBs_thisSM - 1u) {
+      gsrb::ptx::fence_acq_rel_gpu();
+      gsrb::ptx::st_relaxed_gpu(&rec->count, 0u);
+      gsrb::ptx::st_release_gpu(&rec->count2, gen + 1u);
+    } else {
+      gsrb::detail::wait_ne(&rec->count2, gen, gb, smID);
+    }
+  }
+  __syncthreads();
+}
+// Heterosync/cudaLocksBarrierAtomic.cu:125-140.
+inline __device__ void cudaBarrierAtomicLocal(unsigned int* perSMBarrierBuffers, const unsigned int smID,
+                                              const unsigned int numTBs_thisSM, const bool isMasterThread,
+                                              const int MAX_BLOCKS) {
+  (void)isMasterThread;
+  gsrb_compat_local_barrier(perSMBarrierBuffers, smID, numTBs_thisSM, MAX_BLOCKS);
+}
+// Heterosync/cudaLocksBarrierAtomicSRB.cu:179-190.
+inline __device__ void cudaBarrierAtomicLocalSRB(unsigned int* perSMBarrierBuffers, const unsigned int smID,
+                                                 const unsigned int numTBs_thisSM, const bool isMasterThread,
+                                                 const int MAX_BLOCKS) {
+  (void)isMasterThread;
+  gsrb_compat_local_barrier(perSMBarrierBuffers, smID, numTBs_thisSM, MAX_BLOCKS);
+}
+// Synchronous: the first status code a local barrier of this translation unit
+// recorded (0 = none; ~0u if the slot could not be read), then cleared.
+static inline unsigned int gsrb_cudalocks_local_status() {
+  unsigned int st = 0;
+  const unsigned int zero = 0;
+  const size_t off = offsetof(gsrb::BarrierSlot, status);
+  if (cudaMemcpyFromSymbol(&st, gsrb_local_status_slot, sizeof st, off) != cudaSuccess) return ~0u;
+  if (st != 0 && cudaMemcpyToSymbol(gsrb_local_status_slot, &zero, sizeof zero, off) != cudaSuccess) return ~0u;
+  return st;
 }

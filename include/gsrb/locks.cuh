@@ -146,7 +146,16 @@ __device__ __forceinline__ void mutex_sleep_unlock(int32_t* ring, uint32_t slot,
 // Reference-protocol semaphore (lock word + count + writerWaiting [+ priority]):
 // record words [count, lock, writerWaiting, max, priority].  `priority` selects
 // the TPDS'22 priority variant (waiters stand back while posts are pending),
-// `backoff` the EBO flavour.
+// `backoff` the EBO flavour.  The EBO backoff is asymmetric as in the reference
+// (Heterosync/cudaLocksSemaphoreEBO.cu:160-181): a failing writer doubles its
+// pause up to MAX_BACKOFF - 1 loop iterations, a failing reader adds 5; at about
+// 16 ns per iteration that is a 16 us cap for writers and an 80 ns step for
+// readers.  (Equal pauses for both let the readers' retries keep the count
+// below max for seconds at 296 CTAs.)  A reader first checks writerWaiting and
+// the count with plain loads and takes the lock word only when it could enter:
+// the attempt it skips would have changed nothing.
+constexpr uint32_t kSemWriterBackoffCapNs = 16383;
+constexpr uint32_t kSemReaderBackoffStepNs = 80;
 struct RefSem {
   uint32_t* rec;
   __device__ __forceinline__ uint32_t* count() const { return rec; }
@@ -173,7 +182,9 @@ __device__ __forceinline__ bool refsem_wait(RefSem s, bool is_writer, uint32_t m
         if (!ok) break;
       }
       bool entered = false;
-      if (ptx::atom_cas_acquire_gpu(s.lockw(), 0u, 1u) == 0u) {
+      const bool hopeless = !is_writer && (ptx::ld_relaxed_gpu(s.writer_waiting()) != 0u ||
+                                           ptx::ld_relaxed_gpu(s.count()) <= 1u);
+      if (!hopeless && ptx::atom_cas_acquire_gpu(s.lockw(), 0u, 1u) == 0u) {
         const uint32_t c = ptx::ld_relaxed_gpu(s.count());
         if (is_writer) {
           if (c == max_count) {
@@ -191,7 +202,11 @@ __device__ __forceinline__ bool refsem_wait(RefSem s, bool is_writer, uint32_t m
       }
       if (entered) break;
       if (!w.tick()) { ok = false; break; }
-      if (backoff) { __nanosleep(b); b = (b << 1) < kMaxBackoffNs ? (b << 1) : kMaxBackoffNs; }
+      if (backoff) {
+        __nanosleep(b);
+        if (is_writer) b = 2u * b + 1u < kSemWriterBackoffCapNs ? 2u * b + 1u : kSemWriterBackoffCapNs;
+        else b += kSemReaderBackoffStepNs;
+      }
     }
     if (!ok) lock_record_timeout(buf);
   }
