@@ -135,3 +135,12 @@ def test_uniq_semaphore_kernels(orc, tmp_path, ctx, nsm, prim):
 def test_local_exchange_needs_equal_groups(tmp_path, ctx, nsm):
     p, _ = _run(["atomicTreeBarrUniqLocalExchSRB", 4, 2 * nsm + 1, 1], tmp_path)
     assert p.returncode != 0 and "multiple of" in p.stderr
+
+
+@pytest.mark.gpu
+def test_banner_lines_match_the_reference(orc, tmp_path, ctx):
+    # Heterosync/main.cu:2670,2702,2734 print size 2 for the size-120 spin semaphores
+    out, _ = _check(orc, tmp_path, 11, "spinSem120", 8, 8, 1, 1)
+    assert "\nspin_lock_sem_002_001\n" in out
+    out, _ = _check(orc, tmp_path, 37, "atomicTreeBarrUniqSRB", 8, 8, 1, 1)
+    assert "\natomic_tree_barrier_SRB_001\n" in out
