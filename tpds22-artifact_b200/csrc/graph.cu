@@ -68,10 +68,10 @@ __device__ __noinline__ void bfs_solo(const BfsArgs& a, uint32_t L, uint32_t nre
   const Team one{0u, 1u};
   uint32_t levels = 0;
   for (;;) {
-    const uint32_t* qin = a.q[(L - 1) & 1];
-    const uint32_t* hin = a.hq[(L - 1) & 1];
-    uint32_t* qout = a.q[L & 1];
-    uint32_t* hout = a.hq[L & 1];
+    const uint2* qin = reinterpret_cast<const uint2*>(a.q[(L - 1) & 1]);
+    const uint2* hin = reinterpret_cast<const uint2*>(a.hq[(L - 1) & 1]);
+    uint2* qout = reinterpret_cast<uint2*>(a.q[L & 1]);
+    uint2* hout = reinterpret_cast<uint2*>(a.hq[L & 1]);
     if (threadIdx.x == 0) {
       s_c.n_reg = 0;
       s_c.n_big = 0;
@@ -81,19 +81,24 @@ __device__ __noinline__ void bfs_solo(const BfsArgs& a, uint32_t L, uint32_t nre
     unsigned long long m_acc = 0;
     const int32_t Li = (int32_t)L;
     auto push_edge = [&](uint32_t, uint32_t j, bool active) {
-      uint32_t v = 0, d = 0;
+      uint2 r = make_uint2(0u, 0u);
       bool disc = false;
       if (active) {
-        v = __ldg(g.dst + j);
+        const uint32_t v = __ldg(g.dst + j);
         if (__ldcg(a.level + v) == kInf) disc = atomicCAS(a.level + v, kInf, Li) == kInf;
-        if (disc) d = __ldg(g.row + v + 1) - __ldg(g.row + v);
+        if (disc) r = make_uint2(__ldg(g.row + v), __ldg(g.row + v + 1));
       }
-      warp_append(disc && d <= kBigDegree, v, qout, &s_c.n_reg, g.n, a.overflow);
-      warp_append(disc && d > kBigDegree, v, hout, &s_c.n_big, g.n, a.overflow);
+      const uint32_t d = r.y - r.x;
+      warp_append(disc && d <= kBigDegree, r, qout, &s_c.n_reg, g.n, a.overflow);
+      warp_append(disc && d > kBigDegree, r, hout, &s_c.n_big, g.n, a.overflow);
       m_acc += d;
     };
-    expand_hubs(one, g, hin, nbig, push_edge);
-    expand_queue(one, g, qin, nreg, push_edge);
+    expand_hub_ranges(one, hin, nbig, push_edge);
+    const PushSink sink{qout, hout, &s_c.n_reg, &s_c.n_big, g.n, a.overflow};
+    auto lanes = [&](uint32_t b, uint32_t mine, uint32_t kmax) {
+      bfs_push_lanes(g, a.level, Li, b, mine, kmax, false, sink, m_acc);
+    };
+    expand_range_queue(one, qin, nreg, push_edge, lanes);
     const unsigned long long ws = warp_sum_u64(m_acc);
     if (lane_id() == 0 && ws) atomicAdd(&s_c.m_next, ws);
     __syncthreads();
@@ -159,8 +164,7 @@ __device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const B
   const uint32_t dsrc = g.row[a.src + 1] - g.row[a.src];
   if (tid == 0) {
     const bool hub = dsrc > kBigDegree;
-    if (hub) a.hq[0][0] = a.src;
-    else a.q[0][0] = a.src;
+    reinterpret_cast<uint2*>(hub ? a.hq[0] : a.q[0])[0] = make_uint2(g.row[a.src], g.row[a.src + 1]);
     a.cnt[0].n_reg = hub ? 0 : 1;
     a.cnt[0].n_big = hub ? 1 : 0;
     a.cnt[0].m_next = dsrc;
@@ -271,19 +275,20 @@ __device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const B
       continue;
     }
 
-    const uint32_t* qin = a.q[(L - 1) & 1];
-    const uint32_t* hin = a.hq[(L - 1) & 1];
-    uint32_t* qout = a.q[L & 1];
-    uint32_t* hout = a.hq[L & 1];
+    const uint2* qin = reinterpret_cast<const uint2*>(a.q[(L - 1) & 1]);
+    const uint2* hin = reinterpret_cast<const uint2*>(a.hq[(L - 1) & 1]);
+    uint2* qout = reinterpret_cast<uint2*>(a.q[L & 1]);
+    uint2* hout = reinterpret_cast<uint2*>(a.hq[L & 1]);
     LevelCounters* c = &a.cnt[L % 3];
     unsigned long long m_acc = 0;
     const int32_t Li = (int32_t)L;
 
     auto discover = [&](bool disc, uint32_t v) {
-      uint32_t d = 0;
-      if (disc) d = __ldg(g.row + v + 1) - __ldg(g.row + v);
-      warp_append(disc && d <= kBigDegree, v, qout, &c->n_reg, g.n, a.overflow);
-      warp_append(disc && d > kBigDegree, v, hout, &c->n_big, g.n, a.overflow);
+      uint2 r = make_uint2(0u, 0u);
+      if (disc) r = make_uint2(__ldg(g.row + v), __ldg(g.row + v + 1));
+      const uint32_t d = r.y - r.x;
+      warp_append(disc && d <= kBigDegree, r, qout, &c->n_reg, g.n, a.overflow);
+      warp_append(disc && d > kBigDegree, r, hout, &c->n_big, g.n, a.overflow);
       m_acc += d;
     };
     auto push_edge = [&](uint32_t, uint32_t j, bool active) {
@@ -297,11 +302,16 @@ __device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const B
     };
 
     if (dir == DIR_PUSH) {
-      expand_hubs(team, g, hin, nbig, push_edge);
-      expand_queue(team, g, qin, nreg, push_edge);
+      expand_hub_ranges(team, hin, nbig, push_edge);
+      const PushSink sink{qout, hout, &c->n_reg, &c->n_big, g.n, a.overflow};
+      const bool precheck = nf > kPushPrecheckFrontier;
+      auto lanes = [&](uint32_t b, uint32_t mine, uint32_t kmax) {
+        bfs_push_lanes(g, a.level, Li, b, mine, kmax, precheck, sink, m_acc);
+      };
+      expand_range_queue(team, qin, nreg, push_edge, lanes);
     } else if (dir == DIR_TOPO) {
       // topology-driven push: scan every vertex, expand those at level L - 1
-      expand_hubs(team, g, hin, nbig, push_edge);
+      expand_hub_ranges(team, hin, nbig, push_edge);
       const uint32_t lane = lane_id();
       const uint32_t gw = tid >> 5, nw = nthreads >> 5;
       for (uint32_t base = gw * 32u; base < g.n; base += nw * 32u) {
@@ -1110,8 +1120,9 @@ gsrb_status_t graph_scratch(gsrb_graph* G) {
   const size_t n = G->n;
   cudaError_t e = cudaSuccess;
   for (int k = 0; k < 2 && !e; ++k) {
-    e = dalloc(&G->q[k], n);
-    if (!e) e = dalloc(&G->hq[k], n);
+    // 2n words: BFS keeps an edge range (two words) per queued vertex
+    e = dalloc(&G->q[k], 2 * n);
+    if (!e) e = dalloc(&G->hq[k], 2 * n);
     if (!e) e = dalloc(&G->far[k], n);
     if (!e) e = dalloc(&G->contrib[k], n);
   }

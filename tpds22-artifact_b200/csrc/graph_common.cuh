@@ -73,8 +73,9 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 // Warp-aggregated append of `v` (where `pred`) to queue q with counter *cnt.
 // Must be called by all 32 lanes (warp-synchronous).  Returns nothing; the
 // queue capacity is checked by the caller's sizing (<= n distinct vertices).
-__device__ __forceinline__ void warp_append(bool pred, uint32_t v, uint32_t* q, unsigned long long* cnt,
-                                            uint32_t cap, uint32_t* overflow) {
+template <class T>
+__device__ __forceinline__ void warp_append(bool pred, T v, T* q, unsigned long long* cnt, uint32_t cap,
+                                            uint32_t* overflow) {
   const uint32_t mask = __ballot_sync(0xffffffffu, pred);
   if (!mask) return;
   const uint32_t leader = __ffs(mask) - 1;
@@ -91,9 +92,9 @@ __device__ __forceinline__ void warp_append(bool pred, uint32_t v, uint32_t* q, 
 // Warp-aggregated append of up to K values per lane (v[r] where pred[r]) with
 // ONE reservation on the counter for the whole warp: the K appends of a lane
 // step cost one atomic round trip instead of K.  Warp-synchronous.
-template <int K>
-__device__ __forceinline__ void warp_append_k(const bool* pred, const uint32_t* v, uint32_t* q,
-                                              unsigned long long* cnt, uint32_t cap, uint32_t* overflow) {
+template <int K, class T>
+__device__ __forceinline__ void warp_append_k(const bool* pred, const T* v, T* q, unsigned long long* cnt,
+                                              uint32_t cap, uint32_t* overflow) {
   uint32_t mask[K];
   uint32_t tot = 0;
 #pragma unroll
@@ -164,6 +165,137 @@ __device__ __forceinline__ void expand_queue(const Team& t, const DevCSR& g, con
     const uint32_t mine = deg <= kWarpDegree ? deg : 0u;
     const uint32_t kmax = warp_max_u32(mine);
     for (uint32_t k = 0; k < kmax; ++k) f(u, b + k, k < mine);
+  }
+}
+
+// BFS frontier queues hold each vertex's edge range {row[v], row[v+1]} instead
+// of v (the discoverer has loaded both to learn the degree anyway), so a level
+// starts on its edges without first looking the rows up: one dependent round
+// trip less per level.  Queues of n entries, 8 bytes each.
+//
+// Expand a range queue q[0, nq): ranges of more than kWarpDegree edges are
+// walked by the whole warp, calling f(0, edge, active) warp-synchronously; the
+// rest go to `lanes(b, mine, kmax)`, called by all 32 lanes once per 32-entry
+// group with the lane's first edge b, its edge count `mine` (0 for the warp's
+// ranges) and the warp's largest count, so that the callee can keep several of
+// a lane's edges in flight.
+template <class F, class FL>
+__device__ __forceinline__ void expand_range_queue(const Team& t, const uint2* __restrict__ q, uint32_t nq, F& f,
+                                                   FL& lanes) {
+  const uint32_t lane = lane_id();
+  const uint32_t gw = t.warp();
+  const uint32_t nwarps = t.nwarps();
+  for (uint32_t base = gw * 32u; base < nq; base += nwarps * 32u) {
+    const uint32_t i = base + lane;
+    uint32_t b = 0, e = 0;
+    if (i < nq) {
+      const uint2 r = __ldcg(q + i);
+      b = r.x;
+      e = r.y;
+    }
+    const uint32_t deg = e - b;
+    uint32_t coop = __ballot_sync(0xffffffffu, deg > kWarpDegree);
+    while (coop) {
+      const int src = __ffs(coop) - 1;
+      coop &= coop - 1;
+      const uint32_t bb = __shfl_sync(0xffffffffu, b, src);
+      const uint32_t ee = __shfl_sync(0xffffffffu, e, src);
+      for (uint32_t j0 = bb; j0 < ee; j0 += 32) {
+        const uint32_t j = j0 + lane;
+        f(0u, j, j < ee);
+      }
+    }
+    const uint32_t mine = deg <= kWarpDegree ? deg : 0u;
+    lanes(b, mine, warp_max_u32(mine));
+  }
+}
+
+// Expand a queue of hub ranges: every CTA takes an equal slice of every hub.
+template <class F>
+__device__ __forceinline__ void expand_hub_ranges(const Team& t, const uint2* __restrict__ hq, uint32_t nh, F& f) {
+  const uint32_t G = t.ncta;
+  for (uint32_t k = 0; k < nh; ++k) {
+    const uint2 r = __ldcg(hq + k);
+    const uint64_t len = r.y - r.x;
+    const uint32_t s0 = r.x + (uint32_t)(len * t.cta / G);
+    const uint32_t s1 = r.x + (uint32_t)(len * (t.cta + 1) / G);
+    for (uint32_t j0 = s0 + (threadIdx.x & ~31u); j0 < s1; j0 += blockDim.x) {
+      const uint32_t j = j0 + lane_id();
+      f(0u, j, j < s1);
+    }
+  }
+}
+
+// Where a BFS push step puts the vertices it discovers (as edge ranges).
+struct PushSink {
+  uint2* qout;                 // regular queue of the next level
+  uint2* hout;                 // hub queue of the next level
+  unsigned long long* n_reg;   // their counters (global, or shared in the one-CTA phase)
+  unsigned long long* n_big;
+  uint32_t cap;
+  uint32_t* overflow;
+};
+
+// Frontiers up to this size check a destination's level only through the
+// claim itself (compare-and-swap INF -> L) and load its row range alongside
+// the claim; larger ones read the level first and load rows only for claimed
+// vertices (throughput over latency).
+constexpr uint32_t kPushPrecheckFrontier = 16384;
+
+// BFS push over the lane-per-vertex edges of a 32-entry group, four edges per
+// lane in flight: the four destinations are loaded together, their claims are
+// issued together (with the row ranges of the candidates, or after a level
+// check when `precheck`), and the warp reserves queue space once per step for
+// all of them.  Small frontiers thus cost three dependent round trips per four
+// edges (destination, claim and rows, reservation) instead of five per edge.
+// Levels are the same as with one edge at a time (a vertex gets L from
+// whichever claim lands first); only the order of the next queue differs.
+// Warp-synchronous.
+__device__ __forceinline__ void bfs_push_lanes(const DevCSR& g, int32_t* level, int32_t Li, uint32_t b,
+                                               uint32_t mine, uint32_t kmax, bool precheck, const PushSink& s,
+                                               unsigned long long& m_acc) {
+  for (uint32_t k0 = 0; k0 < kmax; k0 += 4) {
+    uint32_t v[4];
+    uint32_t live = 0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      v[r] = 0;
+      if (k0 + r < mine) {
+        v[r] = __ldg(g.dst + b + k0 + r);
+        live |= 1u << r;
+      }
+    }
+    uint2 rg[4];
+    if (precheck) {
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        if (((live >> r) & 1u) && __ldcg(level + v[r]) != kInf) live &= ~(1u << r);
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        if (((live >> r) & 1u) && atomicCAS(level + v[r], kInf, Li) != kInf) live &= ~(1u << r);
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        rg[r] = ((live >> r) & 1u) ? make_uint2(__ldg(g.row + v[r]), __ldg(g.row + v[r] + 1)) : make_uint2(0u, 0u);
+    } else {
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        rg[r] = ((live >> r) & 1u) ? make_uint2(__ldg(g.row + v[r]), __ldg(g.row + v[r] + 1)) : make_uint2(0u, 0u);
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        if (((live >> r) & 1u) && atomicCAS(level + v[r], kInf, Li) != kInf) live &= ~(1u << r);
+    }
+    bool reg[4], big[4];
+    bool any_big = false;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const uint32_t d = ((live >> r) & 1u) ? rg[r].y - rg[r].x : 0u;
+      reg[r] = ((live >> r) & 1u) && d <= kBigDegree;
+      big[r] = ((live >> r) & 1u) && d > kBigDegree;
+      any_big |= big[r];
+      m_acc += d;
+    }
+    warp_append_k<4>(reg, rg, s.qout, s.n_reg, s.cap, s.overflow);
+    if (__any_sync(0xffffffffu, any_big)) warp_append_k<4>(big, rg, s.hout, s.n_big, s.cap, s.overflow);
   }
 }
 
