@@ -385,8 +385,8 @@ def bfs_runs(gsrb, ctx, orc, dg, g, params, cfg, reps=3):
     m_trav = orc.traversed_edges(g, want)
     res = {"m_traversed": m_trav}
     dg.set_policy(params)
-    for name, mode in (("plain_push", gsrb.BFS_PUSH), ("heuristic", gsrb.BFS_HEURISTIC),
-                       ("learned", gsrb.BFS_LEARNED)):
+    for name, mode in (("plain_push", gsrb.BFS_PUSH), ("push_load_balanced", gsrb.BFS_PUSH | gsrb.BFS_FLAG_LB),
+                       ("heuristic", gsrb.BFS_HEURISTIC), ("learned", gsrb.BFS_LEARNED)):
         ts = []
         for _ in range(reps):
             rc, st = dg.bfs(0, out, mode, cfg)

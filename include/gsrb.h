@@ -258,7 +258,12 @@ enum {
   GSRB_BFS_HEURISTIC = 1, /* direction-optimizing with the fixed Beamer thresholds (alpha 15, beta 18) */
   GSRB_BFS_LEARNED = 2,   /* the policy network decides; falls back to the heuristic after a 2x miss */
   GSRB_BFS_PULL = 3,      /* pull every level after the first (trace collection) */
-  GSRB_BFS_TOPO = 4       /* topology-driven push every level (trace collection) */
+  GSRB_BFS_TOPO = 4,      /* topology-driven push every level (trace collection) */
+  /* OR-ed into any mode: push levels with >= 65536 frontier edges expand with
+   * the load balancer of the reference's -l option (per-CTA degree totals,
+   * prefix offsets, every warp the same number of edges; two extra barriers
+   * per such level).  gsrb_bfs only; batches reject it. */
+  GSRB_BFS_FLAG_LB = 0x100
 };
 
 /* Copy a host CSR to the device (owned by the graph). */
@@ -269,6 +274,12 @@ gsrb_status_t gsrb_graph_wrap(gsrb_ctx_t ctx, uint32_t n, uint64_t m, const uint
 gsrb_status_t gsrb_graph_free(gsrb_graph_t g);
 /* nhubs: vertices of degree > 128, whose rows PageRank splits into 2048-edge chunks. */
 gsrb_status_t gsrb_graph_info(gsrb_graph_t g, uint32_t* n, uint64_t* m, uint32_t* nhubs);
+/* 1 if every edge (u, v) has its reverse (v, u), else 0; tested when the graph
+ * is created (hash sums of the edges and of their reverses).  Pull levels of a
+ * BFS and the pull PageRank read a row as the vertex's in-edges, so on a
+ * graph that is not symmetric BFS never pulls (GSRB_BFS_PULL and gsrb_pagerank
+ * return GSRB_ERR_UNSUPPORTED; gsrb_pagerank_residual pushes and takes any graph). */
+gsrb_status_t gsrb_graph_is_symmetric(gsrb_graph_t g, int32_t* symmetric);
 /* Policy network weights (gsrb_mlp_* layout, gsrb_mlp_param_count() floats). */
 gsrb_status_t gsrb_graph_set_policy(gsrb_graph_t g, const float* h_weights, size_t count);
 /* Copy up to max_records 48-byte per-level trace records of the last traversal. */

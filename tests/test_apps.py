@@ -80,6 +80,16 @@ def test_bfs_app_matches_oracle(ctx, orc, gr_files, tmp_path, variant, name):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["push", "heuristic"])
+def test_bfs_app_load_balanced(ctx, orc, gr_files, tmp_path, mode):
+    # -l: the reference's load-balanced expansion (GSRB_BFS_FLAG_LB)
+    path, g = gr_files["rmat12"]
+    out = tmp_path / "levels.txt"
+    _run("bfs_gsrb", ["-l", "-s", "3", "-m", mode, "-o", str(out), str(path)], block_factor="1")
+    assert np.array_equal(_read_levels(out, g.nnodes), orc.bfs(g, 3))
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("mode", ["push", "pull", "topo", "learned"])
 def test_bfs_app_modes(gsrb, ctx, orc, gr_files, tmp_path, mode):
     path, g = gr_files["rmat12"]

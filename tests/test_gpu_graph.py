@@ -115,3 +115,62 @@ def test_bfs_trace_records(gsrb, ctx, orc, graphs):
     # the frontier of level L holds the vertices at level L - 1
     assert tr["nf"].tolist() == sizes[:len(tr)].tolist()
     assert set(tr["dir"].tolist()) <= {0, 1, 3}  # 3: levels run by a single CTA
+
+
+def _fan_graph(gsrb):
+    # directed: 0 -> 1..200000; every tenth of those -> 8 fresh vertices, the rest
+    # have no out-edges, so a large push level's queue interleaves zero-degree
+    # entries with short ranges (the load balancer's owner search must skip them)
+    n1 = 200000
+    src = [np.zeros(n1, np.uint32)]
+    dst = [np.arange(1, n1 + 1, dtype=np.uint32)]
+    parents = np.arange(10, n1 + 1, 10, dtype=np.uint32)
+    fresh = n1 + 1 + np.arange(parents.size * 8, dtype=np.uint32)
+    src.append(np.repeat(parents, 8))
+    dst.append(fresh)
+    n = int(fresh[-1]) + 1
+    return gsrb.csr_from_edges(n, np.concatenate(src), np.concatenate(dst), symmetrize=False)
+
+
+@pytest.mark.parametrize("name", ["rmat16", "grid64", "isolated", "fan"])
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("shape", [(2, 256), (1, 512), (4, 128)])
+def test_bfs_load_balanced_levels_exact(gsrb, ctx, orc, graphs, name, mode, shape):
+    g = _fan_graph(gsrb) if name == "fan" else graphs[name]
+    dg = ctx.graph(g)
+    out = ctx.array(g.nnodes, np.int32)
+    c = gsrb.cfg(variant=gsrb.BAR_FANOUT, ctas_per_sm=shape[0], threads=shape[1], wake_lines=4)
+    rc, st = dg.bfs(0, out, mode | gsrb.BFS_FLAG_LB, c)
+    gsrb.check(rc, "bfs lb")
+    ctx.check_status("bfs lb")
+    want = orc.bfs(g, 0)
+    assert np.array_equal(out.download(), want)
+    assert st.edges == orc.traversed_edges(g, want)
+    dg.free()
+
+
+def test_bfs_load_balanced_flag_rejected_by_batches(gsrb, ctx, graphs):
+    g = graphs["rmat12"]
+    dg = ctx.graph(g)
+    out = ctx.array(g.nnodes, np.int32)
+    b = gsrb.Batch(ctx, [dg], gsrb.cfg(variant=gsrb.BAR_FANOUT, ctas_per_sm=1, threads=256, wake_lines=4))
+    assert b.bfs([0], [out], gsrb.BFS_PUSH | gsrb.BFS_FLAG_LB) == gsrb.ERR_ARG
+    b.free()
+    dg.free()
+
+
+def test_directed_graph_never_pulls(gsrb, ctx, orc, graphs):
+    # rows are out-edges; a pull level would read them as in-edges, so on a
+    # directed graph the heuristic and the policy push, and the pull-only
+    # forms refuse
+    g = _fan_graph(gsrb)
+    dg = ctx.graph(g)
+    assert not dg.symmetric and ctx.graph(graphs["rmat12"]).symmetric
+    out = ctx.array(g.nnodes, np.int32)
+    want = orc.bfs(g, 0)
+    for mode in (gsrb.BFS_HEURISTIC, gsrb.BFS_PUSH, gsrb.BFS_TOPO):
+        gsrb.check(dg.bfs(0, out, mode)[0], "bfs")
+        assert np.array_equal(out.download(), want)
+    assert dg.bfs(0, out, gsrb.BFS_PULL)[0] == gsrb.ERR_UNSUPPORTED
+    assert dg.pagerank(ctx.array(g.nnodes, np.float32), 0.85, 5)[0] == gsrb.ERR_UNSUPPORTED
+    dg.free()

@@ -21,7 +21,9 @@
 // push-residual algorithm until no residual exceeds epsilon = 1e-6 (-x caps
 // the rounds, as in the reference), or with -u the pull form for -x
 // iterations (default 50).
-// -l is accepted for compatibility: hub vertices are always split across CTAs.
+// -l: BFS expands large push levels with the load balancer (GSRB_BFS_FLAG_LB,
+// the reference's thread-block load balancer); SSSP accepts -l and expands as
+// usual (hub vertices are always split across CTAs).
 #include <getopt.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -42,6 +44,7 @@
 namespace {
 
 int g_quiet = 0, g_device = 0, g_start = 0, g_delta = 10000, g_iters = -1, g_no_rank = 0, g_top = 0, g_pull = 0;
+int g_lb = 0;
 int g_variant = -1, g_mode = GSRB_BFS_HEURISTIC;
 const char* g_output = nullptr;
 const char* g_policy = nullptr;
@@ -104,7 +107,7 @@ void parse_args(int argc, char** argv) {
         break;
       }
       case 'b': g_variant = atoi(optarg); break;
-      case 'l': break;
+      case 'l': g_lb = 1; break;
       case 's':
         g_start = atoi(optarg);
         if (g_start < 0) { usage(argv[0]); exit(EXIT_FAILURE); }
@@ -253,7 +256,7 @@ int main(int argc, char** argv) {
     int32_t* d = nullptr;
     CHECK(gsrb_malloc((void**)&d, sizeof(int32_t) * (n ? n : 1)));
     if (GSRB_APP == 1) {
-      rc = gsrb_bfs(ctx, g, (uint32_t)g_start, d, g_mode, &cfg, &st);
+      rc = gsrb_bfs(ctx, g, (uint32_t)g_start, d, g_mode | (g_lb ? GSRB_BFS_FLAG_LB : 0), &cfg, &st);
       if (rc != GSRB_OK) die("gsrb_bfs", rc);
       printf("Kernel time (ms) %f\n", st.kernel_ms);
       printf("levels: %u\n", st.levels);

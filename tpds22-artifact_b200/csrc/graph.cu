@@ -43,6 +43,11 @@ struct BfsArgs {
   uint32_t* out;       // [0] levels, [1] fallback level (0 = none), [2] policy decisions, [3] overflow
   unsigned long long* out_edges;
   uint32_t* solo;      // [0] last level, [1] nu, [2] prev_nf, [3] solo levels, [4..5] mu, [6..7] edges
+  bool symmetric;      // rows are also in-edge lists: pull levels allowed
+  bool lb;             // load-balanced expansion of large push levels (GSRB_BFS_FLAG_LB)
+  uint32_t* lb_pre;    // [n] edge offset of each regular-queue entry
+  uint32_t* lb_own;    // [m / kLbChunk + 2] entry owning each chunk's first edge
+  uint32_t* lb_part;   // [kLbMaxCtas] per-CTA edge totals
 };
 
 // Single-CTA phase: when a push level's frontier fits one pass of one CTA
@@ -148,6 +153,138 @@ __device__ __noinline__ void bfs_solo(const BfsArgs& a, uint32_t L, uint32_t nre
   }
 }
 
+// Block-wide exclusive prefix sum of x (blockDim.x a multiple of 32, <= 1024);
+// *total receives the block's sum.  `s` holds 32 words of shared memory.
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t* s, uint32_t* total) {
+  const uint32_t lane = lane_id(), wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  uint32_t inc = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= (uint32_t)o) inc += y;
+  }
+  if (lane == 31) s[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t v = lane < nw ? s[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= (uint32_t)o) v += y;
+    }
+    s[lane] = v;
+  }
+  __syncthreads();
+  const uint32_t before = wid ? s[wid - 1] : 0u;
+  *total = s[nw - 1];
+  __syncthreads();
+  return before + inc - x;
+}
+
+// Load-balanced expansion of a push level's regular queue (the reference's
+// thread-block load balancer, apps/bfs/kernel_gsrb.cu:312-399, inspector
+// :360-383, with its prefix sum and binary-search edge assignment): every warp
+// gets the same number of edges whatever the degrees.
+//   1. each CTA sums the degrees of its slice of the queue;      (team barrier)
+//   2. each CTA offsets its slice by the totals of the CTAs before it, writes
+//      every entry's first-edge offset (lb_pre) and, for every kLbChunk-edge
+//      chunk that starts inside an entry's edges, the entry (lb_own);  (barrier)
+//   3. warps take chunks grid-stride; a warp walks its chunk 32 edges at a
+//      time with a window of 32 queue entries, each lane finding its edge's
+//      entry by a binary search over the window's offsets in registers.
+// Returns false if a team barrier failed.
+template <int V, class F>
+__device__ __forceinline__ bool bfs_lb_expand(gsrb::GridSync<V>& bar, const BfsArgs& a, const Team& team,
+                                              const uint2* __restrict__ qin, uint32_t nq, F& push_edge) {
+  __shared__ uint32_t s_scan[32];
+  __shared__ uint32_t s_off, s_tot;
+  const uint32_t G = team.ncta, c = team.cta;
+  const uint32_t s0 = (uint32_t)((uint64_t)nq * c / G), s1 = (uint32_t)((uint64_t)nq * (c + 1) / G);
+  // 1. slice totals
+  uint32_t local = 0;
+  for (uint32_t i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
+    const uint2 r = __ldcg(qin + i);
+    local += r.y - r.x;
+  }
+  uint32_t tsum = 0;
+  (void)block_exclusive_scan(local, s_scan, &tsum);
+  if (threadIdx.x == 0) a.lb_part[c] = tsum;
+  if (!bar.sync()) return false;
+  // 2. offsets, owners of chunk starts
+  uint32_t off = 0, tot = 0;
+  for (uint32_t k = threadIdx.x; k < G; k += blockDim.x) {
+    const uint32_t v = __ldcg(a.lb_part + k);
+    tot += v;
+    if (k < c) off += v;
+  }
+  uint32_t t1 = 0, t2 = 0;
+  (void)block_exclusive_scan(off, s_scan, &t1);
+  (void)block_exclusive_scan(tot, s_scan, &t2);
+  if (threadIdx.x == 0) {
+    s_off = t1;
+    s_tot = t2;
+  }
+  __syncthreads();
+  uint32_t carry = s_off;
+  const uint32_t W = s_tot;
+  for (uint32_t base = s0; base < s1; base += blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    uint32_t d = 0;
+    if (i < s1) {
+      const uint2 r = __ldcg(qin + i);
+      d = r.y - r.x;
+    }
+    uint32_t tile = 0;
+    const uint32_t ex = block_exclusive_scan(d, s_scan, &tile);
+    if (i < s1) {
+      const uint32_t P = carry + ex;
+      a.lb_pre[i] = P;
+      for (uint32_t k = (P + kLbChunk - 1) / kLbChunk; k * kLbChunk < P + d; ++k) a.lb_own[k] = i;
+    }
+    carry += tile;
+  }
+  if (!bar.sync()) return false;
+  // 3. edge-balanced walk
+  const uint32_t lane = lane_id();
+  const uint32_t nchunks = (W + kLbChunk - 1) / kLbChunk;
+  for (uint32_t chunk = team.warp(); chunk < nchunks; chunk += team.nwarps()) {
+    uint32_t o = __ldcg(a.lb_own + chunk);
+    uint32_t t0 = chunk * kLbChunk;
+    const uint32_t t_end = min(t0 + kLbChunk, W);
+    for (;;) {
+      const uint32_t wi = o + lane;
+      uint32_t p = W, b = 0;
+      if (wi < nq) {
+        p = __ldcg(a.lb_pre + wi);
+        b = __ldcg(&qin[wi].x);
+      }
+      const uint32_t p_next = o + 32 < nq ? __ldcg(a.lb_pre + o + 32) : W;
+      const uint32_t t_lim = min(t_end, p_next);
+      const uint32_t t = t0 + lane;
+      // largest window slot j with p_j <= t (offsets are non-decreasing)
+      uint32_t j = 0;
+#pragma unroll
+      for (uint32_t st = 16; st > 0; st >>= 1) {
+        const uint32_t pc = __shfl_sync(0xffffffffu, p, j + st);
+        if (pc <= t) j += st;
+      }
+      const uint32_t pj = __shfl_sync(0xffffffffu, p, j), bj = __shfl_sync(0xffffffffu, b, j);
+      push_edge(0u, bj + (t - pj), t < t_lim);
+      if (t0 + 32 <= t_lim) {
+        o += __shfl_sync(0xffffffffu, j, 31);
+        t0 += 32;
+        if (t0 == t_end) break;
+      } else if (t_lim == t_end) {
+        break;
+      } else {
+        o += 32;  // the window's entries end before the chunk does
+        t0 = t_lim;
+      }
+    }
+  }
+  return true;
+}
+
 // The traversal body, relative to a team (the whole grid, or one instance's
 // CTA range in a batch, synchronised by `bar`).
 template <int V>
@@ -238,6 +375,8 @@ __device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const B
         ++decisions;
       }
     }
+    // a pull level reads rows as in-edges: only on symmetric graphs
+    if (nd == DIR_PULL && !a.symmetric) nd = DIR_PUSH;
     dir = nd;
     if (team.cta == 0 && threadIdx.x == 0) {
       // the counter set of level L + 1 was last read before barrier L - 1
@@ -303,12 +442,20 @@ __device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const B
 
     if (dir == DIR_PUSH) {
       expand_hub_ranges(team, hin, nbig, push_edge);
-      const PushSink sink{qout, hout, &c->n_reg, &c->n_big, g.n, a.overflow};
-      const bool precheck = nf > kPushPrecheckFrontier;
-      auto lanes = [&](uint32_t b, uint32_t mine, uint32_t kmax) {
-        bfs_push_lanes(g, a.level, Li, b, mine, kmax, precheck, sink, m_acc);
-      };
-      expand_range_queue(team, qin, nreg, push_edge, lanes);
+      if (a.lb && team.ncta > 1 && mf >= kLbMinEdges) {
+        // uniform across the team: every CTA takes the two extra barriers
+        if (!bfs_lb_expand(bar, a, team, qin, nreg, push_edge)) {
+          ok = false;
+          break;
+        }
+      } else {
+        const PushSink sink{qout, hout, &c->n_reg, &c->n_big, g.n, a.overflow};
+        const bool precheck = nf > kPushPrecheckFrontier;
+        auto lanes = [&](uint32_t b, uint32_t mine, uint32_t kmax) {
+          bfs_push_lanes(g, a.level, Li, b, mine, kmax, precheck, sink, m_acc);
+        };
+        expand_range_queue(team, qin, nreg, push_edge, lanes);
+      }
     } else if (dir == DIR_TOPO) {
       // topology-driven push: scan every vertex, expand those at level L - 1
       expand_hub_ranges(team, hin, nbig, push_edge);
@@ -1107,6 +1254,10 @@ struct gsrb_graph {
   uint32_t* hub_done = nullptr;   // [nhubs] chunk counters
   MLPWeights* mlp = nullptr;
   bool mlp_set = false;
+  uint32_t* lb_pre = nullptr;   // [n] load-balanced BFS: edge offset of each queue entry
+  uint32_t* lb_own = nullptr;   // [m / kLbChunk + 2] queue entry owning each chunk's first edge
+  uint32_t* lb_part = nullptr;  // [kLbMaxCtas] per-CTA edge totals
+  bool symmetric = false;       // every edge (u, v) has its reverse (v, u)
 };
 
 namespace {
@@ -1114,6 +1265,55 @@ namespace {
 template <class T>
 cudaError_t dalloc(T** p, size_t count) {
   return cudaMalloc((void**)p, sizeof(T) * (count ? count : 1));
+}
+
+DevCSR dev_csr(const gsrb_graph* G) {
+  DevCSR d;
+  d.n = G->n;
+  d.m = G->m;
+  d.row = G->row;
+  d.dst = G->dst;
+  d.w = G->w;
+  return d;
+}
+
+// splitmix64's output mix (Steele, Lea, Flood, OOPSLA'14), as a hash of an edge.
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+// Symmetry test of a CSR: sums (mod 2^64) of two hashes of every edge (u, v)
+// and of its reverse (v, u).  The edge multiset equals its reverse exactly
+// when the graph is symmetric; then both pairs of sums agree, and otherwise
+// they differ except with probability about 2^-128.  One warp per row.
+__global__ void __launch_bounds__(256) edge_hash_kernel(DevCSR g, unsigned long long* sums) {
+  const uint32_t lane = lane_id();
+  const uint32_t w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  unsigned long long f1 = 0, r1 = 0, f2 = 0, r2 = 0;
+  for (uint32_t u = w0; u < g.n; u += nw) {
+    const uint32_t b = g.row[u], e = g.row[u + 1];
+    for (uint32_t j = b + lane; j < e; j += 32) {
+      const uint32_t v = g.dst[j];
+      const unsigned long long fw = ((unsigned long long)u << 32) | v, rv = ((unsigned long long)v << 32) | u;
+      f1 += mix64(fw);
+      r1 += mix64(rv);
+      f2 += mix64(fw ^ 0x5851f42d4c957f2dull);
+      r2 += mix64(rv ^ 0x5851f42d4c957f2dull);
+    }
+  }
+  f1 = warp_sum_u64(f1);
+  r1 = warp_sum_u64(r1);
+  f2 = warp_sum_u64(f2);
+  r2 = warp_sum_u64(r2);
+  if (lane == 0) {
+    atomicAdd(sums + 0, f1);
+    atomicAdd(sums + 1, r1);
+    atomicAdd(sums + 2, f2);
+    atomicAdd(sums + 3, r2);
+  }
 }
 
 gsrb_status_t graph_scratch(gsrb_graph* G) {
@@ -1135,6 +1335,9 @@ gsrb_status_t graph_scratch(gsrb_graph* G) {
   if (!e) e = dalloc(&G->trace, G->trace_cap);
   if (!e) e = dalloc(&G->mlp, 1);
   if (!e) e = cudaMemset(G->mlp, 0, sizeof(MLPWeights));
+  if (!e) e = dalloc(&G->lb_pre, n);
+  if (!e) e = dalloc(&G->lb_own, (size_t)G->m / kLbChunk + 2);
+  if (!e) e = dalloc(&G->lb_part, kLbMaxCtas);
   // PageRank hub chunks (degree > kPrHubDegree), built on the host from row_start
   if (!e) {
     std::vector<uint32_t> hrow(n + 1);
@@ -1159,6 +1362,18 @@ gsrb_status_t graph_scratch(gsrb_graph* G) {
     if (!e) e = cudaMemcpy(G->hub_c0, c0.data(), sizeof(uint32_t) * c0.size(), cudaMemcpyHostToDevice);
     if (!e && !ch.empty())
       e = cudaMemcpy(G->chunk_hub, ch.data(), sizeof(uint32_t) * ch.size(), cudaMemcpyHostToDevice);
+  }
+  // symmetric? (pull directions and pull PageRank read a row as in-edges)
+  if (!e) {
+    unsigned long long* sums = reinterpret_cast<unsigned long long*>(G->lb_part);
+    e = cudaMemset(sums, 0, 4 * sizeof(unsigned long long));
+    if (!e) {
+      edge_hash_kernel<<<1184, 256>>>(dev_csr(G), sums);
+      e = cudaGetLastError();
+    }
+    unsigned long long h[4] = {0, 0, 0, 0};
+    if (!e) e = cudaMemcpy(h, sums, sizeof h, cudaMemcpyDeviceToHost);
+    G->symmetric = h[0] == h[1] && h[2] == h[3];
   }
   if (!e) e = cudaDeviceSynchronize();
   if (e) return cuda_err(e, "graph scratch");
@@ -1189,17 +1404,11 @@ void graph_free(gsrb_graph* G) {
   cudaFree(G->hub_part);
   cudaFree(G->hub_done);
   cudaFree(G->mlp);
+  cudaFree(G->lb_pre);
+  cudaFree(G->lb_own);
+  cudaFree(G->lb_part);
 }
 
-DevCSR dev_csr(const gsrb_graph* G) {
-  DevCSR d;
-  d.n = G->n;
-  d.m = G->m;
-  d.row = G->row;
-  d.dst = G->dst;
-  d.w = G->w;
-  return d;
-}
 
 gsrb_cfg_t graph_cfg(gsrb_ctx* ctx, const gsrb_cfg_t* in) {
   gsrb_cfg_t c = resolve_cfg(ctx, in);
@@ -1295,6 +1504,12 @@ gsrb_status_t gsrb_graph_info(gsrb_graph_t G, uint32_t* n, uint64_t* m, uint32_t
   return GSRB_OK;
 }
 
+gsrb_status_t gsrb_graph_is_symmetric(gsrb_graph_t G, int32_t* symmetric) {
+  if (!G || !symmetric) return GSRB_ERR_ARG;
+  *symmetric = G->symmetric ? 1 : 0;
+  return GSRB_OK;
+}
+
 gsrb_status_t gsrb_graph_set_policy(gsrb_graph_t G, const float* h_weights, size_t count) {
   if (!G || !h_weights || count != sizeof(MLPWeights) / sizeof(float)) return GSRB_ERR_ARG;
   GSRB_CUDA(cudaMemcpy(G->mlp, h_weights, sizeof(MLPWeights), cudaMemcpyHostToDevice));
@@ -1316,14 +1531,23 @@ gsrb_status_t gsrb_graph_trace(gsrb_graph_t G, void* h_out, uint32_t max_records
 
 gsrb_status_t gsrb_bfs(gsrb_ctx_t ctx, gsrb_graph_t G, uint32_t src, int32_t* d_level, int32_t mode,
                        const gsrb_cfg_t* cfgin, gsrb_traversal_stats_t* stats) {
+  const bool lb = (mode & GSRB_BFS_FLAG_LB) != 0;
+  mode &= ~GSRB_BFS_FLAG_LB;
   if (!ctx || !G || !d_level || src >= G->n || mode < 0 || mode > GSRB_BFS_TOPO) return GSRB_ERR_ARG;
   if (mode == GSRB_BFS_LEARNED && !G->mlp_set) return GSRB_ERR_STATE;
+  if (mode == GSRB_BFS_PULL && !G->symmetric) return GSRB_ERR_UNSUPPORTED;
   gsrb_cfg_t c = graph_cfg(ctx, cfgin);
   const void* fn = bfs_fn(c.variant);
   if (!fn) return GSRB_ERR_UNSUPPORTED;
   const int grid = grid_of(ctx, c);
   if (grid % c.cluster || c.threads % 32 || c.threads > kGraphMaxThreads) return GSRB_ERR_ARG;
+  if (lb && grid > (int)kLbMaxCtas) return GSRB_ERR_ARG;
   BfsArgs a;
+  a.symmetric = G->symmetric;
+  a.lb = lb;
+  a.lb_pre = G->lb_pre;
+  a.lb_own = G->lb_own;
+  a.lb_part = G->lb_part;
   a.g = dev_csr(G);
   a.src = src;
   a.level = d_level;
@@ -1404,6 +1628,7 @@ gsrb_status_t gsrb_sssp(gsrb_ctx_t ctx, gsrb_graph_t G, uint32_t src, int32_t* d
 gsrb_status_t gsrb_pagerank(gsrb_ctx_t ctx, gsrb_graph_t G, float alpha, int32_t iters, float* d_rank,
                             const gsrb_cfg_t* cfgin, gsrb_traversal_stats_t* stats) {
   if (!ctx || !G || !d_rank || iters < 0 || !(alpha >= 0.f && alpha < 1.f)) return GSRB_ERR_ARG;
+  if (!G->symmetric) return GSRB_ERR_UNSUPPORTED;  // a row is summed as the vertex's in-edges
   gsrb_cfg_t c = graph_cfg(ctx, cfgin);
   const void* fn = pr_fn(c.variant);
   if (!fn) return GSRB_ERR_UNSUPPORTED;
@@ -1520,6 +1745,11 @@ BfsArgs bfs_args(gsrb_graph* G, uint32_t src, int32_t* level, int32_t mode) {
   a.out = G->flags + 4;
   a.out_edges = (unsigned long long*)((char*)G->flags + 64);
   a.solo = G->flags + 8;
+  a.symmetric = G->symmetric;
+  a.lb = false;
+  a.lb_pre = G->lb_pre;
+  a.lb_own = G->lb_own;
+  a.lb_part = G->lb_part;
   return a;
 }
 

@@ -20,6 +20,9 @@ constexpr uint32_t kBigDegree = 4096;       // vertices above this are expanded 
 constexpr uint32_t kWarpDegree = 32;        // above this a warp expands the vertex cooperatively
 constexpr uint32_t kPrHubDegree = 128;      // PageRank: above this a vertex's edges are cut into chunks
 constexpr uint32_t kPrChunk = 2048;         // PageRank: edges per hub chunk (one warp each)
+constexpr uint32_t kLbChunk = 256;          // load-balanced BFS: edges per warp chunk
+constexpr uint32_t kLbMaxCtas = 8192;       // load-balanced BFS: largest team (per-CTA totals)
+constexpr unsigned long long kLbMinEdges = 65536;  // load-balanced BFS: smaller push levels expand as usual
 
 struct DevCSR {
   uint32_t n;

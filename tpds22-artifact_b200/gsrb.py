@@ -155,6 +155,7 @@ _SIGS = {
     "gsrb_graph_upload": (C.c_int32, [_P, C.POINTER(HostCSR), C.POINTER(_P)]),
     "gsrb_graph_free": (C.c_int32, [_P]),
     "gsrb_graph_info": (C.c_int32, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
+    "gsrb_graph_is_symmetric": (C.c_int32, [_P, C.POINTER(C.c_int32)]),
     "gsrb_graph_set_policy": (C.c_int32, [_P, _P, C.c_size_t]),
     "gsrb_graph_trace": (C.c_int32, [_P, _P, C.c_uint32, C.POINTER(C.c_uint32)]),
     "gsrb_bfs": (C.c_int32, [_P, _P, C.c_uint32, _P, C.c_int32, C.POINTER(Cfg), C.c_void_p]),
@@ -184,6 +185,7 @@ _SIGS = {
 SEM_REF_SPIN, SEM_REF_EBO, SEM_REF_PRIORITY, SEM_REF_PRIORITY_EBO, SEM_PRIORITY = range(5)
 MUTEX_SPIN, MUTEX_EBO, MUTEX_FA, MUTEX_SLEEP = range(4)
 BFS_PUSH, BFS_HEURISTIC, BFS_LEARNED, BFS_PULL, BFS_TOPO = range(5)
+BFS_FLAG_LB = 0x100  # OR-ed into a mode: load-balanced expansion of large push levels
 
 
 class TraversalStats(C.Structure):
@@ -435,6 +437,12 @@ class DeviceGraph:
             self.free()
         except Exception:
             pass
+
+    @property
+    def symmetric(self) -> bool:
+        v = C.c_int32()
+        check(_lib().gsrb_graph_is_symmetric(self.h, C.byref(v)), "graph_is_symmetric")
+        return bool(v.value)
 
     def set_policy(self, weights: np.ndarray):
         w = np.ascontiguousarray(weights, dtype=np.float32)
