@@ -569,6 +569,125 @@ struct SsspArgs {
   unsigned long long* out_edges;
 };
 
+// Where an SSSP relax step puts the vertices whose distance it lowered.
+struct RelaxSink {
+  uint32_t* qout;               // near queue of the next round
+  uint32_t* hout;               // near hub queue
+  unsigned long long* n_reg;
+  unsigned long long* n_big;
+  uint32_t* fout;               // far pile
+  unsigned long long* fc;
+  uint32_t stamp;               // near-queue stamp of this round
+  uint32_t fgen;                // far-pile generation
+  long long T;                  // near threshold
+};
+
+// Relax four edges per lane at once: edge r of the lane is j[r] (where bit r of
+// `act` is set), leaving a vertex at distance du[r].  Every dependent step is
+// issued for all four before the next (destinations and weights, distance
+// probes, the atomicMin claims, the stamps, the degrees of vertices entering
+// the near queue), and the warp reserves queue space once per step.
+// Warp-synchronous.
+__device__ __forceinline__ void sssp_relax4e(const SsspArgs& a, const long long* du, const uint32_t* j, uint32_t act,
+                                             const RelaxSink& s, unsigned long long& my_edges) {
+  const DevCSR& g = a.g;
+  uint32_t v[4];
+  long long nd[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const bool on = (act >> r) & 1u;
+    v[r] = on ? __ldg(g.dst + j[r]) : 0u;
+    nd[r] = on ? du[r] + (long long)__ldg(g.w + j[r]) : (long long)kInf;
+    my_edges += on ? 1u : 0u;
+  }
+  int32_t cur[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) cur[r] = nd[r] < (long long)kInf ? __ldcg(a.dist + v[r]) : kInf;
+  bool imp[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+    imp[r] = nd[r] < (long long)cur[r] && nd[r] < (long long)atomicMin(a.dist + v[r], (int32_t)nd[r]);
+  bool to_near[4], to_far[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    to_near[r] = imp[r] && nd[r] < s.T && atomicExch(a.mark + v[r], s.stamp) != s.stamp;
+    to_far[r] = imp[r] && nd[r] >= s.T && atomicExch(a.fmark + v[r], s.fgen) != s.fgen;
+  }
+  uint32_t d[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) d[r] = to_near[r] ? __ldg(g.row + v[r] + 1) - __ldg(g.row + v[r]) : 0u;
+  bool reg[4], big[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    reg[r] = to_near[r] && d[r] <= kBigDegree;
+    big[r] = to_near[r] && d[r] > kBigDegree;
+  }
+  warp_append_k<4>(reg, v, s.qout, s.n_reg, g.n, a.overflow);
+  warp_append_k<4>(big, v, s.hout, s.n_big, g.n, a.overflow);
+  warp_append_k<4>(to_far, v, s.fout, s.fc, g.n, a.overflow);
+}
+
+// The same from one vertex: edge r is jbase + r * stride while below jend.
+__device__ __forceinline__ void sssp_relax4(const SsspArgs& a, long long du, uint32_t jbase, uint32_t stride,
+                                            uint32_t jend, const RelaxSink& s, unsigned long long& my_edges) {
+  long long dd[4];
+  uint32_t j[4];
+  uint32_t act = 0;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    dd[r] = du;
+    j[r] = jbase + (uint32_t)r * stride;
+    if (j[r] < jend) act |= 1u << r;
+  }
+  sssp_relax4e(a, dd, j, act, s, my_edges);
+}
+
+// A list of vertices relaxed edge-balanced: their edge counts' prefix p[0..cnt]
+// (p[cnt] = total), first edges b[] and distances d[] in shared memory.  Thread
+// x of nthr takes edges (x & ~31) + lane + k * nthr, four per step, each
+// finding its vertex by binary search over p.  Warp-synchronous loops.
+__device__ __forceinline__ void sssp_relax_list(const SsspArgs& a, const uint32_t* p, const uint32_t* b,
+                                                const int32_t* d, uint32_t cnt, uint32_t x, uint32_t nthr,
+                                                const RelaxSink& s, unsigned long long& my_edges) {
+  const uint32_t total = p[cnt];
+  for (uint32_t t0 = (x & ~31u) + lane_id(); t0 - lane_id() < total; t0 += 4u * nthr) {
+    long long du[4];
+    uint32_t j[4];
+    uint32_t act = 0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const uint32_t t = t0 + (uint32_t)r * nthr;
+      du[r] = 0;
+      j[r] = 0;
+      if (t < total) {
+        uint32_t lo = 0, hi = cnt;  // largest i with p[i] <= t
+        while (hi - lo > 1) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if (p[mid] <= t) lo = mid;
+          else hi = mid;
+        }
+        j[r] = b[lo] + (t - p[lo]);
+        du[r] = d[lo];
+        act |= 1u << r;
+      }
+    }
+    sssp_relax4e(a, du, j, act, s, my_edges);
+  }
+}
+
+// Hub queues up to this long are relaxed edge-balanced over the whole team
+// (each CTA builds the hubs' edge prefix in shared memory); longer ones fall
+// back to every CTA taking a slice of every hub.
+constexpr uint32_t kHubList = 2048;
+
+// Vertices of the regular queue with more edges than this are relaxed by their
+// whole CTA (after the CTA's warps have walked their queue groups), so that one
+// warp does not walk thousands of edges while the rest of the grid waits at
+// the round's barrier (the thread-block tier of the reference's nested
+// parallelism, LONESTAR/rt/include/internal.h.prehip:99-158).
+constexpr uint32_t kCtaDegree = 256;
+constexpr uint32_t kCtaListCap = 256;
+
 template <int V>
 __device__ __forceinline__ void sssp_run(gsrb::GridSync<V>& bar, bool ok, const SsspArgs& a, const Team team) {
   const DevCSR& g = a.g;
@@ -694,11 +813,49 @@ __device__ __forceinline__ void sssp_run(gsrb::GridSync<V>& bar, bool ok, const 
       warp_append(to_near && d > kBigDegree, v, hout, &c->n_big, g.n, a.overflow);
       warp_append(to_far, v, fout, fc, g.n, a.overflow);
     };
-    expand_hubs(team, g, hin, nbig, relax);
+    const RelaxSink sink{qout, hout, &c->n_reg, &c->n_big, fout, fc, stamp, fgen, T};
+    // vertex lists relaxed edge-balanced: edge prefix, first edge, distance
+    __shared__ uint32_t s_lp[kHubList + 1], s_lb[kHubList];
+    __shared__ int32_t s_ld[kHubList];
+    __shared__ uint32_t s_scan[32];
+    // builds the list's arrays from vertex ids (CTA-wide)
+    auto build_list = [&](auto id_of, uint32_t cnt) {
+      uint32_t carry = 0;
+      for (uint32_t base = 0; base < cnt; base += blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        uint32_t d = 0;
+        if (i < cnt) {
+          const uint32_t u = id_of(i);
+          const uint32_t b = __ldg(g.row + u);
+          d = __ldg(g.row + u + 1) - b;
+          s_lb[i] = b;
+          s_ld[i] = __ldcg(a.dist + u);
+        }
+        uint32_t tile = 0;
+        const uint32_t ex = block_exclusive_scan(d, s_scan, &tile);
+        if (i < cnt) s_lp[i] = carry + ex;
+        carry += tile;
+      }
+      if (threadIdx.x == 0) s_lp[cnt] = carry;
+      __syncthreads();
+    };
+    if (nbig <= kHubList) {
+      // hubs: every CTA builds the same list; the team's threads share its edges
+      build_list([&](uint32_t i) { return __ldcg(hin + i); }, nbig);
+      sssp_relax_list(a, s_lp, s_lb, s_ld, nbig, team.tid(), team.nthreads(), sink, my_edges);
+      __syncthreads();
+    } else {
+      expand_hubs(team, g, hin, nbig, relax);
+    }
     {
-      // regular queue: vertices of degree > kWarpDegree edge-parallel across the
-      // warp; smaller ones one lane each with 4 edges per lane in flight through
-      // every dependent step (ids and weights, distance probe, atomicMin, stamp)
+      // regular queue: vertices of degree > kCtaDegree go to the CTA's list
+      // (relaxed edge-balanced by the whole CTA below); degree > kWarpDegree
+      // edge-parallel across the warp; the rest one lane each; every tier
+      // keeps four edges per lane in flight
+      __shared__ uint32_t s_cta_u[kCtaListCap];
+      __shared__ uint32_t s_ncta;
+      if (threadIdx.x == 0) s_ncta = 0;
+      __syncthreads();
       const uint32_t lane = lane_id();
       const uint32_t gw = team.warp(), nwarps = team.nwarps();
       for (uint32_t base = gw * 32u; base < nreg; base += nwarps * 32u) {
@@ -710,52 +867,33 @@ __device__ __forceinline__ void sssp_run(gsrb::GridSync<V>& bar, bool ok, const 
           e = __ldg(g.row + u + 1);
         }
         const uint32_t deg = e - b;
-        uint32_t coop = __ballot_sync(0xffffffffu, deg > kWarpDegree);
+        bool warp_tier = deg > kWarpDegree;
+        if (deg > kCtaDegree) {
+          const uint32_t slot = atomicAdd(&s_ncta, 1u);
+          if (slot < kCtaListCap) {
+            s_cta_u[slot] = u;
+            warp_tier = false;
+          }
+        }
+        uint32_t coop = __ballot_sync(0xffffffffu, warp_tier);
         while (coop) {
           const int src = __ffs(coop) - 1;
           coop &= coop - 1;
           const uint32_t uu = __shfl_sync(0xffffffffu, u, src);
           const uint32_t bb = __shfl_sync(0xffffffffu, b, src), ee = __shfl_sync(0xffffffffu, e, src);
-          for (uint32_t j0 = bb; j0 < ee; j0 += 32) relax(uu, j0 + lane, j0 + lane < ee);
+          const long long du = (long long)__ldcg(a.dist + uu);
+          for (uint32_t j0 = bb; j0 < ee; j0 += 128) sssp_relax4(a, du, j0 + lane, 32u, ee, sink, my_edges);
         }
         const uint32_t mine = deg <= kWarpDegree ? deg : 0u;
         const uint32_t kmax = warp_max_u32(mine);
         const long long du = mine ? (long long)__ldcg(a.dist + u) : 0;
-        for (uint32_t k0 = 0; k0 < kmax; k0 += 4) {
-          uint32_t v[4];
-          long long nd[4];
-          bool to_near[4], to_far[4];
-#pragma unroll
-          for (int r = 0; r < 4; ++r) {
-            const bool act = k0 + r < mine;
-            v[r] = act ? __ldg(g.dst + b + k0 + r) : 0u;
-            nd[r] = act ? du + (long long)__ldg(g.w + b + k0 + r) : (long long)kInf;
-            my_edges += act ? 1u : 0u;
-          }
-          int32_t cur[4];
-#pragma unroll
-          for (int r = 0; r < 4; ++r) cur[r] = (k0 + r < mine) ? __ldcg(a.dist + v[r]) : kInf;
-          bool imp[4];
-#pragma unroll
-          for (int r = 0; r < 4; ++r) imp[r] = nd[r] < (long long)cur[r] && nd[r] < (long long)atomicMin(a.dist + v[r], (int32_t)nd[r]);
-#pragma unroll
-          for (int r = 0; r < 4; ++r) {
-            to_near[r] = imp[r] && nd[r] < T && atomicExch(a.mark + v[r], stamp) != stamp;
-            to_far[r] = imp[r] && nd[r] >= T && atomicExch(a.fmark + v[r], fgen) != fgen;
-          }
-          uint32_t d[4];
-#pragma unroll
-          for (int r = 0; r < 4; ++r) d[r] = to_near[r] ? __ldg(g.row + v[r] + 1) - __ldg(g.row + v[r]) : 0u;
-          bool reg[4], big[4];
-#pragma unroll
-          for (int r = 0; r < 4; ++r) {
-            reg[r] = to_near[r] && d[r] <= kBigDegree;
-            big[r] = to_near[r] && d[r] > kBigDegree;
-          }
-          warp_append_k<4>(reg, v, qout, &c->n_reg, g.n, a.overflow);
-          warp_append_k<4>(big, v, hout, &c->n_big, g.n, a.overflow);
-          warp_append_k<4>(to_far, v, fout, fc, g.n, a.overflow);
-        }
+        for (uint32_t k0 = 0; k0 < kmax; k0 += 4) sssp_relax4(a, du, b + k0, 1u, b + mine, sink, my_edges);
+      }
+      __syncthreads();
+      const uint32_t ncta = min(s_ncta, kCtaListCap);
+      if (ncta) {
+        build_list([&](uint32_t i) { return s_cta_u[i]; }, ncta);
+        sssp_relax_list(a, s_lp, s_lb, s_ld, ncta, threadIdx.x, blockDim.x, sink, my_edges);
       }
     }
     relaxed_edges += my_edges;
