@@ -196,7 +196,7 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t* s
 template <int V, class F>
 __device__ __forceinline__ bool bfs_lb_expand(gsrb::GridSync<V>& bar, const BfsArgs& a, const Team& team,
                                               const uint2* __restrict__ qin, uint32_t nq, F& push_edge) {
-  __shared__ uint32_t s_scan[32];
+  uint32_t* s_scan = list_smem().scan;
   __shared__ uint32_t s_off, s_tot;
   const uint32_t G = team.ncta, c = team.cta;
   const uint32_t s0 = (uint32_t)((uint64_t)nq * c / G), s1 = (uint32_t)((uint64_t)nq * (c + 1) / G);
@@ -283,6 +283,33 @@ __device__ __forceinline__ bool bfs_lb_expand(gsrb::GridSync<V>& bar, const BfsA
     }
   }
   return true;
+}
+
+// A push level's hub queue (2..kHubList ranges) expanded edge-balanced over the
+// team: every CTA builds the ranges' edge prefix in shared memory (the same in
+// every CTA, so no barrier is needed) and its threads take edges grid-stride.
+__device__ __forceinline__ void bfs_push_hubs(const BfsArgs& a, const Team& team, const uint2* __restrict__ hin,
+                                           uint32_t nbig, int32_t Li, const PushSink sink,
+                                           unsigned long long& m_acc) {
+  ListSmem& L_ = list_smem();
+  uint32_t carry = 0;
+  for (uint32_t base = 0; base < nbig; base += blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    uint32_t d = 0;
+    if (i < nbig) {
+      const uint2 r = __ldcg(hin + i);
+      L_.b[i] = r.x;
+      d = r.y - r.x;
+    }
+    uint32_t tile = 0;
+    const uint32_t ex = block_exclusive_scan(d, L_.scan, &tile);
+    if (i < nbig) L_.p[i] = carry + ex;
+    carry += tile;
+  }
+  if (threadIdx.x == 0) L_.p[nbig] = carry;
+  __syncthreads();
+  bfs_push_list(a.g, a.level, Li, L_.p, L_.b, nbig, team.tid(), team.nthreads(), sink, m_acc);
+  __syncthreads();
 }
 
 // The traversal body, relative to a team (the whole grid, or one instance's
@@ -441,7 +468,12 @@ __device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const B
     };
 
     if (dir == DIR_PUSH) {
-      expand_hub_ranges(team, hin, nbig, push_edge);
+      if (nbig > 1 && nbig <= kHubList) {
+        // hubs edge-balanced over the team: every CTA builds the same prefix
+        bfs_push_hubs(a, team, hin, nbig, Li, PushSink{qout, hout, &c->n_reg, &c->n_big, g.n, a.overflow}, m_acc);
+      } else {
+        expand_hub_ranges(team, hin, nbig, push_edge);
+      }
       if (a.lb && team.ncta > 1 && mf >= kLbMinEdges) {
         // uniform across the team: every CTA takes the two extra barriers
         if (!bfs_lb_expand(bar, a, team, qin, nreg, push_edge)) {
@@ -660,25 +692,15 @@ __device__ __forceinline__ void sssp_relax_list(const SsspArgs& a, const uint32_
       du[r] = 0;
       j[r] = 0;
       if (t < total) {
-        uint32_t lo = 0, hi = cnt;  // largest i with p[i] <= t
-        while (hi - lo > 1) {
-          const uint32_t mid = (lo + hi) >> 1;
-          if (p[mid] <= t) lo = mid;
-          else hi = mid;
-        }
-        j[r] = b[lo] + (t - p[lo]);
-        du[r] = d[lo];
+        const uint32_t o = list_owner(p, cnt, t);
+        j[r] = b[o] + (t - p[o]);
+        du[r] = d[o];
         act |= 1u << r;
       }
     }
     sssp_relax4e(a, du, j, act, s, my_edges);
   }
 }
-
-// Hub queues up to this long are relaxed edge-balanced over the whole team
-// (each CTA builds the hubs' edge prefix in shared memory); longer ones fall
-// back to every CTA taking a slice of every hub.
-constexpr uint32_t kHubList = 2048;
 
 // Vertices of the regular queue with more edges than this are relaxed by their
 // whole CTA (after the CTA's warps have walked their queue groups), so that one
@@ -815,9 +837,11 @@ __device__ __forceinline__ void sssp_run(gsrb::GridSync<V>& bar, bool ok, const 
     };
     const RelaxSink sink{qout, hout, &c->n_reg, &c->n_big, fout, fc, stamp, fgen, T};
     // vertex lists relaxed edge-balanced: edge prefix, first edge, distance
-    __shared__ uint32_t s_lp[kHubList + 1], s_lb[kHubList];
-    __shared__ int32_t s_ld[kHubList];
-    __shared__ uint32_t s_scan[32];
+    ListSmem& L_ = list_smem();
+    uint32_t* s_lp = L_.p;
+    uint32_t* s_lb = L_.b;
+    int32_t* s_ld = L_.d;
+    uint32_t* s_scan = L_.scan;
     // builds the list's arrays from vertex ids (CTA-wide)
     auto build_list = [&](auto id_of, uint32_t cnt) {
       uint32_t carry = 0;

@@ -245,6 +245,53 @@ struct PushSink {
 // vertices (throughput over latency).
 constexpr uint32_t kPushPrecheckFrontier = 16384;
 
+// BFS push of four edges per lane at once: edge r of the lane is j[r] (where
+// bit r of `act` is set).  The four destinations are loaded together, their
+// claims (compare-and-swap INF -> L) are issued together (with the row ranges
+// of the candidates, or after a level check when `precheck`), and the warp
+// reserves queue space once per step for all of them.  Levels are the same as
+// with one edge at a time (a vertex gets L from whichever claim lands first);
+// only the order of the next queue differs.  Warp-synchronous.
+__device__ __forceinline__ void bfs_push4e(const DevCSR& g, int32_t* level, int32_t Li, const uint32_t* j,
+                                           uint32_t act, bool precheck, const PushSink& s,
+                                           unsigned long long& m_acc) {
+  uint32_t v[4];
+  uint32_t live = act;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) v[r] = ((live >> r) & 1u) ? __ldg(g.dst + j[r]) : 0u;
+  uint2 rg[4];
+  if (precheck) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+      if (((live >> r) & 1u) && __ldcg(level + v[r]) != kInf) live &= ~(1u << r);
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+      if (((live >> r) & 1u) && atomicCAS(level + v[r], kInf, Li) != kInf) live &= ~(1u << r);
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+      rg[r] = ((live >> r) & 1u) ? make_uint2(__ldg(g.row + v[r]), __ldg(g.row + v[r] + 1)) : make_uint2(0u, 0u);
+  } else {
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+      rg[r] = ((live >> r) & 1u) ? make_uint2(__ldg(g.row + v[r]), __ldg(g.row + v[r] + 1)) : make_uint2(0u, 0u);
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+      if (((live >> r) & 1u) && atomicCAS(level + v[r], kInf, Li) != kInf) live &= ~(1u << r);
+  }
+  bool reg[4], big[4];
+  bool any_big = false;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const uint32_t d = ((live >> r) & 1u) ? rg[r].y - rg[r].x : 0u;
+    reg[r] = ((live >> r) & 1u) && d <= kBigDegree;
+    big[r] = ((live >> r) & 1u) && d > kBigDegree;
+    any_big |= big[r];
+    m_acc += d;
+  }
+  warp_append_k<4>(reg, rg, s.qout, s.n_reg, s.cap, s.overflow);
+  if (__any_sync(0xffffffffu, any_big)) warp_append_k<4>(big, rg, s.hout, s.n_big, s.cap, s.overflow);
+}
+
 // BFS push over the lane-per-vertex edges of a 32-entry group, four edges per
 // lane in flight: the four destinations are loaded together, their claims are
 // issued together (with the row ranges of the candidates, or after a level
@@ -253,7 +300,8 @@ constexpr uint32_t kPushPrecheckFrontier = 16384;
 // edges (destination, claim and rows, reservation) instead of five per edge.
 // Levels are the same as with one edge at a time (a vertex gets L from
 // whichever claim lands first); only the order of the next queue differs.
-// Warp-synchronous.
+// Warp-synchronous.  (bfs_push4e does the same for arbitrary edge indices; this
+// contiguous form keeps fewer registers live in the level loop.)
 __device__ __forceinline__ void bfs_push_lanes(const DevCSR& g, int32_t* level, int32_t Li, uint32_t b,
                                                uint32_t mine, uint32_t kmax, bool precheck, const PushSink& s,
                                                unsigned long long& m_acc) {
@@ -299,6 +347,60 @@ __device__ __forceinline__ void bfs_push_lanes(const DevCSR& g, int32_t* level, 
     }
     warp_append_k<4>(reg, rg, s.qout, s.n_reg, s.cap, s.overflow);
     if (__any_sync(0xffffffffu, any_big)) warp_append_k<4>(big, rg, s.hout, s.n_big, s.cap, s.overflow);
+  }
+}
+
+// Largest i in [0, cnt) with p[i] <= t (p non-decreasing, p[0] <= t).
+__device__ __forceinline__ uint32_t list_owner(const uint32_t* p, uint32_t cnt, uint32_t t) {
+  uint32_t lo = 0, hi = cnt;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (p[mid] <= t) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Hub queues up to this long are expanded edge-balanced over the whole team
+// (each CTA builds the hubs' edge prefix in shared memory, no barrier needed);
+// longer ones fall back to every CTA taking a slice of every hub in turn.
+constexpr uint32_t kHubList = 2048;
+
+// Shared-memory lists of the edge-balanced tiers (one instance per CTA, shared
+// by every traversal kernel that inlines them): edge prefix, first edges,
+// source distances (SSSP), and scan scratch.
+struct ListSmem {
+  uint32_t p[kHubList + 1];
+  uint32_t b[kHubList];
+  int32_t d[kHubList];
+  uint32_t scan[32];
+};
+__device__ __forceinline__ ListSmem& list_smem() {
+  __shared__ ListSmem s;
+  return s;
+}
+
+// BFS push of a list of ranges, edge-balanced: prefix p[0..cnt] and first edges
+// b[] in shared memory; thread x of nthr takes edges (x & ~31) + lane + k * nthr,
+// four per step, each finding its range by binary search.  Warp-synchronous.
+__device__ __forceinline__ void bfs_push_list(const DevCSR& g, int32_t* level, int32_t Li, const uint32_t* p,
+                                              const uint32_t* b, uint32_t cnt, uint32_t x, uint32_t nthr,
+                                              const PushSink& s, unsigned long long& m_acc) {
+  const uint32_t total = p[cnt];
+  for (uint32_t t0 = (x & ~31u) + lane_id(); t0 - lane_id() < total; t0 += 4u * nthr) {
+    uint32_t j[4];
+    uint32_t act = 0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const uint32_t t = t0 + (uint32_t)r * nthr;
+      j[r] = 0;
+      if (t < total) {
+        const uint32_t o = list_owner(p, cnt, t);
+        j[r] = b[o] + (t - p[o]);
+        act |= 1u << r;
+      }
+    }
+    bfs_push4e(g, level, Li, j, act, true, s, m_acc);
   }
 }
 
