@@ -1191,6 +1191,92 @@ struct PrrArgs {
   unsigned long long* out_edges;
 };
 
+// Where a residual push step puts the vertices whose residual crossed epsilon.
+struct PrrSink {
+  uint32_t* qout;
+  uint32_t* hout;
+  unsigned long long* n_reg;
+  unsigned long long* n_big;
+  uint32_t stamp;  // a vertex enters the next worklist at most once per round
+};
+
+// Push residual along four edges per lane at once: edge r of the lane is j[r]
+// (bit r of `act`), carrying upd[r].  The four destinations, then the four
+// residual additions, then the four worklist stamps are issued together, and
+// the warp reserves queue space once per step (apps/pr/kernel_gsrb.cu:430-470:
+// r[dst] += alpha * res / outdeg, pushed when it crosses epsilon).
+// Warp-synchronous.
+__device__ __forceinline__ void prr_push4e(const PrrArgs& a, const float* upd, const uint32_t* j, uint32_t act,
+                                           const PrrSink& s, unsigned long long& pushes) {
+  const DevCSR& g = a.g;
+  uint32_t w[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) w[r] = ((act >> r) & 1u) ? __ldg(g.dst + j[r]) : 0u;
+  bool cross[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    cross[r] = false;
+    if ((act >> r) & 1u) {
+      const float prev = atomicAdd(a.r + w[r], upd[r]);
+      cross[r] = prev + upd[r] > a.eps && prev < a.eps;
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 4; ++r) cross[r] = cross[r] && atomicExch(a.mark + w[r], s.stamp) != s.stamp;
+  bool reg[4], big[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const uint32_t d = cross[r] ? __ldg(g.row + w[r] + 1) - __ldg(g.row + w[r]) : 0u;
+    reg[r] = cross[r] && d <= kBigDegree;
+    big[r] = cross[r] && d > kBigDegree;
+    pushes += cross[r] ? 1u : 0u;
+  }
+  warp_append_k<4>(reg, w, s.qout, s.n_reg, g.n, a.overflow);
+  warp_append_k<4>(big, w, s.hout, s.n_big, g.n, a.overflow);
+}
+
+// The same from one vertex: edge r is jbase + r * stride while below jend.
+__device__ __forceinline__ void prr_push4(const PrrArgs& a, float upd, uint32_t jbase, uint32_t stride, uint32_t jend,
+                                          const PrrSink& s, unsigned long long& pushes) {
+  float u4[4];
+  uint32_t j[4];
+  uint32_t act = 0;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    u4[r] = upd;
+    j[r] = jbase + (uint32_t)r * stride;
+    if (j[r] < jend) act |= 1u << r;
+  }
+  prr_push4e(a, u4, j, act, s, pushes);
+}
+
+// A list of vertices pushed edge-balanced: edge prefix p[0..cnt], first edges
+// b[], updates (float bits) d[] in shared memory; thread x of nthr takes edges
+// (x & ~31) + lane + k * nthr, four per step.  Warp-synchronous loops.
+__device__ __forceinline__ void prr_push_list(const PrrArgs& a, const uint32_t* p, const uint32_t* b,
+                                              const int32_t* d, uint32_t cnt, uint32_t x, uint32_t nthr,
+                                              const PrrSink& s, unsigned long long& pushes) {
+  const uint32_t total = p[cnt];
+  for (uint32_t t0 = (x & ~31u) + lane_id(); t0 - lane_id() < total; t0 += 4u * nthr) {
+    float upd[4];
+    uint32_t j[4];
+    uint32_t act = 0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const uint32_t t = t0 + (uint32_t)r * nthr;
+      upd[r] = 0.f;
+      j[r] = 0;
+      if (t < total) {
+        const uint32_t o = list_owner(p, cnt, t);
+        j[r] = b[o] + (t - p[o]);
+        upd[r] = __int_as_float(d[o]);
+        act |= 1u << r;
+      }
+    }
+    prr_push4e(a, upd, j, act, s, pushes);
+  }
+}
+
 template <int V>
 __global__ void __launch_bounds__(1024)
 pr_residual_kernel(gsrb::GridBarrier gb, PrrArgs a) {
@@ -1266,8 +1352,31 @@ pr_residual_kernel(gsrb::GridBarrier gb, PrrArgs a) {
       warp_append(cross && d > kBigDegree, w, hout, &c->n_big, g.n, a.overflow);
       pushes += cross ? 1u : 0u;
     };
+    const PrrSink sink{qout, hout, &c->n_reg, &c->n_big, stamp};
+    ListSmem& L_ = list_smem();
+    // builds an edge-balanced list from vertex ids and their updates (CTA-wide)
+    auto build_list = [&](auto id_of, auto upd_of, uint32_t cnt) {
+      uint32_t carry = 0;
+      for (uint32_t base = 0; base < cnt; base += blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        uint32_t d = 0;
+        if (i < cnt) {
+          const uint32_t u = id_of(i);
+          const uint32_t b = __ldg(g.row + u);
+          d = __ldg(g.row + u + 1) - b;
+          L_.b[i] = b;
+          L_.d[i] = __float_as_int(upd_of(i, u));
+        }
+        uint32_t tile = 0;
+        const uint32_t ex = block_exclusive_scan(d, L_.scan, &tile);
+        if (i < cnt) L_.p[i] = carry + ex;
+        carry += tile;
+      }
+      if (threadIdx.x == 0) L_.p[cnt] = carry;
+      __syncthreads();
+    };
     if (nbig) {
-      // hubs: take the residual once, then split the edges across the grid
+      // hubs: take the residual once, then share the edges across the grid
       for (uint32_t k = tid; k < nbig; k += nthreads) {
         const uint32_t u = __ldcg(hin + k);
         const float res = atomicExch(a.r + u, 0.f);
@@ -1276,21 +1385,35 @@ pr_residual_kernel(gsrb::GridBarrier gb, PrrArgs a) {
       }
       ok = bar.sync();
       if (!ok) break;
-      auto hub_edge = [&](uint32_t u, uint32_t j, bool active) {
-        bool cross = false;
-        uint32_t w = 0;
-        if (active) {
-          w = __ldg(g.dst + j);
-          const float upd = __ldcg(a.hub_upd + u);
-          const float prev = atomicAdd(a.r + w, upd);
-          cross = prev + upd > a.eps && prev < a.eps;
-        }
-        push(cross, w);
-      };
-      expand_hubs(team, g, hin, nbig, hub_edge);
+      if (nbig <= kHubList) {
+        build_list([&](uint32_t i) { return __ldcg(hin + i); },
+                   [&](uint32_t, uint32_t u) { return __ldcg(a.hub_upd + u); }, nbig);
+        prr_push_list(a, L_.p, L_.b, L_.d, nbig, tid, nthreads, sink, pushes);
+        __syncthreads();
+      } else {
+        auto hub_edge = [&](uint32_t u, uint32_t j, bool active) {
+          bool cross = false;
+          uint32_t w = 0;
+          if (active) {
+            w = __ldg(g.dst + j);
+            const float upd = __ldcg(a.hub_upd + u);
+            const float prev = atomicAdd(a.r + w, upd);
+            cross = prev + upd > a.eps && prev < a.eps;
+          }
+          push(cross, w);
+        };
+        expand_hubs(team, g, hin, nbig, hub_edge);
+      }
     }
-    // regular worklist: a lane per vertex (exchange once), edges per lane or
-    // per warp for degree > kWarpDegree
+    // regular worklist: a lane per vertex exchanges its residual once; edges
+    // of degree > kCtaDegree vertices go to the CTA's edge-balanced list,
+    // degree > kWarpDegree across the warp, the rest per lane, four edges per
+    // lane in flight
+    __shared__ uint32_t s_cta_u[kCtaListCap];
+    __shared__ float s_cta_upd[kCtaListCap];
+    __shared__ uint32_t s_ncta;
+    if (threadIdx.x == 0) s_ncta = 0;
+    __syncthreads();
     for (uint32_t base = (tid >> 5) * 32u; base < nreg; base += nthreads) {
       const uint32_t i = base + lane;
       uint32_t u = 0, b = 0, e = 0;
@@ -1304,36 +1427,32 @@ pr_residual_kernel(gsrb::GridBarrier gb, PrrArgs a) {
         upd = e > b ? res * a.alpha / (float)(e - b) : 0.f;
       }
       const uint32_t deg = e - b;
-      uint32_t coop = __ballot_sync(0xffffffffu, deg > kWarpDegree);
+      bool warp_tier = deg > kWarpDegree;
+      if (deg > kCtaDegree) {
+        const uint32_t slot = atomicAdd(&s_ncta, 1u);
+        if (slot < kCtaListCap) {
+          s_cta_u[slot] = u;
+          s_cta_upd[slot] = upd;
+          warp_tier = false;
+        }
+      }
+      uint32_t coop = __ballot_sync(0xffffffffu, warp_tier);
       while (coop) {
         const int src = __ffs(coop) - 1;
         coop &= coop - 1;
         const uint32_t bb = __shfl_sync(0xffffffffu, b, src), ee = __shfl_sync(0xffffffffu, e, src);
         const float uu = __shfl_sync(0xffffffffu, upd, src);
-        for (uint32_t j0 = bb; j0 < ee; j0 += 32) {
-          const uint32_t j = j0 + lane;
-          bool cross = false;
-          uint32_t w = 0;
-          if (j < ee) {
-            w = __ldg(g.dst + j);
-            const float prev = atomicAdd(a.r + w, uu);
-            cross = prev + uu > a.eps && prev < a.eps;
-          }
-          push(cross, w);
-        }
+        for (uint32_t j0 = bb; j0 < ee; j0 += 128) prr_push4(a, uu, j0 + lane, 32u, ee, sink, pushes);
       }
       const uint32_t mine = deg <= kWarpDegree ? deg : 0u;
       const uint32_t kmax = warp_max_u32(mine);
-      for (uint32_t k = 0; k < kmax; ++k) {
-        bool cross = false;
-        uint32_t w = 0;
-        if (k < mine) {
-          w = __ldg(g.dst + b + k);
-          const float prev = atomicAdd(a.r + w, upd);
-          cross = prev + upd > a.eps && prev < a.eps;
-        }
-        push(cross, w);
-      }
+      for (uint32_t k0 = 0; k0 < kmax; k0 += 4) prr_push4(a, upd, b + k0, 1u, b + mine, sink, pushes);
+    }
+    __syncthreads();
+    const uint32_t ncta = min(s_ncta, kCtaListCap);
+    if (ncta) {
+      build_list([&](uint32_t i) { return s_cta_u[i]; }, [&](uint32_t i, uint32_t) { return s_cta_upd[i]; }, ncta);
+      prr_push_list(a, L_.p, L_.b, L_.d, ncta, threadIdx.x, blockDim.x, sink, pushes);
     }
     ok = bar.sync();
   }
