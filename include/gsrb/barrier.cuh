@@ -255,8 +255,9 @@ __device__ __forceinline__ bool flip_wait(const GridBarrier& gb, uint32_t n, uin
 // ---- counter + fan-out wake-up lines (V_FANOUT, V_CLUSTER_FANOUT) -------------
 // Arrivals (one per unit) go to the counter line slot->count with a release
 // RMW (fence.acq_rel + relaxed atom); the unit whose arrival completes the
-// episode acquires (fence.acq_rel), resets the counter and writes the new
-// generation into all kFanoutLines wake-up lines (second half of the flip
+// episode resets the counter, then one fence.acq_rel acquires the other
+// arrivals and orders the reset before the new generation, which it writes
+// into all kFanoutLines wake-up lines (second half of the flip
 // area; all of them, so they always hold the same value whatever R a later
 // launch uses); unit u polls line u % R with ld.acquire.  Keeping the polled
 // lines apart from the counter line means the polling loads never queue in
@@ -272,8 +273,10 @@ __device__ __forceinline__ uint32_t fanout_count(const GridBarrier& gb) {
 __device__ __forceinline__ bool fanout_arrive(const GridBarrier& gb, uint32_t n, uint32_t epoch) {
   ptx::fence_acq_rel_gpu();
   if (ptx::atom_add_relaxed_gpu(&gb.slot->count, 1u) != n - 1u) return false;
-  ptx::fence_acq_rel_gpu();
+  // reset before the fence, so that the fence orders it before the generation
+  // stores (a CTA that sees the new generation arrives on a reset counter)
   ptx::st_relaxed_gpu(&gb.slot->count, 0u);
+  ptx::fence_acq_rel_gpu();
   for (uint32_t r = 0; r < kFanoutLines; ++r) ptx::st_relaxed_gpu(fanout_line(gb, r), epoch + 1u);
   return true;
 }
@@ -343,7 +346,9 @@ constexpr size_t kLfWords = 2 * (size_t)kLfGlobal + 2 * (size_t)kLfGroups * kLfL
 // the group's last arrival acquires and arrives on the root counter for the
 // group; the root's last arrival resets the counters it completed and publishes
 // the generation to every wake-up line.  Every RMW is a release (fence.acq_rel
-// before a relaxed atom); a completer acquires with a second fence.
+// before a relaxed atom); a completer resets its counter and then fences, which
+// acquires the arrivals it completed and orders the reset before its next
+// arrival or the generation stores.
 __device__ __forceinline__ bool hier_arrive(const GridBarrier& gb, uint32_t idx, uint32_t n, uint32_t epoch) {
   const uint32_t G = gb.ngroups;
   ptx::fence_acq_rel_gpu();
@@ -351,13 +356,14 @@ __device__ __forceinline__ bool hier_arrive(const GridBarrier& gb, uint32_t idx,
     const uint32_t g = idx % G;
     uint32_t* gc = &gb.groups[g].count;
     if (ptx::atom_add_relaxed_gpu(gc, 1u) != group_size(n, G, g) - 1u) return false;
-    ptx::fence_acq_rel_gpu();
+    // reset before the fence: the fence orders it before the root arrival
     ptx::st_relaxed_gpu(gc, 0u);
+    ptx::fence_acq_rel_gpu();
     n = G;
   }
   if (ptx::atom_add_relaxed_gpu(&gb.slot->count, 1u) != n - 1u) return false;
-  ptx::fence_acq_rel_gpu();
   ptx::st_relaxed_gpu(&gb.slot->count, 0u);
+  ptx::fence_acq_rel_gpu();
   for (uint32_t r = 0; r < kFanoutLines; ++r) ptx::st_relaxed_gpu(fanout_line(gb, r), epoch + 1u);
   return true;
 }
