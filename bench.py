@@ -22,7 +22,7 @@ measured on the same device in the same run (disable with --no-extras):
                     batched + learned in one CUDA-graph launch; aggregate GTEPS
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload barrier|reduce|scan|bfs|sssp|pr] [--graph rmat|grid] [--scale 22]
+                  [--workload barrier|reduce|scan|bfs|sssp|pr|prr] [--graph rmat|grid] [--scale 22]
                   [--k 8] [--fma 0] [--cfg JSON] [--no-extras]
 
 --impl reference times the reference's CPU implementation of the path on the
@@ -360,7 +360,7 @@ def scan_numbers(gsrb, ctx, orc, tune, cache, n=1 << 28, reps=5, fixed=None):
 # --------------------------------------------------------------------- graphs
 def train_policy(gsrb, ctx, pol):
     """Per-level traces of training graphs (not the evaluation graphs) -> MLP."""
-    graphs = [gsrb.rmat(s, 16, seed=SEED + 1000 + s) for s in (14, 16, 18, 20, 21)]
+    graphs = [gsrb.rmat(s, 16, seed=SEED + 1000 + s) for s in (14, 16, 18, 20, 21, 22)]
     graphs += [gsrb.grid2d(256, 256, seed=SEED + 7), gsrb.grid2d(1024, 64, seed=SEED + 8),
                gsrb.grid2d(1024, 1024, seed=SEED + 9), gsrb.grid2d(2048, 512, seed=SEED + 10)]
     X, Y, M = [], [], []
@@ -399,6 +399,9 @@ def bfs_runs(gsrb, ctx, orc, dg, g, params, cfg, reps=3):
         if mode == gsrb.BFS_LEARNED:
             res[name]["policy_decisions"] = int(st.decisions)
             res[name]["fallback_level"] = int(st.aux)
+            if st.levels <= 64:
+                # per-level schedule (0 push, 1 pull, 2 topology push, 3 one-CTA push)
+                res[name]["dirs"] = [int(x) for x in dg.trace(64)["dir"][: int(st.levels)]]
     res["learned_vs_plain"] = round(res["plain_push"]["ms"] / res["learned"]["ms"], 3)
     return res
 
@@ -566,7 +569,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="barrier", choices=["barrier", "reduce", "scan", "bfs", "sssp", "pr"])
+    ap.add_argument("--workload", default="barrier", choices=["barrier", "reduce", "scan", "bfs", "sssp", "pr", "prr"])
     ap.add_argument("--graph", default="rmat", choices=["rmat", "grid"], help="graph of the bfs/sssp/pr workloads")
     ap.add_argument("--scale", type=int, default=22, help="log2 vertices of the bfs/sssp/pr workload graph")
     ap.add_argument("--iters", type=int, default=50, help="PageRank iterations (pr workload)")
@@ -628,6 +631,15 @@ def main():
                 r = bfs_runs(gsrb, ctx, orc, dg, g, gsrb.mlp_init(1), c, reps=args.steps)
             elif args.workload == "sssp":
                 r = sssp_runs(gsrb, ctx, orc, dg, g, [("delta", args.delta)], c)
+            elif args.workload == "prr":
+                # the reference's push-residual PageRank (epsilon 1e-6, to an empty worklist)
+                out = ctx.array(g.nnodes, np.float32)
+                ts = []
+                for _ in range(args.steps):
+                    rc, st = dg.pagerank_residual(out, 0.85, 1e-6, 2**31 - 1, c)
+                    gsrb.check(rc, "pagerank_residual")
+                    ts.append(st.kernel_ms)
+                r = {"n": g.nnodes, "m": g.nedges, "ms": ts, "rounds": int(st.levels), "pushes": int(st.edges)}
             else:
                 out = ctx.array(g.nnodes, np.float32)
                 ts = []

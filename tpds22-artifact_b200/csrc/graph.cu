@@ -59,6 +59,8 @@ struct BfsArgs {
 // ends.  Small-frontier levels of high-diameter graphs (meshes, road
 // networks) then cost no grid barrier.
 constexpr uint32_t kSoloMaxLevels = 16384;
+// The policy's topology-push output must exceed this logit (probability 0.88).
+constexpr float kTopoLogit = 2.f;
 
 // The single-CTA phase, run by every thread of the team's first CTA from level
 // L (whose frontier, nreg + nbig vertices of level L-1, is in the global
@@ -389,7 +391,10 @@ __device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const B
           level_features(feat, g.n, g.m, L, nf, mf, nu, mu, prev_nf, dir);
           mlp_forward_smem(&s_mlp, feat, out);
           if (threadIdx.x == 0) {
-            s_dir = out[0] > 0.f ? DIR_PULL : (out[1] > 0.f ? DIR_TOPO : DIR_PUSH);
+            // the topology push scans all n vertices: taken only on a confident
+            // output; the first level always pushes (its frontier is the source,
+            // and the training labels hold no pull decision for it)
+            s_dir = (out[0] > 0.f && L > 1) ? DIR_PULL : (out[1] > kTopoLogit ? DIR_TOPO : DIR_PUSH);
             s_pred = out[2];
           }
         }

@@ -42,6 +42,9 @@ def level_times(trace: np.ndarray, total_ms: float | None = None) -> np.ndarray:
     return d
 
 
+TOPO_MARGIN = 0.8
+
+
 def _weight(t_a: float, t_b: float) -> float:
     """Cost-sensitive sample weight: |log2(t_a / t_b)| clipped to [0.05, 4].
     A level where the two directions take about the same time hardly matters;
@@ -92,7 +95,9 @@ def features_labels(rec: dict):
             Y[i, 0] = 1.0 if t_pull[i] < t_push[i] else 0.0
             M[i, 0] = _weight(t_push[i], t_pull[i])
         if i < len(t_topo) and np.isfinite(t_push[i]) and np.isfinite(t_topo[i]):
-            Y[i, 1] = 1.0 if t_topo[i] < t_push[i] else 0.0
+            # the topology push scans every vertex: label it only where it wins
+            # clearly (by 20 %), so that near-ties teach the safe worklist push
+            Y[i, 1] = 1.0 if t_topo[i] < TOPO_MARGIN * t_push[i] else 0.0
             M[i, 1] = _weight(t_push[i], t_topo[i])
         nxt = int(tr[i + 1]["nf"]) if i + 1 < L else 0
         Y[i, 2] = np.log2(1.0 + nxt)
