@@ -174,3 +174,20 @@ def test_directed_graph_never_pulls(gsrb, ctx, orc, graphs):
     assert dg.bfs(0, out, gsrb.BFS_PULL)[0] == gsrb.ERR_UNSUPPORTED
     assert dg.pagerank(ctx.array(g.nnodes, np.float32), 0.85, 5)[0] == gsrb.ERR_UNSUPPORTED
     dg.free()
+
+
+@pytest.mark.parametrize("name,delta", [("rmat16", 10000), ("rmat16", 300), ("grid256", 2000)])
+@pytest.mark.parametrize("shape", [(1, 64), (1, 128)])
+def test_sssp_reserved_queue_chunks(gsrb, ctx, orc, graphs, name, delta, shape):
+    # few warps (n >= 63 x warps), so the near queue is filled through
+    # per-warp reservations with hole slots that the next round skips
+    g = gsrb.grid2d(256, 256, seed=5) if name == "grid256" else graphs[name]
+    dg = ctx.graph(g)
+    out = ctx.array(g.nnodes, np.int32)
+    c = gsrb.cfg(variant=gsrb.BAR_FANOUT, ctas_per_sm=shape[0], threads=shape[1], wake_lines=4)
+    assert 63 * (ctx.num_sms * shape[0] * shape[1] // 32) <= g.nnodes
+    rc, st = dg.sssp(0, out, delta, c)
+    gsrb.check(rc, "sssp")
+    ctx.check_status("sssp")
+    assert np.array_equal(out.download(), orc.dijkstra(g, 0))
+    dg.free()

@@ -617,6 +617,8 @@ struct RelaxSink {
   uint32_t stamp;               // near-queue stamp of this round
   uint32_t fgen;                // far-pile generation
   long long T;                  // near threshold
+  WarpRes* res;                 // the warp's near-queue reservation
+  uint32_t near_cap;            // near-queue capacity in slots (holes included)
 };
 
 // Relax four edges per lane at once: edge r of the lane is j[r] (where bit r of
@@ -659,7 +661,8 @@ __device__ __forceinline__ void sssp_relax4e(const SsspArgs& a, const long long*
     reg[r] = to_near[r] && d[r] <= kBigDegree;
     big[r] = to_near[r] && d[r] > kBigDegree;
   }
-  warp_append_k<4>(reg, v, s.qout, s.n_reg, g.n, a.overflow);
+  if (s.res->chunk) warp_append_res<4>(reg, v, s.qout, s.n_reg, s.near_cap, a.overflow, *s.res);
+  else warp_append_k<4>(reg, v, s.qout, s.n_reg, g.n, a.overflow);
   warp_append_k<4>(big, v, s.hout, s.n_big, g.n, a.overflow);
   warp_append_k<4>(to_far, v, s.fout, s.fc, g.n, a.overflow);
 }
@@ -836,11 +839,15 @@ __device__ __forceinline__ void sssp_run(gsrb::GridSync<V>& bar, bool ok, const 
       }
       uint32_t d = 0;
       if (to_near) d = __ldg(g.row + v + 1) - __ldg(g.row + v);
-      warp_append(to_near && d <= kBigDegree, v, qout, &c->n_reg, g.n, a.overflow);
+      // (the near queue's slots may include reservation holes: 2n of them)
+      warp_append(to_near && d <= kBigDegree, v, qout, &c->n_reg, 2u * g.n, a.overflow);
       warp_append(to_near && d > kBigDegree, v, hout, &c->n_big, g.n, a.overflow);
       warp_append(to_far, v, fout, fc, g.n, a.overflow);
     };
-    const RelaxSink sink{qout, hout, &c->n_reg, &c->n_big, fout, fc, stamp, fgen, T};
+    // near-queue reservations in chunks of 64 slots when the queue (2n slots)
+    // can hold the holes of every warp
+    WarpRes res{0ull, 0u, 63ull * team.nwarps() <= g.n ? 64u : 0u};
+    const RelaxSink sink{qout, hout, &c->n_reg, &c->n_big, fout, fc, stamp, fgen, T, &res, 2u * g.n};
     // vertex lists relaxed edge-balanced: edge prefix, first edge, distance
     ListSmem& L_ = list_smem();
     uint32_t* s_lp = L_.p;
@@ -892,8 +899,10 @@ __device__ __forceinline__ void sssp_run(gsrb::GridSync<V>& bar, bool ok, const 
         uint32_t u = 0, b = 0, e = 0;
         if (i < nreg) {
           u = __ldcg(qin + i);
-          b = __ldg(g.row + u);
-          e = __ldg(g.row + u + 1);
+          if (u != kHole) {
+            b = __ldg(g.row + u);
+            e = __ldg(g.row + u + 1);
+          }
         }
         const uint32_t deg = e - b;
         bool warp_tier = deg > kWarpDegree;
@@ -925,6 +934,7 @@ __device__ __forceinline__ void sssp_run(gsrb::GridSync<V>& bar, bool ok, const 
         sssp_relax_list(a, s_lp, s_lb, s_ld, ncta, threadIdx.x, blockDim.x, sink, my_edges);
       }
     }
+    warp_res_close(qout, 2u * g.n, res);
     relaxed_edges += my_edges;
     ++step;
     ok = bar.sync();

@@ -121,6 +121,65 @@ __device__ __forceinline__ void warp_append_k(const bool* pred, const T* v, T* q
   }
 }
 
+// Queue slots reserved by a warp in chunks: one atomic on the shared counter
+// per chunk instead of one per warp step (every warp of a large round appends
+// at almost every step, and those atomics serialise on one L2 line).  Slots a
+// warp reserved but did not fill hold kHole, which readers skip; a queue then
+// holds at most (chunk - 1) holes per warp more than its entries.
+constexpr uint32_t kHole = 0xffffffffu;
+struct WarpRes {
+  unsigned long long base;  // next reserved slot (warp-uniform)
+  uint32_t left;            // reserved slots not yet filled
+  uint32_t chunk;           // slots per reservation (0: no reservation, append directly)
+};
+
+template <int K, class T>
+__device__ __forceinline__ void warp_append_res(const bool* pred, const T* v, T* q, unsigned long long* cnt,
+                                                uint32_t cap, uint32_t* overflow, WarpRes& res) {
+  uint32_t mask[K];
+  uint32_t tot = 0;
+#pragma unroll
+  for (int r = 0; r < K; ++r) {
+    mask[r] = __ballot_sync(0xffffffffu, pred[r]);
+    tot += __popc(mask[r]);
+  }
+  if (!tot) return;
+  if (tot > res.left) {
+    for (uint32_t i = lane_id(); i < res.left; i += 32) {
+      const unsigned long long pos = res.base + i;
+      if (pos < cap) q[pos] = (T)kHole;
+    }
+    const uint32_t want = tot > res.chunk ? tot : res.chunk;
+    unsigned long long b = 0;
+    if (lane_id() == 0) b = atomicAdd(cnt, (unsigned long long)want);
+    res.base = __shfl_sync(0xffffffffu, b, 0);
+    res.left = want;
+  }
+  const uint32_t lt = lanemask_lt();
+  unsigned long long base = res.base;
+#pragma unroll
+  for (int r = 0; r < K; ++r) {
+    if (pred[r]) {
+      const unsigned long long pos = base + __popc(mask[r] & lt);
+      if (pos < cap) q[pos] = v[r];
+      else atomicExch(overflow, 1u);
+    }
+    base += __popc(mask[r]);
+  }
+  res.base = base;
+  res.left -= tot;
+}
+
+// Fills the warp's unused reserved slots with holes (end of a round).
+template <class T>
+__device__ __forceinline__ void warp_res_close(T* q, uint32_t cap, WarpRes& res) {
+  for (uint32_t i = lane_id(); i < res.left; i += 32) {
+    const unsigned long long pos = res.base + i;
+    if (pos < cap) q[pos] = (T)kHole;
+  }
+  res.left = 0;
+}
+
 __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
