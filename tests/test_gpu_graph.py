@@ -93,6 +93,22 @@ def test_pagerank_residual_converges_to_the_fixed_point(gsrb, ctx, orc, graphs, 
     assert st.levels >= 1
 
 
+@pytest.mark.parametrize("shape", [(1, 64), (1, 128)])
+def test_pagerank_residual_reserved_worklist_chunks(gsrb, ctx, orc, graphs, shape):
+    # few warps (n >= 63 x warps): the worklist is filled through per-warp
+    # reservations whose hole slots the next round skips
+    g = graphs["rmat16"]
+    assert 63 * (ctx.num_sms * shape[0] * shape[1] // 32) <= g.nnodes
+    dg = ctx.graph(g)
+    out = ctx.array(g.nnodes, np.float32)
+    c = gsrb.cfg(variant=gsrb.BAR_FANOUT, ctas_per_sm=shape[0], threads=shape[1], wake_lines=4)
+    rc, st = dg.pagerank_residual(out, 0.85, 1e-6, c=c)
+    gsrb.check(rc, "pagerank_residual")
+    ctx.check_status("pagerank_residual")
+    assert orc.normalized_l1(out.download(), orc.pagerank(g, 0.85, 400)) <= 2e-5
+    dg.free()
+
+
 def test_pagerank_residual_round_cap(gsrb, ctx, graphs):
     g = graphs["rmat12"]
     dg = ctx.graph(g)

@@ -1213,6 +1213,7 @@ struct PrrSink {
   unsigned long long* n_reg;
   unsigned long long* n_big;
   uint32_t stamp;  // a vertex enters the next worklist at most once per round
+  WarpRes* res;    // the warp's worklist reservation (chunk 0: direct appends)
 };
 
 // Push residual along four edges per lane at once: edge r of the lane is j[r]
@@ -1246,7 +1247,8 @@ __device__ __forceinline__ void prr_push4e(const PrrArgs& a, const float* upd, c
     big[r] = cross[r] && d > kBigDegree;
     pushes += cross[r] ? 1u : 0u;
   }
-  warp_append_k<4>(reg, w, s.qout, s.n_reg, g.n, a.overflow);
+  if (s.res->chunk) warp_append_res<4>(reg, w, s.qout, s.n_reg, 2u * g.n, a.overflow, *s.res);
+  else warp_append_k<4>(reg, w, s.qout, s.n_reg, g.n, a.overflow);
   warp_append_k<4>(big, w, s.hout, s.n_big, g.n, a.overflow);
 }
 
@@ -1363,11 +1365,15 @@ pr_residual_kernel(gsrb::GridBarrier gb, PrrArgs a) {
       uint32_t d = 0;
       if (cross) cross = atomicExch(a.mark + w, stamp) != stamp;
       if (cross) d = __ldg(g.row + w + 1) - __ldg(g.row + w);
-      warp_append(cross && d <= kBigDegree, w, qout, &c->n_reg, g.n, a.overflow);
+      // (the worklist's slots may include reservation holes: 2n of them)
+      warp_append(cross && d <= kBigDegree, w, qout, &c->n_reg, 2u * g.n, a.overflow);
       warp_append(cross && d > kBigDegree, w, hout, &c->n_big, g.n, a.overflow);
       pushes += cross ? 1u : 0u;
     };
-    const PrrSink sink{qout, hout, &c->n_reg, &c->n_big, stamp};
+    // worklist reservations in chunks of 64 slots when the queue (2n slots)
+    // can hold the holes of every warp (see WarpRes)
+    WarpRes wres{0ull, 0u, 63ull * (nthreads >> 5) <= g.n ? 64u : 0u};
+    const PrrSink sink{qout, hout, &c->n_reg, &c->n_big, stamp, &wres};
     ListSmem& L_ = list_smem();
     // builds an edge-balanced list from vertex ids and their updates (CTA-wide)
     auto build_list = [&](auto id_of, auto upd_of, uint32_t cnt) {
@@ -1433,8 +1439,8 @@ pr_residual_kernel(gsrb::GridBarrier gb, PrrArgs a) {
       const uint32_t i = base + lane;
       uint32_t u = 0, b = 0, e = 0;
       float upd = 0.f;
-      if (i < nreg) {
-        u = __ldcg(qin + i);
+      if (i < nreg) u = __ldcg(qin + i);
+      if (i < nreg && u != kHole) {
         b = __ldg(g.row + u);
         e = __ldg(g.row + u + 1);
         const float res = atomicExch(a.r + u, 0.f);
@@ -1469,6 +1475,7 @@ pr_residual_kernel(gsrb::GridBarrier gb, PrrArgs a) {
       build_list([&](uint32_t i) { return s_cta_u[i]; }, [&](uint32_t i, uint32_t) { return s_cta_upd[i]; }, ncta);
       prr_push_list(a, L_.p, L_.b, L_.d, ncta, threadIdx.x, blockDim.x, sink, pushes);
     }
+    warp_res_close(qout, 2u * g.n, wres);
     ok = bar.sync();
   }
   const unsigned long long ws = warp_sum_u64(pushes);
