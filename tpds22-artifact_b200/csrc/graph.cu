@@ -101,7 +101,7 @@ __device__ __noinline__ void bfs_solo(const BfsArgs& a, uint32_t L, uint32_t nre
       m_acc += d;
     };
     expand_hub_ranges(one, hin, nbig, push_edge);
-    const PushSink sink{qout, hout, &s_c.n_reg, &s_c.n_big, g.n, a.overflow};
+    const PushSink sink{qout, hout, &s_c.n_reg, &s_c.n_big, g.n, a.overflow, nullptr, nullptr, 0u};
     auto lanes = [&](uint32_t b, uint32_t mine, uint32_t kmax) {
       bfs_push_lanes(g, a.level, Li, b, mine, kmax, false, sink, m_acc);
     };
@@ -117,9 +117,11 @@ __device__ __noinline__ void bfs_solo(const BfsArgs& a, uint32_t L, uint32_t nre
     if (stop) {
       if (threadIdx.x == 0) {
         a.cnt[L % 3].n_reg = nr;
+        a.cnt[L % 3].n_real = nr;
         a.cnt[L % 3].n_big = nb;
         a.cnt[L % 3].m_next = mf;
         a.cnt[(L + 1) % 3].n_reg = 0;
+        a.cnt[(L + 1) % 3].n_real = 0;
         a.cnt[(L + 1) % 3].n_big = 0;
         a.cnt[(L + 1) % 3].m_next = 0;
         a.solo[0] = L;
@@ -331,11 +333,11 @@ __device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const B
   if (tid == 0) {
     const bool hub = dsrc > kBigDegree;
     reinterpret_cast<uint2*>(hub ? a.hq[0] : a.q[0])[0] = make_uint2(g.row[a.src], g.row[a.src + 1]);
-    a.cnt[0].n_reg = hub ? 0 : 1;
+    a.cnt[0].n_reg = a.cnt[0].n_real = hub ? 0 : 1;
     a.cnt[0].n_big = hub ? 1 : 0;
     a.cnt[0].m_next = dsrc;
-    a.cnt[1].n_reg = a.cnt[1].n_big = a.cnt[1].m_next = 0;
-    a.cnt[2].n_reg = a.cnt[2].n_big = a.cnt[2].m_next = 0;
+    a.cnt[1].n_reg = a.cnt[1].n_real = a.cnt[1].n_big = a.cnt[1].m_next = 0;
+    a.cnt[2].n_reg = a.cnt[2].n_real = a.cnt[2].n_big = a.cnt[2].m_next = 0;
   }
   ok = bar.sync() && ok;
 
@@ -351,9 +353,10 @@ __device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const B
   unsigned long long last_mf = 0;
   for (; ok; ++L) {
     const LevelCounters cur = {__ldcg(&a.cnt[(L - 1) % 3].n_reg), __ldcg(&a.cnt[(L - 1) % 3].n_big),
-                               __ldcg(&a.cnt[(L - 1) % 3].m_next), 0};
+                               __ldcg(&a.cnt[(L - 1) % 3].m_next), __ldcg(&a.cnt[(L - 1) % 3].n_real)};
+    // nreg counts queue slots (the expansion's bound), n_real the entries
     const uint32_t nreg = (uint32_t)cur.n_reg, nbig = (uint32_t)cur.n_big;
-    const uint32_t nf = nreg + nbig;
+    const uint32_t nf = (uint32_t)cur.n_real + nbig;
     if (nf == 0) break;
     const unsigned long long mf = cur.m_next;
     if (L > 1) {
@@ -413,6 +416,7 @@ __device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const B
     if (team.cta == 0 && threadIdx.x == 0) {
       // the counter set of level L + 1 was last read before barrier L - 1
       a.cnt[(L + 1) % 3].n_reg = 0;
+      a.cnt[(L + 1) % 3].n_real = 0;
       a.cnt[(L + 1) % 3].n_big = 0;
       a.cnt[(L + 1) % 3].m_next = 0;
       if (L - 1 < a.trace_cap) {
@@ -453,12 +457,18 @@ __device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const B
     LevelCounters* c = &a.cnt[L % 3];
     unsigned long long m_acc = 0;
     const int32_t Li = (int32_t)L;
+    // regular-queue slots reserved per warp in chunks of 64 (one counter atomic
+    // per chunk) when the queue's 2n slots can hold every warp's holes
+    WarpRes res{0ull, 0u, 63ull * team.nwarps() <= g.n ? 64u : 0u};
+    uint32_t real_w = 0;  // regular entries this warp appended (warp-uniform)
+    const PushSink sink{qout, hout, &c->n_reg, &c->n_big, g.n, a.overflow, &res, &real_w, 2u * g.n};
 
     auto discover = [&](bool disc, uint32_t v) {
       uint2 r = make_uint2(0u, 0u);
       if (disc) r = make_uint2(__ldg(g.row + v), __ldg(g.row + v + 1));
       const uint32_t d = r.y - r.x;
-      warp_append(disc && d <= kBigDegree, r, qout, &c->n_reg, g.n, a.overflow);
+      const bool reg1[1] = {disc && d <= kBigDegree};
+      push_append_reg<1>(reg1, &r, sink);
       warp_append(disc && d > kBigDegree, r, hout, &c->n_big, g.n, a.overflow);
       m_acc += d;
     };
@@ -475,7 +485,7 @@ __device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const B
     if (dir == DIR_PUSH) {
       if (nbig > 1 && nbig <= kHubList) {
         // hubs edge-balanced over the team: every CTA builds the same prefix
-        bfs_push_hubs(a, team, hin, nbig, Li, PushSink{qout, hout, &c->n_reg, &c->n_big, g.n, a.overflow}, m_acc);
+        bfs_push_hubs(a, team, hin, nbig, Li, sink, m_acc);
       } else {
         expand_hub_ranges(team, hin, nbig, push_edge);
       }
@@ -486,7 +496,6 @@ __device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const B
           break;
         }
       } else {
-        const PushSink sink{qout, hout, &c->n_reg, &c->n_big, g.n, a.overflow};
         const bool precheck = nf > kPushPrecheckFrontier;
         auto lanes = [&](uint32_t b, uint32_t mine, uint32_t kmax) {
           bfs_push_lanes(g, a.level, Li, b, mine, kmax, precheck, sink, m_acc);
@@ -554,9 +563,11 @@ __device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const B
         discover(found, v);
       }
     }
-    // per-warp edge sums of the new frontier
+    // per-warp edge sums and entry counts of the new frontier
+    warp_res_close(qout, 2u * g.n, res, make_uint2(0u, 0u));
     const unsigned long long ws = warp_sum_u64(m_acc);
     if (lane_id() == 0 && ws) atomicAdd(&c->m_next, ws);
+    if (lane_id() == 0 && real_w) atomicAdd(&c->n_real, (unsigned long long)real_w);
     ok = bar.sync();
   }
   if (team.cta == 0 && threadIdx.x == 0) {
@@ -661,7 +672,7 @@ __device__ __forceinline__ void sssp_relax4e(const SsspArgs& a, const long long*
     reg[r] = to_near[r] && d[r] <= kBigDegree;
     big[r] = to_near[r] && d[r] > kBigDegree;
   }
-  if (s.res->chunk) warp_append_res<4>(reg, v, s.qout, s.n_reg, s.near_cap, a.overflow, *s.res);
+  if (s.res->chunk) warp_append_res<4>(reg, v, s.qout, s.n_reg, s.near_cap, a.overflow, *s.res, kHole);
   else warp_append_k<4>(reg, v, s.qout, s.n_reg, g.n, a.overflow);
   warp_append_k<4>(big, v, s.hout, s.n_big, g.n, a.overflow);
   warp_append_k<4>(to_far, v, s.fout, s.fc, g.n, a.overflow);
@@ -934,7 +945,7 @@ __device__ __forceinline__ void sssp_run(gsrb::GridSync<V>& bar, bool ok, const 
         sssp_relax_list(a, s_lp, s_lb, s_ld, ncta, threadIdx.x, blockDim.x, sink, my_edges);
       }
     }
-    warp_res_close(qout, 2u * g.n, res);
+    warp_res_close(qout, 2u * g.n, res, kHole);
     relaxed_edges += my_edges;
     ++step;
     ok = bar.sync();
@@ -1247,7 +1258,7 @@ __device__ __forceinline__ void prr_push4e(const PrrArgs& a, const float* upd, c
     big[r] = cross[r] && d > kBigDegree;
     pushes += cross[r] ? 1u : 0u;
   }
-  if (s.res->chunk) warp_append_res<4>(reg, w, s.qout, s.n_reg, 2u * g.n, a.overflow, *s.res);
+  if (s.res->chunk) warp_append_res<4>(reg, w, s.qout, s.n_reg, 2u * g.n, a.overflow, *s.res, kHole);
   else warp_append_k<4>(reg, w, s.qout, s.n_reg, g.n, a.overflow);
   warp_append_k<4>(big, w, s.hout, s.n_big, g.n, a.overflow);
 }
@@ -1475,7 +1486,7 @@ pr_residual_kernel(gsrb::GridBarrier gb, PrrArgs a) {
       build_list([&](uint32_t i) { return s_cta_u[i]; }, [&](uint32_t i, uint32_t) { return s_cta_upd[i]; }, ncta);
       prr_push_list(a, L_.p, L_.b, L_.d, ncta, threadIdx.x, blockDim.x, sink, pushes);
     }
-    warp_res_close(qout, 2u * g.n, wres);
+    warp_res_close(qout, 2u * g.n, wres, kHole);
     ok = bar.sync();
   }
   const unsigned long long ws = warp_sum_u64(pushes);
@@ -1623,8 +1634,9 @@ gsrb_status_t graph_scratch(gsrb_graph* G) {
   const size_t n = G->n;
   cudaError_t e = cudaSuccess;
   for (int k = 0; k < 2 && !e; ++k) {
-    // 2n words: BFS keeps an edge range (two words) per queued vertex
-    e = dalloc(&G->q[k], 2 * n);
+    // 4n words: BFS keeps an edge range (two words) per queue slot, and up to
+    // 2n slots (entries plus reservation holes)
+    e = dalloc(&G->q[k], 4 * n);
     if (!e) e = dalloc(&G->hq[k], 2 * n);
     if (!e) e = dalloc(&G->far[k], n);
     if (!e) e = dalloc(&G->contrib[k], n);
@@ -1638,7 +1650,7 @@ gsrb_status_t graph_scratch(gsrb_graph* G) {
   if (!e) e = dalloc(&G->trace, G->trace_cap);
   if (!e) e = dalloc(&G->mlp, 1);
   if (!e) e = cudaMemset(G->mlp, 0, sizeof(MLPWeights));
-  if (!e) e = dalloc(&G->lb_pre, n);
+  if (!e) e = dalloc(&G->lb_pre, 2 * n);  // one per queue slot (holes included)
   if (!e) e = dalloc(&G->lb_own, (size_t)G->m / kLbChunk + 2);
   if (!e) e = dalloc(&G->lb_part, kLbMaxCtas);
   // PageRank hub chunks (degree > kPrHubDegree), built on the host from row_start

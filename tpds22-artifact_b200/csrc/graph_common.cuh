@@ -51,7 +51,7 @@ struct LevelCounters {
   unsigned long long n_reg;   // regular-queue appends
   unsigned long long n_big;   // hub-queue appends
   unsigned long long m_next;  // out-edges of appended vertices
-  unsigned long long pad;
+  unsigned long long n_real;  // BFS: regular entries (n_reg counts slots, reservation holes included)
 };
 
 // The CTAs working on one traversal: the whole grid for a single traversal, a
@@ -134,8 +134,8 @@ struct WarpRes {
 };
 
 template <int K, class T>
-__device__ __forceinline__ void warp_append_res(const bool* pred, const T* v, T* q, unsigned long long* cnt,
-                                                uint32_t cap, uint32_t* overflow, WarpRes& res) {
+__device__ __forceinline__ uint32_t warp_append_res(const bool* pred, const T* v, T* q, unsigned long long* cnt,
+                                                    uint32_t cap, uint32_t* overflow, WarpRes& res, T hole) {
   uint32_t mask[K];
   uint32_t tot = 0;
 #pragma unroll
@@ -143,11 +143,11 @@ __device__ __forceinline__ void warp_append_res(const bool* pred, const T* v, T*
     mask[r] = __ballot_sync(0xffffffffu, pred[r]);
     tot += __popc(mask[r]);
   }
-  if (!tot) return;
+  if (!tot) return 0;
   if (tot > res.left) {
     for (uint32_t i = lane_id(); i < res.left; i += 32) {
       const unsigned long long pos = res.base + i;
-      if (pos < cap) q[pos] = (T)kHole;
+      if (pos < cap) q[pos] = hole;
     }
     const uint32_t want = tot > res.chunk ? tot : res.chunk;
     unsigned long long b = 0;
@@ -168,14 +168,15 @@ __device__ __forceinline__ void warp_append_res(const bool* pred, const T* v, T*
   }
   res.base = base;
   res.left -= tot;
+  return tot;
 }
 
 // Fills the warp's unused reserved slots with holes (end of a round).
 template <class T>
-__device__ __forceinline__ void warp_res_close(T* q, uint32_t cap, WarpRes& res) {
+__device__ __forceinline__ void warp_res_close(T* q, uint32_t cap, WarpRes& res, T hole) {
   for (uint32_t i = lane_id(); i < res.left; i += 32) {
     const unsigned long long pos = res.base + i;
-    if (pos < cap) q[pos] = (T)kHole;
+    if (pos < cap) q[pos] = hole;
   }
   res.left = 0;
 }
@@ -296,7 +297,27 @@ struct PushSink {
   unsigned long long* n_big;
   uint32_t cap;
   uint32_t* overflow;
+  WarpRes* res;                // regular-queue reservation (null: append directly)
+  uint32_t* real;              // regular entries appended by this warp (with res)
+  uint32_t rcap;               // regular-queue slots (with res)
 };
+
+// Appends the regular entries of a push step: through the warp's reservation
+// when there is one (counting the entries), else directly.
+template <int K>
+__device__ __forceinline__ void push_append_reg(const bool* reg, const uint2* rg, const PushSink& s) {
+  if (s.res && s.res->chunk) {
+    *s.real += warp_append_res<K>(reg, rg, s.qout, s.n_reg, s.rcap, s.overflow, *s.res, make_uint2(0u, 0u));
+  } else {
+    if (s.real) {
+      uint32_t tot = 0;
+#pragma unroll
+      for (int r = 0; r < K; ++r) tot += __popc(__ballot_sync(0xffffffffu, reg[r]));
+      *s.real += tot;
+    }
+    warp_append_k<K>(reg, rg, s.qout, s.n_reg, s.cap, s.overflow);
+  }
+}
 
 // Frontiers up to this size check a destination's level only through the
 // claim itself (compare-and-swap INF -> L) and load its row range alongside
@@ -347,7 +368,7 @@ __device__ __forceinline__ void bfs_push4e(const DevCSR& g, int32_t* level, int3
     any_big |= big[r];
     m_acc += d;
   }
-  warp_append_k<4>(reg, rg, s.qout, s.n_reg, s.cap, s.overflow);
+  push_append_reg<4>(reg, rg, s);
   if (__any_sync(0xffffffffu, any_big)) warp_append_k<4>(big, rg, s.hout, s.n_big, s.cap, s.overflow);
 }
 
@@ -404,7 +425,7 @@ __device__ __forceinline__ void bfs_push_lanes(const DevCSR& g, int32_t* level, 
       any_big |= big[r];
       m_acc += d;
     }
-    warp_append_k<4>(reg, rg, s.qout, s.n_reg, s.cap, s.overflow);
+    push_append_reg<4>(reg, rg, s);
     if (__any_sync(0xffffffffu, any_big)) warp_append_k<4>(big, rg, s.hout, s.n_big, s.cap, s.overflow);
   }
 }
