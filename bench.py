@@ -362,11 +362,15 @@ def train_policy(gsrb, ctx, pol):
     """Per-level traces of training graphs (not the evaluation graphs) -> MLP."""
     graphs = [gsrb.rmat(s, 16, seed=SEED + 1000 + s) for s in (14, 16, 18, 20, 21, 22)]
     graphs += [gsrb.grid2d(256, 256, seed=SEED + 7), gsrb.grid2d(1024, 64, seed=SEED + 8),
-               gsrb.grid2d(1024, 1024, seed=SEED + 9), gsrb.grid2d(2048, 512, seed=SEED + 10)]
+               gsrb.grid2d(1024, 1024, seed=SEED + 9), gsrb.grid2d(2048, 512, seed=SEED + 10),
+               gsrb.grid2d(4096, 1024, seed=SEED + 11)]
     X, Y, M = [], [], []
+    cands = pol.launch_candidates()
+    launch = []
     for g in graphs:
         dg = ctx.graph(g)
-        x, y, m, _ = pol.collect(ctx, dg, 0, reps=2)
+        x, y, m, info = pol.collect(ctx, dg, 0, reps=2, launch_cfgs=cands)
+        launch.append([g.nnodes, g.nedges] + [round(float(t), 3) for t in info["launch_ms"]])
         X.append(x)
         Y.append(y)
         M.append(m)
@@ -376,10 +380,13 @@ def train_policy(gsrb, ctx, pol):
     params, hist = pol.train(ctx, X, Y, M, steps=3000)
     acc = pol.accuracy(ctx, params, X, Y, M)
     return params, {"levels": int(len(X)), "train_s": round(time.time() - t0, 2), "loss_first": float(hist[0]),
-                    "loss_last": float(hist[-1]), **acc}
+                    "loss_last": float(hist[-1]), **acc,
+                    "launch_labels": {"candidates": [gsrb.VARIANT_NAMES[c.variant] + f" {c.ctas_per_sm}x{c.threads}"
+                                                     for c in cands],
+                                      "n_m_ms0_ms1": launch}}
 
 
-def bfs_runs(gsrb, ctx, orc, dg, g, params, cfg, reps=3):
+def bfs_runs(gsrb, ctx, orc, dg, g, params, cfg, reps=3, launch=None):
     out = ctx.array(g.nnodes, np.int32)
     want = orc.bfs(g, 0)
     m_trav = orc.traversed_edges(g, want)
@@ -403,6 +410,34 @@ def bfs_runs(gsrb, ctx, orc, dg, g, params, cfg, reps=3):
                 # per-level schedule (0 push, 1 pull, 2 topology push, 3 one-CTA push)
                 res[name]["dirs"] = [int(x) for x in dg.trace(64)["dir"][: int(st.levels)]]
     res["learned_vs_plain"] = round(res["plain_push"]["ms"] / res["learned"]["ms"], 3)
+    if launch is not None:
+        # the policy's head 3 also picks the launch (barrier variant and CTA
+        # shape) between two fixed candidates, with no autotuning; the learned
+        # traversal's time under each candidate shows whether it chose well
+        each = []
+        for c in launch:
+            ts = []
+            for _ in range(reps):
+                rc, st = dg.bfs(0, out, gsrb.BFS_LEARNED, c)
+                gsrb.check(rc, "bfs learned (launch candidate)")
+                ts.append(st.kernel_ms)
+            each.append(round(statistics.median(ts), 3))
+        dg.set_launch_choices(*launch)
+        ts = []
+        for _ in range(reps):
+            rc, st = dg.bfs(0, out, gsrb.BFS_LEARNED)
+            gsrb.check(rc, "bfs learned (own launch)")
+            ts.append(st.kernel_ms)
+        ok = bool(np.array_equal(out.download(), want))
+        k, z = dg.policy_launch(0)
+        dg.set_launch_choices(None, None)
+        t = statistics.median(ts)
+        res["learned_own_launch"] = {"ms": round(t, 3), "GTEPS": round(m_trav / (t * 1e-3) / 1e9, 3),
+                                     "launch": int(st.launch) - 1, "head3": round(z, 3),
+                                     "candidates_ms": each,
+                                     "candidates": [gsrb.VARIANT_NAMES[c.variant] + f" {c.ctas_per_sm}x{c.threads}"
+                                                    for c in launch],
+                                     "bit_exact": ok}
     return res
 
 
@@ -433,7 +468,7 @@ def graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, verify_pr=True):
     best, _, _ = tune.tune_bfs(ctx, dg, 0, gsrb.BFS_HEURISTIC, reps=1)
     cache["bfs_rmat"] = best
     cfg = tune.cfg_from(best)
-    res["rmat22"]["bfs"] = bfs_runs(gsrb, ctx, orc, dg, rm, params, cfg)
+    res["rmat22"]["bfs"] = bfs_runs(gsrb, ctx, orc, dg, rm, params, cfg, launch=pol.launch_candidates())
     res["rmat22"]["sssp"] = sssp_runs(gsrb, ctx, orc, dg, rm, [("reference_delta", 10000), ("delta_256", 256)], cfg)
     out = ctx.array(rm.nnodes, np.float32)
     rc, st = dg.pagerank(out, 0.85, 50, cfg)
@@ -465,7 +500,8 @@ def graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, verify_pr=True):
     best, _, _ = tune.tune_bfs(ctx, dg, 0, gsrb.BFS_PUSH, reps=1)
     cache["bfs_grid"] = best
     cfg = tune.cfg_from(best)
-    res["grid2048"] = {"n": gr.nnodes, "m": gr.nedges, "bfs": bfs_runs(gsrb, ctx, orc, dg, gr, params, cfg, reps=2)}
+    res["grid2048"] = {"n": gr.nnodes, "m": gr.nedges,
+                       "bfs": bfs_runs(gsrb, ctx, orc, dg, gr, params, cfg, reps=2, launch=pol.launch_candidates())}
     res["grid2048"]["sssp"] = sssp_runs(gsrb, ctx, orc, dg, gr, [("reference_delta", 10000), ("delta_4096", 4096)],
                                         cfg)
     dg.free()

@@ -249,7 +249,8 @@ typedef struct gsrb_traversal_stats {
   uint64_t edges;         /* BFS: out-edges of reached vertices (the TEPS numerator);
                              SSSP: edges relaxed */
   float kernel_ms;        /* CUDA-event time of the traversal launch */
-  uint32_t _pad;
+  uint32_t launch;        /* BFS (learned, cfg NULL, launch choices set): 1 + the index of the
+                             launch configuration the policy picked; else 0 */
 } gsrb_traversal_stats_t;
 
 /* BFS direction modes. */
@@ -282,6 +283,14 @@ gsrb_status_t gsrb_graph_info(gsrb_graph_t g, uint32_t* n, uint64_t* m, uint32_t
 gsrb_status_t gsrb_graph_is_symmetric(gsrb_graph_t g, int32_t* symmetric);
 /* Policy network weights (gsrb_mlp_* layout, gsrb_mlp_param_count() floats). */
 gsrb_status_t gsrb_graph_set_policy(gsrb_graph_t g, const float* h_weights, size_t count);
+/* Two launch configurations (barrier variant, CTAs per SM, threads) for
+ * learned traversals: gsrb_bfs in GSRB_BFS_LEARNED mode with cfg == NULL then
+ * runs the one head 3 of the policy picks.  Both NULL: forget them. */
+gsrb_status_t gsrb_graph_set_launch_choices(gsrb_graph_t g, const gsrb_cfg_t* cfg0, const gsrb_cfg_t* cfg1);
+/* The policy's launch choice for a BFS from src: head 3 evaluated on the host
+ * on the first level's features (frontier = src); *choice = 1 if it is > 0,
+ * else 0; *score (may be NULL) = head 3.  GSRB_ERR_STATE without a policy. */
+gsrb_status_t gsrb_graph_policy_launch(gsrb_graph_t g, uint32_t src, int32_t* choice, float* score);
 /* Copy up to max_records 48-byte per-level trace records of the last traversal. */
 gsrb_status_t gsrb_graph_trace(gsrb_graph_t g, void* h_out, uint32_t max_records, uint32_t* records);
 /* BFS levels from src into d_level (int32[n]; INT32_MAX = unreachable).
@@ -333,7 +342,9 @@ gsrb_status_t gsrb_exec_free(gsrb_exec_t exec);
 /* ---- the learned policy: a 12 -> 32 -> 32 -> 4 FP32 MLP -----------------------------
  * Parameter layout (floats): w1[32][12], b1[32], w2[32][32], b2[32], w3[4][32], b3[4].
  * Heads: [0] logit(pull faster than push), [1] logit(topology push faster than
- * worklist push), [2] log2(1 + next frontier size), [3] spare.  Loss: masked
+ * worklist push), [2] log2(1 + next frontier size), [3] log2(t0 / t1), the
+ * traversal time under launch configuration 0 over that under configuration 1
+ * (gsrb_graph_set_launch_choices; read on the first level only).  Loss: masked
  * BCE-with-logits on heads 0-1, masked 0.5*(z-y)^2 on heads 2-3, batch mean.
  * No counterpart in the reference (its traversals use fixed schedules). */
 size_t gsrb_mlp_param_count(void);

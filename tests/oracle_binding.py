@@ -30,6 +30,7 @@ _lib.orc_gr_read.argtypes = [C.c_char_p, C.POINTER(C.c_uint32), C.POINTER(C.c_ui
                              C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.POINTER(C.c_uint32)),
                              C.POINTER(C.POINTER(C.c_int32))]
 _lib.orc_free.argtypes = [_P]
+_lib.orc_mlp_forward.argtypes = [_P, _P, C.c_int, _P]
 _lib.orc_heterosync_golden.argtypes = [C.c_int] * 7 + [_P, C.c_int]
 _lib.orc_heterosync_storage_locs.restype = C.c_int
 _lib.orc_heterosync_storage_locs.argtypes = [C.c_int] * 5
@@ -74,6 +75,15 @@ def max_rel_err(gpu, ref, floor=1e-30):
     gpu = np.ascontiguousarray(gpu, dtype=np.float32)
     ref = np.ascontiguousarray(ref, dtype=np.float64)
     return float(_lib.orc_max_rel_err_f32_f64(_p(gpu), _p(ref), gpu.size, floor))
+
+
+def mlp_forward(params, X):
+    """FP64 forward pass of the policy network: X[B][12] -> [B][4]."""
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    out = np.zeros((X.shape[0], 4), np.float64)
+    _lib.orc_mlp_forward(_p(p), _p(X), X.shape[0], _p(out))
+    return out
 
 
 def bfs(g, src=0):

@@ -207,3 +207,60 @@ def test_sssp_reserved_queue_chunks(gsrb, ctx, orc, graphs, name, delta, shape):
     ctx.check_status("sssp")
     assert np.array_equal(out.download(), orc.dijkstra(g, 0))
     dg.free()
+
+
+def _head3_only(gsrb, bias):
+    """Policy weights whose head 3 is the constant `bias` (hidden layers zero)
+    and whose other heads say "push" and predict nothing."""
+    w = np.zeros(gsrb.mlp_param_count(), np.float32)
+    w[-1] = bias  # b3[3]
+    return w
+
+
+@pytest.mark.parametrize("bias", [-1.5, 2.0])
+def test_policy_picks_the_launch(gsrb, ctx, orc, graphs, bias):
+    g = graphs["rmat16"]
+    dg = ctx.graph(g)
+    dg.set_policy(_head3_only(gsrb, bias))
+    c0 = gsrb.cfg(variant=gsrb.BAR_CCG, ctas_per_sm=2, threads=512, cluster=1)
+    c1 = gsrb.cfg(variant=gsrb.BAR_FLIP, ctas_per_sm=1, threads=256, cluster=1)
+    k, z = dg.policy_launch(0)
+    assert z == pytest.approx(bias) and k == (1 if bias > 0 else 0)
+    out = ctx.array(g.nnodes, np.int32)
+    want = orc.bfs(g, 0)
+    # without launch choices the default shape runs and stats.launch stays 0
+    rc, st = dg.bfs(0, out, gsrb.BFS_LEARNED)
+    gsrb.check(rc, "learned bfs")
+    assert st.launch == 0 and np.array_equal(out.download(), want)
+    dg.set_launch_choices(c0, c1)
+    rc, st = dg.bfs(0, out, gsrb.BFS_LEARNED)
+    gsrb.check(rc, "learned bfs, own launch")
+    assert st.launch == 1 + k
+    assert np.array_equal(out.download(), want)
+    # an explicit cfg overrides the choice; other modes never consult it
+    rc, st = dg.bfs(0, out, gsrb.BFS_LEARNED, c0)
+    gsrb.check(rc)
+    assert st.launch == 0
+    rc, st = dg.bfs(0, out, gsrb.BFS_HEURISTIC)
+    gsrb.check(rc)
+    assert st.launch == 0 and np.array_equal(out.download(), want)
+    dg.set_launch_choices(None, None)
+    rc, st = dg.bfs(0, out, gsrb.BFS_LEARNED)
+    gsrb.check(rc)
+    assert st.launch == 0
+    out.free()
+    dg.free()
+
+
+def test_policy_launch_score_matches_the_oracle_forward(gsrb, ctx, orc, graphs):
+    g = graphs["grid64"]
+    dg = ctx.graph(g)
+    w = gsrb.mlp_init(77)
+    dg.set_policy(w)
+    for src in (0, 5, 1000):
+        deg = int(g.row_start[src + 1] - g.row_start[src])
+        x = gsrb.level_features(g.nnodes, g.nedges, 1, 1, deg, g.nnodes - 1, g.nedges - deg, 1, 0)
+        want = orc.mlp_forward(w, np.asarray(x, np.float32)[None, :])[0, 3]
+        k, z = dg.policy_launch(src)
+        assert z == pytest.approx(want, rel=1e-4, abs=1e-5) and k == (1 if z > 0 else 0)
+    dg.free()

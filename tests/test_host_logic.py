@@ -188,3 +188,37 @@ def test_trace_files_roundtrip_and_labels(gsrb, pol, tmp_path):
     assert Y[1, 0] == 0.0 and M[1, 0] < 0.2
     # next-frontier regression target
     assert Y[0, 2] == pytest.approx(math.log2(11)) and Y[3, 2] == 0.0
+
+
+def test_launch_label_first_level_only(gsrb, pol, tmp_path):
+    push = _fake_trace(gsrb, [1, 10, 300, 50], [16, 160, 4800, 800])
+    rec = {"n": 1000, "m": 16000, "src": 0, "push": push, "pull": push.copy(), "topo": push.copy(),
+           "push_ns": np.array([100.0, 900.0, 4000.0, np.nan]),
+           "pull_ns": np.array([5000.0, 1000.0, 400.0, np.nan]),
+           "topo_ns": np.array([300.0, 900.0, 8000.0, np.nan]),
+           "launch_ms": np.array([2.0, 0.5])}
+    path = tmp_path / "traces.npz"
+    pol.save_traces(path, [rec])
+    back = pol.load_traces(path)
+    assert np.array_equal(back[0]["launch_ms"], [2.0, 0.5])
+    X, Y, M = pol.dataset(back)
+    # no sampled sources: one launch row, the first level's features, after the 4 level rows
+    assert X.shape == (5, 12) and not M[:4, 3].any() and not M[4, :3].any()
+    np.testing.assert_array_equal(X[4], gsrb.level_features(1000, 16000, 1, 1, 16, 999, 16000 - 16, 1, 0))
+    np.testing.assert_array_equal(X[4], X[0])
+    # configuration 1 is 4x faster: head 3 target log2(t0 / t1) = 2
+    assert Y[4, 3] == pytest.approx(2.0) and M[4, 3] == pol.LAUNCH_WEIGHT
+    # sampled sources: one row per source degree, all with the graph's label
+    rec["launch_degs"] = np.array([16, 3, 40])
+    pol.save_traces(path, [rec])
+    X, Y, M = pol.dataset(pol.load_traces(path))
+    assert X.shape == (7, 12) and np.all(Y[4:, 3] == Y[4, 3]) and np.all(M[4:, 3] == pol.LAUNCH_WEIGHT)
+    np.testing.assert_array_equal(X[5], gsrb.level_features(1000, 16000, 1, 1, 3, 999, 16000 - 3, 1, 0))
+    # the target is clipped to [-4, 4]
+    rec["launch_ms"] = np.array([1.0, 1000.0])
+    _, Y, _ = pol.features_labels(rec)
+    assert np.all(Y[4:, 3] == -4.0)
+    # traces without launch times carry no launch rows
+    del rec["launch_ms"]
+    X, _, M = pol.features_labels(rec)
+    assert X.shape == (4, 12) and not M[:, 3].any()

@@ -1568,6 +1568,9 @@ struct gsrb_graph {
   uint32_t* hub_done = nullptr;   // [nhubs] chunk counters
   MLPWeights* mlp = nullptr;
   bool mlp_set = false;
+  MLPWeights mlp_host{};        // host copy of the policy weights (the launch choice runs on the host)
+  gsrb_cfg_t launch[2]{};       // the two launch configurations head 3 chooses between
+  bool launch_set = false;
   uint32_t* lb_pre = nullptr;   // [n] load-balanced BFS: edge offset of each queue entry
   uint32_t* lb_own = nullptr;   // [m / kLbChunk + 2] queue entry owning each chunk's first edge
   uint32_t* lb_part = nullptr;  // [kLbMaxCtas] per-CTA edge totals
@@ -1748,6 +1751,7 @@ gsrb_status_t finish_stats(gsrb_graph* G, gsrb_traversal_stats_t* st, float ms) 
     st->edges = edges;
     st->kernel_ms = ms;
     st->trace_records = h[4] < G->trace_cap ? h[4] : G->trace_cap;
+    st->launch = 0;
   }
   if (h[0]) return GSRB_ERR_OVERFLOW;
   if (h[7]) return GSRB_ERR_TIMEOUT;
@@ -1828,7 +1832,70 @@ gsrb_status_t gsrb_graph_is_symmetric(gsrb_graph_t G, int32_t* symmetric) {
 gsrb_status_t gsrb_graph_set_policy(gsrb_graph_t G, const float* h_weights, size_t count) {
   if (!G || !h_weights || count != sizeof(MLPWeights) / sizeof(float)) return GSRB_ERR_ARG;
   GSRB_CUDA(cudaMemcpy(G->mlp, h_weights, sizeof(MLPWeights), cudaMemcpyHostToDevice));
+  memcpy(&G->mlp_host, h_weights, sizeof(MLPWeights));
   G->mlp_set = true;
+  return GSRB_OK;
+}
+
+gsrb_status_t gsrb_graph_set_launch_choices(gsrb_graph_t G, const gsrb_cfg_t* cfg0, const gsrb_cfg_t* cfg1) {
+  if (!G) return GSRB_ERR_ARG;
+  if (!cfg0 && !cfg1) {
+    G->launch_set = false;
+    return GSRB_OK;
+  }
+  if (!cfg0 || !cfg1) return GSRB_ERR_ARG;
+  const gsrb_cfg_t* in[2] = {cfg0, cfg1};
+  for (int k = 0; k < 2; ++k) {
+    const gsrb_cfg_t c = graph_cfg(G->ctx, in[k]);
+    if (!bfs_fn(c.variant)) return GSRB_ERR_UNSUPPORTED;
+    const int grid = grid_of(G->ctx, c);
+    if (grid <= 0 || grid % c.cluster || c.threads % 32 || c.threads > kGraphMaxThreads) return GSRB_ERR_ARG;
+    G->launch[k] = c;
+  }
+  G->launch_set = true;
+  return GSRB_OK;
+}
+
+namespace {
+
+// Host forward pass of the policy network (the layout of MLPWeights; ReLU on
+// the two hidden layers).  Used for the per-traversal launch choice, which is
+// taken before the launch.
+void mlp_forward_host(const MLPWeights& W, const float* x, float* out) {
+  float h1[kHid], h2[kHid];
+  for (int j = 0; j < kHid; ++j) {
+    float z = W.b1[j];
+    for (int i = 0; i < kFeat; ++i) z += W.w1[j][i] * x[i];
+    h1[j] = z > 0.f ? z : 0.f;
+  }
+  for (int j = 0; j < kHid; ++j) {
+    float z = W.b2[j];
+    for (int k = 0; k < kHid; ++k) z += W.w2[j][k] * h1[k];
+    h2[j] = z > 0.f ? z : 0.f;
+  }
+  for (int o = 0; o < kOut; ++o) {
+    float z = W.b3[o];
+    for (int k = 0; k < kHid; ++k) z += W.w3[o][k] * h2[k];
+    out[o] = z;
+  }
+}
+
+}  // namespace
+
+gsrb_status_t gsrb_graph_policy_launch(gsrb_graph_t G, uint32_t src, int32_t* choice, float* score) {
+  if (!G || !choice || src >= G->n) return GSRB_ERR_ARG;
+  if (!G->mlp_set) return GSRB_ERR_STATE;
+  // the first level's features, as the traversal computes them: the frontier
+  // is the source, every other vertex and edge is unvisited
+  uint32_t r[2];
+  GSRB_CUDA(cudaMemcpyAsync(r, G->row + src, sizeof(r), cudaMemcpyDeviceToHost, G->ctx->stream));
+  GSRB_CUDA(cudaStreamSynchronize(G->ctx->stream));
+  const uint32_t dsrc = r[1] - r[0];
+  float feat[kFeat], out[kOut];
+  level_features(feat, G->n, G->m, 1, 1, dsrc, G->n - 1, (unsigned long long)G->m - dsrc, 1, DIR_PUSH);
+  mlp_forward_host(G->mlp_host, feat, out);
+  *choice = out[3] > 0.f ? 1 : 0;
+  if (score) *score = out[3];
   return GSRB_OK;
 }
 
@@ -1852,6 +1919,16 @@ gsrb_status_t gsrb_bfs(gsrb_ctx_t ctx, gsrb_graph_t G, uint32_t src, int32_t* d_
   if (mode == GSRB_BFS_LEARNED && !G->mlp_set) return GSRB_ERR_STATE;
   if (mode == GSRB_BFS_PULL && !G->symmetric) return GSRB_ERR_UNSUPPORTED;
   gsrb_cfg_t c = graph_cfg(ctx, cfgin);
+  uint32_t launch = 0;
+  if (mode == GSRB_BFS_LEARNED && !cfgin && G->launch_set) {
+    // the policy's head 3 picks the launch configuration (barrier variant and
+    // CTA shape) from the first level's features
+    int32_t k = 0;
+    gsrb_status_t st = gsrb_graph_policy_launch(G, src, &k, nullptr);
+    if (st) return st;
+    c = G->launch[k];
+    launch = 1u + (uint32_t)k;
+  }
   const void* fn = bfs_fn(c.variant);
   if (!fn) return GSRB_ERR_UNSUPPORTED;
   const int grid = grid_of(ctx, c);
@@ -1894,7 +1971,9 @@ gsrb_status_t gsrb_bfs(gsrb_ctx_t ctx, gsrb_graph_t G, uint32_t src, int32_t* d_
   GSRB_CUDA(cudaEventSynchronize(ctx->events[63]));
   float ms = 0;
   GSRB_CUDA(cudaEventElapsedTime(&ms, ctx->events[62], ctx->events[63]));
-  return finish_stats(G, stats, ms);
+  st = finish_stats(G, stats, ms);
+  if (stats) stats->launch = launch;
+  return st;
 }
 
 gsrb_status_t gsrb_sssp(gsrb_ctx_t ctx, gsrb_graph_t G, uint32_t src, int32_t* d_dist, int32_t delta,

@@ -157,6 +157,8 @@ _SIGS = {
     "gsrb_graph_info": (C.c_int32, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
     "gsrb_graph_is_symmetric": (C.c_int32, [_P, C.POINTER(C.c_int32)]),
     "gsrb_graph_set_policy": (C.c_int32, [_P, _P, C.c_size_t]),
+    "gsrb_graph_set_launch_choices": (C.c_int32, [_P, C.POINTER(Cfg), C.POINTER(Cfg)]),
+    "gsrb_graph_policy_launch": (C.c_int32, [_P, C.c_uint32, C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
     "gsrb_graph_trace": (C.c_int32, [_P, _P, C.c_uint32, C.POINTER(C.c_uint32)]),
     "gsrb_bfs": (C.c_int32, [_P, _P, C.c_uint32, _P, C.c_int32, C.POINTER(Cfg), C.c_void_p]),
     "gsrb_sssp": (C.c_int32, [_P, _P, C.c_uint32, _P, C.c_int32, C.POINTER(Cfg), C.c_void_p]),
@@ -191,7 +193,7 @@ BFS_FLAG_LB = 0x100  # OR-ed into a mode: load-balanced expansion of large push 
 class TraversalStats(C.Structure):
     _fields_ = [("levels", C.c_uint32), ("aux", C.c_uint32), ("decisions", C.c_uint32),
                 ("trace_records", C.c_uint32), ("edges", C.c_uint64), ("kernel_ms", C.c_float),
-                ("_pad", C.c_uint32)]
+                ("launch", C.c_uint32)]
 
 
 TRACE_DTYPE = np.dtype([("level", "<u4"), ("dir", "<u4"), ("nf", "<u4"), ("nu", "<u4"), ("mf", "<u8"),
@@ -447,6 +449,18 @@ class DeviceGraph:
     def set_policy(self, weights: np.ndarray):
         w = np.ascontiguousarray(weights, dtype=np.float32)
         check(_lib().gsrb_graph_set_policy(self.h, w.ctypes.data, w.size), "set_policy")
+
+    def set_launch_choices(self, c0: Cfg | None, c1: Cfg | None):
+        """The two launch configurations head 3 of the policy chooses between
+        for learned traversals run without a cfg (None, None: forget them)."""
+        check(_lib().gsrb_graph_set_launch_choices(self.h, C.byref(c0) if c0 is not None else None,
+                                                   C.byref(c1) if c1 is not None else None), "set_launch_choices")
+
+    def policy_launch(self, src: int = 0):
+        """(choice, head 3) of the policy for a BFS from src."""
+        k, z = C.c_int32(), C.c_float()
+        check(_lib().gsrb_graph_policy_launch(self.h, src, C.byref(k), C.byref(z)), "policy_launch")
+        return int(k.value), float(z.value)
 
     def trace(self, max_records=1 << 16) -> np.ndarray:
         out = np.zeros(max_records, dtype=TRACE_DTYPE)

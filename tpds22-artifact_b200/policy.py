@@ -13,6 +13,12 @@ direction).  Those times label each level:
     (both weighted by |log2 of the time ratio|: the loss follows the cost of a
     wrong choice, not the count of levels)
     head 2: log2(1 + size of the next frontier) (squared error)
+    head 3: log2(t0 / t1), the heuristic traversal's time under launch
+            configuration 0 over that under configuration 1 (squared error;
+            gsrb_graph_set_launch_choices).  The library reads it on the first
+            level's features only, whose frontier is the source, so it is
+            trained on extra rows: the first-level features of a sample of
+            sources (their degrees), all carrying the graph's label.
 
 Features are computed by gsrb_level_features, the host twin of the function the
 traversal kernel evaluates on the device.  The policy changes only which
@@ -43,6 +49,21 @@ def level_times(trace: np.ndarray, total_ms: float | None = None) -> np.ndarray:
 
 
 TOPO_MARGIN = 0.8
+# weight of one launch row, and the sources sampled per graph for them (a few
+# rows per graph against thousands of level rows)
+LAUNCH_WEIGHT = 10.0
+LAUNCH_SOURCES = 16
+
+
+def launch_candidates():
+    """The two launch configurations head 3 chooses between: the call-wide
+    default shape (2 x 512 threads per SM, grid.sync barrier), which suits
+    power-law graphs whose few levels carry millions of edges, and 2 x 256
+    threads per SM with the split-counter barrier, which suits meshes whose
+    thousands of thin levels are barrier-bound."""
+    g = _g()
+    return (g.cfg(variant=g.BAR_CCG, ctas_per_sm=2, threads=512, cluster=1),
+            g.cfg(variant=g.BAR_FLIP, ctas_per_sm=2, threads=256, cluster=1))
 
 
 def _weight(t_a: float, t_b: float) -> float:
@@ -53,13 +74,38 @@ def _weight(t_a: float, t_b: float) -> float:
     return float(min(4.0, max(0.05, r)))
 
 
-def collect_traces(ctx, dgraph, src: int = 0, reps: int = 1) -> dict:
-    """Raw material of one graph: the per-level trace of the worklist push, the
-    pull and the topology push traversals (the fastest of `reps` runs per
-    level) and the graph's size.  Storable with save_traces."""
+def launch_times(ctx, dgraph, cfgs, src: int = 0, reps: int = 2) -> np.ndarray:
+    """Kernel time (ms, fastest of `reps`) of the heuristic BFS from src under
+    each launch configuration."""
     g = _g()
     out = ctx.array(dgraph.n, np.int32)
+    t = np.zeros(len(cfgs))
+    for k, c in enumerate(cfgs):
+        best = np.inf
+        for _ in range(reps):
+            rc, st = dgraph.bfs(src, out, g.BFS_HEURISTIC, c)
+            g.check(rc, "bfs (launch labels)")
+            best = min(best, float(st.kernel_ms))
+        t[k] = best
+    out.free()
+    return t
+
+
+def collect_traces(ctx, dgraph, src: int = 0, reps: int = 1, launch_cfgs=None) -> dict:
+    """Raw material of one graph: the per-level trace of the worklist push, the
+    pull and the topology push traversals (the fastest of `reps` runs per
+    level), the graph's size and, with launch_cfgs, the heuristic traversal's
+    time under each of the two launch configurations.  Storable with
+    save_traces."""
+    g = _g()
     rec = {"n": int(dgraph.n), "m": int(dgraph.m), "src": int(src)}
+    if launch_cfgs is not None:
+        rec["launch_ms"] = launch_times(ctx, dgraph, launch_cfgs, src, max(reps, 2))
+        deg = dgraph.host.degrees()
+        rng = np.random.default_rng(rec["n"] * 1_000_003 + rec["m"])
+        pick = rng.integers(0, rec["n"], LAUNCH_SOURCES - 1)
+        rec["launch_degs"] = np.concatenate([[deg[src]], deg[pick]]).astype(np.int64)
+    out = ctx.array(dgraph.n, np.int32)
     for name, mode in (("push", g.BFS_PUSH), ("pull", g.BFS_PULL), ("topo", g.BFS_TOPO)):
         best = None
         for _ in range(reps):
@@ -103,14 +149,27 @@ def features_labels(rec: dict):
         Y[i, 2] = np.log2(1.0 + nxt)
         M[i, 2] = 1.0
         prev_dir = 1 if Y[i, 0] > 0.5 and M[i, 0] > 0 else 0
+    if rec.get("launch_ms") is not None:
+        # launch rows: the first level's features from each sampled source
+        t0, t1 = (max(float(x), 1e-6) for x in rec["launch_ms"])
+        degs = rec.get("launch_degs")
+        degs = [int(tr[0]["mf"])] if degs is None else [int(d) for d in degs]
+        Xl = np.stack([g.level_features(n, m, 1, 1, d, n - 1, m - d, 1, 0) for d in degs]).astype(np.float32)
+        Yl = np.zeros((len(degs), 4), np.float32)
+        Ml = np.zeros((len(degs), 4), np.float32)
+        Yl[:, 3] = float(np.clip(np.log2(t0 / t1), -4.0, 4.0))
+        Ml[:, 3] = LAUNCH_WEIGHT
+        X, Y, M = np.concatenate([X, Xl]), np.concatenate([Y, Yl]), np.concatenate([M, Ml])
     return X, Y, M
 
 
-def collect(ctx, dgraph, src: int = 0, reps: int = 1):
-    """Per-level features, labels and masks of one graph from three traversals."""
-    rec = collect_traces(ctx, dgraph, src, reps)
+def collect(ctx, dgraph, src: int = 0, reps: int = 1, launch_cfgs=None):
+    """Per-level features, labels and masks of one graph from three traversals
+    (and two more per launch configuration with launch_cfgs)."""
+    rec = collect_traces(ctx, dgraph, src, reps, launch_cfgs)
     X, Y, M = features_labels(rec)
-    return X, Y, M, {"push": rec["push_ns"], "pull": rec["pull_ns"], "topo": rec["topo_ns"]}
+    return X, Y, M, {"push": rec["push_ns"], "pull": rec["pull_ns"], "topo": rec["topo_ns"],
+                     "launch_ms": rec.get("launch_ms")}
 
 
 def save_traces(path, recs) -> None:
@@ -120,6 +179,10 @@ def save_traces(path, recs) -> None:
     arrays = {"count": np.array([len(recs)], np.int64)}
     for k, rec in enumerate(recs):
         arrays[f"g{k}_meta"] = np.array([rec["n"], rec["m"], rec["src"]], np.int64)
+        if rec.get("launch_ms") is not None:
+            arrays[f"g{k}_launch_ms"] = np.asarray(rec["launch_ms"], np.float64)
+        if rec.get("launch_degs") is not None:
+            arrays[f"g{k}_launch_degs"] = np.asarray(rec["launch_degs"], np.int64)
         for name in ("push", "pull", "topo"):
             arrays[f"g{k}_{name}"] = rec[name]
             arrays[f"g{k}_{name}_ns"] = np.asarray(rec[name + "_ns"], np.float64)
@@ -132,6 +195,9 @@ def load_traces(path) -> list:
     for k in range(int(z["count"][0])):
         n, m, src = (int(x) for x in z[f"g{k}_meta"])
         rec = {"n": n, "m": m, "src": src}
+        for key in ("launch_ms", "launch_degs"):
+            if f"g{k}_{key}" in z:
+                rec[key] = z[f"g{k}_{key}"]
         for name in ("push", "pull", "topo"):
             rec[name] = z[f"g{k}_{name}"]
             rec[name + "_ns"] = z[f"g{k}_{name}_ns"]
@@ -166,6 +232,10 @@ def accuracy(ctx, params, X, Y, M):
     sel = M[:, 2] > 0
     if sel.any():
         res["head2_within_2x"] = float(np.mean(np.abs(out[sel, 2] - Y[sel, 2]) <= 1.0))
+    sel = M[:, 3] > 0
+    if sel.any():
+        # launch choice: the sign of head 3 against the sign of the measured ratio
+        res["head3_launch_acc"] = float(np.mean((out[sel, 3] > 0) == (Y[sel, 3] > 0)))
     return res
 
 
