@@ -508,6 +508,86 @@ def graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, verify_pr=True):
     return res
 
 
+class _At:
+    """A device address inside an allocation (a segment's start)."""
+
+    def __init__(self, ptr, dtype):
+        self.ptr, self.dtype = ptr, dtype
+
+
+def segment_numbers(gsrb, ctx, orc, cache, k=64, reps=5, fixed=None):
+    """k segments of uneven lengths (2^U(10, 22) elements): one batched launch
+    against one persistent launch per segment (the reference's form: one array
+    per launch), issued from the host and captured into one CUDA graph."""
+    rng = np.random.default_rng(SEED + 64)
+    lens = np.round(2.0 ** rng.uniform(10, 22, k)).astype(np.uint64)
+    off = np.concatenate([[0], np.cumsum(lens)]).astype(np.uint64)
+    n = int(off[-1])
+    peak, src = hbm_peak()
+    res = {"segments": k, "elements": n, "min_len": int(lens.min()), "max_len": int(lens.max()),
+           "peak_source": src, "cold_l2": True}
+    a = gsrb.uniform_i32(SEED + 1, n, 0, 127)
+    u = gsrb.uniform_i32(SEED + 2, n, 0, 15).astype(np.uint32)
+    da, du = ctx.to_device(a), ctx.to_device(u)
+    dsum = ctx.array(k, np.int64).zero()
+    dscan = ctx.array(n, np.uint32)
+    tune_cfg = gsrb.cfg(**{kk: v for kk, v in cache.get("reduce", {}).items() if kk in dict(gsrb.Cfg._fields_)})
+    cs = gsrb.cfg(**{kk: v for kk, v in cache.get("scan", {}).items() if kk in dict(gsrb.Cfg._fields_)})
+
+    def per_segment(kind):
+        for i in range(k):
+            s0, ln = int(off[i]), int(lens[i])
+            if kind == "reduce":
+                gsrb.check(ctx.reduce_i32(_At(da.ptr + 4 * s0, np.int32), ln, _At(dsum.ptr + 8 * i, np.int64),
+                                          tune_cfg))
+            else:
+                gsrb.check(ctx.scan(_At(du.ptr + 4 * s0, np.uint32), _At(dscan.ptr + 4 * s0, np.uint32), ln, cs))
+
+    cb = gsrb.cfg(**{kk: v for kk, v in fixed.items() if kk in dict(gsrb.Cfg._fields_)}) if fixed else None
+    if fixed:
+        res["cfg"] = fixed
+
+    def batched(kind):
+        if kind == "reduce":
+            gsrb.check(ctx.reduce_i32_segments(da, off, dsum, cb))
+        else:
+            gsrb.check(ctx.scan_u32_segments(du, dscan, off, cb))
+
+    def timed(fn):
+        ts = []
+        for i in range(2 + reps):
+            ctx.l2_flush()
+            ctx.record(4)
+            fn()
+            ctx.record(5)
+            if i >= 2:
+                ts.append(ctx.elapsed_ms(4, 5))
+        ctx.check_status("segments")
+        return statistics.median(ts)
+
+    want_sum = [orc.sum_i32(a[int(off[i]):int(off[i + 1])]) for i in range(k)]
+    want_scan = np.concatenate([orc.scan_u32(u[int(off[i]):int(off[i + 1])]) for i in range(k)])
+    for kind, nbytes in (("reduce", 4 * n), ("scan", 8 * n)):
+        check = (lambda: dsum.download().tolist() == want_sum) if kind == "reduce" else \
+            (lambda: bool(np.array_equal(dscan.download(), want_scan)))
+        tb = timed(lambda: batched(kind))
+        ok_b = check()
+        ts = timed(lambda: per_segment(kind))
+        ok_s = check()
+        cg = gsrb.CudaGraph(ctx)
+        with cg:
+            per_segment(kind)
+        tg = timed(cg.launch)
+        cg.free()
+        res[kind] = {"batched_ms": round(tb, 4), "batched_GB_s": round(nbytes / (tb * 1e-3) / 1e9, 1),
+                     "batched_hbm_frac": round(nbytes / (tb * 1e-3) / 1e9 / peak, 4),
+                     "per_segment_ms": round(ts, 4), "per_segment_graph_ms": round(tg, 4),
+                     "speedup_vs_per_segment_graph": round(tg / tb, 3), "bit_exact": bool(ok_b and ok_s)}
+    for x in (da, du, dsum, dscan):
+        x.free()
+    return res
+
+
 def batch_numbers(gsrb, ctx, orc, params):
     rng = np.random.default_rng(SEED)
     scales = rng.integers(14, 21, 64)
@@ -605,7 +685,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="barrier", choices=["barrier", "reduce", "scan", "bfs", "sssp", "pr", "prr"])
+    ap.add_argument("--workload", default="barrier", choices=["barrier", "reduce", "scan", "segments", "bfs", "sssp", "pr",
+                                                              "prr"])
     ap.add_argument("--graph", default="rmat", choices=["rmat", "grid"], help="graph of the bfs/sssp/pr workloads")
     ap.add_argument("--scale", type=int, default=22, help="log2 vertices of the bfs/sssp/pr workload graph")
     ap.add_argument("--iters", type=int, default=50, help="PageRank iterations (pr workload)")
@@ -658,6 +739,8 @@ def main():
             r = reduce_numbers(gsrb, ctx, orc, tune, cache, reps=args.steps, fixed=args.cfg, n=args.reduce_n)
         elif args.workload == "scan":
             r = scan_numbers(gsrb, ctx, orc, tune, cache, n=args.scan_n, reps=args.steps, fixed=args.cfg)
+        elif args.workload == "segments":
+            r = segment_numbers(gsrb, ctx, orc, cache, reps=args.steps, fixed=args.cfg)
         else:
             g = (gsrb.grid2d(1 << (args.scale // 2), 1 << (args.scale - args.scale // 2), seed=SEED)
                  if args.graph == "grid" else gsrb.rmat(args.scale, 16, seed=SEED))
@@ -761,6 +844,7 @@ def main():
         line["policy"] = pinfo
         line["graphs"] = graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, not args.skip_pr_check)
         line["batch"] = batch_numbers(gsrb, ctx, orc, params)
+        line["segments"] = segment_numbers(gsrb, ctx, orc, cache)
         line["extras_wall_s"] = round(time.time() - extras_t0, 1)
         if dist.rank == 0:
             line["cpu_baseline"] = cpu_barrier_baseline(orc)

@@ -180,6 +180,32 @@ gsrb_status_t gsrb_scan_u32(gsrb_ctx_t ctx, const uint32_t* d_in, uint32_t* d_ou
                             const gsrb_cfg_t* cfg);
 gsrb_status_t gsrb_scan_f32(gsrb_ctx_t ctx, const float* d_in, float* d_out, size_t n, const gsrb_cfg_t* cfg);
 
+/* ---- batched reduce / scan segments (no counterpart in the reference) -------------
+ * k independent segments of uneven lengths, segment i = elements
+ * [h_off[i], h_off[i+1]) of d_in (host offsets, non-decreasing, 1 <= k <= 127,
+ * total < 2^47), in one persistent launch.  Segment i gets CTAs
+ * [first_i, first_i + count_i): first_i = i + floor((grid - k) * (h_off[i] -
+ * h_off[0]) / (h_off[k] - h_off[0])) (every segment at least one CTA, the rest
+ * in proportion to length), and synchronises them on its own sub-grid barrier
+ * (slot 1 + i).  The layout is computed on the device from the launch
+ * parameters, so nothing is copied per call and calls can be captured
+ * (gsrb_capture_begin/end).  cfg == NULL: GSRB_BAR_FANOUT, 2 x 512 threads per
+ * SM; cfg->variant must be GSRB_BAR_FANOUT, GSRB_BAR_FLIP or GSRB_BAR_FLAT; grid
+ * >= k.  Asynchronous; a bounded wait that ran out is reported by
+ * gsrb_ctx_status. */
+/* d_out[i] = int64 sum of segment i (0 for an empty segment), bit-exact. */
+gsrb_status_t gsrb_reduce_i32_segments(gsrb_ctx_t ctx, const int32_t* d_in, const uint64_t* h_off, int32_t k,
+                                       int64_t* d_out, const gsrb_cfg_t* cfg);
+/* Exclusive uint32 prefix sum within each segment (wrapping; each segment starts
+ * at 0), written at the same offsets of d_out.  Not in place.  A segment is
+ * scanned in rounds of cfg->tile elements per CTA (rounded up to whole tiles of
+ * 16 x threads; 0 = 4 tiles), chunk sums and one sub-grid barrier per round, so
+ * that the rescan re-reads L2. */
+gsrb_status_t gsrb_scan_u32_segments(gsrb_ctx_t ctx, const uint32_t* d_in, uint32_t* d_out, const uint64_t* h_off,
+                                     int32_t k, const gsrb_cfg_t* cfg);
+/* Host: the CTA layout those calls use for a grid of `grid` CTAs (first[k], count[k]). */
+gsrb_status_t gsrb_segments_layout(const uint64_t* h_off, int32_t k, int32_t grid, uint32_t* first, uint32_t* count);
+
 /* ---- lock state, mutexes and semaphores (the Heterosync cudaLocks layer) -------
  * The reference-named host API (cudaLocksInit, cudaMutexCreate*, ...) is in
  * gsrb/cudaLocks.h and the device API in gsrb/cudaLocks.cuh; these are the

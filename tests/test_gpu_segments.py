@@ -1,0 +1,128 @@
+"""Batched reduce / scan segments (one persistent launch, a sub-grid barrier per
+segment): bit-exact against the serial oracle per segment."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+VARIANTS = [4, 8, 9]  # FLAT, FLIP, FANOUT
+
+
+def _uneven_offsets(seed, k, lo=0, hi=1 << 18):
+    rng = np.random.default_rng(seed)
+    lens = rng.integers(lo, hi, k)
+    lens[rng.integers(0, k, max(1, k // 8))] = 0  # some empty segments
+    return np.concatenate([[0], np.cumsum(lens)]).astype(np.uint64)
+
+
+def _reduce_segments(gsrb, ctx, a, off, cfg=None):
+    d = ctx.to_device(a) if a.size else ctx.array(1, np.int32)
+    out = ctx.array(len(off) - 1, np.int64).zero()
+    gsrb.check(ctx.reduce_i32_segments(d, off, out, cfg), "reduce_i32_segments")
+    ctx.check_status("reduce_i32_segments")
+    return out.download()
+
+
+def _scan_segments(gsrb, ctx, a, off, cfg=None):
+    d = ctx.to_device(a) if a.size else ctx.array(1, np.uint32)
+    out = ctx.array(max(a.size, 1), np.uint32).zero()
+    gsrb.check(ctx.scan_u32_segments(d, out, off, cfg), "scan_u32_segments")
+    ctx.check_status("scan_u32_segments")
+    return out.download()[: a.size]
+
+
+def _want_scan(orc, a, off):
+    want = np.zeros(a.size, np.uint32)
+    for i in range(len(off) - 1):
+        s, e = int(off[i]), int(off[i + 1])
+        if e > s:
+            want[s:e] = orc.scan_u32(a[s:e])
+    return want
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+@pytest.mark.parametrize("k", [1, 7, 64, 127])
+def test_reduce_segments_exact(gsrb, ctx, orc, variant, k):
+    off = _uneven_offsets(k, k)
+    a = gsrb.uniform_i32(0x5EED2022 + k, int(off[-1]), -1000, 1000)
+    got = _reduce_segments(gsrb, ctx, a, off, gsrb.cfg(variant=variant, ctas_per_sm=2, threads=256))
+    want = [orc.sum_i32(a[int(off[i]):int(off[i + 1])]) if off[i + 1] > off[i] else 0 for i in range(k)]
+    assert got.tolist() == want
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+@pytest.mark.parametrize("k", [1, 7, 64, 127])
+def test_scan_segments_exact(gsrb, ctx, orc, variant, k):
+    off = _uneven_offsets(100 + k, k)
+    a = gsrb.uniform_i32(0x5EED2022 + k, int(off[-1]), 0, 15).astype(np.uint32)
+    got = _scan_segments(gsrb, ctx, a, off, gsrb.cfg(variant=variant, ctas_per_sm=2, threads=256))
+    assert np.array_equal(got, _want_scan(orc, a, off))
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_scan_segments_many_rounds(gsrb, ctx, orc, variant):
+    # one tile per CTA per round: tens of rounds per segment, so the double
+    # buffered round sums are reused many times
+    off = np.array([0, 1_000_003, 1_000_004, 1_700_000, 3_000_001], np.uint64)
+    a = gsrb.uniform_i32(21, int(off[-1]), 0, 2**31 - 1).astype(np.uint32) * np.uint32(5)
+    c = gsrb.cfg(variant=variant, ctas_per_sm=1, threads=128, tile=1)
+    assert np.array_equal(_scan_segments(gsrb, ctx, a, off, c), _want_scan(orc, a, off))
+
+
+@pytest.mark.parametrize("threads", [64, 512, 1024])
+def test_segments_odd_offsets_and_tiny_segments(gsrb, ctx, orc, threads):
+    # lengths 0..9 and a few large ones, so slices start at every alignment and
+    # many segments have fewer elements than CTAs
+    lens = np.array([0, 1, 2, 3, 5, 7, 9, 0, 0, 1, 100_003, 3, 1 << 20, 6, 8, 4, 2, 1], np.uint64)
+    off = np.concatenate([[0], np.cumsum(lens)]).astype(np.uint64)
+    cfg = gsrb.cfg(variant=9, ctas_per_sm=1, threads=threads)
+    a = gsrb.uniform_i32(7, int(off[-1]), -(1 << 30), 1 << 30)
+    got = _reduce_segments(gsrb, ctx, a, off, cfg)
+    want = [orc.sum_i32(a[int(off[i]):int(off[i + 1])]) if off[i + 1] > off[i] else 0 for i in range(len(lens))]
+    assert got.tolist() == want
+    u = gsrb.uniform_i32(8, int(off[-1]), 0, 2**31 - 1).astype(np.uint32) * np.uint32(3)  # wraps
+    assert np.array_equal(_scan_segments(gsrb, ctx, u, off, cfg), _want_scan(orc, u, off))
+
+
+def test_segments_default_cfg_large_and_all_empty(gsrb, ctx, orc):
+    # one 2^24 segment beside small ones, the default launch shape
+    lens = np.array([1 << 24, 17, 0, 1 << 16], np.uint64)
+    off = np.concatenate([[0], np.cumsum(lens)]).astype(np.uint64)
+    a = gsrb.uniform_i32(0x5EED2022, int(off[-1]), 0, 127)
+    got = _reduce_segments(gsrb, ctx, a, off)
+    assert got.tolist() == [orc.sum_i32(a[int(off[i]):int(off[i + 1])]) if lens[i] else 0 for i in range(4)]
+    u = gsrb.uniform_i32(5, int(off[-1]), 0, 15).astype(np.uint32)
+    assert np.array_equal(_scan_segments(gsrb, ctx, u, off), _want_scan(orc, u, off))
+    # every segment empty: sums are 0 and nothing is read
+    off0 = np.zeros(9, np.uint64)
+    assert _reduce_segments(gsrb, ctx, np.zeros(0, np.int32), off0).tolist() == [0] * 8
+
+
+def test_segments_rejects_bad_arguments(gsrb, ctx):
+    d = ctx.array(16, np.int32)
+    out = ctx.array(200, np.int64)
+    assert ctx.reduce_i32_segments(d, np.array([0, 8, 4], np.uint64), out) == gsrb.ERR_ARG  # decreasing
+    assert ctx.reduce_i32_segments(d, np.arange(129, dtype=np.uint64), out) == gsrb.ERR_ARG  # k = 128
+    c = gsrb.cfg(variant=9, ctas_per_sm=1, threads=256, grid_override=4)
+    assert ctx.reduce_i32_segments(d, np.arange(6, dtype=np.uint64), out, c) == gsrb.ERR_ARG  # grid < k
+    assert ctx.reduce_i32_segments(d, np.array([0, 16], np.uint64), out,
+                                   gsrb.cfg(variant=6)) == gsrb.ERR_UNSUPPORTED  # grid.sync is whole-grid
+    u = ctx.array(16, np.uint32)
+    assert ctx.scan_u32_segments(u, u, np.array([0, 16], np.uint64)) == gsrb.ERR_ARG  # in place
+
+
+def test_segments_graph_replay(gsrb, ctx, orc):
+    off = _uneven_offsets(3, 40)
+    a = gsrb.uniform_i32(11, int(off[-1]), 0, 127)
+    d = ctx.to_device(a)
+    out = ctx.array(40, np.int64).zero()
+    want = [orc.sum_i32(a[int(off[i]):int(off[i + 1])]) if off[i + 1] > off[i] else 0 for i in range(40)]
+    cg = gsrb.CudaGraph(ctx)
+    with cg:
+        gsrb.check(ctx.reduce_i32_segments(d, off, out))
+    for _ in range(3):
+        out.zero()
+        cg.launch()
+        ctx.check_status("replay")
+        assert out.download().tolist() == want
+    cg.free()

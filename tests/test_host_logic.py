@@ -222,3 +222,25 @@ def test_launch_label_first_level_only(gsrb, pol, tmp_path):
     del rec["launch_ms"]
     X, _, M = pol.features_labels(rec)
     assert X.shape == (4, 12) and not M[:, 3].any()
+
+
+def test_segments_layout(gsrb):
+    # every segment gets at least one CTA, the rest go in proportion to length,
+    # the teams tile the grid in order
+    rng = np.random.default_rng(1)
+    for k, grid in ((1, 296), (5, 5), (64, 296), (127, 296), (127, 1184)):
+        lens = rng.integers(0, 1 << 20, k)
+        lens[::7] = 0
+        off = np.concatenate([[0], np.cumsum(lens)]).astype(np.uint64)
+        first, count = gsrb.segments_layout(off, grid)
+        assert first[0] == 0 and np.all(count >= 1) and int(count.sum()) == grid
+        assert np.array_equal(first[1:], first[:-1] + count[:-1])
+        if lens.sum():
+            extra = count.astype(np.int64) - 1
+            share = (grid - k) * lens / lens.sum()
+            assert np.all(np.abs(extra - share) <= 1.0 + 1e-9)
+    # no elements at all: one CTA each, the last segment the rest
+    first, count = gsrb.segments_layout(np.zeros(4, np.uint64), 10)
+    assert count.tolist() == [1, 1, 8]
+    with pytest.raises(gsrb.GsrbError):
+        gsrb.segments_layout(np.arange(6, dtype=np.uint64), 4)  # grid < k

@@ -1,0 +1,420 @@
+// Batched reduce and scan: k independent segments of uneven lengths in one
+// persistent launch, each on its own sub-grid barrier.
+//
+// Reference: the single-array forms reduce() (Reduce/reduce_gsrb.cu:289-404)
+// and sum_scan_blelloch (scan/scan_gsrb.cu:486-804), which take one array per
+// launch and synchronise the whole grid per level.  Here the segments of a
+// call share one launch: segment i gets CTAs [first_i, first_i + count_i), in
+// proportion to its length and at least one, and barrier slot 1 + i (sub-grid
+// barriers carved from the same state block as the whole-grid barrier, as the
+// batched traversals do).  The layout is a pure function of the offsets, the
+// number of segments and the grid, so every CTA computes it itself from the
+// launch parameters: nothing is copied to the device per call, and a call can
+// be captured into a CUDA graph and replayed.
+//
+//   reduce  each CTA sums a contiguous slice of its segment (int64), stores
+//           the partial, arrives on the segment's barrier; the combiner (the
+//           completing CTA for the fan-out protocol, else the segment's first
+//           CTA after a wait) adds the segment's partials in CTA order.
+//   scan    (exclusive, uint32) in rounds, so that the re-read comes from L2:
+//           in round j the team's CTAs take consecutive chunks of `chunk`
+//           elements (CTA r the r-th); chunk sums -> segment barrier -> every
+//           CTA adds the round's sums of the CTAs before it to the running
+//           total of the earlier rounds -> rescan of the chunk in tiles of
+//           16 x blockDim elements staged through shared memory (coalesced
+//           loads and stores whatever the offsets' alignment).  One round has
+//           grid x chunk elements in flight (about 38 MB at the default shape),
+//           so the rescan re-reads L2, not HBM.  The round sums are double
+//           buffered: a CTA writes round j + 2's sum only after the barrier of
+//           round j + 1, which every CTA reaches after reading round j's.
+#include "internal.h"
+
+#include <string.h>
+
+using namespace gsrbrt;
+
+namespace {
+
+constexpr int kMaxSegments = kSlots - 1;
+
+struct SegParams {
+  gsrb::GridBarrier gb;   // slot 1's descriptor (nparticipants/first_cta set per segment)
+  uint64_t flip_stride;   // words between consecutive slots' flip areas
+  uint32_t k;
+  uint32_t chunk;         // scan: elements per CTA per round (whole tiles of kScanV x blockDim)
+  uint64_t off[kMaxSegments + 1];
+};
+
+// First CTA of segment i: i + floor(left * off[i] / total), left = grid - k
+// (so every segment has at least one CTA and the rest go in proportion to
+// length); with no elements at all, segment i < k - 1 gets CTA i and the last
+// segment the rest.  Strictly increasing in i; first(k) = grid.
+__host__ __device__ __forceinline__ uint32_t seg_first(const uint64_t* off, uint32_t k, uint32_t grid, uint32_t i) {
+  const uint64_t total = off[k] - off[0];
+  if (i >= k) return grid;
+  if (total == 0) return i;
+  const uint64_t left = (uint64_t)(grid - k);
+  return i + (uint32_t)((left * (off[i] - off[0])) / total);
+}
+
+// Segment of CTA b (the last i with seg_first(i) <= b).
+__host__ __device__ __forceinline__ uint32_t seg_of(const uint64_t* off, uint32_t k, uint32_t grid, uint32_t b) {
+  uint32_t lo = 0, hi = k - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) >> 1;
+    if (seg_first(off, k, grid, mid) <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+struct SegTeam {
+  uint32_t seg, first, count, rank;
+  uint64_t a, b;  // this CTA's slice [a, b) (absolute element indices)
+};
+
+__device__ __forceinline__ SegTeam seg_team(const SegParams& p) {
+  SegTeam t;
+  t.seg = seg_of(p.off, p.k, gridDim.x, blockIdx.x);
+  t.first = seg_first(p.off, p.k, gridDim.x, t.seg);
+  t.count = seg_first(p.off, p.k, gridDim.x, t.seg + 1) - t.first;
+  t.rank = blockIdx.x - t.first;
+  const uint64_t o0 = p.off[t.seg], o1 = p.off[t.seg + 1];
+  const uint64_t len = o1 - o0;
+  uint64_t per = (len + t.count - 1) / t.count;
+  per = (per + 3) & ~3ull;
+  t.a = o0 + per * t.rank;
+  if (t.a > o1) t.a = o1;
+  t.b = t.a + per < o1 ? t.a + per : o1;
+  return t;
+}
+
+__device__ __forceinline__ gsrb::GridBarrier seg_barrier(const SegParams& p, const SegTeam& t) {
+  gsrb::GridBarrier gb = p.gb;
+  gb.slot += t.seg;
+  gb.flip += p.flip_stride * t.seg;
+  gb.nparticipants = t.count;
+  gb.first_cta = t.first;
+  return gb;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide sum, valid in every thread (fixed order).
+template <typename T>
+__device__ __forceinline__ T block_sum(T v, T* buf) {
+  v = warp_sum(v);
+  const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane == 0) buf[w] = v;
+  __syncthreads();
+  T s = lane < nw ? buf[lane] : T(0);
+  return warp_sum(s);
+}
+
+// Sum of in[a, b) by the CTA: 16-byte loads over the aligned body, four in
+// flight per thread, scalar head and tail.
+__device__ __forceinline__ long long slice_sum_i32(const int32_t* __restrict__ in, uint64_t a, uint64_t b) {
+  const uint32_t tid = threadIdx.x, T = blockDim.x;
+  long long acc = 0;
+  uint64_t h = a;
+  while (h < b && (reinterpret_cast<uintptr_t>(in + h) & 15u)) ++h;
+  const uint64_t nv = (b - h) >> 2;
+  const uint64_t t0 = h + (nv << 2);
+  for (uint64_t i = a + tid; i < h; i += T) acc += __ldg(in + i);
+  const int4* v = reinterpret_cast<const int4*>(in + h);
+  uint64_t i = tid;
+  for (; i + 3ull * T < nv; i += 4ull * T) {
+    const int4 x0 = __ldcs(v + i), x1 = __ldcs(v + i + T), x2 = __ldcs(v + i + 2ull * T), x3 = __ldcs(v + i + 3ull * T);
+    acc += (long long)x0.x + x0.y + x0.z + x0.w;
+    acc += (long long)x1.x + x1.y + x1.z + x1.w;
+    acc += (long long)x2.x + x2.y + x2.z + x2.w;
+    acc += (long long)x3.x + x3.y + x3.z + x3.w;
+  }
+  for (; i < nv; i += T) {
+    const int4 x = __ldcs(v + i);
+    acc += (long long)x.x + x.y + x.z + x.w;
+  }
+  for (uint64_t j = t0 + tid; j < b; j += T) acc += __ldg(in + j);
+  return acc;
+}
+
+__device__ __forceinline__ uint32_t slice_sum_u32(const uint32_t* __restrict__ in, uint64_t a, uint64_t b) {
+  const uint32_t tid = threadIdx.x, T = blockDim.x;
+  uint32_t acc = 0;
+  uint64_t h = a;
+  while (h < b && (reinterpret_cast<uintptr_t>(in + h) & 15u)) ++h;
+  const uint64_t nv = (b - h) >> 2;
+  const uint64_t t0 = h + (nv << 2);
+  for (uint64_t i = a + tid; i < h; i += T) acc += __ldg(in + i);
+  const uint4* v = reinterpret_cast<const uint4*>(in + h);
+  uint64_t i = tid;
+  for (; i + 3ull * T < nv; i += 4ull * T) {
+    const uint4 x0 = __ldcg(v + i), x1 = __ldcg(v + i + T), x2 = __ldcg(v + i + 2ull * T), x3 = __ldcg(v + i + 3ull * T);
+    acc += (x0.x + x0.y) + (x0.z + x0.w) + (x1.x + x1.y) + (x1.z + x1.w);
+    acc += (x2.x + x2.y) + (x2.z + x2.w) + (x3.x + x3.y) + (x3.z + x3.w);
+  }
+  for (; i < nv; i += T) {
+    const uint4 x = __ldcg(v + i);
+    acc += (x.x + x.y) + (x.z + x.w);
+  }
+  for (uint64_t j = t0 + tid; j < b; j += T) acc += __ldg(in + j);
+  return acc;
+}
+
+template <int V>
+__global__ void __launch_bounds__(1024)
+reduce_segments_kernel(SegParams p, const int32_t* __restrict__ in, long long* __restrict__ partials,
+                       long long* __restrict__ out) {
+  __shared__ gsrb::BarrierShared bsh;
+  __shared__ long long buf[32];
+  __shared__ uint32_t s_comb;
+  const SegTeam t = seg_team(p);
+  gsrb::GridSync<V> bar;
+  const bool ok = bar.init(seg_barrier(p, t), &bsh);
+  long long s = 0;
+  if (ok) s = slice_sum_i32(in, t.a, t.b);
+  s = block_sum(s, buf);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+  bar.arrive();
+  bool done = true, combiner;
+  if (gsrb::GridSync<V>::kCompleter) {
+    if (threadIdx.x == 0) s_comb = bar.arrived_done;
+    __syncthreads();
+    combiner = s_comb != 0u;
+  } else {
+    combiner = t.rank == 0;
+    if (!gsrb::GridSync<V>::kSplit || combiner) done = bar.wait();
+  }
+  if (ok && done && combiner) {
+    long long c = 0;
+    for (uint32_t j = threadIdx.x; j < t.count; j += blockDim.x) c += __ldcg(partials + t.first + j);
+    c = block_sum(c, buf);
+    if (threadIdx.x == 0) out[t.seg] = c;
+  }
+  bar.finish();
+}
+
+// Elements per thread of a scan tile, and the shared-memory word of tile
+// element e: one pad word per 32 elements, so that the coalesced fill (32
+// consecutive elements per warp) and the per-thread reads (kScanV consecutive
+// elements per lane, lanes kScanV apart) both touch 32 distinct banks.
+constexpr uint32_t kScanV = 16;
+__device__ __forceinline__ uint32_t tpos(uint32_t e) { return e + (e >> 5); }
+
+// Exclusive scan of one tile of up to kScanV * blockDim elements starting at
+// `base` (n elements valid), offset by `carry`; returns the tile's total.  All
+// kScanV loads of a thread are issued before the first is used.
+__device__ __forceinline__ uint32_t scan_tile_u32(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                                                  uint64_t base, uint32_t n, uint32_t carry, uint32_t* tile,
+                                                  uint32_t* wsum) {
+  const uint32_t tid = threadIdx.x, T = blockDim.x;
+  const uint32_t lane = tid & 31u, w = tid >> 5, nw = T >> 5;
+  uint32_t x[kScanV];
+#pragma unroll
+  for (uint32_t r = 0; r < kScanV; ++r) {
+    const uint32_t j = r * T + tid;
+    x[r] = j < n ? __ldcg(in + base + j) : 0u;
+  }
+#pragma unroll
+  for (uint32_t r = 0; r < kScanV; ++r) tile[tpos(r * T + tid)] = x[r];
+  __syncthreads();
+  uint32_t sum = 0;
+#pragma unroll
+  for (uint32_t r = 0; r < kScanV; ++r) {
+    const uint32_t v = tile[tpos(kScanV * tid + r)];
+    x[r] = sum;
+    sum += v;
+  }
+  // block exclusive scan of the per-thread sums
+  uint32_t inc = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+    if ((int)lane >= o) inc += y;
+  }
+  if (lane == 31) wsum[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    uint32_t v = lane < nw ? wsum[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, v, o);
+      if ((int)lane >= o) v += y;
+    }
+    wsum[lane] = v;  // inclusive warp prefix; wsum[31] = tile total
+  }
+  __syncthreads();
+  const uint32_t excl = carry + (w ? wsum[w - 1] : 0u) + (inc - sum);
+#pragma unroll
+  for (uint32_t r = 0; r < kScanV; ++r) tile[tpos(kScanV * tid + r)] = excl + x[r];
+  __syncthreads();
+#pragma unroll
+  for (uint32_t r = 0; r < kScanV; ++r) {
+    const uint32_t j = r * T + tid;
+    if (j < n) __stcs(out + base + j, tile[tpos(j)]);
+  }
+  const uint32_t total = wsum[31];
+  __syncthreads();  // tile and wsum are reused by the next tile
+  return total;
+}
+
+template <int V>
+__global__ void __launch_bounds__(1024)
+scan_segments_kernel(SegParams p, const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                     uint32_t* __restrict__ partials) {
+  __shared__ gsrb::BarrierShared bsh;
+  __shared__ uint32_t buf[32];
+  __shared__ uint32_t wsum[32];
+  extern __shared__ uint32_t tile[];  // tpos(kScanV * blockDim) words
+  const SegTeam t = seg_team(p);
+  gsrb::GridSync<V> bar;
+  bool ok = bar.init(seg_barrier(p, t), &bsh);
+  const uint64_t o0 = p.off[t.seg], o1 = p.off[t.seg + 1];
+  const uint64_t C = p.chunk, R = C * t.count;
+  const uint64_t rounds = (o1 - o0 + R - 1) / R;  // the same in every CTA of the team
+  const uint32_t step = kScanV * blockDim.x;
+  uint32_t base_carry = 0;
+  for (uint64_t j = 0; j < rounds && ok; ++j) {
+    const uint64_t a0 = o0 + j * R + C * t.rank;
+    const uint64_t a = a0 < o1 ? a0 : o1;
+    const uint64_t b = a + C < o1 ? a + C : o1;
+    uint32_t* part = partials + (j & 1) * gridDim.x + t.first;
+    uint32_t s = slice_sum_u32(in, a, b);
+    s = block_sum(s, buf);
+    if (threadIdx.x == 0) part[t.rank] = s;
+    ok = bar.sync() && ok;
+    if (!ok) break;
+    // this round's sums of the team: before this CTA, and in total
+    uint32_t pre = 0, tot = 0;
+    for (uint32_t r = threadIdx.x; r < t.count; r += blockDim.x) {
+      const uint32_t x = __ldcg(part + r);
+      tot += x;
+      if (r < t.rank) pre += x;
+    }
+    pre = block_sum(pre, buf);
+    tot = block_sum(tot, buf);
+    uint32_t c = base_carry + pre;
+    for (uint64_t x = a; x < b; x += step) {
+      const uint64_t left = b - x;
+      const uint32_t n = left < step ? (uint32_t)left : step;
+      c += scan_tile_u32(in, out, x, n, c, tile, wsum);
+    }
+    base_carry += tot;
+  }
+  bar.finish();
+}
+
+const void* reduce_segments_fn(int v) {
+  switch (v) {  // sub-grid protocols whose state does not depend on the team size
+    case gsrb::V_FLAT: return (const void*)reduce_segments_kernel<gsrb::V_FLAT>;
+    case gsrb::V_FLIP: return (const void*)reduce_segments_kernel<gsrb::V_FLIP>;
+    case gsrb::V_FANOUT: return (const void*)reduce_segments_kernel<gsrb::V_FANOUT>;
+    default: return nullptr;
+  }
+}
+
+const void* scan_segments_fn(int v) {
+  switch (v) {
+    case gsrb::V_FLAT: return (const void*)scan_segments_kernel<gsrb::V_FLAT>;
+    case gsrb::V_FLIP: return (const void*)scan_segments_kernel<gsrb::V_FLIP>;
+    case gsrb::V_FANOUT: return (const void*)scan_segments_kernel<gsrb::V_FANOUT>;
+    default: return nullptr;
+  }
+}
+
+// Shared checks and the launch parameters of a segmented call.
+gsrb_status_t seg_setup(gsrb_ctx* ctx, const gsrb_cfg_t* cfgin, const uint64_t* h_off, int32_t k,
+                        const void* (*pick)(int), gsrb_cfg_t* c, int* grid, const void** fn, SegParams* p) {
+  if (!ctx || !h_off || k <= 0 || k > kMaxSegments) return GSRB_ERR_ARG;
+  for (int32_t i = 0; i < k; ++i)
+    if (h_off[i + 1] < h_off[i]) return GSRB_ERR_ARG;
+  if (h_off[k] - h_off[0] >= (1ull << 47)) return GSRB_ERR_ARG;
+  *c = resolve_cfg(ctx, cfgin);
+  if (!cfgin) {
+    c->variant = gsrb::V_FANOUT;
+    c->ctas_per_sm = 2;
+    c->threads = 512;
+  }
+  c->cluster = 1;
+  if (c->threads % 32 || c->threads > 1024 || c->threads < 64) return GSRB_ERR_ARG;
+  *fn = pick(c->variant);
+  if (!*fn) return GSRB_ERR_UNSUPPORTED;
+  *grid = grid_of(ctx, *c);
+  if (*grid < k || *grid > 65535) return GSRB_ERR_ARG;
+  memset(p, 0, sizeof(*p));
+  p->gb = make_barrier(ctx, *c, 1, 1u, 0u, 0u);
+  p->flip_stride = (uint64_t)kMaxFlip * 32u;
+  p->k = (uint32_t)k;
+  // scan rounds: cfg->tile elements per CTA (rounded to whole tiles), 0 = 4 tiles
+  const uint32_t tile_elems = kScanV * (uint32_t)c->threads;
+  uint32_t chunk = c->tile > 0 ? (uint32_t)c->tile : 4u * tile_elems;
+  chunk = (chunk + tile_elems - 1) / tile_elems * tile_elems;
+  if (chunk > (1u << 24)) return GSRB_ERR_ARG;
+  p->chunk = chunk;
+  for (int32_t i = 0; i <= k; ++i) p->off[i] = h_off[i];
+  return GSRB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+gsrb_status_t gsrb_segments_layout(const uint64_t* h_off, int32_t k, int32_t grid, uint32_t* first, uint32_t* count) {
+  if (!h_off || k <= 0 || k > kMaxSegments || grid < k) return GSRB_ERR_ARG;
+  for (int32_t i = 0; i < k; ++i) {
+    if (h_off[i + 1] < h_off[i]) return GSRB_ERR_ARG;
+    const uint32_t f = seg_first(h_off, (uint32_t)k, (uint32_t)grid, (uint32_t)i);
+    if (first) first[i] = f;
+    if (count) count[i] = seg_first(h_off, (uint32_t)k, (uint32_t)grid, (uint32_t)i + 1) - f;
+  }
+  return GSRB_OK;
+}
+
+gsrb_status_t gsrb_reduce_i32_segments(gsrb_ctx_t ctx, const int32_t* d_in, const uint64_t* h_off, int32_t k,
+                                       int64_t* d_out, const gsrb_cfg_t* cfgin) {
+  if (!d_out || !h_off || (k > 0 && h_off[k] > h_off[0] && !d_in)) return GSRB_ERR_ARG;
+  if (!ctx) return GSRB_ERR_ARG;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  gsrb_cfg_t c;
+  int grid = 0;
+  const void* fn = nullptr;
+  SegParams p;
+  gsrb_status_t st = seg_setup(ctx, cfgin, h_off, k, reduce_segments_fn, &c, &grid, &fn, &p);
+  if (st) return st;
+  void* part = nullptr;
+  st = scratch(ctx, sizeof(long long) * (size_t)grid, &part);
+  if (st) return st;
+  long long* partials = (long long*)part;
+  long long* out = (long long*)d_out;
+  void* args[] = {&p, &d_in, &partials, &out};
+  return launch_persistent(ctx, fn, grid, c.threads, 0, 1, coop_of(c), args);
+}
+
+gsrb_status_t gsrb_scan_u32_segments(gsrb_ctx_t ctx, const uint32_t* d_in, uint32_t* d_out, const uint64_t* h_off,
+                                     int32_t k, const gsrb_cfg_t* cfgin) {
+  if (!h_off || (k > 0 && h_off[k] > h_off[0] && (!d_in || !d_out || d_in == d_out))) return GSRB_ERR_ARG;
+  if (!ctx) return GSRB_ERR_ARG;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  gsrb_cfg_t c;
+  int grid = 0;
+  const void* fn = nullptr;
+  SegParams p;
+  gsrb_status_t st = seg_setup(ctx, cfgin, h_off, k, scan_segments_fn, &c, &grid, &fn, &p);
+  if (st) return st;
+  void* part = nullptr;
+  st = scratch(ctx, sizeof(uint32_t) * 2 * (size_t)grid, &part);
+  if (st) return st;
+  uint32_t* partials = (uint32_t*)part;
+  const uint32_t tw = kScanV * (uint32_t)c.threads;
+  const size_t smem = sizeof(uint32_t) * (size_t)(tw + (tw >> 5));
+  void* args[] = {&p, &d_in, &d_out, &partials};
+  return launch_persistent(ctx, fn, grid, c.threads, smem, 1, coop_of(c), args);
+}
+
+}  // extern "C"

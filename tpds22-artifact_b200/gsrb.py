@@ -149,6 +149,9 @@ _SIGS = {
     "gsrb_gr_write": (C.c_int32, [C.c_char_p, C.POINTER(HostCSR), C.c_int32]),
     "gsrb_scan_u32": (C.c_int32, [_P, _P, _P, C.c_size_t, C.POINTER(Cfg)]),
     "gsrb_scan_f32": (C.c_int32, [_P, _P, _P, C.c_size_t, C.POINTER(Cfg)]),
+    "gsrb_reduce_i32_segments": (C.c_int32, [_P, _P, _P, C.c_int32, _P, C.POINTER(Cfg)]),
+    "gsrb_scan_u32_segments": (C.c_int32, [_P, _P, _P, _P, C.c_int32, C.POINTER(Cfg)]),
+    "gsrb_segments_layout": (C.c_int32, [_P, C.c_int32, C.c_int32, _P, _P]),
     "gsrb_semaphore_bench": (C.c_int32, [_P, C.POINTER(Cfg), C.c_int32, C.c_uint32, C.c_int32, C.c_int32,
                                          C.c_int32, _P]),
     "gsrb_mutex_bench": (C.c_int32, [_P, C.POINTER(Cfg), C.c_int32, C.c_int32, C.c_int32, _P]),
@@ -401,6 +404,19 @@ class Context:
         fn = _lib().gsrb_scan_f32 if d_in.dtype == np.float32 else _lib().gsrb_scan_u32
         return fn(self.h, d_in.ptr, d_out.ptr, n, C.byref(c) if c is not None else None)
 
+    # -- batched segments ----------------------------------------------------------
+    def reduce_i32_segments(self, d_in: DeviceArray, offsets, d_out: DeviceArray, c: Cfg | None = None) -> int:
+        """int64 sums of the segments [offsets[i], offsets[i+1]) of d_in, one launch."""
+        off = np.ascontiguousarray(offsets, dtype=np.uint64)
+        return _lib().gsrb_reduce_i32_segments(self.h, d_in.ptr, off.ctypes.data, len(off) - 1, d_out.ptr,
+                                               C.byref(c) if c is not None else None)
+
+    def scan_u32_segments(self, d_in: DeviceArray, d_out: DeviceArray, offsets, c: Cfg | None = None) -> int:
+        """Exclusive uint32 prefix sums within each segment, one launch."""
+        off = np.ascontiguousarray(offsets, dtype=np.uint64)
+        return _lib().gsrb_scan_u32_segments(self.h, d_in.ptr, d_out.ptr, off.ctypes.data, len(off) - 1,
+                                             C.byref(c) if c is not None else None)
+
     # -- locks ------------------------------------------------------------------
     def semaphore_bench(self, c: Cfg, kind: int, capacity: int, writer_every: int, iters: int, incs: int,
                         counters: DeviceArray) -> int:
@@ -587,6 +603,17 @@ def mlp_init(seed: int) -> np.ndarray:
     p = np.zeros(mlp_param_count(), dtype=np.float32)
     check(_lib().gsrb_mlp_init(seed, p.ctypes.data), "mlp_init")
     return p
+
+
+def segments_layout(offsets, grid: int):
+    """(first, count) CTAs of each segment for a batched segment launch of `grid` CTAs."""
+    off = np.ascontiguousarray(offsets, dtype=np.uint64)
+    k = len(off) - 1
+    first = np.zeros(max(k, 1), np.uint32)
+    count = np.zeros(max(k, 1), np.uint32)
+    check(_lib().gsrb_segments_layout(off.ctypes.data, k, grid, first.ctypes.data, count.ctypes.data),
+          "segments_layout")
+    return first[:k], count[:k]
 
 
 def level_features(n, m, level, nf, mf, nu, mu, prev_nf, prev_dir) -> np.ndarray:
