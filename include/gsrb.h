@@ -190,7 +190,7 @@ gsrb_status_t gsrb_scan_f32(gsrb_ctx_t ctx, const float* d_in, float* d_out, siz
  * (slot 1 + i).  The layout is computed on the device from the launch
  * parameters, so nothing is copied per call and calls can be captured
  * (gsrb_capture_begin/end).  cfg == NULL: GSRB_BAR_FANOUT, 2 x 512 threads per
- * SM; cfg->variant must be GSRB_BAR_FANOUT, GSRB_BAR_FLIP or GSRB_BAR_FLAT; grid
+ * SM for the reduce, 4 x 256 for the scan; cfg->variant must be GSRB_BAR_FANOUT, GSRB_BAR_FLIP or GSRB_BAR_FLAT; grid
  * >= k.  Asynchronous; a bounded wait that ran out is reported by
  * gsrb_ctx_status. */
 /* d_out[i] = int64 sum of segment i (0 for an empty segment), bit-exact. */

@@ -24,9 +24,11 @@
 //           16 x blockDim elements staged through shared memory (coalesced
 //           loads and stores whatever the offsets' alignment).  One round has
 //           grid x chunk elements in flight (about 38 MB at the default shape),
-//           so the rescan re-reads L2, not HBM.  The round sums are double
-//           buffered: a CTA writes round j + 2's sum only after the barrier of
-//           round j + 1, which every CTA reaches after reading round j's.
+//           so the rescan re-reads L2, not HBM.  The barrier is split: a CTA
+//           arrives for round j, reads round j + 1's chunk sum from HBM, then
+//           waits.  The round sums are double buffered: a CTA writes round
+//           j + 1's sum only after the barrier of round j, which every CTA
+//           reaches after reading round j - 1's.
 #include "internal.h"
 
 #include <string.h>
@@ -280,17 +282,32 @@ scan_segments_kernel(SegParams p, const uint32_t* __restrict__ in, uint32_t* __r
   const uint64_t rounds = (o1 - o0 + R - 1) / R;  // the same in every CTA of the team
   const uint32_t step = kScanV * blockDim.x;
   uint32_t base_carry = 0;
-  for (uint64_t j = 0; j < rounds && ok; ++j) {
+  auto chunk = [&](uint64_t j, uint64_t* a, uint64_t* b) {
     const uint64_t a0 = o0 + j * R + C * t.rank;
-    const uint64_t a = a0 < o1 ? a0 : o1;
-    const uint64_t b = a + C < o1 ? a + C : o1;
-    uint32_t* part = partials + (j & 1) * gridDim.x + t.first;
-    uint32_t s = slice_sum_u32(in, a, b);
-    s = block_sum(s, buf);
-    if (threadIdx.x == 0) part[t.rank] = s;
-    ok = bar.sync() && ok;
+    *a = a0 < o1 ? a0 : o1;
+    *b = *a + C < o1 ? *a + C : o1;
+  };
+  uint64_t a = o0, b = o0;
+  if (rounds && ok) {
+    chunk(0, &a, &b);
+    const uint32_t s = block_sum(slice_sum_u32(in, a, b), buf);
+    if (threadIdx.x == 0) partials[t.first + t.rank] = s;
+    bar.arrive();
+  }
+  for (uint64_t j = 0; j < rounds && ok; ++j) {
+    // split phase: the next round's chunk sum is read from HBM while this
+    // round's barrier completes (a full barrier for the protocols without a
+    // split form, still correct)
+    uint64_t na = b, nb = b;
+    uint32_t s_next = 0;
+    if (j + 1 < rounds) {
+      chunk(j + 1, &na, &nb);
+      s_next = block_sum(slice_sum_u32(in, na, nb), buf);
+    }
+    ok = bar.wait() && ok;
     if (!ok) break;
     // this round's sums of the team: before this CTA, and in total
+    const uint32_t* part = partials + (j & 1) * gridDim.x + t.first;
     uint32_t pre = 0, tot = 0;
     for (uint32_t r = threadIdx.x; r < t.count; r += blockDim.x) {
       const uint32_t x = __ldcg(part + r);
@@ -306,6 +323,14 @@ scan_segments_kernel(SegParams p, const uint32_t* __restrict__ in, uint32_t* __r
       c += scan_tile_u32(in, out, x, n, c, tile, wsum);
     }
     base_carry += tot;
+    if (j + 1 < rounds) {
+      // round j + 1's buffer held round j - 1's sums, which every CTA has read
+      // before arriving at barrier j
+      if (threadIdx.x == 0) partials[((j + 1) & 1) * gridDim.x + t.first + t.rank] = s_next;
+      bar.arrive();
+      a = na;
+      b = nb;
+    }
   }
   bar.finish();
 }
@@ -330,7 +355,8 @@ const void* scan_segments_fn(int v) {
 
 // Shared checks and the launch parameters of a segmented call.
 gsrb_status_t seg_setup(gsrb_ctx* ctx, const gsrb_cfg_t* cfgin, const uint64_t* h_off, int32_t k,
-                        const void* (*pick)(int), gsrb_cfg_t* c, int* grid, const void** fn, SegParams* p) {
+                        const void* (*pick)(int), int def_ctas, int def_threads, gsrb_cfg_t* c, int* grid,
+                        const void** fn, SegParams* p) {
   if (!ctx || !h_off || k <= 0 || k > kMaxSegments) return GSRB_ERR_ARG;
   for (int32_t i = 0; i < k; ++i)
     if (h_off[i + 1] < h_off[i]) return GSRB_ERR_ARG;
@@ -338,8 +364,8 @@ gsrb_status_t seg_setup(gsrb_ctx* ctx, const gsrb_cfg_t* cfgin, const uint64_t* 
   *c = resolve_cfg(ctx, cfgin);
   if (!cfgin) {
     c->variant = gsrb::V_FANOUT;
-    c->ctas_per_sm = 2;
-    c->threads = 512;
+    c->ctas_per_sm = def_ctas;
+    c->threads = def_threads;
   }
   c->cluster = 1;
   if (c->threads % 32 || c->threads > 1024 || c->threads < 64) return GSRB_ERR_ARG;
@@ -385,7 +411,7 @@ gsrb_status_t gsrb_reduce_i32_segments(gsrb_ctx_t ctx, const int32_t* d_in, cons
   int grid = 0;
   const void* fn = nullptr;
   SegParams p;
-  gsrb_status_t st = seg_setup(ctx, cfgin, h_off, k, reduce_segments_fn, &c, &grid, &fn, &p);
+  gsrb_status_t st = seg_setup(ctx, cfgin, h_off, k, reduce_segments_fn, 2, 512, &c, &grid, &fn, &p);
   if (st) return st;
   void* part = nullptr;
   st = scratch(ctx, sizeof(long long) * (size_t)grid, &part);
@@ -405,7 +431,7 @@ gsrb_status_t gsrb_scan_u32_segments(gsrb_ctx_t ctx, const uint32_t* d_in, uint3
   int grid = 0;
   const void* fn = nullptr;
   SegParams p;
-  gsrb_status_t st = seg_setup(ctx, cfgin, h_off, k, scan_segments_fn, &c, &grid, &fn, &p);
+  gsrb_status_t st = seg_setup(ctx, cfgin, h_off, k, scan_segments_fn, 4, 256, &c, &grid, &fn, &p);
   if (st) return st;
   void* part = nullptr;
   st = scratch(ctx, sizeof(uint32_t) * 2 * (size_t)grid, &part);
