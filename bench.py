@@ -515,7 +515,7 @@ class _At:
         self.ptr, self.dtype = ptr, dtype
 
 
-def segment_numbers(gsrb, ctx, orc, cache, k=64, reps=5, fixed=None):
+def segment_numbers(gsrb, ctx, orc, tune, cache, k=64, reps=5, fixed=None):
     """k segments of uneven lengths (2^U(10, 22) elements): one batched launch
     against one persistent launch per segment (the reference's form: one array
     per launch), issued from the host and captured into one CUDA graph."""
@@ -543,15 +543,19 @@ def segment_numbers(gsrb, ctx, orc, cache, k=64, reps=5, fixed=None):
             else:
                 gsrb.check(ctx.scan(_At(du.ptr + 4 * s0, np.uint32), _At(dscan.ptr + 4 * s0, np.uint32), ln, cs))
 
-    cb = gsrb.cfg(**{kk: v for kk, v in fixed.items() if kk in dict(gsrb.Cfg._fields_)}) if fixed else None
-    if fixed:
-        res["cfg"] = fixed
+    # the batched calls' configurations: fixed, or picked by the autotuner
+    cb = {}
+    for kind, (din, dout) in (("reduce", (da, dsum)), ("scan", (du, dscan))):
+        best = fixed if fixed else tune.tune_segments(ctx, kind, din, dout, off)[0]
+        cache["segments_" + kind] = best
+        cb[kind] = gsrb.cfg(**{kk: v for kk, v in best.items() if kk in dict(gsrb.Cfg._fields_)})
+        res.setdefault("cfg", {})[kind] = best
 
     def batched(kind):
         if kind == "reduce":
-            gsrb.check(ctx.reduce_i32_segments(da, off, dsum, cb))
+            gsrb.check(ctx.reduce_i32_segments(da, off, dsum, cb[kind]))
         else:
-            gsrb.check(ctx.scan_u32_segments(du, dscan, off, cb))
+            gsrb.check(ctx.scan_u32_segments(du, dscan, off, cb[kind]))
 
     def timed(fn):
         ts = []
@@ -740,7 +744,7 @@ def main():
         elif args.workload == "scan":
             r = scan_numbers(gsrb, ctx, orc, tune, cache, n=args.scan_n, reps=args.steps, fixed=args.cfg)
         elif args.workload == "segments":
-            r = segment_numbers(gsrb, ctx, orc, cache, reps=args.steps, fixed=args.cfg)
+            r = segment_numbers(gsrb, ctx, orc, tune, cache, reps=args.steps, fixed=args.cfg)
         else:
             g = (gsrb.grid2d(1 << (args.scale // 2), 1 << (args.scale - args.scale // 2), seed=SEED)
                  if args.graph == "grid" else gsrb.rmat(args.scale, 16, seed=SEED))
@@ -844,7 +848,7 @@ def main():
         line["policy"] = pinfo
         line["graphs"] = graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, not args.skip_pr_check)
         line["batch"] = batch_numbers(gsrb, ctx, orc, params)
-        line["segments"] = segment_numbers(gsrb, ctx, orc, cache)
+        line["segments"] = segment_numbers(gsrb, ctx, orc, tune, cache)
         line["extras_wall_s"] = round(time.time() - extras_t0, 1)
         if dist.rank == 0:
             line["cpu_baseline"] = cpu_barrier_baseline(orc)

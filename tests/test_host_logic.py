@@ -96,6 +96,12 @@ def test_autotune_candidates_and_cfg_roundtrip(gsrb, tune):
         if p.exists():
             p.unlink()
     assert tune.load_cache(ROOT / "does-not-exist.json") == {}
+    # segment calls: only the protocols whose state does not depend on the team size
+    for kind in ("reduce", "scan"):
+        sc = tune.segment_candidates(kind)
+        assert {c["variant"] for c in sc} == {gsrb.BAR_FANOUT, gsrb.BAR_FLIP, gsrb.BAR_FLAT}
+        assert all(c["ctas_per_sm"] * c["threads"] <= 2048 for c in sc)
+    assert {c["tile"] for c in tune.segment_candidates("reduce")} == {0}
 
 
 def _bench_env():

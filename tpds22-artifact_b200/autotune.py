@@ -116,6 +116,40 @@ def tune_reduce(ctx, d_in, n: int, reps: int = 5):
     return table[0][1], table[0][0], table
 
 
+def segment_candidates(kind: str):
+    """Shapes and sub-grid protocols for the batched segment calls (protocols
+    whose state does not depend on the team size; for the scan also the round
+    length, 0 = 4 tiles of 16 x threads)."""
+    g = _g()
+    out = []
+    for k, threads in ((2, 512), (4, 256), (2, 256), (1, 1024)):
+        for cand in (dict(variant=g.BAR_FANOUT, wake_lines=4), dict(variant=g.BAR_FLIP, fanin_groups=1),
+                     dict(variant=g.BAR_FLAT)):
+            for tile in ((0, 8 * 16 * threads) if kind == "scan" else (0,)):
+                out.append(dict(cand, ctas_per_sm=k, threads=threads, tile=tile))
+    return out
+
+
+def tune_segments(ctx, kind: str, d_in, d_out, offsets, reps: int = 3):
+    """Best configuration of gsrb_reduce_i32_segments (kind "reduce", d_out =
+    the sums) or gsrb_scan_u32_segments (kind "scan"), timed cold (L2 flushed)."""
+    g = _g()
+    table = []
+    for cand in segment_candidates(kind):
+        c = g.cfg(**cand)
+
+        def run():
+            ctx.l2_flush()
+            if kind == "reduce":
+                return ctx.reduce_i32_segments(d_in, offsets, d_out, c)
+            return ctx.scan_u32_segments(d_in, d_out, offsets, c)
+        t = _median_ms(ctx, run, reps)
+        if t is not None:
+            table.append((t, cand))
+    table.sort(key=lambda x: x[0])
+    return table[0][1], table[0][0], table
+
+
 def tune_bfs(ctx, dgraph, src: int, mode: int, reps: int = 2):
     g = _g()
     out = ctx.array(dgraph.n, np.int32)
