@@ -364,24 +364,50 @@ typedef struct {
   int episodes;
   atomic_uint* stamps; /* one per thread, each on its own line (stride 16) */
   atomic_ullong stale;
+  int stall_permille;  /* injected stalls: chance per stall point, in 1/1000 */
+  atomic_ullong stalls;
 } srb_t;
 
 typedef struct {
   srb_t* b;
   int id;
+  uint64_t rng;
 } srb_arg;
+
+/* Injected stall: with probability permille/1000 the thread yields or sleeps
+ * 5-100 us (xorshift64 per thread, seeded), so that arrivals, the completer's
+ * reset-then-publish and the critical sections are reordered across threads. */
+static int maybe_stall(uint64_t* rng, int permille) {
+  if (permille <= 0) return 0;
+  uint64_t x = *rng;
+  x ^= x << 13;
+  x ^= x >> 7;
+  x ^= x << 17;
+  *rng = x;
+  if ((int)(x % 1000u) >= permille) return 0;
+  if ((x >> 20) & 1u) {
+    sched_yield();
+  } else {
+    struct timespec ts = {0, (long)(5000 + (x >> 32) % 95000)};
+    nanosleep(&ts, NULL);
+  }
+  return 1;
+}
 
 static unsigned gsize(unsigned n, unsigned g, unsigned i) { return n / g + (i < n % g ? 1u : 0u); }
 
-static void srb_sync(srb_t* b, int id, unsigned* epoch) {
+static void srb_sync(srb_t* b, int id, unsigned* epoch, uint64_t* rng) {
   const unsigned e = *epoch;
   int done = 0;
   unsigned n = (unsigned)b->nthreads;
+  unsigned long long st = 0;
+  st += maybe_stall(rng, b->stall_permille); /* late arrival */
   if (b->ngroups > 1 && n > (unsigned)b->ngroups) {
     unsigned g = (unsigned)id % (unsigned)b->ngroups;
     unsigned gs = gsize(n, (unsigned)b->ngroups, g);
     if (atomic_fetch_add_explicit(&b->groups[g].count, 1, memory_order_acq_rel) == gs - 1) {
       atomic_store_explicit(&b->groups[g].count, 0, memory_order_relaxed);
+      st += maybe_stall(rng, b->stall_permille); /* group completer slow to go on */
       n = (unsigned)b->ngroups;
       goto root;
     }
@@ -390,9 +416,11 @@ static void srb_sync(srb_t* b, int id, unsigned* epoch) {
 root:
   if (atomic_fetch_add_explicit(&b->count, 1, memory_order_acq_rel) == n - 1) {
     atomic_store_explicit(&b->count, 0, memory_order_relaxed);
+    st += maybe_stall(rng, b->stall_permille); /* between the reset and the publish */
     atomic_store_explicit(&b->epoch, e + 1, memory_order_release);
     done = 1;
   }
+  if (st) atomic_fetch_add(&b->stalls, st);
 wait:
   if (!done) {
     unsigned spins = 0;
@@ -414,16 +442,21 @@ static void* srb_worker(void* p) {
   for (int e = 0; e < b->episodes; ++e) {
     unsigned stamp = 0x9e3779b9u * (unsigned)(e + 1);
     atomic_store_explicit(&b->stamps[a->id * 16], stamp, memory_order_relaxed);
-    srb_sync(b, a->id, &epoch);
+    srb_sync(b, a->id, &epoch, &a->rng);
     int peer = (a->id + 1 + e) % b->nthreads;
     if (atomic_load_explicit(&b->stamps[peer * 16], memory_order_relaxed) != stamp) ++bad;
-    srb_sync(b, a->id, &epoch);
+    srb_sync(b, a->id, &epoch, &a->rng);
   }
   atomic_fetch_add(&b->stale, bad);
   return NULL;
 }
 
 double orc_cpu_srb_barrier(int nthreads, int ngroups, int episodes, uint64_t* stale) {
+  return orc_cpu_srb_barrier_stalls(nthreads, ngroups, episodes, 0, 0, stale, NULL);
+}
+
+double orc_cpu_srb_barrier_stalls(int nthreads, int ngroups, int episodes, int stall_permille, uint64_t seed,
+                                  uint64_t* stale, uint64_t* stalls) {
   if (nthreads < 1) nthreads = 1;
   if (nthreads > 1024) nthreads = 1024;
   srb_t* b = (srb_t*)aligned_alloc(64, sizeof(srb_t));
@@ -431,6 +464,7 @@ double orc_cpu_srb_barrier(int nthreads, int ngroups, int episodes, uint64_t* st
   b->ngroups = ngroups;
   b->nthreads = nthreads;
   b->episodes = episodes;
+  b->stall_permille = stall_permille;
   b->groups = (grp_t*)aligned_alloc(64, sizeof(grp_t) * (size_t)(ngroups > 0 ? ngroups : 1));
   memset(b->groups, 0, sizeof(grp_t) * (size_t)(ngroups > 0 ? ngroups : 1));
   b->stamps = (atomic_uint*)aligned_alloc(64, sizeof(atomic_uint) * 16 * (size_t)nthreads);
@@ -441,11 +475,14 @@ double orc_cpu_srb_barrier(int nthreads, int ngroups, int episodes, uint64_t* st
   for (int t = 0; t < nthreads; ++t) {
     args[t].b = b;
     args[t].id = t;
+    args[t].rng = (seed + 1u) * 0x9e3779b97f4a7c15ull ^ (uint64_t)(t + 1) * 0xbf58476d1ce4e5b9ull;
+    if (!args[t].rng) args[t].rng = 1;
     pthread_create(&th[t], NULL, srb_worker, &args[t]);
   }
   for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);
   double t1 = now_s();
   if (stale) *stale = atomic_load(&b->stale);
+  if (stalls) *stalls = atomic_load(&b->stalls);
   free(th);
   free(args);
   free(b->stamps);
@@ -471,18 +508,23 @@ typedef struct {
   atomic_uint max_readers;
   atomic_uint violations;
   int capacity, writer_every, iters, incs;
+  int stall_permille;
+  atomic_ullong stalls;
 } sem_t_;
 
 typedef struct {
   sem_t_* s;
   int id;
+  uint64_t rng;
 } sem_arg;
 
 static void* sem_worker(void* p) {
   sem_arg* a = (sem_arg*)p;
   sem_t_* s = a->s;
   const int writer = (a->id % s->writer_every) == 0;
+  unsigned long long st = 0;
   for (int it = 0; it < s->iters; ++it) {
+    st += maybe_stall(&a->rng, s->stall_permille); /* before the acquire */
     if (writer) {
       unsigned my = atomic_fetch_add(&s->ticket, 1);
       atomic_fetch_add(&s->state, 1u << 17);
@@ -496,7 +538,10 @@ static void* sem_worker(void* p) {
         sched_yield();
       }
       if (atomic_fetch_add(&s->inside, 1000) != 0) atomic_fetch_add(&s->violations, 1);
-      for (int k = 0; k < s->incs; ++k) s->W = s->W + 1;
+      for (int k = 0; k < s->incs; ++k) {
+        s->W = s->W + 1;
+        if (k == 0) st += maybe_stall(&a->rng, s->stall_permille); /* holding it */
+      }
       atomic_fetch_sub(&s->inside, 1000);
       atomic_fetch_sub_explicit(&s->state, 1u << 16, memory_order_release);
       atomic_fetch_add_explicit(&s->serving, 1, memory_order_release);
@@ -514,16 +559,27 @@ static void* sem_worker(void* p) {
       unsigned mr = atomic_load(&s->max_readers);
       while (in > mr && !atomic_compare_exchange_weak(&s->max_readers, &mr, in)) {
       }
-      for (int k = 0; k < s->incs; ++k) atomic_fetch_add_explicit(&s->R, 1, memory_order_relaxed);
+      for (int k = 0; k < s->incs; ++k) {
+        atomic_fetch_add_explicit(&s->R, 1, memory_order_relaxed);
+        if (k == 0) st += maybe_stall(&a->rng, s->stall_permille); /* holding it */
+      }
       atomic_fetch_sub(&s->inside, 1);
       atomic_fetch_sub_explicit(&s->state, 1, memory_order_release);
     }
   }
+  if (st) atomic_fetch_add(&s->stalls, st);
   return NULL;
 }
 
 double orc_cpu_semaphore(int nthreads, int capacity, int writer_every, int iters, int incs, uint64_t* W,
                          uint64_t* R, uint32_t* max_readers, uint32_t* violations) {
+  return orc_cpu_semaphore_stalls(nthreads, capacity, writer_every, iters, incs, 0, 0, W, R, max_readers,
+                                  violations, NULL);
+}
+
+double orc_cpu_semaphore_stalls(int nthreads, int capacity, int writer_every, int iters, int incs,
+                                int stall_permille, uint64_t seed, uint64_t* W, uint64_t* R,
+                                uint32_t* max_readers, uint32_t* violations, uint64_t* stalls) {
   if (nthreads < 1) nthreads = 1;
   if (writer_every < 1) writer_every = 1;
   sem_t_* s = (sem_t_*)aligned_alloc(64, sizeof(sem_t_));
@@ -532,12 +588,15 @@ double orc_cpu_semaphore(int nthreads, int capacity, int writer_every, int iters
   s->writer_every = writer_every;
   s->iters = iters;
   s->incs = incs;
+  s->stall_permille = stall_permille;
   pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * (size_t)nthreads);
   sem_arg* args = (sem_arg*)malloc(sizeof(sem_arg) * (size_t)nthreads);
   double t0 = now_s();
   for (int t = 0; t < nthreads; ++t) {
     args[t].s = s;
     args[t].id = t;
+    args[t].rng = (seed + 7u) * 0x9e3779b97f4a7c15ull ^ (uint64_t)(t + 1) * 0x94d049bb133111ebull;
+    if (!args[t].rng) args[t].rng = 1;
     pthread_create(&th[t], NULL, sem_worker, &args[t]);
   }
   for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);
@@ -546,6 +605,7 @@ double orc_cpu_semaphore(int nthreads, int capacity, int writer_every, int iters
   if (R) *R = atomic_load(&s->R);
   if (max_readers) *max_readers = atomic_load(&s->max_readers);
   if (violations) *violations = atomic_load(&s->violations);
+  if (stalls) *stalls = atomic_load(&s->stalls);
   free(th);
   free(args);
   free(s);

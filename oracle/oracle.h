@@ -74,6 +74,13 @@ int orc_heterosync_storage_locs(int syncPrim, int numLdSt, int numTBs, int numSM
  * barrier, reads a peer's stamp, crosses again.  Returns ns per barrier episode;
  * *stale receives the number of stale reads (must be 0). */
 double orc_cpu_srb_barrier(int nthreads, int ngroups, int episodes, uint64_t* stale);
+/* The same with injected stalls: at each stall point (before an arrival, in a
+ * group completer, between the root completer's counter reset and its
+ * publish) a participant yields or sleeps 5-100 us with probability
+ * stall_permille / 1000 (seeded per participant); *stalls (may be NULL)
+ * receives how many stalls were taken. */
+double orc_cpu_srb_barrier_stalls(int nthreads, int ngroups, int episodes, int stall_permille, uint64_t seed,
+                                  uint64_t* stale, uint64_t* stalls);
 
 /* Host-thread model of the reader/writer priority semaphore semantics: `nthreads`
  * holders (every `writer_every`-th is a writer) each acquire `iters` times, add
@@ -82,6 +89,11 @@ double orc_cpu_srb_barrier(int nthreads, int ngroups, int episodes, uint64_t* st
  * number of simultaneous readers seen. */
 double orc_cpu_semaphore(int nthreads, int capacity, int writer_every, int iters, int incs,
                          uint64_t* W, uint64_t* R, uint32_t* max_readers, uint32_t* violations);
+/* The same with injected stalls (before each acquire and while holding the
+ * semaphore; see orc_cpu_srb_barrier_stalls). */
+double orc_cpu_semaphore_stalls(int nthreads, int capacity, int writer_every, int iters, int incs,
+                                int stall_permille, uint64_t seed, uint64_t* W, uint64_t* R,
+                                uint32_t* max_readers, uint32_t* violations, uint64_t* stalls);
 
 /* FP64 forward + backward of the policy MLP (12 -> 32 -> 32 -> 4, ReLU; layout
  * of gsrb_mlp_param_count()): masked BCE-with-logits on outputs 0-1, masked

@@ -39,6 +39,13 @@ _lib.orc_cpu_srb_barrier.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_ui
 _lib.orc_cpu_semaphore.restype = C.c_double
 _lib.orc_cpu_semaphore.argtypes = [C.c_int] * 5 + [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                                    C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+_lib.orc_cpu_srb_barrier_stalls.restype = C.c_double
+_lib.orc_cpu_srb_barrier_stalls.argtypes = [C.c_int] * 4 + [C.c_uint64, C.POINTER(C.c_uint64),
+                                                            C.POINTER(C.c_uint64)]
+_lib.orc_cpu_semaphore_stalls.restype = C.c_double
+_lib.orc_cpu_semaphore_stalls.argtypes = [C.c_int] * 6 + [C.c_uint64, C.POINTER(C.c_uint64),
+                                                          C.POINTER(C.c_uint64), C.POINTER(C.c_uint32),
+                                                          C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]
 
 INF = 2**31 - 1
 
@@ -148,6 +155,21 @@ def cpu_srb_barrier(nthreads, ngroups, episodes):
     stale = C.c_uint64()
     ns = _lib.orc_cpu_srb_barrier(nthreads, ngroups, episodes, C.byref(stale))
     return float(ns), int(stale.value)
+
+
+def cpu_srb_barrier_stalls(nthreads, ngroups, episodes, permille, seed):
+    stale, stalls = C.c_uint64(), C.c_uint64()
+    ns = _lib.orc_cpu_srb_barrier_stalls(nthreads, ngroups, episodes, permille, seed, C.byref(stale),
+                                         C.byref(stalls))
+    return float(ns), int(stale.value), int(stalls.value)
+
+
+def cpu_semaphore_stalls(nthreads, capacity, writer_every, iters, incs, permille, seed):
+    W, R, stalls = C.c_uint64(), C.c_uint64(), C.c_uint64()
+    mr, viol = C.c_uint32(), C.c_uint32()
+    rate = _lib.orc_cpu_semaphore_stalls(nthreads, capacity, writer_every, iters, incs, permille, seed,
+                                         C.byref(W), C.byref(R), C.byref(mr), C.byref(viol), C.byref(stalls))
+    return float(rate), int(W.value), int(R.value), int(mr.value), int(viol.value), int(stalls.value)
 
 
 def cpu_semaphore(nthreads, capacity, writer_every, iters, incs):

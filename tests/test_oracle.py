@@ -100,6 +100,21 @@ def test_cpu_barrier_model_no_stale_reads(orc):
         assert stale == 0 and ns > 0
 
 
+@pytest.mark.parametrize("nt,ng", [(5, 0), (8, 3), (12, 4)])
+def test_cpu_barrier_model_injected_stalls(orc, nt, ng):
+    # late arrivals and a completer stalled between its counter reset and its
+    # publish: no participant may run ahead into the next episode
+    ns, stale, stalls = orc.cpu_srb_barrier_stalls(nt, ng, 300, 40, nt * 31 + ng)
+    assert stale == 0 and stalls > 0
+
+
+def test_cpu_semaphore_model_injected_stalls(orc):
+    rate, W, R, mr, viol, stalls = orc.cpu_semaphore_stalls(8, 3, 4, 150, 8, 60, 2022)
+    writers = sum(1 for t in range(8) if t % 4 == 0)
+    assert W == writers * 150 * 8 and R == (8 - writers) * 150 * 8
+    assert viol == 0 and 1 <= mr <= 3 and stalls > 0
+
+
 def test_cpu_semaphore_model_exact_counts(orc):
     rate, W, R, mr, viol = orc.cpu_semaphore(6, 2, 3, 200, 10)
     writers = sum(1 for t in range(6) if t % 3 == 0)
