@@ -252,6 +252,12 @@ enum { GSRB_MUTEX_SPIN = 0, GSRB_MUTEX_EBO = 1, GSRB_MUTEX_FA = 2, GSRB_MUTEX_SL
  * Reference: kernelSpinLockSemaphorePriority, Heterosync/main.cu:962-1040. */
 gsrb_status_t gsrb_semaphore_bench(gsrb_ctx_t ctx, const gsrb_cfg_t* cfg, int32_t kind, uint32_t capacity,
                                    int32_t writer_every, int32_t iters, int32_t incs, uint32_t* d_counters);
+/* Fault test: a semaphore of `capacity` (GSRB_SEM_PRIORITY protocol) is posted
+ * once by a CTA that never waited on it (an over-post), then waited on by that
+ * CTA as a reader and as a writer.  Both waits see the count above its maximum
+ * and fail at once; returns GSRB_ERR_INVARIANT (synchronous).  d_out: 2 uint32,
+ * 1 where the reader / writer wait succeeded, else 0. */
+gsrb_status_t gsrb_semaphore_fault_overpost(gsrb_ctx_t ctx, uint32_t capacity, uint32_t* d_out);
 /* Mutex microbenchmark: every CTA locks `iters` times and adds 1 to W `incs`
  * times with a plain read-modify-write.  Same counter layout.  Synchronous.
  * Reference: kernelSpinLockMutex / EBO / FA / Sleep, Heterosync/main.cu:574-700. */

@@ -57,6 +57,9 @@ struct LockWait {
 __device__ __forceinline__ void lock_record_timeout(const void* buf) {
   ptx::atom_cas_acq_rel_gpu(lock_status_word(buf), 0u, GSRB_DEV_LOCK_TIMEOUT);
 }
+__device__ __forceinline__ void lock_record_invariant(const void* buf) {
+  ptx::atom_cas_acq_rel_gpu(lock_status_word(buf), 0u, GSRB_DEV_INVARIANT);
+}
 
 __device__ __forceinline__ bool cta_bcast(bool v) {
   __shared__ int s_flag;
@@ -245,7 +248,10 @@ __device__ __forceinline__ bool refsem_post(RefSem s, bool is_writer, uint32_t m
 //   writer leaves : red.release count += max, serving += 1 (never waits)
 // Mutual exclusion and the capacity bound rest on the single CAS-ed count
 // word; the queue and ticket words only order writers and hold readers back
-// while a writer waits (writer precedence).
+// while a writer waits (writer precedence).  Every change of the count is an
+// atomic read-modify-write, so in correct use it never exceeds max; a waiter
+// that reads more than max has seen an over-post (a post without its wait)
+// and reports GSRB_DEV_INVARIANT instead of waiting for its deadline.
 struct PrioritySem {
   uint32_t* rec;
   __device__ __forceinline__ uint32_t* count() const { return rec; }
@@ -267,7 +273,8 @@ __device__ __forceinline__ bool psem_wait(PrioritySem s, bool is_writer, const v
       for (;;) {
         if (ptx::ld_relaxed_gpu(s.queued()) == 0u) {
           const uint32_t c = ptx::ld_relaxed_gpu(s.count());
-          if (c > 1u && c <= mx && ptx::atom_cas_acquire_gpu(s.count(), c, c - 1u) == c) break;
+          if (c > mx) { lock_record_invariant(buf); ok = false; break; }  // over-post
+          if (c > 1u && ptx::atom_cas_acquire_gpu(s.count(), c, c - 1u) == c) break;
         }
         if (!w.tick()) { ok = false; break; }
         __nanosleep(b);
@@ -282,14 +289,16 @@ __device__ __forceinline__ bool psem_wait(PrioritySem s, bool is_writer, const v
       }
       if (ok) {
         for (;;) {
-          if (ptx::ld_relaxed_gpu(s.count()) == mx && ptx::atom_cas_acquire_gpu(s.count(), mx, 0u) == mx) break;
+          const uint32_t c = ptx::ld_relaxed_gpu(s.count());
+          if (c > mx) { lock_record_invariant(buf); ok = false; break; }  // over-post
+          if (c == mx && ptx::atom_cas_acquire_gpu(s.count(), mx, 0u) == mx) break;
           if (!w.tick()) { ok = false; break; }
           if (spin_ns) __nanosleep(spin_ns);
         }
       }
       ptx::red_add_relaxed_gpu(s.queued(), 0xffffffffu);
     }
-    if (!ok) lock_record_timeout(buf);
+    if (!ok) lock_record_timeout(buf);  // no-op after an invariant report (first code wins)
   }
   return cta_bcast(ok);
 }

@@ -366,6 +366,11 @@ typedef struct {
   atomic_ullong stale;
   int stall_permille;  /* injected stalls: chance per stall point, in 1/1000 */
   atomic_ullong stalls;
+  int kill_id;         /* participant that leaves for good before kill_episode (-1: none) */
+  int kill_episode;
+  double deadline_s;   /* bound on each wait (0: none) */
+  atomic_int abort;    /* set by the first wait that ran out; every waiter then gives up */
+  atomic_ullong timeouts;
 } srb_t;
 
 typedef struct {
@@ -396,7 +401,7 @@ static int maybe_stall(uint64_t* rng, int permille) {
 
 static unsigned gsize(unsigned n, unsigned g, unsigned i) { return n / g + (i < n % g ? 1u : 0u); }
 
-static void srb_sync(srb_t* b, int id, unsigned* epoch, uint64_t* rng) {
+static int srb_sync(srb_t* b, int id, unsigned* epoch, uint64_t* rng) {
   const unsigned e = *epoch;
   int done = 0;
   unsigned n = (unsigned)b->nthreads;
@@ -420,18 +425,26 @@ root:
     atomic_store_explicit(&b->epoch, e + 1, memory_order_release);
     done = 1;
   }
-  if (st) atomic_fetch_add(&b->stalls, st);
 wait:
+  if (st) atomic_fetch_add(&b->stalls, st);
   if (!done) {
     unsigned spins = 0;
+    const double t0 = b->deadline_s > 0 ? now_s() : 0.0;
     while (atomic_load_explicit(&b->epoch, memory_order_acquire) == e) {
       if (++spins > 4096) {
         sched_yield();
         spins = 0;
+        if (atomic_load_explicit(&b->abort, memory_order_relaxed)) return 0;
+        if (b->deadline_s > 0 && now_s() - t0 > b->deadline_s) {
+          atomic_store(&b->abort, 1);
+          atomic_fetch_add(&b->timeouts, 1);
+          return 0;
+        }
       }
     }
   }
   *epoch = e + 1;
+  return 1;
 }
 
 static void* srb_worker(void* p) {
@@ -440,23 +453,38 @@ static void* srb_worker(void* p) {
   unsigned epoch = atomic_load_explicit(&b->epoch, memory_order_acquire);
   unsigned long long bad = 0;
   for (int e = 0; e < b->episodes; ++e) {
+    if (a->id == b->kill_id && e == b->kill_episode) break; /* leaves, never arrives again */
     unsigned stamp = 0x9e3779b9u * (unsigned)(e + 1);
     atomic_store_explicit(&b->stamps[a->id * 16], stamp, memory_order_relaxed);
-    srb_sync(b, a->id, &epoch, &a->rng);
+    if (!srb_sync(b, a->id, &epoch, &a->rng)) break;
     int peer = (a->id + 1 + e) % b->nthreads;
     if (atomic_load_explicit(&b->stamps[peer * 16], memory_order_relaxed) != stamp) ++bad;
-    srb_sync(b, a->id, &epoch, &a->rng);
+    if (!srb_sync(b, a->id, &epoch, &a->rng)) break;
   }
   atomic_fetch_add(&b->stale, bad);
   return NULL;
 }
 
+static double srb_run(int nthreads, int ngroups, int episodes, int stall_permille, uint64_t seed, int kill_id,
+                      int kill_episode, int deadline_ms, uint64_t* stale, uint64_t* stalls, uint64_t* timeouts);
+
 double orc_cpu_srb_barrier(int nthreads, int ngroups, int episodes, uint64_t* stale) {
-  return orc_cpu_srb_barrier_stalls(nthreads, ngroups, episodes, 0, 0, stale, NULL);
+  return srb_run(nthreads, ngroups, episodes, 0, 0, -1, 0, 0, stale, NULL, NULL);
 }
 
 double orc_cpu_srb_barrier_stalls(int nthreads, int ngroups, int episodes, int stall_permille, uint64_t seed,
                                   uint64_t* stale, uint64_t* stalls) {
+  return srb_run(nthreads, ngroups, episodes, stall_permille, seed, -1, 0, 0, stale, stalls, NULL);
+}
+
+double orc_cpu_srb_barrier_kill(int nthreads, int ngroups, int episodes, int kill_id, int kill_episode,
+                                int deadline_ms, uint64_t* stale, uint64_t* timeouts) {
+  return srb_run(nthreads, ngroups, episodes, 0, 0, kill_id, kill_episode, deadline_ms > 0 ? deadline_ms : 1,
+                 stale, NULL, timeouts);
+}
+
+static double srb_run(int nthreads, int ngroups, int episodes, int stall_permille, uint64_t seed, int kill_id,
+                      int kill_episode, int deadline_ms, uint64_t* stale, uint64_t* stalls, uint64_t* timeouts) {
   if (nthreads < 1) nthreads = 1;
   if (nthreads > 1024) nthreads = 1024;
   srb_t* b = (srb_t*)aligned_alloc(64, sizeof(srb_t));
@@ -465,6 +493,9 @@ double orc_cpu_srb_barrier_stalls(int nthreads, int ngroups, int episodes, int s
   b->nthreads = nthreads;
   b->episodes = episodes;
   b->stall_permille = stall_permille;
+  b->kill_id = kill_id;
+  b->kill_episode = kill_episode;
+  b->deadline_s = deadline_ms * 1e-3;
   b->groups = (grp_t*)aligned_alloc(64, sizeof(grp_t) * (size_t)(ngroups > 0 ? ngroups : 1));
   memset(b->groups, 0, sizeof(grp_t) * (size_t)(ngroups > 0 ? ngroups : 1));
   b->stamps = (atomic_uint*)aligned_alloc(64, sizeof(atomic_uint) * 16 * (size_t)nthreads);
@@ -483,6 +514,7 @@ double orc_cpu_srb_barrier_stalls(int nthreads, int ngroups, int episodes, int s
   double t1 = now_s();
   if (stale) *stale = atomic_load(&b->stale);
   if (stalls) *stalls = atomic_load(&b->stalls);
+  if (timeouts) *timeouts = atomic_load(&b->timeouts);
   free(th);
   free(args);
   free(b->stamps);

@@ -81,6 +81,14 @@ double orc_cpu_srb_barrier(int nthreads, int ngroups, int episodes, uint64_t* st
  * receives how many stalls were taken. */
 double orc_cpu_srb_barrier_stalls(int nthreads, int ngroups, int episodes, int stall_permille, uint64_t seed,
                                   uint64_t* stale, uint64_t* stalls);
+/* The same with a participant that leaves for good: kill_id stops before
+ * episode kill_episode and never arrives again.  Every wait is bounded by
+ * deadline_ms; the first wait that runs out raises an abort flag and every
+ * other waiter gives up at its next poll (the device's abort-word protocol).
+ * Returns when all participants have left; *timeouts receives the number of
+ * waits that ran out (>= 1 when someone was killed before the end). */
+double orc_cpu_srb_barrier_kill(int nthreads, int ngroups, int episodes, int kill_id, int kill_episode,
+                                int deadline_ms, uint64_t* stale, uint64_t* timeouts);
 
 /* Host-thread model of the reader/writer priority semaphore semantics: `nthreads`
  * holders (every `writer_every`-th is a writer) each acquire `iters` times, add

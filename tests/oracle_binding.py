@@ -42,6 +42,8 @@ _lib.orc_cpu_semaphore.argtypes = [C.c_int] * 5 + [C.POINTER(C.c_uint64), C.POIN
 _lib.orc_cpu_srb_barrier_stalls.restype = C.c_double
 _lib.orc_cpu_srb_barrier_stalls.argtypes = [C.c_int] * 4 + [C.c_uint64, C.POINTER(C.c_uint64),
                                                             C.POINTER(C.c_uint64)]
+_lib.orc_cpu_srb_barrier_kill.restype = C.c_double
+_lib.orc_cpu_srb_barrier_kill.argtypes = [C.c_int] * 6 + [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
 _lib.orc_cpu_semaphore_stalls.restype = C.c_double
 _lib.orc_cpu_semaphore_stalls.argtypes = [C.c_int] * 6 + [C.c_uint64, C.POINTER(C.c_uint64),
                                                           C.POINTER(C.c_uint64), C.POINTER(C.c_uint32),
@@ -162,6 +164,13 @@ def cpu_srb_barrier_stalls(nthreads, ngroups, episodes, permille, seed):
     ns = _lib.orc_cpu_srb_barrier_stalls(nthreads, ngroups, episodes, permille, seed, C.byref(stale),
                                          C.byref(stalls))
     return float(ns), int(stale.value), int(stalls.value)
+
+
+def cpu_srb_barrier_kill(nthreads, ngroups, episodes, kill_id, kill_episode, deadline_ms):
+    stale, timeouts = C.c_uint64(), C.c_uint64()
+    _lib.orc_cpu_srb_barrier_kill(nthreads, ngroups, episodes, kill_id, kill_episode, deadline_ms,
+                                  C.byref(stale), C.byref(timeouts))
+    return int(stale.value), int(timeouts.value)
 
 
 def cpu_semaphore_stalls(nthreads, capacity, writer_every, iters, incs, permille, seed):

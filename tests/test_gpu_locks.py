@@ -67,3 +67,17 @@ def test_semaphore_full_residency(gsrb, ctx):
     grid = 8 * ctx.num_sms
     writers = len([b for b in range(grid) if b % 11 == 0])
     assert viol == 0 and tmo == 0 and W == writers * 200 and R == (grid - writers) * 200
+
+
+@pytest.mark.parametrize("cap", [1, 2, 120])
+def test_semaphore_overpost_detected(gsrb, ctx, cap):
+    # a post without its wait pushes the count above its maximum: the next
+    # waits report the invariant at once (no deadline), and the context and
+    # a fresh semaphore work afterwards
+    out = ctx.array(2, np.uint32).zero()
+    assert ctx.semaphore_fault_overpost(cap, out) == gsrb.ERR_INVARIANT
+    assert out.download().tolist() == [0, 0]
+    assert ctx.status()[0] == 0
+    cnt = _counters(ctx)
+    gsrb.check(ctx.semaphore_bench(gsrb.cfg(ctas_per_sm=1, threads=64, timeout_ms=3000), 4, cap, 5, 2, 10, cnt))
+    assert cnt.download().tolist()[6] == 0

@@ -1,5 +1,6 @@
 """The oracle pinned against the reference's golden vectors and known answers (CPU)."""
 import pathlib
+import time
 
 import numpy as np
 import pytest
@@ -106,6 +107,19 @@ def test_cpu_barrier_model_injected_stalls(orc, nt, ng):
     # publish: no participant may run ahead into the next episode
     ns, stale, stalls = orc.cpu_srb_barrier_stalls(nt, ng, 300, 40, nt * 31 + ng)
     assert stale == 0 and stalls > 0
+
+
+@pytest.mark.parametrize("nt,ng,kill", [(4, 0, 2), (8, 3, 0), (8, 3, 7)])
+def test_cpu_barrier_model_killed_participant_times_out(orc, nt, ng, kill):
+    # a participant leaves for good after 50 episodes: the others' bounded
+    # waits run out, the abort flag ends every wait, the run returns
+    t0 = time.time()
+    stale, timeouts = orc.cpu_srb_barrier_kill(nt, ng, 400, kill, 50, 200)
+    assert timeouts >= 1 and stale == 0
+    assert time.time() - t0 < 20
+    # nobody killed: no timeouts
+    stale, timeouts = orc.cpu_srb_barrier_kill(nt, ng, 200, -1, 0, 2000)
+    assert timeouts == 0 and stale == 0
 
 
 def test_cpu_semaphore_model_injected_stalls(orc):

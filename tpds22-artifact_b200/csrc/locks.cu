@@ -174,6 +174,21 @@ semaphore_bench_kernel(uint32_t* rec, const void* statbuf, int writer_every, int
   }
 }
 
+// Fault test: one CTA posts the native priority semaphore without having
+// waited on it (an over-post, the usage error the count gauge catches), then
+// waits on it as a reader and as a writer; both waits must report the
+// invariant at once instead of running into their deadline.
+__global__ void __launch_bounds__(256)
+semaphore_overpost_kernel(uint32_t* rec, const void* statbuf, uint64_t timeout_ns, uint32_t* out) {
+  gsrb::psem_post(gsrb::PrioritySem{rec}, false);
+  const bool r = gsrb::psem_wait(gsrb::PrioritySem{rec}, false, statbuf, timeout_ns, 0);
+  const bool w = gsrb::psem_wait(gsrb::PrioritySem{rec}, true, statbuf, timeout_ns, 0);
+  if (threadIdx.x == 0) {
+    out[0] = r ? 1u : 0u;
+    out[1] = w ? 1u : 0u;
+  }
+}
+
 template <int KIND>
 __global__ void __launch_bounds__(256)
 mutex_bench_kernel(uint32_t* heads, uint32_t* tails, int32_t* ring, uint32_t ring_max, const void* statbuf,
@@ -316,6 +331,25 @@ gsrb_status_t gsrb_semaphore_bench(gsrb_ctx_t ctx, const gsrb_cfg_t* cfgin, int3
     Counters* cc = (Counters*)d_counters;
     void* args[] = {&rec, &statbuf, &writer_every, &iters, &incs, &to, &spin, &cc};
     st = launch_persistent(ctx, fn, grid, c.threads, 0, 1, c.launch_mode == 1 ? 0 : 1, args);
+  }
+  gsrb_status_t st2 = gsrb_locks_status(L, nullptr);
+  gsrb_locks_destroy(L);
+  return st ? st : st2;
+}
+
+gsrb_status_t gsrb_semaphore_fault_overpost(gsrb_ctx_t ctx, uint32_t capacity, uint32_t* d_out) {
+  if (!ctx || !d_out || capacity < 1 || capacity > 60000) return GSRB_ERR_ARG;
+  gsrb_locks_t L = nullptr;
+  gsrb_status_t st = gsrb_locks_create(ctx, 1, 1, 1, 1, &L);
+  if (st) return st;
+  st = gsrb_semaphore_init(L, 0, capacity, 1);
+  if (!st) {
+    std::lock_guard<std::mutex> g(ctx->mu);
+    uint32_t* rec = L->st.d.semaphoreBuffers;
+    const void* statbuf = rec;
+    uint64_t to = 200ull * 1000000ull;  // a missed detection ends in 0.2 s, not a hang
+    void* args[] = {&rec, &statbuf, &to, &d_out};
+    st = launch_plain(ctx, (const void*)semaphore_overpost_kernel, dim3(1), dim3(32), 0, args);
   }
   gsrb_status_t st2 = gsrb_locks_status(L, nullptr);
   gsrb_locks_destroy(L);

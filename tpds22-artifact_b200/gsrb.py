@@ -155,6 +155,7 @@ _SIGS = {
     "gsrb_semaphore_bench": (C.c_int32, [_P, C.POINTER(Cfg), C.c_int32, C.c_uint32, C.c_int32, C.c_int32,
                                          C.c_int32, _P]),
     "gsrb_mutex_bench": (C.c_int32, [_P, C.POINTER(Cfg), C.c_int32, C.c_int32, C.c_int32, _P]),
+    "gsrb_semaphore_fault_overpost": (C.c_int32, [_P, C.c_uint32, _P]),
     "gsrb_graph_upload": (C.c_int32, [_P, C.POINTER(HostCSR), C.POINTER(_P)]),
     "gsrb_graph_free": (C.c_int32, [_P]),
     "gsrb_graph_info": (C.c_int32, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
@@ -422,6 +423,9 @@ class Context:
                         counters: DeviceArray) -> int:
         return _lib().gsrb_semaphore_bench(self.h, C.byref(c), kind, capacity, writer_every, iters, incs,
                                            counters.ptr)
+
+    def semaphore_fault_overpost(self, capacity: int, out: DeviceArray) -> int:
+        return _lib().gsrb_semaphore_fault_overpost(self.h, capacity, out.ptr)
 
     def mutex_bench(self, c: Cfg, kind: int, iters: int, incs: int, counters: DeviceArray) -> int:
         return _lib().gsrb_mutex_bench(self.h, C.byref(c), kind, iters, incs, counters.ptr)
