@@ -671,15 +671,19 @@ def batch_numbers(gsrb, ctx, orc, params):
     return res
 
 
-def cpu_barrier_baseline(orc, seconds=8.0):
+def cpu_barrier_baseline(orc, nctas, seconds=8.0):
+    """The reference's two-level sense-reversing barrier restated on the host
+    cores, with the same participants as the GPU workload: `nctas` CTAs in
+    min(nctas, 148) groups (CTA % 148, as the reference groups by blockIdx %
+    NUM_SM), carried by one thread per core, each arriving for its CTAs in turn."""
     threads = os.cpu_count() or 1
-    groups = 0 if threads <= 4 else max(2, threads // 4)
-    ns, stale = orc.cpu_srb_barrier(threads, groups, 2000)
-    episodes = int(max(2000, min(5_000_000, seconds * 1e9 / max(ns, 1.0) / 2)))
-    ns, stale = orc.cpu_srb_barrier(threads, groups, episodes)
+    groups = min(nctas, 148)
+    ns, stale = orc.cpu_srb_barrier_vcta(threads, nctas, groups, 200)
+    episodes = int(max(200, min(5_000_000, seconds * 1e9 / max(ns, 1.0) / 2)))
+    ns, stale = orc.cpu_srb_barrier_vcta(threads, nctas, groups, episodes)
     return {"value": round(ns, 2), "unit": "ns per barrier", "cores": threads, "kind": "port",
-            "sample": f"{threads} host threads (one per core, standing in for the 1184 CTAs), {groups} groups, "
-                      f"{2 * episodes} barrier episodes, stale reads {stale}"}
+            "sample": f"{nctas} CTAs (the GPU workload's) carried by {threads} host threads, one per core, "
+                      f"{groups} groups, {2 * episodes} barrier episodes, F=0, stale reads {stale}"}
 
 
 # ----------------------------------------------------------------------- main
@@ -718,7 +722,7 @@ def main():
         if dist.rank == 0:
             orc = load_oracle()
             t0 = time.time()
-            samples = [cpu_barrier_baseline(orc, seconds=4.0) for _ in range(max(1, min(args.steps, 3)))]
+            samples = [cpu_barrier_baseline(orc, 148 * args.k, seconds=4.0) for _ in range(max(1, min(args.steps, 3)))]
             v = statistics.median(s["value"] for s in samples)
             line = {"impl": "reference", "metric": "ns per grid barrier", "value": v, "unit": "ns",
                     "n_gpus": args.gpus, "steps": len(samples), "warmup": args.warmup,
@@ -851,7 +855,7 @@ def main():
         line["segments"] = segment_numbers(gsrb, ctx, orc, tune, cache)
         line["extras_wall_s"] = round(time.time() - extras_t0, 1)
         if dist.rank == 0:
-            line["cpu_baseline"] = cpu_barrier_baseline(orc)
+            line["cpu_baseline"] = cpu_barrier_baseline(orc, 148 * args.k)
     line["autotuned"] = cache
 
     if dist.rank == 0:

@@ -361,6 +361,7 @@ typedef struct {
   grp_t* groups;
   int ngroups;
   int nthreads;
+  int nparts;  /* participants (>= nthreads): thread t arrives for t, t + nthreads, ... */
   int episodes;
   atomic_uint* stamps; /* one per thread, each on its own line (stride 16) */
   atomic_ullong stale;
@@ -401,31 +402,34 @@ static int maybe_stall(uint64_t* rng, int permille) {
 
 static unsigned gsize(unsigned n, unsigned g, unsigned i) { return n / g + (i < n % g ? 1u : 0u); }
 
+/* One arrival of participant `vid` (of b->nparts) in episode e; returns 1 if
+ * it completed the episode and published it. */
+static int srb_arrive(srb_t* b, unsigned vid, unsigned e, uint64_t* rng, unsigned long long* st) {
+  unsigned n = (unsigned)b->nparts;
+  if (b->ngroups > 1 && n > (unsigned)b->ngroups) {
+    unsigned g = vid % (unsigned)b->ngroups;
+    unsigned gs = gsize(n, (unsigned)b->ngroups, g);
+    if (atomic_fetch_add_explicit(&b->groups[g].count, 1, memory_order_acq_rel) != gs - 1) return 0;
+    atomic_store_explicit(&b->groups[g].count, 0, memory_order_relaxed);
+    *st += maybe_stall(rng, b->stall_permille); /* group completer slow to go on */
+    n = (unsigned)b->ngroups;
+  }
+  if (atomic_fetch_add_explicit(&b->count, 1, memory_order_acq_rel) != n - 1) return 0;
+  atomic_store_explicit(&b->count, 0, memory_order_relaxed);
+  *st += maybe_stall(rng, b->stall_permille); /* between the reset and the publish */
+  atomic_store_explicit(&b->epoch, e + 1, memory_order_release);
+  return 1;
+}
+
+/* A host thread arrives for each participant it stands for (vid = id,
+ * id + nthreads, ...), then waits for the episode to be published. */
 static int srb_sync(srb_t* b, int id, unsigned* epoch, uint64_t* rng) {
   const unsigned e = *epoch;
   int done = 0;
-  unsigned n = (unsigned)b->nthreads;
   unsigned long long st = 0;
   st += maybe_stall(rng, b->stall_permille); /* late arrival */
-  if (b->ngroups > 1 && n > (unsigned)b->ngroups) {
-    unsigned g = (unsigned)id % (unsigned)b->ngroups;
-    unsigned gs = gsize(n, (unsigned)b->ngroups, g);
-    if (atomic_fetch_add_explicit(&b->groups[g].count, 1, memory_order_acq_rel) == gs - 1) {
-      atomic_store_explicit(&b->groups[g].count, 0, memory_order_relaxed);
-      st += maybe_stall(rng, b->stall_permille); /* group completer slow to go on */
-      n = (unsigned)b->ngroups;
-      goto root;
-    }
-    goto wait;
-  }
-root:
-  if (atomic_fetch_add_explicit(&b->count, 1, memory_order_acq_rel) == n - 1) {
-    atomic_store_explicit(&b->count, 0, memory_order_relaxed);
-    st += maybe_stall(rng, b->stall_permille); /* between the reset and the publish */
-    atomic_store_explicit(&b->epoch, e + 1, memory_order_release);
-    done = 1;
-  }
-wait:
+  for (unsigned v = (unsigned)id; v < (unsigned)b->nparts; v += (unsigned)b->nthreads)
+    done |= srb_arrive(b, v, e, rng, &st);
   if (st) atomic_fetch_add(&b->stalls, st);
   if (!done) {
     unsigned spins = 0;
@@ -465,32 +469,39 @@ static void* srb_worker(void* p) {
   return NULL;
 }
 
-static double srb_run(int nthreads, int ngroups, int episodes, int stall_permille, uint64_t seed, int kill_id,
-                      int kill_episode, int deadline_ms, uint64_t* stale, uint64_t* stalls, uint64_t* timeouts);
+static double srb_run(int nthreads, int nparts, int ngroups, int episodes, int stall_permille, uint64_t seed,
+                      int kill_id, int kill_episode, int deadline_ms, uint64_t* stale, uint64_t* stalls,
+                      uint64_t* timeouts);
 
 double orc_cpu_srb_barrier(int nthreads, int ngroups, int episodes, uint64_t* stale) {
-  return srb_run(nthreads, ngroups, episodes, 0, 0, -1, 0, 0, stale, NULL, NULL);
+  return srb_run(nthreads, 0, ngroups, episodes, 0, 0, -1, 0, 0, stale, NULL, NULL);
+}
+
+double orc_cpu_srb_barrier_vcta(int nthreads, int nctas, int ngroups, int episodes, uint64_t* stale) {
+  return srb_run(nthreads, nctas, ngroups, episodes, 0, 0, -1, 0, 0, stale, NULL, NULL);
 }
 
 double orc_cpu_srb_barrier_stalls(int nthreads, int ngroups, int episodes, int stall_permille, uint64_t seed,
                                   uint64_t* stale, uint64_t* stalls) {
-  return srb_run(nthreads, ngroups, episodes, stall_permille, seed, -1, 0, 0, stale, stalls, NULL);
+  return srb_run(nthreads, 0, ngroups, episodes, stall_permille, seed, -1, 0, 0, stale, stalls, NULL);
 }
 
 double orc_cpu_srb_barrier_kill(int nthreads, int ngroups, int episodes, int kill_id, int kill_episode,
                                 int deadline_ms, uint64_t* stale, uint64_t* timeouts) {
-  return srb_run(nthreads, ngroups, episodes, 0, 0, kill_id, kill_episode, deadline_ms > 0 ? deadline_ms : 1,
+  return srb_run(nthreads, 0, ngroups, episodes, 0, 0, kill_id, kill_episode, deadline_ms > 0 ? deadline_ms : 1,
                  stale, NULL, timeouts);
 }
 
-static double srb_run(int nthreads, int ngroups, int episodes, int stall_permille, uint64_t seed, int kill_id,
-                      int kill_episode, int deadline_ms, uint64_t* stale, uint64_t* stalls, uint64_t* timeouts) {
+static double srb_run(int nthreads, int nparts, int ngroups, int episodes, int stall_permille, uint64_t seed,
+                      int kill_id, int kill_episode, int deadline_ms, uint64_t* stale, uint64_t* stalls,
+                      uint64_t* timeouts) {
   if (nthreads < 1) nthreads = 1;
   if (nthreads > 1024) nthreads = 1024;
   srb_t* b = (srb_t*)aligned_alloc(64, sizeof(srb_t));
   memset(b, 0, sizeof(*b));
   b->ngroups = ngroups;
   b->nthreads = nthreads;
+  b->nparts = nparts > nthreads ? nparts : nthreads;
   b->episodes = episodes;
   b->stall_permille = stall_permille;
   b->kill_id = kill_id;

@@ -74,6 +74,11 @@ int orc_heterosync_storage_locs(int syncPrim, int numLdSt, int numTBs, int numSM
  * barrier, reads a peer's stamp, crosses again.  Returns ns per barrier episode;
  * *stale receives the number of stale reads (must be 0). */
 double orc_cpu_srb_barrier(int nthreads, int ngroups, int episodes, uint64_t* stale);
+/* The same barrier with `nctas` participants (the CTAs of a grid) carried by
+ * `nthreads` host threads: thread t arrives for participants t, t + nthreads,
+ * ... in turn (group counters by participant % ngroups, as the reference
+ * groups CTAs by blockIdx % NUM_SM), then waits once for the episode. */
+double orc_cpu_srb_barrier_vcta(int nthreads, int nctas, int ngroups, int episodes, uint64_t* stale);
 /* The same with injected stalls: at each stall point (before an arrival, in a
  * group completer, between the root completer's counter reset and its
  * publish) a participant yields or sleeps 5-100 us with probability

@@ -42,6 +42,8 @@ _lib.orc_cpu_semaphore.argtypes = [C.c_int] * 5 + [C.POINTER(C.c_uint64), C.POIN
 _lib.orc_cpu_srb_barrier_stalls.restype = C.c_double
 _lib.orc_cpu_srb_barrier_stalls.argtypes = [C.c_int] * 4 + [C.c_uint64, C.POINTER(C.c_uint64),
                                                             C.POINTER(C.c_uint64)]
+_lib.orc_cpu_srb_barrier_vcta.restype = C.c_double
+_lib.orc_cpu_srb_barrier_vcta.argtypes = [C.c_int] * 4 + [C.POINTER(C.c_uint64)]
 _lib.orc_cpu_srb_barrier_kill.restype = C.c_double
 _lib.orc_cpu_srb_barrier_kill.argtypes = [C.c_int] * 6 + [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
 _lib.orc_cpu_semaphore_stalls.restype = C.c_double
@@ -164,6 +166,12 @@ def cpu_srb_barrier_stalls(nthreads, ngroups, episodes, permille, seed):
     ns = _lib.orc_cpu_srb_barrier_stalls(nthreads, ngroups, episodes, permille, seed, C.byref(stale),
                                          C.byref(stalls))
     return float(ns), int(stale.value), int(stalls.value)
+
+
+def cpu_srb_barrier_vcta(nthreads, nctas, ngroups, episodes):
+    stale = C.c_uint64()
+    ns = _lib.orc_cpu_srb_barrier_vcta(nthreads, nctas, ngroups, episodes, C.byref(stale))
+    return float(ns), int(stale.value)
 
 
 def cpu_srb_barrier_kill(nthreads, ngroups, episodes, kill_id, kill_episode, deadline_ms):

@@ -122,6 +122,13 @@ def test_cpu_barrier_model_killed_participant_times_out(orc, nt, ng, kill):
     assert timeouts == 0 and stale == 0
 
 
+@pytest.mark.parametrize("nt,nctas,ng", [(4, 1184, 148), (8, 296, 148), (3, 10, 0), (16, 1184, 148)])
+def test_cpu_barrier_model_many_ctas_per_thread(orc, nt, nctas, ng):
+    # host threads carrying many participants each (the grid's CTAs)
+    ns, stale = orc.cpu_srb_barrier_vcta(nt, nctas, ng, 300)
+    assert stale == 0 and ns > 0
+
+
 def test_cpu_semaphore_model_injected_stalls(orc):
     rate, W, R, mr, viol, stalls = orc.cpu_semaphore_stalls(8, 3, 4, 150, 8, 60, 2022)
     writers = sum(1 for t in range(8) if t % 4 == 0)
