@@ -223,8 +223,10 @@ def l2_atomic_peak(ctx):
     ctx.probe_l2_atomics(ctas, 200, 0)
     ms = min(ctx.probe_l2_atomics(ctas, iters, 0) for _ in range(3))
     rate = ctas * iters / (ms * 1e-3)
-    ctx.probe_l2_atomics(1, 1000, 1)
-    ms1 = min(ctx.probe_l2_atomics(1, 20000, 1) for _ in range(3))
+    # the round trip is one CTA's dependent chain: the fastest of several runs
+    # after a longer warm-up (a single slow sample once doubled it)
+    ctx.probe_l2_atomics(1, 5000, 1)
+    ms1 = min(ctx.probe_l2_atomics(1, 20000, 1) for _ in range(7))
     return rate, ms1 * 1e6 / 20000
 
 
@@ -363,7 +365,7 @@ def train_policy(gsrb, ctx, pol):
     graphs = [gsrb.rmat(s, 16, seed=SEED + 1000 + s) for s in (14, 16, 18, 20, 21, 22)]
     graphs += [gsrb.grid2d(256, 256, seed=SEED + 7), gsrb.grid2d(1024, 64, seed=SEED + 8),
                gsrb.grid2d(1024, 1024, seed=SEED + 9), gsrb.grid2d(2048, 512, seed=SEED + 10),
-               gsrb.grid2d(4096, 1024, seed=SEED + 11)]
+               gsrb.grid2d(4096, 1024, seed=SEED + 11), gsrb.grid2d(3072, 1536, seed=SEED + 12)]
     X, Y, M = [], [], []
     cands = pol.launch_candidates()
     launch = []

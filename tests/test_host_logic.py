@@ -196,6 +196,24 @@ def test_trace_files_roundtrip_and_labels(gsrb, pol, tmp_path):
     assert Y[0, 2] == pytest.approx(math.log2(11)) and Y[3, 2] == 0.0
 
 
+def test_level_rows_capped_per_graph(gsrb, pol):
+    # a long traversal (a mesh) weighs as much as LEVEL_CAP levels in total
+    L = 4 * pol.LEVEL_CAP
+    nfs = [1] + [2] * (L - 1)
+    push = _fake_trace(gsrb, nfs, [4] * L)
+    t = np.full(L, 100.0)
+    rec = {"n": 100000, "m": 400000, "src": 0, "push": push, "pull": push.copy(), "topo": push.copy(),
+           "push_ns": t, "pull_ns": t * 2, "topo_ns": t * 2}
+    X, Y, M = pol.features_labels(rec)
+    assert X.shape == (L, 12)
+    assert M[:, 2].sum() == pytest.approx(pol.LEVEL_CAP)
+    short = _fake_trace(gsrb, [1, 10, 300, 50], [16, 160, 4800, 800])
+    rec2 = dict(rec, push=short, pull=short.copy(), topo=short.copy(), push_ns=t[:4], pull_ns=t[:4] * 2,
+                topo_ns=t[:4] * 2)
+    _, _, M2 = pol.features_labels(rec2)
+    assert M2[:, 2].sum() == 4.0
+
+
 def test_launch_label_first_level_only(gsrb, pol, tmp_path):
     push = _fake_trace(gsrb, [1, 10, 300, 50], [16, 160, 4800, 800])
     rec = {"n": 1000, "m": 16000, "src": 0, "push": push, "pull": push.copy(), "topo": push.copy(),

@@ -49,6 +49,12 @@ def level_times(trace: np.ndarray, total_ms: float | None = None) -> np.ndarray:
 
 
 TOPO_MARGIN = 0.8
+# level rows of one graph count as at most LEVEL_CAP rows: a mesh has thousands
+# of near-identical levels and an R-MAT graph six to ten, and without the cap
+# the meshes decide the fit of every head (one added 4.7 M-vertex mesh once
+# made the next-frontier head miss R-MAT's second level by more than 2x, so
+# every R-MAT traversal fell back to the heuristic)
+LEVEL_CAP = 64
 # weight of one launch row, and the sources sampled per graph for them (a few
 # rows per graph against thousands of level rows)
 LAUNCH_WEIGHT = 10.0
@@ -149,6 +155,8 @@ def features_labels(rec: dict):
         Y[i, 2] = np.log2(1.0 + nxt)
         M[i, 2] = 1.0
         prev_dir = 1 if Y[i, 0] > 0.5 and M[i, 0] > 0 else 0
+    if L > LEVEL_CAP:
+        M[:, :3] *= LEVEL_CAP / L
     if rec.get("launch_ms") is not None:
         # launch rows: the first level's features from each sampled source
         t0, t1 = (max(float(x), 1e-6) for x in rec["launch_ms"])
