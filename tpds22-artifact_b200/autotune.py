@@ -122,7 +122,7 @@ def segment_candidates(kind: str):
     length, 0 = 4 tiles of 16 x threads)."""
     g = _g()
     out = []
-    for k, threads in ((2, 512), (4, 256), (2, 256), (1, 1024)):
+    for k, threads in ((2, 512), (4, 256), (8, 128), (2, 256), (1, 1024)):
         for cand in (dict(variant=g.BAR_FANOUT, wake_lines=4), dict(variant=g.BAR_FLIP, fanin_groups=1),
                      dict(variant=g.BAR_FLAT)):
             for tile in ((0, 8 * 16 * threads) if kind == "scan" else (0,)):
