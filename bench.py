@@ -589,7 +589,18 @@ def segment_numbers(gsrb, ctx, orc, tune, cache, k=64, reps=5, fixed=None):
                      "batched_hbm_frac": round(nbytes / (tb * 1e-3) / 1e9 / peak, 4),
                      "per_segment_ms": round(ts, 4), "per_segment_graph_ms": round(tg, 4),
                      "speedup_vs_per_segment_graph": round(tg / tb, 3), "bit_exact": bool(ok_b and ok_s)}
-    for x in (da, du, dsum, dscan):
+    # FP32 segments with the scan's configuration, within 1e-5 relative per element
+    f = gsrb.uniform_f32(SEED + 3, n)
+    df, dfo = ctx.to_device(f), ctx.array(n, np.float32)
+    tf = timed(lambda: gsrb.check(ctx.scan_segments(df, dfo, off, cb["scan"])))
+    got = dfo.download()
+    err = max((orc.max_rel_err(got[int(off[i]) + 1:int(off[i + 1])],
+                               orc.scan_f32_f64(f[int(off[i]):int(off[i + 1])])[1:])
+               for i in range(k) if off[i + 1] > off[i] + 1), default=0.0)
+    res["scan_f32"] = {"batched_ms": round(tf, 4), "batched_GB_s": round(8 * n / (tf * 1e-3) / 1e9, 1),
+                       "batched_hbm_frac": round(8 * n / (tf * 1e-3) / 1e9 / peak, 4),
+                       "max_rel_err": err, "within_1e-5": bool(err <= 1e-5)}
+    for x in (da, du, dsum, dscan, df, dfo):
         x.free()
     return res
 

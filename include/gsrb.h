@@ -203,6 +203,10 @@ gsrb_status_t gsrb_reduce_i32_segments(gsrb_ctx_t ctx, const int32_t* d_in, cons
  * that the rescan re-reads L2. */
 gsrb_status_t gsrb_scan_u32_segments(gsrb_ctx_t ctx, const uint32_t* d_in, uint32_t* d_out, const uint64_t* h_off,
                                      int32_t k, const gsrb_cfg_t* cfg);
+/* The same for FP32: chunk sums and carries in FP64, each tile scanned in FP32
+ * (within 1e-5 relative of an FP64 prefix, as gsrb_scan_f32). */
+gsrb_status_t gsrb_scan_f32_segments(gsrb_ctx_t ctx, const float* d_in, float* d_out, const uint64_t* h_off,
+                                     int32_t k, const gsrb_cfg_t* cfg);
 /* Host: the CTA layout those calls use for a grid of `grid` CTAs (first[k], count[k]). */
 gsrb_status_t gsrb_segments_layout(const uint64_t* h_off, int32_t k, int32_t grid, uint32_t* first, uint32_t* count);
 

@@ -59,6 +59,31 @@ def test_scan_segments_exact(gsrb, ctx, orc, variant, k):
     assert np.array_equal(got, _want_scan(orc, a, off))
 
 
+REL_TOL_F32 = 1e-5
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+@pytest.mark.parametrize("k", [1, 9, 127])
+def test_scan_f32_segments_within_tolerance(gsrb, ctx, orc, variant, k):
+    # FP32 values U[0,1): every element within 1e-5 relative of the FP64 prefix
+    # of its segment (the first element of a segment is exactly 0)
+    off = _uneven_offsets(200 + k, k, hi=1 << 19)
+    a = gsrb.uniform_f32(0x5EED2022 + k, int(off[-1]))
+    d = ctx.to_device(a) if a.size else ctx.array(1, np.float32)
+    out = ctx.array(max(a.size, 1), np.float32).zero()
+    c = gsrb.cfg(variant=variant, ctas_per_sm=2, threads=256, tile=1 if k == 9 else 0)
+    gsrb.check(ctx.scan_segments(d, out, off, c), "scan_f32_segments")
+    ctx.check_status("scan_f32_segments")
+    got = out.download()[: a.size]
+    for i in range(k):
+        s0, e0 = int(off[i]), int(off[i + 1])
+        if e0 == s0:
+            continue
+        assert got[s0] == 0.0
+        if e0 - s0 > 1:
+            assert orc.max_rel_err(got[s0 + 1:e0], orc.scan_f32_f64(a[s0:e0])[1:]) <= REL_TOL_F32
+
+
 @pytest.mark.parametrize("variant", VARIANTS)
 def test_scan_segments_many_rounds(gsrb, ctx, orc, variant):
     # one tile per CTA per round: tens of rounds per segment, so the double

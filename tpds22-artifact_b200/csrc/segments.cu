@@ -146,26 +146,46 @@ __device__ __forceinline__ long long slice_sum_i32(const int32_t* __restrict__ i
   return acc;
 }
 
-__device__ __forceinline__ uint32_t slice_sum_u32(const uint32_t* __restrict__ in, uint64_t a, uint64_t b) {
-  const uint32_t tid = threadIdx.x, T = blockDim.x;
-  uint32_t acc = 0;
+// Scan element traits: uint32 scans wrap (bit-exact against cpu_sum_scan);
+// FP32 scans keep chunk sums and carries in FP64 and scan within a tile in
+// FP32 (the error of an element is then a few ulps of its prefix).
+template <typename T> struct ScanT;
+template <> struct ScanT<uint32_t> {
+  using Acc = uint32_t;
+  using Vec = uint4;
+  __device__ static __forceinline__ Acc vsum(uint4 x) { return (x.x + x.y) + (x.z + x.w); }
+  __device__ static __forceinline__ uint32_t out(Acc carry, uint32_t e) { return carry + e; }
+};
+template <> struct ScanT<float> {
+  using Acc = double;
+  using Vec = float4;
+  __device__ static __forceinline__ Acc vsum(float4 x) { return ((double)x.x + x.y) + ((double)x.z + x.w); }
+  __device__ static __forceinline__ float out(Acc carry, float e) { return (float)(carry + (double)e); }
+};
+
+// Sum of in[a, b) by the CTA (per thread, in the accumulation type): 16-byte
+// loads over the aligned body, four in flight per thread, kept in L2 for the
+// rescan; scalar head and tail.
+template <typename T>
+__device__ __forceinline__ typename ScanT<T>::Acc slice_sum(const T* __restrict__ in, uint64_t a, uint64_t b) {
+  using Acc = typename ScanT<T>::Acc;
+  using Vec = typename ScanT<T>::Vec;
+  const uint32_t tid = threadIdx.x, NT = blockDim.x;
+  Acc acc = 0;
   uint64_t h = a;
   while (h < b && (reinterpret_cast<uintptr_t>(in + h) & 15u)) ++h;
   const uint64_t nv = (b - h) >> 2;
   const uint64_t t0 = h + (nv << 2);
-  for (uint64_t i = a + tid; i < h; i += T) acc += __ldg(in + i);
-  const uint4* v = reinterpret_cast<const uint4*>(in + h);
+  for (uint64_t i = a + tid; i < h; i += NT) acc += (Acc)__ldg(in + i);
+  const Vec* v = reinterpret_cast<const Vec*>(in + h);
   uint64_t i = tid;
-  for (; i + 3ull * T < nv; i += 4ull * T) {
-    const uint4 x0 = __ldcg(v + i), x1 = __ldcg(v + i + T), x2 = __ldcg(v + i + 2ull * T), x3 = __ldcg(v + i + 3ull * T);
-    acc += (x0.x + x0.y) + (x0.z + x0.w) + (x1.x + x1.y) + (x1.z + x1.w);
-    acc += (x2.x + x2.y) + (x2.z + x2.w) + (x3.x + x3.y) + (x3.z + x3.w);
+  for (; i + 3ull * NT < nv; i += 4ull * NT) {
+    const Vec x0 = __ldcg(v + i), x1 = __ldcg(v + i + NT), x2 = __ldcg(v + i + 2ull * NT), x3 = __ldcg(v + i + 3ull * NT);
+    acc += ScanT<T>::vsum(x0) + ScanT<T>::vsum(x1);
+    acc += ScanT<T>::vsum(x2) + ScanT<T>::vsum(x3);
   }
-  for (; i < nv; i += T) {
-    const uint4 x = __ldcg(v + i);
-    acc += (x.x + x.y) + (x.z + x.w);
-  }
-  for (uint64_t j = t0 + tid; j < b; j += T) acc += __ldg(in + j);
+  for (; i < nv; i += NT) acc += ScanT<T>::vsum(__ldcg(v + i));
+  for (uint64_t j = t0 + tid; j < b; j += NT) acc += (Acc)__ldg(in + j);
   return acc;
 }
 
@@ -212,68 +232,71 @@ __device__ __forceinline__ uint32_t tpos(uint32_t e) { return e + (e >> 5); }
 // Exclusive scan of one tile of up to kScanV * blockDim elements starting at
 // `base` (n elements valid), offset by `carry`; returns the tile's total.  All
 // kScanV loads of a thread are issued before the first is used.
-__device__ __forceinline__ uint32_t scan_tile_u32(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
-                                                  uint64_t base, uint32_t n, uint32_t carry, uint32_t* tile,
-                                                  uint32_t* wsum) {
-  const uint32_t tid = threadIdx.x, T = blockDim.x;
-  const uint32_t lane = tid & 31u, w = tid >> 5, nw = T >> 5;
-  uint32_t x[kScanV];
+template <typename T>
+__device__ __forceinline__ typename ScanT<T>::Acc scan_tile(const T* __restrict__ in, T* __restrict__ out,
+                                                            uint64_t base, uint32_t n,
+                                                            typename ScanT<T>::Acc carry, T* tile, T* wsum) {
+  const uint32_t tid = threadIdx.x, NT = blockDim.x;
+  const uint32_t lane = tid & 31u, w = tid >> 5, nw = NT >> 5;
+  T x[kScanV];
 #pragma unroll
   for (uint32_t r = 0; r < kScanV; ++r) {
-    const uint32_t j = r * T + tid;
-    x[r] = j < n ? __ldcg(in + base + j) : 0u;
+    const uint32_t j = r * NT + tid;
+    x[r] = j < n ? __ldcg(in + base + j) : T(0);
   }
 #pragma unroll
-  for (uint32_t r = 0; r < kScanV; ++r) tile[tpos(r * T + tid)] = x[r];
+  for (uint32_t r = 0; r < kScanV; ++r) tile[tpos(r * NT + tid)] = x[r];
   __syncthreads();
-  uint32_t sum = 0;
+  T sum = 0;
 #pragma unroll
   for (uint32_t r = 0; r < kScanV; ++r) {
-    const uint32_t v = tile[tpos(kScanV * tid + r)];
+    const T v = tile[tpos(kScanV * tid + r)];
     x[r] = sum;
     sum += v;
   }
   // block exclusive scan of the per-thread sums
-  uint32_t inc = sum;
+  T inc = sum;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+    const T y = __shfl_up_sync(0xffffffffu, inc, o);
     if ((int)lane >= o) inc += y;
   }
   if (lane == 31) wsum[w] = inc;
   __syncthreads();
   if (w == 0) {
-    uint32_t v = lane < nw ? wsum[lane] : 0u;
+    T v = lane < nw ? wsum[lane] : T(0);
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, v, o);
+      const T y = __shfl_up_sync(0xffffffffu, v, o);
       if ((int)lane >= o) v += y;
     }
     wsum[lane] = v;  // inclusive warp prefix; wsum[31] = tile total
   }
   __syncthreads();
-  const uint32_t excl = carry + (w ? wsum[w - 1] : 0u) + (inc - sum);
+  const T excl = (w ? wsum[w - 1] : T(0)) + (inc - sum);
 #pragma unroll
-  for (uint32_t r = 0; r < kScanV; ++r) tile[tpos(kScanV * tid + r)] = excl + x[r];
+  for (uint32_t r = 0; r < kScanV; ++r) tile[tpos(kScanV * tid + r)] = ScanT<T>::out(carry, excl + x[r]);
   __syncthreads();
 #pragma unroll
   for (uint32_t r = 0; r < kScanV; ++r) {
-    const uint32_t j = r * T + tid;
+    const uint32_t j = r * NT + tid;
     if (j < n) __stcs(out + base + j, tile[tpos(j)]);
   }
-  const uint32_t total = wsum[31];
+  const typename ScanT<T>::Acc total = wsum[31];
   __syncthreads();  // tile and wsum are reused by the next tile
   return total;
 }
 
-template <int V>
+template <int V, typename T>
 __global__ void __launch_bounds__(1024)
-scan_segments_kernel(SegParams p, const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
-                     uint32_t* __restrict__ partials) {
+scan_segments_kernel(SegParams p, const T* __restrict__ in, T* __restrict__ out,
+                     typename ScanT<T>::Acc* __restrict__ partials) {
+  using Acc = typename ScanT<T>::Acc;
   __shared__ gsrb::BarrierShared bsh;
-  __shared__ uint32_t buf[32];
-  __shared__ uint32_t wsum[32];
-  extern __shared__ uint32_t tile[];  // tpos(kScanV * blockDim) words
+  __shared__ Acc buf[32];
+  __shared__ T wsum[32];
+  extern __shared__ __align__(16) unsigned char tile_raw[];  // tpos(kScanV * blockDim) elements
+  T* tile = reinterpret_cast<T*>(tile_raw);
   const SegTeam t = seg_team(p);
   gsrb::GridSync<V> bar;
   bool ok = bar.init(seg_barrier(p, t), &bsh);
@@ -281,7 +304,7 @@ scan_segments_kernel(SegParams p, const uint32_t* __restrict__ in, uint32_t* __r
   const uint64_t C = p.chunk, R = C * t.count;
   const uint64_t rounds = (o1 - o0 + R - 1) / R;  // the same in every CTA of the team
   const uint32_t step = kScanV * blockDim.x;
-  uint32_t base_carry = 0;
+  Acc base_carry = 0;
   auto chunk = [&](uint64_t j, uint64_t* a, uint64_t* b) {
     const uint64_t a0 = o0 + j * R + C * t.rank;
     *a = a0 < o1 ? a0 : o1;
@@ -290,7 +313,7 @@ scan_segments_kernel(SegParams p, const uint32_t* __restrict__ in, uint32_t* __r
   uint64_t a = o0, b = o0;
   if (rounds && ok) {
     chunk(0, &a, &b);
-    const uint32_t s = block_sum(slice_sum_u32(in, a, b), buf);
+    const Acc s = block_sum(slice_sum(in, a, b), buf);
     if (threadIdx.x == 0) partials[t.first + t.rank] = s;
     bar.arrive();
   }
@@ -299,28 +322,28 @@ scan_segments_kernel(SegParams p, const uint32_t* __restrict__ in, uint32_t* __r
     // round's barrier completes (a full barrier for the protocols without a
     // split form, still correct)
     uint64_t na = b, nb = b;
-    uint32_t s_next = 0;
+    Acc s_next = 0;
     if (j + 1 < rounds) {
       chunk(j + 1, &na, &nb);
-      s_next = block_sum(slice_sum_u32(in, na, nb), buf);
+      s_next = block_sum(slice_sum(in, na, nb), buf);
     }
     ok = bar.wait() && ok;
     if (!ok) break;
     // this round's sums of the team: before this CTA, and in total
-    const uint32_t* part = partials + (j & 1) * gridDim.x + t.first;
-    uint32_t pre = 0, tot = 0;
+    const Acc* part = partials + (j & 1) * gridDim.x + t.first;
+    Acc pre = 0, tot = 0;
     for (uint32_t r = threadIdx.x; r < t.count; r += blockDim.x) {
-      const uint32_t x = __ldcg(part + r);
+      const Acc x = __ldcg(part + r);
       tot += x;
       if (r < t.rank) pre += x;
     }
     pre = block_sum(pre, buf);
     tot = block_sum(tot, buf);
-    uint32_t c = base_carry + pre;
+    Acc c = base_carry + pre;
     for (uint64_t x = a; x < b; x += step) {
       const uint64_t left = b - x;
       const uint32_t n = left < step ? (uint32_t)left : step;
-      c += scan_tile_u32(in, out, x, n, c, tile, wsum);
+      c += scan_tile<T>(in, out, x, n, c, tile, wsum);
     }
     base_carry += tot;
     if (j + 1 < rounds) {
@@ -344,11 +367,12 @@ const void* reduce_segments_fn(int v) {
   }
 }
 
+template <typename T>
 const void* scan_segments_fn(int v) {
   switch (v) {
-    case gsrb::V_FLAT: return (const void*)scan_segments_kernel<gsrb::V_FLAT>;
-    case gsrb::V_FLIP: return (const void*)scan_segments_kernel<gsrb::V_FLIP>;
-    case gsrb::V_FANOUT: return (const void*)scan_segments_kernel<gsrb::V_FANOUT>;
+    case gsrb::V_FLAT: return (const void*)scan_segments_kernel<gsrb::V_FLAT, T>;
+    case gsrb::V_FLIP: return (const void*)scan_segments_kernel<gsrb::V_FLIP, T>;
+    case gsrb::V_FANOUT: return (const void*)scan_segments_kernel<gsrb::V_FANOUT, T>;
     default: return nullptr;
   }
 }
@@ -385,6 +409,29 @@ gsrb_status_t seg_setup(gsrb_ctx* ctx, const gsrb_cfg_t* cfgin, const uint64_t* 
   p->chunk = chunk;
   for (int32_t i = 0; i <= k; ++i) p->off[i] = h_off[i];
   return GSRB_OK;
+}
+
+template <typename T>
+gsrb_status_t scan_segments(gsrb_ctx* ctx, const T* d_in, T* d_out, const uint64_t* h_off, int32_t k,
+                            const gsrb_cfg_t* cfgin) {
+  if (!h_off || (k > 0 && h_off[k] > h_off[0] && (!d_in || !d_out || d_in == d_out))) return GSRB_ERR_ARG;
+  if (!ctx) return GSRB_ERR_ARG;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  gsrb_cfg_t c;
+  int grid = 0;
+  const void* fn = nullptr;
+  SegParams p;
+  gsrb_status_t st = seg_setup(ctx, cfgin, h_off, k, scan_segments_fn<T>, 4, 256, &c, &grid, &fn, &p);
+  if (st) return st;
+  using Acc = typename ScanT<T>::Acc;
+  void* part = nullptr;
+  st = scratch(ctx, sizeof(Acc) * 2 * (size_t)grid, &part);
+  if (st) return st;
+  Acc* partials = (Acc*)part;
+  const uint32_t tw = kScanV * (uint32_t)c.threads;
+  const size_t smem = sizeof(T) * (size_t)(tw + (tw >> 5));
+  void* args[] = {&p, &d_in, &d_out, &partials};
+  return launch_persistent(ctx, fn, grid, c.threads, smem, 1, coop_of(c), args);
 }
 
 }  // namespace
@@ -424,23 +471,12 @@ gsrb_status_t gsrb_reduce_i32_segments(gsrb_ctx_t ctx, const int32_t* d_in, cons
 
 gsrb_status_t gsrb_scan_u32_segments(gsrb_ctx_t ctx, const uint32_t* d_in, uint32_t* d_out, const uint64_t* h_off,
                                      int32_t k, const gsrb_cfg_t* cfgin) {
-  if (!h_off || (k > 0 && h_off[k] > h_off[0] && (!d_in || !d_out || d_in == d_out))) return GSRB_ERR_ARG;
-  if (!ctx) return GSRB_ERR_ARG;
-  std::lock_guard<std::mutex> g(ctx->mu);
-  gsrb_cfg_t c;
-  int grid = 0;
-  const void* fn = nullptr;
-  SegParams p;
-  gsrb_status_t st = seg_setup(ctx, cfgin, h_off, k, scan_segments_fn, 4, 256, &c, &grid, &fn, &p);
-  if (st) return st;
-  void* part = nullptr;
-  st = scratch(ctx, sizeof(uint32_t) * 2 * (size_t)grid, &part);
-  if (st) return st;
-  uint32_t* partials = (uint32_t*)part;
-  const uint32_t tw = kScanV * (uint32_t)c.threads;
-  const size_t smem = sizeof(uint32_t) * (size_t)(tw + (tw >> 5));
-  void* args[] = {&p, &d_in, &d_out, &partials};
-  return launch_persistent(ctx, fn, grid, c.threads, smem, 1, coop_of(c), args);
+  return scan_segments<uint32_t>(ctx, d_in, d_out, h_off, k, cfgin);
+}
+
+gsrb_status_t gsrb_scan_f32_segments(gsrb_ctx_t ctx, const float* d_in, float* d_out, const uint64_t* h_off,
+                                     int32_t k, const gsrb_cfg_t* cfgin) {
+  return scan_segments<float>(ctx, d_in, d_out, h_off, k, cfgin);
 }
 
 }  // extern "C"

@@ -151,6 +151,7 @@ _SIGS = {
     "gsrb_scan_f32": (C.c_int32, [_P, _P, _P, C.c_size_t, C.POINTER(Cfg)]),
     "gsrb_reduce_i32_segments": (C.c_int32, [_P, _P, _P, C.c_int32, _P, C.POINTER(Cfg)]),
     "gsrb_scan_u32_segments": (C.c_int32, [_P, _P, _P, _P, C.c_int32, C.POINTER(Cfg)]),
+    "gsrb_scan_f32_segments": (C.c_int32, [_P, _P, _P, _P, C.c_int32, C.POINTER(Cfg)]),
     "gsrb_segments_layout": (C.c_int32, [_P, C.c_int32, C.c_int32, _P, _P]),
     "gsrb_semaphore_bench": (C.c_int32, [_P, C.POINTER(Cfg), C.c_int32, C.c_uint32, C.c_int32, C.c_int32,
                                          C.c_int32, _P]),
@@ -413,10 +414,13 @@ class Context:
                                                C.byref(c) if c is not None else None)
 
     def scan_u32_segments(self, d_in: DeviceArray, d_out: DeviceArray, offsets, c: Cfg | None = None) -> int:
-        """Exclusive uint32 prefix sums within each segment, one launch."""
+        """Exclusive prefix sums within each segment, one launch (uint32, or
+        FP32 when d_in is float32)."""
         off = np.ascontiguousarray(offsets, dtype=np.uint64)
-        return _lib().gsrb_scan_u32_segments(self.h, d_in.ptr, d_out.ptr, off.ctypes.data, len(off) - 1,
-                                             C.byref(c) if c is not None else None)
+        fn = _lib().gsrb_scan_f32_segments if d_in.dtype == np.float32 else _lib().gsrb_scan_u32_segments
+        return fn(self.h, d_in.ptr, d_out.ptr, off.ctypes.data, len(off) - 1, C.byref(c) if c is not None else None)
+
+    scan_segments = scan_u32_segments
 
     # -- locks ------------------------------------------------------------------
     def semaphore_bench(self, c: Cfg, kind: int, capacity: int, writer_every: int, iters: int, incs: int,
