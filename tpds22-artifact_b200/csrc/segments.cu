@@ -16,7 +16,8 @@
 //           the partial, arrives on the segment's barrier; the combiner (the
 //           completing CTA for the fan-out protocol, else the segment's first
 //           CTA after a wait) adds the segment's partials in CTA order.
-//   scan    (exclusive, uint32) in rounds, so that the re-read comes from L2:
+//   scan    (exclusive; uint32 wrapping, or FP32 with FP64 chunk sums and
+//           carries) in rounds, so that the re-read comes from L2:
 //           in round j the team's CTAs take consecutive chunks of `chunk`
 //           elements (CTA r the r-th); chunk sums -> segment barrier -> every
 //           CTA adds the round's sums of the CTAs before it to the running
