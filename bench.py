@@ -38,6 +38,7 @@ import importlib.util
 import json
 import os
 import pathlib
+import re
 import statistics
 import subprocess
 import sys
@@ -78,6 +79,26 @@ def hbm_peak():
         return float(json.loads(PEAKS.read_text())["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
     except Exception:
         return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
+
+
+def wall(fn):
+    """(seconds, result) of one call: the CPU-baseline leg's clock."""
+    t0 = time.perf_counter()
+    r = fn()
+    return time.perf_counter() - t0, r
+
+
+def cpu_info():
+    """Host CPU model and logical core count (recorded with every CPU baseline)."""
+    model = "unknown"
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"cpu_model": model, "nproc": os.cpu_count() or 1}
 
 
 # ---------------------------------------------------------------- distributed
@@ -291,7 +312,7 @@ def semaphore_numbers(gsrb, ctx):
 
 
 # --------------------------------------------------------------- data kernels
-def reduce_numbers(gsrb, ctx, orc, tune, cache, reps=10, fixed=None, n=1 << 24):
+def reduce_numbers(gsrb, ctx, orc, tune, cache, reps=10, fixed=None, n=1 << 24, cpu=False):
     a = gsrb.uniform_i32(SEED, n, 0, 127)
     d = ctx.to_device(a)
     out = ctx.array(1, np.int64).zero()
@@ -312,11 +333,19 @@ def reduce_numbers(gsrb, ctx, orc, tune, cache, reps=10, fixed=None, n=1 << 24):
     peak, src = hbm_peak()
     gbs = 4 * n / (t * 1e-3) / 1e9
     d.free()
-    return {"n": n, "ms": round(t, 5), "GB_s": round(gbs, 1), "hbm_frac": round(gbs / peak, 4),
-            "peak_source": src, "bit_exact": ok, "cold_l2": True, "cfg": best}
+    res = {"n": n, "ms": round(t, 5), "GB_s": round(gbs, 1), "hbm_frac": round(gbs / peak, 4),
+           "peak_source": src, "bit_exact": ok, "cold_l2": True, "cfg": best}
+    if cpu:
+        thr = os.cpu_count() or 1
+        t1 = statistics.median(wall(lambda: orc.sum_i32(a))[0] for _ in range(5))
+        tm = statistics.median(wall(lambda: orc.sum_i32(a, threads=thr))[0] for _ in range(5))
+        res["cpu"] = {"kind": "port", "serial_ms": round(t1 * 1e3, 3), "serial_GB_s": round(4 * n / t1 / 1e9, 2),
+                      "mt_ms": round(tm * 1e3, 3), "mt_GB_s": round(4 * n / tm / 1e9, 2), "threads": thr,
+                      "sample": f"the same {n} int32, int64 sum, median of 5", **cpu_info()}
+    return res
 
 
-def scan_numbers(gsrb, ctx, orc, tune, cache, n=1 << 28, reps=5, fixed=None):
+def scan_numbers(gsrb, ctx, orc, tune, cache, n=1 << 28, reps=5, fixed=None, cpu=False):
     peak, src = hbm_peak()
     res = {"n": n, "peak_source": src}
     a = gsrb.uniform_i32(SEED, n, 0, 15).astype(np.uint32)
@@ -342,8 +371,22 @@ def scan_numbers(gsrb, ctx, orc, tune, cache, n=1 << 28, reps=5, fixed=None):
         ctx.check_status("scan")
         got = dout.download()
         if kind == "u32":
-            ok = bool(np.array_equal(got, orc.scan_u32(a, threads=os.cpu_count() or 1)))
+            thr = os.cpu_count() or 1
+            t_mt, want = wall(lambda: orc.scan_u32(a, threads=thr))
+            ok = bool(np.array_equal(got, want))
             check = {"bit_exact": ok}
+            if cpu:
+                t_ref, ref_out = wall(lambda: orc.ref_cpu_sum_scan(a))
+                res["cpu"] = {"kind": "reference" if ref_out is not None else "port",
+                              "serial_ms": round(t_ref * 1e3, 1) if ref_out is not None else None,
+                              "serial_GB_s": round(8 * n / t_ref / 1e9, 2) if ref_out is not None else None,
+                              "serial_matches": bool(np.array_equal(ref_out, want)) if ref_out is not None else None,
+                              "mt_ms": round(t_mt * 1e3, 1), "mt_GB_s": round(8 * n / t_mt / 1e9, 2), "threads": thr,
+                              "sample": f"the same {n} uint32: the reference's cpu_sum_scan (scan/main.cu:11-21, "
+                                        f"oracle/_ref) on one core; the two-pass blocked scan on all cores",
+                              **cpu_info()}
+                del ref_out
+            del want
         else:
             ref = orc.scan_f32_f64(a)
             err = orc.max_rel_err(got[1:], ref[1:])
@@ -388,11 +431,19 @@ def train_policy(gsrb, ctx, pol):
                                       "n_m_ms0_ms1": launch}}
 
 
-def bfs_runs(gsrb, ctx, orc, dg, g, params, cfg, reps=3, launch=None):
+def bfs_runs(gsrb, ctx, orc, dg, g, params, cfg, reps=3, launch=None, cpu=False):
     out = ctx.array(g.nnodes, np.int32)
-    want = orc.bfs(g, 0)
+    t_cpu, want = wall(lambda: orc.bfs(g, 0))
     m_trav = orc.traversed_edges(g, want)
     res = {"m_traversed": m_trav}
+    if cpu:
+        thr = os.cpu_count() or 1
+        t_mt, got = wall(lambda: orc.bfs(g, 0, threads=thr))
+        res["cpu"] = {"kind": "port", "serial_ms": round(t_cpu * 1e3, 2),
+                      "serial_GTEPS": round(m_trav / t_cpu / 1e9, 4), "mt_ms": round(t_mt * 1e3, 2),
+                      "mt_GTEPS": round(m_trav / t_mt / 1e9, 4), "mt_matches": bool(np.array_equal(got, want)),
+                      "threads": thr, "sample": "one whole BFS from vertex 0: queue BFS on one core, "
+                                                "level-synchronous BFS on all cores"}
     dg.set_policy(params)
     for name, mode in (("plain_push", gsrb.BFS_PUSH), ("push_load_balanced", gsrb.BFS_PUSH | gsrb.BFS_FLAG_LB),
                        ("heuristic", gsrb.BFS_HEURISTIC), ("learned", gsrb.BFS_LEARNED)):
@@ -445,9 +496,13 @@ def bfs_runs(gsrb, ctx, orc, dg, g, params, cfg, reps=3, launch=None):
 
 def sssp_runs(gsrb, ctx, orc, dg, g, deltas, cfg, verify=True):
     out = ctx.array(g.nnodes, np.int32)
-    want = orc.dijkstra(g, 0) if verify else None
+    t_cpu, want = wall(lambda: orc.dijkstra(g, 0)) if verify else (None, None)
     m_trav = orc.traversed_edges(g, want) if verify else g.nedges
     res = {}
+    if verify:
+        res["cpu"] = {"kind": "port", "serial_ms": round(t_cpu * 1e3, 2),
+                      "serial_GTEPS": round(m_trav / t_cpu / 1e9, 4), "threads": 1,
+                      "sample": "one whole binary-heap Dijkstra from vertex 0 on one core"}
     for name, delta in deltas:
         rc, st = dg.sssp(0, out, delta, cfg)
         gsrb.check(rc, "sssp")
@@ -460,7 +515,7 @@ def sssp_runs(gsrb, ctx, orc, dg, g, deltas, cfg, verify=True):
     return res
 
 
-def graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, verify_pr=True):
+def graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, verify_pr=True, ref_gpu=True):
     res = {}
     t0 = time.time()
     rm = gsrb.rmat(22, 16, a=0.57, b=0.19, c=0.19, seed=SEED, wlo=1, whi=255)
@@ -470,7 +525,7 @@ def graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, verify_pr=True):
     best, _, _ = tune.tune_bfs(ctx, dg, 0, gsrb.BFS_HEURISTIC, reps=1)
     cache["bfs_rmat"] = best
     cfg = tune.cfg_from(best)
-    res["rmat22"]["bfs"] = bfs_runs(gsrb, ctx, orc, dg, rm, params, cfg, launch=pol.launch_candidates())
+    res["rmat22"]["bfs"] = bfs_runs(gsrb, ctx, orc, dg, rm, params, cfg, launch=pol.launch_candidates(), cpu=True)
     res["rmat22"]["sssp"] = sssp_runs(gsrb, ctx, orc, dg, rm, [("reference_delta", 10000), ("delta_256", 256)], cfg)
     out = ctx.array(rm.nnodes, np.float32)
     rc, st = dg.pagerank(out, 0.85, 50, cfg)
@@ -479,10 +534,19 @@ def graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, verify_pr=True):
     gsrb.check(rc, "pagerank")
     per_iter_bytes = 4 * (rm.nnodes + 1) + 4 * rm.nedges + 8 * rm.nnodes
     l1 = orc.normalized_l1(out.download(), orc.pagerank(rm, 0.85, 50)) if verify_pr else None
+    thr = os.cpu_count() or 1
+    t_pr1 = wall(lambda: orc.pagerank(rm, 0.85, 5))[0] / 5
+    t_prm = wall(lambda: orc.pagerank(rm, 0.85, 5, threads=thr))[0] / 5
+    pr_cpu = {"kind": "port", "serial_ms_per_iter": round(t_pr1 * 1e3, 2),
+              "serial_edges_per_s": round(rm.nedges / t_pr1, 1), "mt_ms_per_iter": round(t_prm * 1e3, 2),
+              "mt_edges_per_s": round(rm.nedges / t_prm, 1), "threads": thr,
+              "sample": "5 of the 50 FP64 pull iterations, per-iteration time"}
     res["rmat22"]["pagerank"] = {"iters": 50, "ms": round(st.kernel_ms, 3),
                                  "edges_per_s": round(50 * rm.nedges / (st.kernel_ms * 1e-3), 1),
                                  "GB_s_algorithmic": round(50 * per_iter_bytes / (st.kernel_ms * 1e-3) / 1e9, 1),
-                                 "l1_vs_fp64": l1, "within_1e-6": (l1 <= 1e-6) if l1 is not None else None}
+                                 "hbm_frac": round(50 * per_iter_bytes / (st.kernel_ms * 1e-3) / 1e9 / hbm_peak()[0], 4),
+                                 "l1_vs_fp64": l1, "within_1e-6": (l1 <= 1e-6) if l1 is not None else None,
+                                 "cpu": pr_cpu}
     # the reference's push-residual algorithm (epsilon 1e-6, run to empty
     # worklist), checked against the pull form run to convergence (200 iterations)
     conv = ctx.array(rm.nnodes, np.float32)
@@ -496,6 +560,8 @@ def graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, verify_pr=True):
                                           "l1_vs_converged_pull": orc.normalized_l1(outr.download(),
                                                                                     conv.download().astype(np.float64))}
     dg.free()
+    if ref_gpu:
+        res["rmat22"]["reference_gpu"] = lonestar_reference(rm)
     del rm
     gr = gsrb.grid2d(2048, 2048, seed=SEED, wlo=1, whi=1000)
     dg = ctx.graph(gr)
@@ -503,10 +569,13 @@ def graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, verify_pr=True):
     cache["bfs_grid"] = best
     cfg = tune.cfg_from(best)
     res["grid2048"] = {"n": gr.nnodes, "m": gr.nedges,
-                       "bfs": bfs_runs(gsrb, ctx, orc, dg, gr, params, cfg, reps=2, launch=pol.launch_candidates())}
+                       "bfs": bfs_runs(gsrb, ctx, orc, dg, gr, params, cfg, reps=2, launch=pol.launch_candidates(),
+                                       cpu=True)}
     res["grid2048"]["sssp"] = sssp_runs(gsrb, ctx, orc, dg, gr, [("reference_delta", 10000), ("delta_4096", 4096)],
                                         cfg)
     dg.free()
+    if ref_gpu:
+        res["grid2048"]["reference_gpu"] = lonestar_reference(gr)
     return res
 
 
@@ -615,10 +684,28 @@ def batch_numbers(gsrb, ctx, orc, params):
     for dg in dgs:
         dg.set_policy(params)
     outs = [ctx.array(g.nnodes, np.int32) for g in graphs]
-    wants = [orc.bfs(g, 0) for g in graphs]
+    t_cpu_bfs, wants = wall(lambda: [orc.bfs(g, 0) for g in graphs])
     m_total = sum(orc.traversed_edges(g, w) for g, w in zip(graphs, wants))
+    thr = os.cpu_count() or 1
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(thr) as ex:  # the oracle's C code runs without the GIL
+        t_mt_bfs, got = wall(lambda: list(ex.map(lambda g: orc.bfs(g, 0), graphs)))
+        mt_ok = all(np.array_equal(a, b) for a, b in zip(got, wants))
+        t_cpu_dij, wants_d = wall(lambda: [orc.dijkstra(g, 0) for g in graphs])
+        t_mt_dij, got = wall(lambda: list(ex.map(lambda g: orc.dijkstra(g, 0), graphs)))
+        mt_ok = mt_ok and all(np.array_equal(a, b) for a, b in zip(got, wants_d))
+    del got
     res = {"graphs": 64, "scales": [int(s) for s in scales], "m_total": int(sum(g.nedges for g in graphs)),
            "m_traversed": int(m_total), "gen_s": round(gen_s, 1)}
+    res["cpu"] = {"kind": "port", "bfs_serial_ms": round(t_cpu_bfs * 1e3, 1),
+                  "bfs_serial_GTEPS": round(m_total / t_cpu_bfs / 1e9, 4),
+                  "bfs_mt_ms": round(t_mt_bfs * 1e3, 1), "bfs_mt_GTEPS": round(m_total / t_mt_bfs / 1e9, 4),
+                  "sssp_serial_ms": round(t_cpu_dij * 1e3, 1),
+                  "sssp_serial_GTEPS": round(m_total / t_cpu_dij / 1e9, 4),
+                  "sssp_mt_ms": round(t_mt_dij * 1e3, 1), "sssp_mt_GTEPS": round(m_total / t_mt_dij / 1e9, 4),
+                  "mt_matches": mt_ok, "threads": thr,
+                  "sample": "all 64 graphs from vertex 0: queue BFS / binary-heap Dijkstra, one graph after "
+                            "another on one core, and one graph per host thread on all cores"}
     # plain: the reference algorithm (worklist push), one whole-grid launch per graph
     plain_cfg = gsrb.cfg(variant=gsrb.BAR_SOFT2, ctas_per_sm=2, threads=256)
     for rep in range(2):
@@ -646,16 +733,34 @@ def batch_numbers(gsrb, ctx, orc, params):
     gsrb.check(rc, "batch stats")
     ok_batch = all(np.array_equal(o.download(), w) for o, w in zip(outs, wants))
     t_batch = statistics.median(ts)
+    # the same batched launch with the fixed direction heuristic instead of the network
+    cgh = gsrb.CudaGraph(ctx)
+    with cgh:
+        gsrb.check(b.bfs([0] * 64, outs, gsrb.BFS_HEURISTIC), "batch bfs heuristic")
+    for o in outs:
+        o.zero()
+    tsh = []
+    for rep in range(3):
+        ctx.record(10)
+        cgh.launch()
+        ctx.record(11)
+        tsh.append(ctx.elapsed_ms(10, 11))
+    ok_heur = all(np.array_equal(o.download(), w) for o, w in zip(outs, wants))
+    t_heur = statistics.median(tsh)
+    cgh.free()
     res["bfs"] = {"plain_ms": round(t_plain, 3), "plain_GTEPS": round(m_total / (t_plain * 1e-3) / 1e9, 3),
                   "plain_bit_exact": ok_plain, "batched_learned_ms": round(t_batch, 3),
                   "batched_learned_GTEPS": round(m_total / (t_batch * 1e-3) / 1e9, 3),
                   "batched_learned_bit_exact": ok_batch, "speedup": round(t_plain / t_batch, 3),
+                  "batched_heuristic_ms": round(t_heur, 3),
+                  "batched_heuristic_GTEPS": round(m_total / (t_heur * 1e-3) / 1e9, 3),
+                  "batched_heuristic_bit_exact": ok_heur,
+                  "learned_vs_heuristic": round(t_heur / t_batch, 3),
                   "policy_decisions": int(sum(s.decisions for s in st)),
                   "fallbacks": int(sum(1 for s in st if s.aux))}
     cg.free()
     # SSSP: plain = one launch per graph with the reference's DELTA (10000);
     # batched = one launch with a tuned bucket width
-    wants_d = [orc.dijkstra(g, 0) for g in graphs]
     for rep in range(2):
         ctx.record(8)
         for dg, o in zip(dgs, outs):
@@ -684,6 +789,137 @@ def batch_numbers(gsrb, ctx, orc, params):
     return res
 
 
+# ------------------------------------------------- the reference's GPU programs
+REF_BIN = ROOT / "baseline" / "_ref"
+_TIME_RE = [re.compile(r"average:\s*([0-9.eE+-]+)\s*ms"), re.compile(r"time \(ms\) is\s*([0-9.eE+-]+)"),
+            re.compile(r"(?i)kernel time \(ms\)(?: is)?\s*([0-9.eE+-]+)"),
+            re.compile(r"time cuda only\(ms\)\s*([0-9.eE+-]+)")]
+
+
+def _ref_run(prog, args, stdin=None, timeout=180):
+    """Runs one of the reference's own programs (recompiled for sm_100a) and
+    returns (time in ms it printed, stdout).  Only co-resident shapes are
+    passed: the GSRB forms spin without a bound."""
+    p = subprocess.run([str(REF_BIN / prog)] + [str(a) for a in args], input=stdin, capture_output=True,
+                       text=True, timeout=timeout)
+    if p.returncode != 0:
+        raise RuntimeError(f"{prog} rc {p.returncode}: {(p.stdout + p.stderr)[-300:]}")
+    for rx in _TIME_RE:
+        m = rx.search(p.stdout)
+        if m:
+            return float(m.group(1)), p.stdout
+    raise RuntimeError(f"{prog}: no time in output")
+
+
+def reference_gpu_numbers(gsrb, ctx):
+    """The reference's own GPU programs (baseline/_ref, built from the
+    reference sources for sm_100a by baseline/build.sh) timed on this GPU in
+    the same run, beside this library on the same shapes.  Every shape is
+    co-resident: Heterosync runs 148*k CTAs of 32 threads (k <= 8, the
+    reference's own MAX_BLOCKS check allows 32 per SM), the reduce and scan run
+    at N where one element per thread needs <= 8 CTAs per SM, the Lonestar
+    programs get block factor 2 (296 CTAs of 32 threads)."""
+    if not (REF_BIN / "allSyncPrims-1kernel").exists():
+        return {"unavailable": "baseline/_ref not built (needs the reference sources)"}
+    out = {"programs": "baseline/_ref, the reference's sources compiled for sm_100a"}
+    iters = 10000
+    # Heterosync barriers: one barrier per iteration, NUM_LDST = 1, 10 launches averaged
+    het = []
+    for k in (1, 8):
+        ntb = 148 * k
+        row = {"ctas": ntb, "threads": 32, "iterations": iters}
+        for name, prim in (("gsrb", "atomicTreeBarrUniqSRB"), ("gcpusrb", "atomicTreeBarrUniqNaiveSRB"),
+                           ("ccg", "atomicTreeBarrUniqCCG"), ("atomic_tree", "atomicTreeBarrUniq")):
+            try:
+                ms, _ = _ref_run("allSyncPrims-1kernel", [prim, 1, ntb, iters])
+                row[name + "_ns"] = round(ms * 1e6 / iters, 1)
+            except Exception as e:  # noqa: BLE001
+                row[name + "_ns"] = f"failed: {str(e)[:120]}"
+        # this library on the same shape (32-thread CTAs, F = 0), its own protocols
+        for name, v in (("native_fanout", gsrb.BAR_FANOUT), ("native_flip", gsrb.BAR_FLIP)):
+            c = gsrb.cfg(variant=v, ctas_per_sm=k, threads=32, wake_lines=2)
+            none = gsrb.cfg(variant=gsrb.BAR_NONE, ctas_per_sm=k, threads=32)
+            t0 = statistics.median(time_barrier(gsrb, ctx, none, 2000, 0, 3, 1))
+            t1 = statistics.median(time_barrier(gsrb, ctx, c, 2000, 0, 3, 1))
+            row[name + "_ns"] = round((t1 - t0) * 1e6 / 2000, 1)
+        het.append(row)
+    out["heterosync_barrier"] = het
+    # reduce: one element per thread, 256 threads per CTA
+    red = []
+    for n in (37_888, 303_104):
+        row = {"n": n}
+        for v in ("gsrb", "ccg"):
+            try:
+                ms, so = _ref_run(f"reduce_{v}", [n, 256])
+                row[v + "_ms"] = ms
+                row[v + "_correct"] = f"Sum: {n}\n" in so
+            except Exception as e:  # noqa: BLE001
+                row[v + "_ms"] = f"failed: {str(e)[:120]}"
+        a = np.ones(n, np.int32)
+        d = ctx.to_device(a)
+        o = ctx.array(1, np.int64).zero()
+        ts = []
+        for i in range(8):
+            ctx.record(4)
+            gsrb.check(ctx.reduce_i32(d, n, o))
+            ctx.record(5)
+            if i >= 3:
+                ts.append(ctx.elapsed_ms(4, 5))
+        row["native_ms"] = round(statistics.median(ts), 5)
+        row["native_correct"] = int(o.download()[0]) == n
+        d.free()
+        o.free()
+        red.append(row)
+    out["reduce"] = red
+    # scan: 64-element tiles of 32-thread CTAs
+    scn = []
+    for n in (9_472, 151_552):
+        row = {"n": n}
+        for v in ("gsrb", "ccg"):
+            try:
+                ms, so = _ref_run(f"scan_{v}", [n])
+                row[v + "_ms"] = ms
+                row[v + "_match"] = "Match: 1" in so
+            except Exception as e:  # noqa: BLE001
+                row[v + "_ms"] = f"failed: {str(e)[:120]}"
+        a = np.ones(n, np.uint32)
+        d, o = ctx.to_device(a), ctx.array(n, np.uint32)
+        ts = []
+        for i in range(8):
+            ctx.record(4)
+            gsrb.check(ctx.scan(d, o, n))
+            ctx.record(5)
+            if i >= 3:
+                ts.append(ctx.elapsed_ms(4, 5))
+        row["native_ms"] = round(statistics.median(ts), 5)
+        row["native_match"] = bool(np.array_equal(o.download(), np.arange(n, dtype=np.uint32)))
+        d.free()
+        o.free()
+        scn.append(row)
+    out["scan"] = scn
+    return out
+
+
+def lonestar_reference(g, timeout=600):
+    """The reference's Lonestar BFS and SSSP (gsrb and ccg builds) on graph g
+    written as .gr v1: the "Kernel time (ms)" each prints, block factor 2 (296
+    CTAs of 32 threads, within the wrapper's own residency cap)."""
+    if not (REF_BIN / "lonestar" / "bfs_gsrb").exists():
+        return {"unavailable": "baseline/_ref not built (needs the reference sources)"}
+    row = {"block_factor": 2}
+    with tempfile.TemporaryDirectory() as td:
+        path = pathlib.Path(td) / "g.gr"
+        g.write_gr(path, with_weights=True)
+        for app, extra in (("bfs", ["-s", 0]), ("sssp", ["-s", 0, "-d", 10000])):
+            for v in ("gsrb", "ccg"):
+                try:
+                    ms, _ = _ref_run(f"lonestar/{app}_{v}", extra + ["-q", path], stdin="2\n", timeout=timeout)
+                    row[f"{app}_{v}_ms"] = ms
+                except Exception as e:  # noqa: BLE001
+                    row[f"{app}_{v}_ms"] = f"failed: {str(e)[:120]}"
+    return row
+
+
 def cpu_barrier_baseline(orc, nctas, seconds=8.0):
     """The reference's two-level sense-reversing barrier restated on the host
     cores, with the same participants as the GPU workload: `nctas` CTAs in
@@ -697,6 +933,116 @@ def cpu_barrier_baseline(orc, nctas, seconds=8.0):
     return {"value": round(ns, 2), "unit": "ns per barrier", "cores": threads, "kind": "port",
             "sample": f"{nctas} CTAs (the GPU workload's) carried by {threads} host threads, one per core, "
                       f"{groups} groups, {2 * episodes} barrier episodes, F=0, stale reads {stale}"}
+
+
+# --------------------------------------------------------------- the summary
+def _get(d, *keys):
+    for k in keys:
+        if not isinstance(d, dict) or k not in d:
+            return None
+        d = d[k]
+    return d
+
+
+def summarize(detail, peak):
+    """One compact entry per benchmark configuration for the JSON line (the
+    full tables go to the detail file): time, throughput, roofline fraction of
+    measured HBM where the kernel is HBM-bound, correctness, and the CPU
+    baseline of the same workload."""
+    out = {}
+    bt = detail.get("barrier_table") or []
+    out["C2_barrier_k8"] = {f"F{r['F']}": {"native_ns": r.get("native"), "ccg_ns": r.get("ccg"),
+                                           "x_ccg": r.get("speedup_vs_ccg"), "variant": r.get("tuned")}
+                            for r in bt if r.get("k") == 8}
+    rg = detail.get("reference_gpu") or {}
+    if "heterosync_barrier" in rg:
+        out["C2_barrier_reference_programs"] = {f"k{r['ctas'] // 148}": {k: v for k, v in r.items() if k.endswith("_ns")}
+                                                for r in rg["heterosync_barrier"]}
+    sem = detail.get("semaphore") or []
+    out["C2_semaphore"] = {f"S{r['S']}": {"acq_per_s": _get(r, "native_priority", "acquires_per_s"),
+                                          "ref_protocol_acq_per_s": _get(r, "ref_priority", "acquires_per_s"),
+                                          "exact": _get(r, "native_priority", "exact")} for r in sem}
+    r = detail.get("reduce_2e24") or {}
+    out["C1_reduce_2e24"] = {"us": round(r["ms"] * 1e3, 2) if "ms" in r else None, "GB_s": r.get("GB_s"),
+                             "hbm_frac": r.get("hbm_frac"), "bit_exact": r.get("bit_exact"),
+                             "variant": _get(r, "cfg", "variant"),
+                             "cpu_serial_GB_s": _get(r, "cpu", "serial_GB_s"), "cpu_mt_GB_s": _get(r, "cpu", "mt_GB_s")}
+    if "reduce" in rg:
+        out["C1_reduce_reference_programs"] = rg["reduce"]
+    sc = detail.get("scan_2e28") or {}
+    out["C3_scan_2e28"] = {"u32_ms": _get(sc, "u32", "ms"), "u32_hbm_frac": _get(sc, "u32", "hbm_frac"),
+                           "u32_bit_exact": _get(sc, "u32", "bit_exact"), "f32_ms": _get(sc, "f32", "ms"),
+                           "f32_hbm_frac": _get(sc, "f32", "hbm_frac"), "f32_max_rel_err": _get(sc, "f32", "max_rel_err"),
+                           "cpu_ref_serial_GB_s": _get(sc, "cpu", "serial_GB_s"), "cpu_mt_GB_s": _get(sc, "cpu", "mt_GB_s")}
+    if "scan" in rg:
+        out["C3_scan_reference_programs"] = rg["scan"]
+    gr = detail.get("graphs") or {}
+    for key, name in (("rmat22", "C4_rmat22"), ("grid2048", "C4_grid2048")):
+        g = gr.get(key) or {}
+        b = g.get("bfs") or {}
+        n, m = g.get("n"), g.get("m")
+        e = {"n": n, "m": m}
+        for arm in ("plain_push", "heuristic", "learned"):
+            e[f"bfs_{arm}_ms"] = _get(b, arm, "ms")
+            e[f"bfs_{arm}_GTEPS"] = _get(b, arm, "GTEPS")
+        if _get(b, "heuristic", "ms") and _get(b, "learned", "ms"):
+            e["bfs_learned_vs_heuristic"] = round(b["heuristic"]["ms"] / b["learned"]["ms"], 3)
+            e["bfs_learned_vs_plain"] = round(b["plain_push"]["ms"] / b["learned"]["ms"], 3)
+        if n and m and _get(b, "heuristic", "ms"):
+            # one traversal's algorithmic bytes: row offsets, edges, level writes
+            byts = 4 * (n + 1) + 4 * m + 4 * n
+            e["bfs_heuristic_hbm_frac"] = round(byts / (b["heuristic"]["ms"] * 1e-3) / 1e9 / peak, 4)
+        e["bfs_bit_exact"] = all(_get(b, a, "bit_exact") for a in ("plain_push", "heuristic", "learned"))
+        ss = g.get("sssp") or {}
+        first = next((v for k, v in ss.items() if k != "cpu"), {})
+        e["sssp_ms"], e["sssp_GTEPS"], e["sssp_bit_exact"] = first.get("ms"), first.get("GTEPS"), first.get("bit_exact")
+        pr = g.get("pagerank") or {}
+        if pr:
+            e["pr50_ms"], e["pr_hbm_frac"], e["pr_l1"] = pr.get("ms"), pr.get("hbm_frac"), pr.get("l1_vs_fp64")
+        e["cpu_bfs_serial_GTEPS"] = _get(b, "cpu", "serial_GTEPS")
+        e["cpu_bfs_mt_GTEPS"] = _get(b, "cpu", "mt_GTEPS")
+        e["cpu_sssp_serial_GTEPS"] = _get(ss, "cpu", "serial_GTEPS")
+        if pr:
+            e["cpu_pr_serial_ms_per_iter"] = _get(pr, "cpu", "serial_ms_per_iter")
+            e["cpu_pr_mt_ms_per_iter"] = _get(pr, "cpu", "mt_ms_per_iter")
+        ref = g.get("reference_gpu")
+        if ref:
+            e["reference_programs_ms"] = ref
+        out[name] = e
+    bb = detail.get("batch") or {}
+    out["C5_batch64"] = {"bfs_plain_GTEPS": _get(bb, "bfs", "plain_GTEPS"),
+                         "bfs_batched_heuristic_GTEPS": _get(bb, "bfs", "batched_heuristic_GTEPS"),
+                         "bfs_batched_learned_GTEPS": _get(bb, "bfs", "batched_learned_GTEPS"),
+                         "bfs_learned_vs_plain": _get(bb, "bfs", "speedup"),
+                         "bfs_learned_vs_heuristic": _get(bb, "bfs", "learned_vs_heuristic"),
+                         "sssp_plain_GTEPS": _get(bb, "sssp", "plain_GTEPS"),
+                         "sssp_batched_GTEPS": _get(bb, "sssp", "batched_GTEPS"),
+                         "sssp_speedup": _get(bb, "sssp", "speedup"),
+                         "bit_exact": all(_get(bb, *k) for k in (("bfs", "plain_bit_exact"),
+                                                                 ("bfs", "batched_learned_bit_exact"),
+                                                                 ("bfs", "batched_heuristic_bit_exact"),
+                                                                 ("sssp", "batched_bit_exact"))),
+                         "cpu_bfs_mt_GTEPS": _get(bb, "cpu", "bfs_mt_GTEPS"),
+                         "cpu_sssp_mt_GTEPS": _get(bb, "cpu", "sssp_mt_GTEPS")}
+    sg = detail.get("segments") or {}
+    out["C5_segments64"] = {"reduce_hbm_frac": _get(sg, "reduce", "batched_hbm_frac"),
+                            "reduce_x_per_segment": _get(sg, "reduce", "speedup_vs_per_segment_graph"),
+                            "scan_hbm_frac": _get(sg, "scan", "batched_hbm_frac"),
+                            "scan_x_per_segment": _get(sg, "scan", "speedup_vs_per_segment_graph"),
+                            "bit_exact": bool(_get(sg, "reduce", "bit_exact") and _get(sg, "scan", "bit_exact"))}
+    pol = detail.get("policy") or {}
+    out["policy"] = {k: pol.get(k) for k in ("levels", "train_s", "loss_first", "loss_last") if k in pol}
+    return out
+
+
+def profile_traffic(name):
+    """DRAM bytes per launch recorded in a kept ncu summary (profiles/<name>.md,
+    the line 'traffic_bytes_per_launch: N'), or None."""
+    try:
+        m = re.search(r"traffic_bytes_per_launch:\s*([0-9]+)", (ROOT / "profiles" / f"{name}.md").read_text())
+        return int(m.group(1)) if m else None
+    except OSError:
+        return None
 
 
 # ----------------------------------------------------------------------- main
@@ -721,6 +1067,10 @@ def main():
     ap.add_argument("--reduce-n", type=int, default=1 << 24)
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--skip-pr-check", action="store_true", help="skip the FP64 CPU PageRank (about 25 s)")
+    ap.add_argument("--no-reference-programs", action="store_true",
+                    help="do not time the reference's own GPU programs (baseline/_ref)")
+    ap.add_argument("--detail", default=str(ROOT / "gpurun_out" / "bench_detail.json"),
+                    help="where the full tables go (the JSON line keeps one summary per configuration)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -735,7 +1085,9 @@ def main():
         if dist.rank == 0:
             orc = load_oracle()
             t0 = time.time()
-            samples = [cpu_barrier_baseline(orc, 148 * args.k, seconds=4.0) for _ in range(max(1, min(args.steps, 3)))]
+            for _ in range(args.warmup):  # untimed warm-up samples
+                cpu_barrier_baseline(orc, 148 * args.k, seconds=0.2)
+            samples = [cpu_barrier_baseline(orc, 148 * args.k, seconds=2.0) for _ in range(max(1, args.steps))]
             v = statistics.median(s["value"] for s in samples)
             line = {"impl": "reference", "metric": "ns per grid barrier", "value": v, "unit": "ns",
                     "n_gpus": args.gpus, "steps": len(samples), "warmup": args.warmup,
@@ -829,9 +1181,9 @@ def main():
     grid = args.k * ctx.num_sms
     arrivals = arrivals_per_episode(gsrb, c, grid)
     achieved = arrivals / (ns * 1e-9)
-    # DRAM bytes of one launch from an ncu capture of this kernel (1184 x 256,
-    # FANOUT): the per-thread FMA seeds, read once, independent of episodes
-    traffic = 1218560 if args.k == 8 and args.fma == 0 else None
+    # DRAM bytes of one launch from the kept ncu capture of this kernel (1184 x
+    # 256, F = 0): the per-thread FMA seeds, read once, independent of episodes
+    traffic = profile_traffic("barrier_bench_kernel_fanout_k8") if args.k == 8 and args.fma == 0 else None
     roofline = {"bound": "l2_atomic", "achieved": round(achieved / 1e9, 4), "peak": round(rate / 1e9, 4),
                 "unit": "G same-address atomics/s", "frac": round(achieved / rate, 4), "traffic": traffic,
                 "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum per launch (ncu); the barrier is "
@@ -851,27 +1203,39 @@ def main():
             "gpu_launches": int(l1 - l0),
             "e2e": {"value": round(e2e_ns, 2), "unit": "ns", "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
                     "note": "per-episode time of the whole step incl. pinned H2D/D2H copies and the FMA phase"},
-            "autotune_top5": [{"ns": t, "cfg": cand} for t, cand in tune_table[:5]]}
+            }
+    detail = {"headline": dict(line), "autotune_top5": [{"ns": t, "cfg": cand} for t, cand in tune_table[:5]]}
 
     if not args.no_extras:
         orc = load_oracle()
         pol = _load("gsrb_policy", PKG / "policy.py")
         extras_t0 = time.time()
-        line["barrier_table"] = barrier_table(gsrb, ctx, tune, cache)
-        line["semaphore"] = semaphore_numbers(gsrb, ctx)
-        line["reduce_2e24"] = reduce_numbers(gsrb, ctx, orc, tune, cache)
-        line["scan_2e28"] = scan_numbers(gsrb, ctx, orc, tune, cache, n=args.scan_n)
+        detail["barrier_table"] = barrier_table(gsrb, ctx, tune, cache)
+        detail["semaphore"] = semaphore_numbers(gsrb, ctx)
+        detail["reduce_2e24"] = reduce_numbers(gsrb, ctx, orc, tune, cache, cpu=dist.rank == 0)
+        detail["scan_2e28"] = scan_numbers(gsrb, ctx, orc, tune, cache, n=args.scan_n, cpu=dist.rank == 0)
         params, pinfo = train_policy(gsrb, ctx, pol)
-        line["policy"] = pinfo
-        line["graphs"] = graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, not args.skip_pr_check)
-        line["batch"] = batch_numbers(gsrb, ctx, orc, params)
-        line["segments"] = segment_numbers(gsrb, ctx, orc, tune, cache)
+        detail["policy"] = pinfo
+        detail["graphs"] = graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, not args.skip_pr_check,
+                                         ref_gpu=not args.no_reference_programs)
+        detail["batch"] = batch_numbers(gsrb, ctx, orc, params)
+        detail["segments"] = segment_numbers(gsrb, ctx, orc, tune, cache)
+        if not args.no_reference_programs:
+            detail["reference_gpu"] = reference_gpu_numbers(gsrb, ctx)
         line["extras_wall_s"] = round(time.time() - extras_t0, 1)
+        line["configs"] = summarize(detail, hbm_peak()[0])
         if dist.rank == 0:
             line["cpu_baseline"] = cpu_barrier_baseline(orc, 148 * args.k)
-    line["autotuned"] = cache
+    detail["autotuned"] = cache
 
     if dist.rank == 0:
+        try:
+            dpath = pathlib.Path(args.detail)
+            dpath.parent.mkdir(parents=True, exist_ok=True)
+            dpath.write_text(json.dumps(detail, indent=1, default=str))
+            line["detail_file"] = str(args.detail)
+        except OSError as e:
+            line["detail_file"] = f"not written: {e}"
         print(json.dumps(line), flush=True)
     ctx.close()
     dist.close()

@@ -162,8 +162,13 @@ gsrb_status_t gsrb_reduce_i32(gsrb_ctx_t ctx, const int32_t* d_in, size_t n, int
  * GSRB_ERR_ARG), grid = 2 CTAs per SM (at most 2048 CTAs).  The first call on a
  * device looks up the array's device address with that device current; make it
  * before any stream capture.  Every call clears the array's barrier words and
- * reuses it, so calls whose kernels overlap on the GPU race.  Synchronous with
- * respect to `stream`; returns GSRB_ERR_TIMEOUT if a bounded wait ran out. */
+ * reuses it, so calls whose kernels overlap on the GPU race.  The looked-up
+ * address is kept for the life of the process: do not call it again after a
+ * cudaDeviceReset of that device.  Synchronous with respect to `stream`;
+ * returns GSRB_ERR_TIMEOUT if a bounded wait (2 s) ran out -- on a GPU shared
+ * with other running kernels this can also mean that the 2-CTAs-per-SM grid
+ * could not all be resident at once (the launch is not cooperative, and the
+ * occupancy check before it cannot see other processes' kernels). */
 gsrb_status_t gsrb_reduce_i32_noalloc(const int32_t* d_in, size_t n, int64_t* d_out, void* stream);
 
 /* ---- scan (three-phase persistent exclusive prefix sum) ---------------------------

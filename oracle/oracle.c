@@ -229,6 +229,189 @@ void orc_pagerank_pull(uint32_t n, const uint32_t* row, const uint32_t* dst, dou
   free(c);
 }
 
+/* The same fixed point for any graph, directed included, in scatter form:
+ * x <- (1 - alpha) + alpha * sum_{u -> v} x_u / outdeg(u), where u -> v are the
+ * CSR rows' out-edges.  This is the fixed point the reference's push-residual
+ * PageRank converges to (LONESTAR/apps/pr/kernel_gsrb.cu:298-336 seeds
+ * p = 1 - alpha and pushes alpha * residual / outdeg along out-edges); on a
+ * symmetric graph it equals orc_pagerank_pull. */
+void orc_pagerank_push(uint32_t n, const uint32_t* row, const uint32_t* dst, double alpha, int iters,
+                       double* x) {
+  double* y = (double*)malloc(sizeof(double) * (n ? n : 1));
+  for (uint32_t v = 0; v < n; ++v) x[v] = 1.0 - alpha;
+  for (int it = 0; it < iters; ++it) {
+    for (uint32_t v = 0; v < n; ++v) y[v] = 1.0 - alpha;
+    for (uint32_t u = 0; u < n; ++u) {
+      uint32_t d = row[u + 1] - row[u];
+      if (!d) continue;
+      double c = alpha * x[u] / (double)d;
+      for (uint32_t j = row[u]; j < row[u + 1]; ++j) y[dst[j]] += c;
+    }
+    memcpy(x, y, sizeof(double) * n);
+  }
+  free(y);
+}
+
+/* Multi-threaded forms for the CPU baseline (same results as orc_bfs and
+ * orc_pagerank_pull).  BFS: level-synchronous top-down; every thread takes
+ * chunks of the frontier from a shared counter, claims unvisited vertices
+ * with a compare-and-swap on their level and appends them to the next
+ * frontier through per-thread buffers.  Levels are unique, so the result does
+ * not depend on the interleaving. */
+typedef struct {
+  uint32_t n;
+  const uint32_t* row;
+  const uint32_t* dst;
+  int32_t* level;
+  uint32_t* cur;
+  uint32_t* next;
+  size_t cur_n;
+  size_t next_n; /* atomic */
+  size_t take;   /* atomic chunk cursor over cur */
+  int32_t depth;
+  int done;
+  pthread_barrier_t bar;
+} bfsmt_t;
+
+#define BFS_MT_CHUNK 256
+#define BFS_MT_BUF 512
+
+static void* bfs_mt_worker(void* p) {
+  bfsmt_t* b = (bfsmt_t*)p;
+  uint32_t buf[BFS_MT_BUF];
+  for (;;) {
+    size_t nb = 0;
+    int32_t nl = b->depth + 1;
+    for (;;) {
+      size_t beg = __atomic_fetch_add(&b->take, BFS_MT_CHUNK, __ATOMIC_RELAXED);
+      if (beg >= b->cur_n) break;
+      size_t end = beg + BFS_MT_CHUNK < b->cur_n ? beg + BFS_MT_CHUNK : b->cur_n;
+      for (size_t i = beg; i < end; ++i) {
+        uint32_t u = b->cur[i];
+        for (uint32_t j = b->row[u]; j < b->row[u + 1]; ++j) {
+          uint32_t v = b->dst[j];
+          int32_t inf = INT32_MAX;
+          if (__atomic_load_n(&b->level[v], __ATOMIC_RELAXED) != INT32_MAX) continue;
+          if (!__atomic_compare_exchange_n(&b->level[v], &inf, nl, 0, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) continue;
+          buf[nb++] = v;
+          if (nb == BFS_MT_BUF) {
+            size_t at = __atomic_fetch_add(&b->next_n, nb, __ATOMIC_RELAXED);
+            memcpy(b->next + at, buf, nb * sizeof(uint32_t));
+            nb = 0;
+          }
+        }
+      }
+    }
+    if (nb) {
+      size_t at = __atomic_fetch_add(&b->next_n, nb, __ATOMIC_RELAXED);
+      memcpy(b->next + at, buf, nb * sizeof(uint32_t));
+    }
+    if (pthread_barrier_wait(&b->bar) == PTHREAD_BARRIER_SERIAL_THREAD) {
+      uint32_t* t = b->cur;
+      b->cur = b->next;
+      b->next = t;
+      b->cur_n = b->next_n;
+      b->next_n = 0;
+      b->take = 0;
+      b->depth += 1;
+      b->done = b->cur_n == 0;
+    }
+    pthread_barrier_wait(&b->bar);
+    if (b->done) return NULL;
+  }
+}
+
+void orc_bfs_mt(uint32_t n, const uint32_t* row, const uint32_t* dst, uint32_t src, int32_t* level, int threads) {
+  for (uint32_t v = 0; v < n; ++v) level[v] = INT32_MAX;
+  if (src >= n) return;
+  if (threads < 1) threads = 1;
+  if (threads > 256) threads = 256;
+  bfsmt_t b;
+  memset(&b, 0, sizeof(b));
+  b.n = n;
+  b.row = row;
+  b.dst = dst;
+  b.level = level;
+  b.cur = (uint32_t*)malloc(sizeof(uint32_t) * (n ? n : 1));
+  b.next = (uint32_t*)malloc(sizeof(uint32_t) * (n ? n : 1));
+  level[src] = 0;
+  b.cur[0] = src;
+  b.cur_n = 1;
+  pthread_barrier_init(&b.bar, NULL, (unsigned)threads);
+  pthread_t th[256];
+  for (int t = 0; t < threads; ++t) pthread_create(&th[t], NULL, bfs_mt_worker, &b);
+  for (int t = 0; t < threads; ++t) pthread_join(th[t], NULL);
+  pthread_barrier_destroy(&b.bar);
+  free(b.cur);
+  free(b.next);
+}
+
+typedef struct {
+  uint32_t n;
+  const uint32_t* row;
+  const uint32_t* dst;
+  double alpha;
+  int iters;
+  double* x;
+  double* c;
+  size_t take; /* atomic chunk cursor */
+  pthread_barrier_t bar;
+} prmt_t;
+
+#define PR_MT_CHUNK 2048
+
+static void* pr_mt_worker(void* p) {
+  prmt_t* b = (prmt_t*)p;
+  for (int it = 0; it < b->iters; ++it) {
+    for (;;) {
+      size_t beg = __atomic_fetch_add(&b->take, PR_MT_CHUNK, __ATOMIC_RELAXED);
+      if (beg >= b->n) break;
+      size_t end = beg + PR_MT_CHUNK < b->n ? beg + PR_MT_CHUNK : b->n;
+      for (size_t u = beg; u < end; ++u) {
+        uint32_t d = b->row[u + 1] - b->row[u];
+        b->c[u] = d ? b->x[u] / (double)d : 0.0;
+      }
+    }
+    if (pthread_barrier_wait(&b->bar) == PTHREAD_BARRIER_SERIAL_THREAD) b->take = 0;
+    pthread_barrier_wait(&b->bar);
+    for (;;) {
+      size_t beg = __atomic_fetch_add(&b->take, PR_MT_CHUNK, __ATOMIC_RELAXED);
+      if (beg >= b->n) break;
+      size_t end = beg + PR_MT_CHUNK < b->n ? beg + PR_MT_CHUNK : b->n;
+      for (size_t v = beg; v < end; ++v) {
+        double s = 0.0;
+        for (uint32_t j = b->row[v]; j < b->row[v + 1]; ++j) s += b->c[b->dst[j]];
+        b->x[v] = (1.0 - b->alpha) + b->alpha * s;
+      }
+    }
+    if (pthread_barrier_wait(&b->bar) == PTHREAD_BARRIER_SERIAL_THREAD) b->take = 0;
+    pthread_barrier_wait(&b->bar);
+  }
+  return NULL;
+}
+
+void orc_pagerank_pull_mt(uint32_t n, const uint32_t* row, const uint32_t* dst, double alpha, int iters,
+                          double* x, int threads) {
+  if (threads < 1) threads = 1;
+  if (threads > 256) threads = 256;
+  prmt_t b;
+  memset(&b, 0, sizeof(b));
+  b.n = n;
+  b.row = row;
+  b.dst = dst;
+  b.alpha = alpha;
+  b.iters = iters;
+  b.x = x;
+  b.c = (double*)malloc(sizeof(double) * (n ? n : 1));
+  for (uint32_t v = 0; v < n; ++v) x[v] = 1.0 - alpha;
+  pthread_barrier_init(&b.bar, NULL, (unsigned)threads);
+  pthread_t th[256];
+  for (int t = 0; t < threads; ++t) pthread_create(&th[t], NULL, pr_mt_worker, &b);
+  for (int t = 0; t < threads; ++t) pthread_join(th[t], NULL);
+  pthread_barrier_destroy(&b.bar);
+  free(b.c);
+}
+
 double orc_normalized_l1(const float* a, const double* b, uint32_t n) {
   double sa = 0.0, sb = 0.0;
   for (uint32_t v = 0; v < n; ++v) {

@@ -12,7 +12,10 @@
  * (Reduce/test_reduce.cu:14-17, scan/main.cu:37-41), the Heterosync replay
  * against the reference's golden loop (Heterosync/main.cu:2987-3166).  The
  * graph oracles (BFS, Dijkstra, PageRank) have no CPU counterpart in the
- * reference; they are pinned by hand-computed fixtures in tests/golden.
+ * reference; they are pinned against the outputs of the reference's own
+ * Lonestar programs (bfs/sssp/pr_ccg built for sm_100a) on six seeded graphs,
+ * frozen in tests/golden/ref_lonestar_golden.npz by
+ * tests/golden/make_ref_lonestar.py, and by hand-computed fixtures.
  */
 #ifndef GSRB_ORACLE_H_
 #define GSRB_ORACLE_H_
@@ -48,6 +51,18 @@ void orc_dijkstra(uint32_t n, const uint32_t* row, const uint32_t* dst, const in
  * vertices without edges contribute nothing. */
 void orc_pagerank_pull(uint32_t n, const uint32_t* row, const uint32_t* dst, double alpha, int iters,
                        double* x);
+/* The same fixed point in scatter form over out-edges, for any graph (the
+ * fixed point of the reference's push-residual PageRank,
+ * LONESTAR/apps/pr/kernel_gsrb.cu:298-336); equals orc_pagerank_pull on a
+ * symmetric graph. */
+void orc_pagerank_push(uint32_t n, const uint32_t* row, const uint32_t* dst, double alpha, int iters,
+                       double* x);
+/* The same BFS and pull PageRank on `threads` host threads (CPU baseline, all
+ * cores): level-synchronous BFS with compare-and-swap claims, PageRank split
+ * over vertex chunks.  Results equal orc_bfs / orc_pagerank_pull. */
+void orc_bfs_mt(uint32_t n, const uint32_t* row, const uint32_t* dst, uint32_t src, int32_t* level, int threads);
+void orc_pagerank_pull_mt(uint32_t n, const uint32_t* row, const uint32_t* dst, double alpha, int iters,
+                          double* x, int threads);
 /* sum_v |a_v/sum(a) - b_v/sum(b)| with `a` FP32 and `b` FP64. */
 double orc_normalized_l1(const float* a, const double* b, uint32_t n);
 /* Directed CSR edges out of reached vertices (value != INT32_MAX): the TEPS numerator. */

@@ -5,8 +5,9 @@
 #                    main() renamed, linked with scan/scan_gsrb.cu whose GPU
 #                    code is compiled but never called.
 # Nothing is copied into the repository; only the built library lands here.
+#   usage: ref_build.sh [reference root]   (default: $GSRB_REFERENCE_ROOT, else /root/reference)
 set -euo pipefail
-REF=${1:-/root/reference}
+REF=${1:-${GSRB_REFERENCE_ROOT:-/root/reference}}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 NVCC=${NVCC:-/usr/local/cuda/bin/nvcc}

@@ -21,6 +21,9 @@ _lib.orc_max_rel_err_f32_f64.argtypes = [_P, _P, C.c_size_t, C.c_double]
 _lib.orc_bfs.argtypes = [C.c_uint32, _P, _P, C.c_uint32, _P]
 _lib.orc_dijkstra.argtypes = [C.c_uint32, _P, _P, _P, C.c_uint32, _P]
 _lib.orc_pagerank_pull.argtypes = [C.c_uint32, _P, _P, C.c_double, C.c_int, _P]
+_lib.orc_pagerank_push.argtypes = [C.c_uint32, _P, _P, C.c_double, C.c_int, _P]
+_lib.orc_bfs_mt.argtypes = [C.c_uint32, _P, _P, C.c_uint32, _P, C.c_int]
+_lib.orc_pagerank_pull_mt.argtypes = [C.c_uint32, _P, _P, C.c_double, C.c_int, _P, C.c_int]
 _lib.orc_normalized_l1.restype = C.c_double
 _lib.orc_normalized_l1.argtypes = [_P, _P, C.c_uint32]
 _lib.orc_traversed_edges.restype = C.c_uint64
@@ -75,6 +78,29 @@ def scan_u32(a, threads=1):
     return out
 
 
+_ref_scan = None
+
+
+def ref_cpu_sum_scan(a):
+    """The reference's own cpu_sum_scan (scan/main.cu:11-21), compiled from the
+    reference sources into oracle/_ref/libref_scan.so by oracle/ref_build.sh;
+    None when that library was not built."""
+    global _ref_scan
+    if _ref_scan is None:
+        path = ROOT / "oracle" / "_ref" / "libref_scan.so"
+        if not path.exists():
+            return None
+        lib = C.CDLL(str(path))
+        fn = getattr(lib, "_Z12cpu_sum_scanPjPKjm")  # cpu_sum_scan(unsigned*, const unsigned*, size_t)
+        fn.restype = None
+        fn.argtypes = [_P, _P, C.c_size_t]
+        _ref_scan = fn
+    a = np.ascontiguousarray(a, dtype=np.uint32)
+    out = np.empty_like(a)
+    _ref_scan(_p(out), _p(a), a.size)
+    return out
+
+
 def scan_f32_f64(a):
     a = np.ascontiguousarray(a, dtype=np.float32)
     out = np.empty(a.size, dtype=np.float64)
@@ -97,9 +123,12 @@ def mlp_forward(params, X):
     return out
 
 
-def bfs(g, src=0):
+def bfs(g, src=0, threads=1):
     out = np.empty(g.nnodes, dtype=np.int32)
-    _lib.orc_bfs(g.nnodes, _p(g.row_start), _p(g.edge_dst), src, _p(out))
+    if threads > 1:
+        _lib.orc_bfs_mt(g.nnodes, _p(g.row_start), _p(g.edge_dst), src, _p(out), threads)
+    else:
+        _lib.orc_bfs(g.nnodes, _p(g.row_start), _p(g.edge_dst), src, _p(out))
     return out
 
 
@@ -109,9 +138,19 @@ def dijkstra(g, src=0):
     return out
 
 
-def pagerank(g, alpha=0.85, iters=50):
+def pagerank(g, alpha=0.85, iters=50, threads=1):
     out = np.empty(g.nnodes, dtype=np.float64)
-    _lib.orc_pagerank_pull(g.nnodes, _p(g.row_start), _p(g.edge_dst), alpha, iters, _p(out))
+    if threads > 1:
+        _lib.orc_pagerank_pull_mt(g.nnodes, _p(g.row_start), _p(g.edge_dst), alpha, iters, _p(out), threads)
+    else:
+        _lib.orc_pagerank_pull(g.nnodes, _p(g.row_start), _p(g.edge_dst), alpha, iters, _p(out))
+    return out
+
+
+def pagerank_push(g, alpha=0.85, iters=200):
+    """The PageRank fixed point over out-edges, for any graph (see orc_pagerank_push)."""
+    out = np.empty(g.nnodes, dtype=np.float64)
+    _lib.orc_pagerank_push(g.nnodes, _p(g.row_start), _p(g.edge_dst), alpha, iters, _p(out))
     return out
 
 

@@ -45,3 +45,22 @@ def test_noalloc_rejects_oversized_input(gsrb, ctx):
     out = ctx.array(1, np.int64).zero()
     d = ctx.array(16, np.int32)
     assert fn(d.ptr, (1 << 32) + 1, out.ptr, None) == gsrb.ERR_ARG
+
+
+@pytest.mark.parametrize("shift", [1, 3])
+def test_noalloc_unaligned_and_small_inputs(gsrb, ctx, shift):
+    # inputs that start 4 or 12 bytes past a 16-byte boundary (the kernel's
+    # scalar head) and sizes at which most CTAs get empty slices
+    fn = _noalloc(gsrb)
+    sizes = [0, 1, 5, 2 * ctx.num_sms - 1, 1_000_003]
+    for n in sizes:
+        a = gsrb.uniform_i32(n + shift, n, -1000, 1000)
+        buf = np.zeros(n + shift + 4, np.int32)
+        buf[shift:shift + n] = a
+        d = ctx.to_device(buf)
+        got = ctx.array(1, np.int64).zero()
+        ctx.sync()
+        for call in range(2):
+            gsrb.check(fn(d.ptr + 4 * shift, n, got.ptr, None), f"noalloc n={n} shift={shift} call {call}")
+            assert int(got.download()[0]) == int(a.astype(np.int64).sum()), f"n={n} shift={shift} call {call}"
+        d.free()
