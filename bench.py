@@ -515,7 +515,7 @@ def sssp_runs(gsrb, ctx, orc, dg, g, deltas, cfg, verify=True):
     return res
 
 
-def graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, verify_pr=True, ref_gpu=True):
+def graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, verify_pr=True, ref_gpu="quick"):
     res = {}
     t0 = time.time()
     rm = gsrb.rmat(22, 16, a=0.57, b=0.19, c=0.19, seed=SEED, wlo=1, whi=255)
@@ -560,8 +560,8 @@ def graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, verify_pr=True, ref_
                                           "l1_vs_converged_pull": orc.normalized_l1(outr.download(),
                                                                                     conv.download().astype(np.float64))}
     dg.free()
-    if ref_gpu:
-        res["rmat22"]["reference_gpu"] = lonestar_reference(rm)
+    if ref_gpu != "none":
+        res["rmat22"]["reference_gpu"] = lonestar_reference(rm, "rmat22", ref_gpu)
     del rm
     gr = gsrb.grid2d(2048, 2048, seed=SEED, wlo=1, whi=1000)
     dg = ctx.graph(gr)
@@ -574,8 +574,8 @@ def graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, verify_pr=True, ref_
     res["grid2048"]["sssp"] = sssp_runs(gsrb, ctx, orc, dg, gr, [("reference_delta", 10000), ("delta_4096", 4096)],
                                         cfg)
     dg.free()
-    if ref_gpu:
-        res["grid2048"]["reference_gpu"] = lonestar_reference(gr)
+    if ref_gpu != "none":
+        res["grid2048"]["reference_gpu"] = lonestar_reference(gr, "grid2048", ref_gpu)
     return res
 
 
@@ -811,18 +811,34 @@ def _ref_run(prog, args, stdin=None, timeout=180):
     raise RuntimeError(f"{prog}: no time in output")
 
 
-def reference_gpu_numbers(gsrb, ctx):
+# The reference's GSRB / GCPUSRB forms with more than one CTA per barrier group
+# (more CTAs than SMs) measured slow on B200 in one run of this file: reduce at
+# N = 303,104 (1184 CTAs of 256 threads) 8.5 s, scan at N = 151,552 (2368 CTAs
+# of 32 threads) 15.8 s, Lonestar bfs_gsrb 38 s and sssp_gsrb 116 s on RMAT-22
+# (block factor 2); on the 2048 x 2048 grid (4095 levels) bfs_gsrb and
+# sssp_gsrb did not finish within 600 s and were killed.  The default run
+# ("quick") times the reference's programs only at shapes that finish in
+# seconds; "full" adds the slow RMAT-22, reduce and scan shapes.  The grid's
+# GSRB / GCPUSRB forms are never run again.
+REF_SLOW_SHAPES = {"reduce_gsrb_303104_ms": 8542.3, "scan_gsrb_151552_ms": 15834.8,
+                   "rmat22_bfs_gsrb_ms": 38140.4, "rmat22_sssp_gsrb_ms": 115862.0,
+                   "grid2048_bfs_gsrb": "not finished within 600 s (killed)",
+                   "grid2048_sssp_gsrb": "not finished within 600 s (killed)"}
+
+
+def reference_gpu_numbers(gsrb, ctx, mode="quick"):
     """The reference's own GPU programs (baseline/_ref, built from the
     reference sources for sm_100a by baseline/build.sh) timed on this GPU in
     the same run, beside this library on the same shapes.  Every shape is
     co-resident: Heterosync runs 148*k CTAs of 32 threads (k <= 8, the
     reference's own MAX_BLOCKS check allows 32 per SM), the reduce and scan run
-    at N where one element per thread needs <= 8 CTAs per SM, the Lonestar
-    programs get block factor 2 (296 CTAs of 32 threads)."""
+    at N where one element per thread needs <= 8 CTAs per SM.  mode "quick"
+    skips the GSRB forms at the shapes in REF_SLOW_SHAPES."""
     if not (REF_BIN / "allSyncPrims-1kernel").exists():
         return {"unavailable": "baseline/_ref not built (needs the reference sources)"}
-    out = {"programs": "baseline/_ref, the reference's sources compiled for sm_100a"}
-    iters = 10000
+    out = {"programs": "baseline/_ref, the reference's sources compiled for sm_100a", "mode": mode,
+           "slow_shapes_recorded": REF_SLOW_SHAPES}
+    iters = 10000 if mode == "full" else 1000
     # Heterosync barriers: one barrier per iteration, NUM_LDST = 1, 10 launches averaged
     het = []
     for k in (1, 8):
@@ -844,11 +860,25 @@ def reference_gpu_numbers(gsrb, ctx):
             row[name + "_ns"] = round((t1 - t0) * 1e6 / 2000, 1)
         het.append(row)
     out["heterosync_barrier"] = het
+
+    def native_time(fn):
+        ts = []
+        for i in range(8):
+            ctx.record(4)
+            fn()
+            ctx.record(5)
+            if i >= 3:
+                ts.append(ctx.elapsed_ms(4, 5))
+        return round(statistics.median(ts), 5)
+
     # reduce: one element per thread, 256 threads per CTA
     red = []
     for n in (37_888, 303_104):
         row = {"n": n}
         for v in ("gsrb", "ccg"):
+            if v == "gsrb" and n > 37_888 and mode != "full":
+                row[v + "_ms"] = f"not run (measured {REF_SLOW_SHAPES['reduce_gsrb_303104_ms']} ms once)"
+                continue
             try:
                 ms, so = _ref_run(f"reduce_{v}", [n, 256])
                 row[v + "_ms"] = ms
@@ -858,14 +888,7 @@ def reference_gpu_numbers(gsrb, ctx):
         a = np.ones(n, np.int32)
         d = ctx.to_device(a)
         o = ctx.array(1, np.int64).zero()
-        ts = []
-        for i in range(8):
-            ctx.record(4)
-            gsrb.check(ctx.reduce_i32(d, n, o))
-            ctx.record(5)
-            if i >= 3:
-                ts.append(ctx.elapsed_ms(4, 5))
-        row["native_ms"] = round(statistics.median(ts), 5)
+        row["native_ms"] = native_time(lambda: gsrb.check(ctx.reduce_i32(d, n, o)))
         row["native_correct"] = int(o.download()[0]) == n
         d.free()
         o.free()
@@ -876,6 +899,9 @@ def reference_gpu_numbers(gsrb, ctx):
     for n in (9_472, 151_552):
         row = {"n": n}
         for v in ("gsrb", "ccg"):
+            if v == "gsrb" and n > 9_472 and mode != "full":
+                row[v + "_ms"] = f"not run (measured {REF_SLOW_SHAPES['scan_gsrb_151552_ms']} ms once)"
+                continue
             try:
                 ms, so = _ref_run(f"scan_{v}", [n])
                 row[v + "_ms"] = ms
@@ -884,14 +910,7 @@ def reference_gpu_numbers(gsrb, ctx):
                 row[v + "_ms"] = f"failed: {str(e)[:120]}"
         a = np.ones(n, np.uint32)
         d, o = ctx.to_device(a), ctx.array(n, np.uint32)
-        ts = []
-        for i in range(8):
-            ctx.record(4)
-            gsrb.check(ctx.scan(d, o, n))
-            ctx.record(5)
-            if i >= 3:
-                ts.append(ctx.elapsed_ms(4, 5))
-        row["native_ms"] = round(statistics.median(ts), 5)
+        row["native_ms"] = native_time(lambda: gsrb.check(ctx.scan(d, o, n)))
         row["native_match"] = bool(np.array_equal(o.download(), np.arange(n, dtype=np.uint32)))
         d.free()
         o.free()
@@ -900,10 +919,12 @@ def reference_gpu_numbers(gsrb, ctx):
     return out
 
 
-def lonestar_reference(g, timeout=600):
-    """The reference's Lonestar BFS and SSSP (gsrb and ccg builds) on graph g
-    written as .gr v1: the "Kernel time (ms)" each prints, block factor 2 (296
-    CTAs of 32 threads, within the wrapper's own residency cap)."""
+def lonestar_reference(g, name, mode="quick", timeout=300):
+    """The reference's Lonestar BFS and SSSP on graph g written as .gr v1: the
+    "Kernel time (ms)" each prints, block factor 2 (296 CTAs of 32 threads,
+    within the wrapper's own residency cap).  The cooperative-groups builds
+    always; the GSRB builds only in mode "full" and never on the grid (see
+    REF_SLOW_SHAPES)."""
     if not (REF_BIN / "lonestar" / "bfs_gsrb").exists():
         return {"unavailable": "baseline/_ref not built (needs the reference sources)"}
     row = {"block_factor": 2}
@@ -912,6 +933,9 @@ def lonestar_reference(g, timeout=600):
         g.write_gr(path, with_weights=True)
         for app, extra in (("bfs", ["-s", 0]), ("sssp", ["-s", 0, "-d", 10000])):
             for v in ("gsrb", "ccg"):
+                if v == "gsrb" and (mode != "full" or name != "rmat22"):
+                    row[f"{app}_{v}_ms"] = f"not run: {REF_SLOW_SHAPES.get(f'{name}_{app}_gsrb_ms', REF_SLOW_SHAPES.get(f'{name}_{app}_gsrb'))}"
+                    continue
                 try:
                     ms, _ = _ref_run(f"lonestar/{app}_{v}", extra + ["-q", path], stdin="2\n", timeout=timeout)
                     row[f"{app}_{v}_ms"] = ms
@@ -1067,8 +1091,9 @@ def main():
     ap.add_argument("--reduce-n", type=int, default=1 << 24)
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--skip-pr-check", action="store_true", help="skip the FP64 CPU PageRank (about 25 s)")
-    ap.add_argument("--no-reference-programs", action="store_true",
-                    help="do not time the reference's own GPU programs (baseline/_ref)")
+    ap.add_argument("--reference-programs", default="quick", choices=["none", "quick", "full"],
+                    help="time the reference's own GPU programs (baseline/_ref): quick = the shapes that finish "
+                         "in seconds, full = also the slow GSRB shapes (minutes)")
     ap.add_argument("--detail", default=str(ROOT / "gpurun_out" / "bench_detail.json"),
                     help="where the full tables go (the JSON line keeps one summary per configuration)")
     args = ap.parse_args()
@@ -1210,19 +1235,33 @@ def main():
         orc = load_oracle()
         pol = _load("gsrb_policy", PKG / "policy.py")
         extras_t0 = time.time()
-        detail["barrier_table"] = barrier_table(gsrb, ctx, tune, cache)
-        detail["semaphore"] = semaphore_numbers(gsrb, ctx)
-        detail["reduce_2e24"] = reduce_numbers(gsrb, ctx, orc, tune, cache, cpu=dist.rank == 0)
-        detail["scan_2e28"] = scan_numbers(gsrb, ctx, orc, tune, cache, n=args.scan_n, cpu=dist.rank == 0)
-        params, pinfo = train_policy(gsrb, ctx, pol)
+        walls = {}
+
+        def timed(key, fn):
+            t = time.time()
+            r = fn()
+            walls[key] = round(time.time() - t, 1)
+            return r
+
+        detail["barrier_table"] = timed("barrier_table", lambda: barrier_table(gsrb, ctx, tune, cache))
+        detail["semaphore"] = timed("semaphore", lambda: semaphore_numbers(gsrb, ctx))
+        detail["reduce_2e24"] = timed("reduce", lambda: reduce_numbers(gsrb, ctx, orc, tune, cache,
+                                                                       cpu=dist.rank == 0))
+        detail["scan_2e28"] = timed("scan", lambda: scan_numbers(gsrb, ctx, orc, tune, cache, n=args.scan_n,
+                                                                 cpu=dist.rank == 0))
+        params, pinfo = timed("policy", lambda: train_policy(gsrb, ctx, pol))
         detail["policy"] = pinfo
-        detail["graphs"] = graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, not args.skip_pr_check,
-                                         ref_gpu=not args.no_reference_programs)
-        detail["batch"] = batch_numbers(gsrb, ctx, orc, params)
-        detail["segments"] = segment_numbers(gsrb, ctx, orc, tune, cache)
-        if not args.no_reference_programs:
-            detail["reference_gpu"] = reference_gpu_numbers(gsrb, ctx)
+        detail["graphs"] = timed("graphs", lambda: graph_numbers(gsrb, ctx, orc, pol, params, tune, cache,
+                                                                 not args.skip_pr_check,
+                                                                 ref_gpu=args.reference_programs))
+        detail["batch"] = timed("batch", lambda: batch_numbers(gsrb, ctx, orc, params))
+        detail["segments"] = timed("segments", lambda: segment_numbers(gsrb, ctx, orc, tune, cache))
+        if args.reference_programs != "none":
+            detail["reference_gpu"] = timed("reference_programs",
+                                            lambda: reference_gpu_numbers(gsrb, ctx, args.reference_programs))
+        detail["wall_s"] = walls
         line["extras_wall_s"] = round(time.time() - extras_t0, 1)
+        line["extras_walls"] = walls
         line["configs"] = summarize(detail, hbm_peak()[0])
         if dist.rank == 0:
             line["cpu_baseline"] = cpu_barrier_baseline(orc, 148 * args.k)

@@ -61,6 +61,9 @@ enum {
   GSRB_BAR_NONE = 99             /* no barrier (phase-only timing baseline) */
 };
 
+/* Data-kernel forms (gsrb_cfg_t.form). */
+enum { GSRB_FORM_AUTO = 0, GSRB_FORM_L2 = 1 };
+
 /* Launch / schedule configuration.  Zero-initialise and call gsrb_cfg_default. */
 typedef struct gsrb_cfg {
   int32_t variant;       /* GSRB_BAR_* */
@@ -75,7 +78,9 @@ typedef struct gsrb_cfg {
   int32_t launch_mode;   /* 0 = cooperative launch when the driver accepts it, 1 = plain launch (default)
                             (both only after the co-residency check; CCG is always cooperative) */
   int32_t wake_lines;    /* FANOUT / CLUSTER_FANOUT / HIER: wake-up lines the generation is published to (0 = 8) */
-  int32_t reserved[5];
+  int32_t form;          /* scan: GSRB_FORM_AUTO (staged in shared memory when the input is 16-byte
+                            aligned and not in place) or GSRB_FORM_L2 (chunks re-read through L2) */
+  int32_t reserved[4];
 } gsrb_cfg_t;
 
 void gsrb_cfg_default(gsrb_cfg_t* cfg);
@@ -267,6 +272,19 @@ gsrb_status_t gsrb_semaphore_bench(gsrb_ctx_t ctx, const gsrb_cfg_t* cfg, int32_
  * and fail at once; returns GSRB_ERR_INVARIANT (synchronous).  d_out: 2 uint32,
  * 1 where the reader / writer wait succeeded, else 0. */
 gsrb_status_t gsrb_semaphore_fault_overpost(gsrb_ctx_t ctx, uint32_t capacity, uint32_t* d_out);
+/* Fault test of a writer that gives up (no counterpart in the reference): one
+ * CTA enters a GSRB_SEM_PRIORITY semaphore as a reader, then waits on it as a
+ * writer while still holding the reader slot, so that wait is served its turn
+ * but runs into a 20 ms deadline on the count; the CTA leaves as a reader and
+ * waits as a writer again.  A served writer that gives up hands its turn on,
+ * so the second writer wait succeeds.  Returns GSRB_ERR_LOCK_TIMEOUT (the first
+ * writer's); d_out: 5 uint32 = [reader entered, first writer entered, second
+ * writer entered, count afterwards, serving afterwards].
+ * A writer that gives up while still waiting for its turn leaves its ticket
+ * unserved: every later writer of that record then runs into its own deadline
+ * until the record is re-created (gsrb_semaphore_init / cudaSemaphoreCreate*),
+ * as after any wait that reported GSRB_ERR_INVARIANT.  Synchronous. */
+gsrb_status_t gsrb_semaphore_fault_writer_timeout(gsrb_ctx_t ctx, uint32_t capacity, uint32_t* d_out);
 /* Mutex microbenchmark: every CTA locks `iters` times and adds 1 to W `incs`
  * times with a plain read-modify-write.  Same counter layout.  Synchronous.
  * Reference: kernelSpinLockMutex / EBO / FA / Sleep, Heterosync/main.cu:574-700. */

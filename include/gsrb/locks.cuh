@@ -295,6 +295,9 @@ __device__ __forceinline__ bool psem_wait(PrioritySem s, bool is_writer, const v
           if (!w.tick()) { ok = false; break; }
           if (spin_ns) __nanosleep(spin_ns);
         }
+        // a writer that was served but gave up on the count hands its turn
+        // on, so the writers queued behind it are not held up by it
+        if (!ok) ptx::red_add_release_gpu(s.serving(), 1u);
       }
       ptx::red_add_relaxed_gpu(s.queued(), 0xffffffffu);
     }

@@ -81,3 +81,16 @@ def test_semaphore_overpost_detected(gsrb, ctx, cap):
     cnt = _counters(ctx)
     gsrb.check(ctx.semaphore_bench(gsrb.cfg(ctas_per_sm=1, threads=64, timeout_ms=3000), 4, cap, 5, 2, 10, cnt))
     assert cnt.download().tolist()[6] == 0
+
+
+@pytest.mark.parametrize("cap", [1, 10])
+def test_semaphore_writer_timeout_hands_turn_on(gsrb, ctx, cap):
+    # a writer that is served but gives up on the count (a reader slot is held
+    # by its own CTA) reports LOCK_TIMEOUT and hands its turn on: the next
+    # writer of the same record is served, and the record ends balanced
+    out = ctx.array(5, np.uint32).zero()
+    assert ctx.semaphore_fault_writer_timeout(cap, out) == gsrb.ERR_LOCK_TIMEOUT
+    r, w1, w2, count, serving = out.download().tolist()
+    assert (r, w1, w2) == (1, 0, 1)
+    assert count == cap + 1 and serving == 2
+    assert ctx.status()[0] == 0

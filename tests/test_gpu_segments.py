@@ -85,6 +85,33 @@ def test_scan_f32_segments_within_tolerance(gsrb, ctx, orc, variant, k):
 
 
 @pytest.mark.parametrize("variant", VARIANTS)
+@pytest.mark.parametrize("k", [1, 9, 127])
+def test_scan_f32_segments_mixed_sign(gsrb, ctx, orc, variant, k):
+    # FP32 values U[-1,1): prefixes cancel, so a relative bound means nothing
+    # near zero.  Bound each element by the L1 mass it was summed from: the
+    # FP32 tile scan and the FP32 result add at most a few ulps of the running
+    # sum of |x| (chunk sums and carries are FP64), so 1e-5 of that mass holds
+    off = _uneven_offsets(300 + k, k, hi=1 << 19)
+    a = (gsrb.uniform_f32(0xC0FFEE + k, int(off[-1])) * np.float32(2.0) - np.float32(1.0)).astype(np.float32)
+    d = ctx.to_device(a) if a.size else ctx.array(1, np.float32)
+    out = ctx.array(max(a.size, 1), np.float32).zero()
+    c = gsrb.cfg(variant=variant, ctas_per_sm=2, threads=256, tile=1 if k == 9 else 0)
+    gsrb.check(ctx.scan_segments(d, out, off, c), "scan_f32_segments")
+    ctx.check_status("scan_f32_segments")
+    got = out.download()[: a.size].astype(np.float64)
+    for i in range(k):
+        s0, e0 = int(off[i]), int(off[i + 1])
+        if e0 == s0:
+            continue
+        seg = a[s0:e0].astype(np.float64)
+        want = np.concatenate([[0.0], np.cumsum(seg)[:-1]])
+        mass = np.concatenate([[0.0], np.cumsum(np.abs(seg))[:-1]])
+        err = np.abs(got[s0:e0] - want)
+        assert got[s0] == 0.0
+        assert np.all(err <= REL_TOL_F32 * mass + 1e-30), f"segment {i}: worst {float((err - REL_TOL_F32 * mass).max())}"
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
 def test_scan_segments_many_rounds(gsrb, ctx, orc, variant):
     # one tile per CTA per round: tens of rounds per segment, so the double
     # buffered round sums are reused many times

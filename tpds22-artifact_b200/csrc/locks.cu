@@ -189,6 +189,30 @@ semaphore_overpost_kernel(uint32_t* rec, const void* statbuf, uint64_t timeout_n
   }
 }
 
+// One CTA, in order: enters as a reader (count max - 1), waits as a writer
+// while still holding the reader slot (the count never reaches max: that wait
+// runs into its short deadline, after its ticket was served), leaves as a
+// reader, then waits as a writer again with the next ticket.  The second
+// writer is served only if the first handed its turn on.
+__global__ void __launch_bounds__(32)
+semaphore_writer_timeout_kernel(uint32_t* rec, const void* statbuf, uint64_t short_ns, uint64_t timeout_ns,
+                                uint32_t* out) {
+  const gsrb::PrioritySem s{rec};
+  const bool r = gsrb::psem_wait(s, false, statbuf, timeout_ns, 0);
+  const bool w1 = gsrb::psem_wait(s, true, statbuf, short_ns, 0);
+  if (r) gsrb::psem_post(s, false);
+  if (w1) gsrb::psem_post(s, true);
+  const bool w2 = gsrb::psem_wait(s, true, statbuf, timeout_ns, 0);
+  if (w2) gsrb::psem_post(s, true);
+  if (threadIdx.x == 0) {
+    out[0] = r ? 1u : 0u;
+    out[1] = w1 ? 1u : 0u;
+    out[2] = w2 ? 1u : 0u;
+    out[3] = gsrb::ptx::ld_relaxed_gpu(rec);      // count after the run (max when balanced)
+    out[4] = gsrb::ptx::ld_relaxed_gpu(rec + 4);  // serving
+  }
+}
+
 template <int KIND>
 __global__ void __launch_bounds__(256)
 mutex_bench_kernel(uint32_t* heads, uint32_t* tails, int32_t* ring, uint32_t ring_max, const void* statbuf,
@@ -350,6 +374,26 @@ gsrb_status_t gsrb_semaphore_fault_overpost(gsrb_ctx_t ctx, uint32_t capacity, u
     uint64_t to = 200ull * 1000000ull;  // a missed detection ends in 0.2 s, not a hang
     void* args[] = {&rec, &statbuf, &to, &d_out};
     st = launch_plain(ctx, (const void*)semaphore_overpost_kernel, dim3(1), dim3(32), 0, args);
+  }
+  gsrb_status_t st2 = gsrb_locks_status(L, nullptr);
+  gsrb_locks_destroy(L);
+  return st ? st : st2;
+}
+
+gsrb_status_t gsrb_semaphore_fault_writer_timeout(gsrb_ctx_t ctx, uint32_t capacity, uint32_t* d_out) {
+  if (!ctx || !d_out || capacity < 1 || capacity > 60000) return GSRB_ERR_ARG;
+  gsrb_locks_t L = nullptr;
+  gsrb_status_t st = gsrb_locks_create(ctx, 1, 1, 1, 1, &L);
+  if (st) return st;
+  st = gsrb_semaphore_init(L, 0, capacity, 1);
+  if (!st) {
+    std::lock_guard<std::mutex> g(ctx->mu);
+    uint32_t* rec = L->st.d.semaphoreBuffers;
+    const void* statbuf = rec;
+    uint64_t short_ns = 20ull * 1000000ull;  // the writer that must give up: 20 ms
+    uint64_t to = 500ull * 1000000ull;       // every other wait: 0.5 s
+    void* args[] = {&rec, &statbuf, &short_ns, &to, &d_out};
+    st = launch_plain(ctx, (const void*)semaphore_writer_timeout_kernel, dim3(1), dim3(32), 0, args);
   }
   gsrb_status_t st2 = gsrb_locks_status(L, nullptr);
   gsrb_locks_destroy(L);

@@ -50,6 +50,8 @@ BAR_CLUSTER_FANOUT = 10
 BAR_HIER = 11
 BAR_LOCKFREE = 12
 BAR_NONE = 99
+FORM_AUTO = 0
+FORM_L2 = 1
 VARIANT_NAMES = {
     BAR_CLUSTER: "gsrb_cluster",
     BAR_CLUSTER_ALLPOLL: "gsrb_cluster_allpoll",
@@ -88,7 +90,8 @@ class Cfg(C.Structure):
         ("grid_override", C.c_int32),
         ("launch_mode", C.c_int32),
         ("wake_lines", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("form", C.c_int32),
+        ("reserved", C.c_int32 * 4),
     ]
 
     def as_dict(self):
@@ -157,6 +160,7 @@ _SIGS = {
                                          C.c_int32, _P]),
     "gsrb_mutex_bench": (C.c_int32, [_P, C.POINTER(Cfg), C.c_int32, C.c_int32, C.c_int32, _P]),
     "gsrb_semaphore_fault_overpost": (C.c_int32, [_P, C.c_uint32, _P]),
+    "gsrb_semaphore_fault_writer_timeout": (C.c_int32, [_P, C.c_uint32, _P]),
     "gsrb_graph_upload": (C.c_int32, [_P, C.POINTER(HostCSR), C.POINTER(_P)]),
     "gsrb_graph_free": (C.c_int32, [_P]),
     "gsrb_graph_info": (C.c_int32, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
@@ -430,6 +434,9 @@ class Context:
 
     def semaphore_fault_overpost(self, capacity: int, out: DeviceArray) -> int:
         return _lib().gsrb_semaphore_fault_overpost(self.h, capacity, out.ptr)
+
+    def semaphore_fault_writer_timeout(self, capacity: int, out: DeviceArray) -> int:
+        return _lib().gsrb_semaphore_fault_writer_timeout(self.h, capacity, out.ptr)
 
     def mutex_bench(self, c: Cfg, kind: int, iters: int, incs: int, counters: DeviceArray) -> int:
         return _lib().gsrb_mutex_bench(self.h, C.byref(c), kind, iters, incs, counters.ptr)
