@@ -313,28 +313,54 @@ def semaphore_numbers(gsrb, ctx):
 
 # --------------------------------------------------------------- data kernels
 def reduce_numbers(gsrb, ctx, orc, tune, cache, reps=10, fixed=None, n=1 << 24, cpu=False):
-    a = gsrb.uniform_i32(SEED, n, 0, 127)
-    d = ctx.to_device(a)
-    out = ctx.array(1, np.int64).zero()
-    best = fixed or tune.tune_reduce(ctx, d, n, reps=3)[0]
+    """The C1 reduce: 2^24 int32 U[0,127], grid 148 x 2 CTAs x 256 threads.
+    Timed as a stream of reductions: launches back to back over several
+    inputs that together exceed twice the L2 (each launch reads its input from
+    HBM); value = per-launch time.  The configuration is the fastest of the
+    library's own barrier protocols at the C1 shape (grid.sync is timed beside
+    it); the fastest over every shape is reported too, and so is one launch
+    alone after an L2 flush (the launch overhead included)."""
+    nb = int(min(64, max(2, -(-2 * ctx.l2_bytes // (4 * n)))))
+    inputs = [gsrb.uniform_i32(SEED + i, n, 0, 127) for i in range(nb)]
+    bufs = [ctx.to_device(a) for a in inputs]
+    out = ctx.array(nb, np.int64).zero()
+    if fixed:
+        best, table = fixed, []
+    else:
+        best, _, table = tune.tune_reduce(ctx, bufs, n, out, k=2, threads=256)
     cache["reduce"] = best
     c = tune.cfg_from(best)
-    times = []
-    for i in range(3 + reps):
-        ctx.l2_flush()  # 64 MiB fits in L2: time it cold
-        ctx.record(4)
-        gsrb.check(ctx.reduce_i32(d, n, out, c))
-        ctx.record(5)
-        if i >= 3:
-            times.append(ctx.elapsed_ms(4, 5))
+    times = [tune.reduce_stream_ms(ctx, bufs, n, out, c, passes=max(1, reps // 2)) for _ in range(3)]
     ctx.check_status("reduce")
-    ok = int(out.download()[0]) == orc.sum_i32(a)
+    got = out.download()
+    ok = all(int(got[i]) == orc.sum_i32(inputs[i]) for i in range(nb))
     t = statistics.median(times)
     peak, src = hbm_peak()
     gbs = 4 * n / (t * 1e-3) / 1e9
-    d.free()
     res = {"n": n, "ms": round(t, 5), "GB_s": round(gbs, 1), "hbm_frac": round(gbs / peak, 4),
-           "peak_source": src, "bit_exact": ok, "cold_l2": True, "cfg": best}
+           "peak_source": src, "bit_exact": ok, "cfg": best,
+           "timing": f"{nb} inputs of {4 * n} B ({4 * n * nb} B in all, > 2x L2) reduced in turn, back to back, "
+                     "the launches replayed from a CUDA graph; per-launch time"}
+    ccg = [r for r in table if r[1]["variant"] == gsrb.BAR_CCG]
+    if ccg:
+        res["ccg_ms"] = round(min(r[0] for r in ccg), 5)
+    if not fixed:
+        anyb, tany, _ = tune.tune_reduce(ctx, bufs, n, out)
+        res["tuned_any_shape"] = {"ms": round(tany, 5), "hbm_frac": round(4 * n / (tany * 1e-3) / 1e9 / peak, 4),
+                                  "cfg": anyb}
+    # one launch alone, L2 flushed before it (launch latency and ramp included)
+    single = []
+    for i in range(8):
+        ctx.l2_flush()
+        ctx.record(4)
+        gsrb.check(ctx.reduce_i32(bufs[0], n, out.at(0), c))
+        ctx.record(5)
+        if i >= 3:
+            single.append(ctx.elapsed_ms(4, 5))
+    res["single_launch_cold_us"] = round(statistics.median(single) * 1e3, 2)
+    for bb in bufs:
+        bb.free()
+    a = inputs[0]
     if cpu:
         thr = os.cpu_count() or 1
         t1 = statistics.median(wall(lambda: orc.sum_i32(a))[0] for _ in range(5))
@@ -503,19 +529,46 @@ def sssp_runs(gsrb, ctx, orc, dg, g, deltas, cfg, verify=True):
         res["cpu"] = {"kind": "port", "serial_ms": round(t_cpu * 1e3, 2),
                       "serial_GTEPS": round(m_trav / t_cpu / 1e9, 4), "threads": 1,
                       "sample": "one whole binary-heap Dijkstra from vertex 0 on one core"}
-    for name, delta in deltas:
-        rc, st = dg.sssp(0, out, delta, cfg)
-        gsrb.check(rc, "sssp")
-        rc, st = dg.sssp(0, out, delta, cfg)
-        gsrb.check(rc, "sssp")
+    for name, delta, *rest in deltas:
+        c = rest[0] if rest else cfg  # an arm may bring its own launch configuration (None: the default
+        # one, or the SSSP policy's choice when delta is SSSP_DELTA_LEARNED)
+        ts = []
+        for _ in range(3):
+            rc, st = dg.sssp(0, out, delta, c)
+            gsrb.check(rc, "sssp")
+            ts.append(st.kernel_ms)
+        ms = statistics.median(ts[1:])
         ok = bool(np.array_equal(out.download(), want)) if verify else None
-        res[name] = {"delta": delta, "ms": round(st.kernel_ms, 3),
-                     "GTEPS": round(m_trav / (st.kernel_ms * 1e-3) / 1e9, 3), "rounds": int(st.levels),
+        res[name] = {"delta": int(st.delta), "launch": int(st.launch), "ms": round(ms, 3),
+                     "GTEPS": round(m_trav / (ms * 1e-3) / 1e9, 3), "rounds": int(st.levels),
                      "buckets": int(st.aux), "edges_relaxed": int(st.edges), "bit_exact": ok}
     return res
 
 
-def graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, verify_pr=True, ref_gpu="quick"):
+def train_sssp_policy(gsrb, ctx, pol):
+    """SSSP policy from timed runs of training graphs (not the evaluated ones):
+    every width of policy.SSSP_DELTAS under both launch candidates."""
+    graphs = [gsrb.rmat(s, 16, seed=SEED + 2000 + s) for s in (14, 16, 18, 20, 21)]
+    graphs += [gsrb.grid2d(w, h, seed=SEED + 2100 + w + h, wlo=1, whi=1000)
+               for w, h in ((256, 256), (1024, 64), (512, 512), (1024, 1024), (2048, 256))]
+    X, Y, M, rows = [], [], [], []
+    t0 = time.time()
+    for g in graphs:
+        dg = ctx.graph(g)
+        x, y, m, info = pol.sssp_collect(ctx, dg, reps=1)
+        rows.append({"n": g.nnodes, "m": g.nedges, "delta_label_log2": round(info["y2"], 3),
+                     "launch_label": round(info["y3"], 3)})
+        X.append(x)
+        Y.append(y)
+        M.append(m)
+        dg.free()
+    X, Y, M = np.concatenate(X), np.concatenate(Y), np.concatenate(M)
+    params, hist = pol.sssp_train(ctx, X, Y, M, steps=3000)
+    return params, {"graphs": rows, "rows": int(len(X)), "collect_and_train_s": round(time.time() - t0, 1),
+                    "loss_first": float(hist[0]), "loss_last": float(hist[-1])}
+
+
+def graph_numbers(gsrb, ctx, orc, pol, params, sparams, tune, cache, verify_pr=True, ref_gpu="quick"):
     res = {}
     t0 = time.time()
     rm = gsrb.rmat(22, 16, a=0.57, b=0.19, c=0.19, seed=SEED, wlo=1, whi=255)
@@ -526,7 +579,12 @@ def graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, verify_pr=True, ref_
     cache["bfs_rmat"] = best
     cfg = tune.cfg_from(best)
     res["rmat22"]["bfs"] = bfs_runs(gsrb, ctx, orc, dg, rm, params, cfg, launch=pol.launch_candidates(), cpu=True)
-    res["rmat22"]["sssp"] = sssp_runs(gsrb, ctx, orc, dg, rm, [("reference_delta", 10000), ("delta_256", 256)], cfg)
+    dg.set_sssp_policy(sparams)
+    dg.set_launch_choices(*pol.launch_candidates())
+    res["rmat22"]["sssp"] = sssp_runs(gsrb, ctx, orc, dg, rm, [("learned", gsrb.SSSP_DELTA_LEARNED, None),
+                                                              ("reference_delta", 10000, None),
+                                                              ("reference_delta_tuned_cfg", 10000),
+                                                              ("delta_256", 256, None)], cfg)
     out = ctx.array(rm.nnodes, np.float32)
     rc, st = dg.pagerank(out, 0.85, 50, cfg)
     gsrb.check(rc, "pagerank")
@@ -571,8 +629,12 @@ def graph_numbers(gsrb, ctx, orc, pol, params, tune, cache, verify_pr=True, ref_
     res["grid2048"] = {"n": gr.nnodes, "m": gr.nedges,
                        "bfs": bfs_runs(gsrb, ctx, orc, dg, gr, params, cfg, reps=2, launch=pol.launch_candidates(),
                                        cpu=True)}
-    res["grid2048"]["sssp"] = sssp_runs(gsrb, ctx, orc, dg, gr, [("reference_delta", 10000), ("delta_4096", 4096)],
-                                        cfg)
+    dg.set_sssp_policy(sparams)
+    dg.set_launch_choices(*pol.launch_candidates())
+    res["grid2048"]["sssp"] = sssp_runs(gsrb, ctx, orc, dg, gr, [("learned", gsrb.SSSP_DELTA_LEARNED, None),
+                                                                ("reference_delta", 10000, None),
+                                                                ("reference_delta_tuned_cfg", 10000),
+                                                                ("delta_4096", 4096, None)], cfg)
     dg.free()
     if ref_gpu != "none":
         res["grid2048"]["reference_gpu"] = lonestar_reference(gr, "grid2048", ref_gpu)
@@ -674,7 +736,7 @@ def segment_numbers(gsrb, ctx, orc, tune, cache, k=64, reps=5, fixed=None):
     return res
 
 
-def batch_numbers(gsrb, ctx, orc, params):
+def batch_numbers(gsrb, ctx, orc, params, sparams=None):
     rng = np.random.default_rng(SEED)
     scales = rng.integers(14, 21, 64)
     t0 = time.time()
@@ -769,20 +831,41 @@ def batch_numbers(gsrb, ctx, orc, params):
         ctx.record(9)
         t_plain = ctx.elapsed_ms(8, 9)
     ok_plain = all(np.array_equal(o.download(), w) for o, w in zip(outs, wants_d))
-    ts = []
-    for rep in range(3):
-        ctx.record(10)
-        gsrb.check(b.sssp([0] * 64, outs, 256), "batch sssp")
-        ctx.record(11)
-        ts.append(ctx.elapsed_ms(10, 11))
-    rc, _ = b.stats()
-    gsrb.check(rc, "batch sssp stats")
-    ok_batch = all(np.array_equal(o.download(), w) for o, w in zip(outs, wants_d))
-    t_batch = statistics.median(ts)
+    def batched_sssp(delta):
+        for o in outs:
+            o.zero()
+        ts = []
+        for rep in range(3):
+            ctx.record(10)
+            gsrb.check(b.sssp([0] * 64, outs, delta), "batch sssp")
+            ctx.record(11)
+            ts.append(ctx.elapsed_ms(10, 11))
+        rc, st = b.stats()
+        gsrb.check(rc, "batch sssp stats")
+        ok = all(np.array_equal(o.download(), w) for o, w in zip(outs, wants_d))
+        return statistics.median(ts), ok, st
+
+    t_fixed, ok_fixed, _ = batched_sssp(10000)
+    t_256, ok_256, _ = batched_sssp(256)
     res["sssp"] = {"plain_ms": round(t_plain, 3), "plain_GTEPS": round(m_total / (t_plain * 1e-3) / 1e9, 3),
-                   "plain_bit_exact": ok_plain, "batched_ms": round(t_batch, 3),
-                   "batched_GTEPS": round(m_total / (t_batch * 1e-3) / 1e9, 3), "batched_bit_exact": ok_batch,
-                   "speedup": round(t_plain / t_batch, 3)}
+                   "plain_bit_exact": ok_plain,
+                   "batched_fixed_delta_ms": round(t_fixed, 3),
+                   "batched_fixed_delta_GTEPS": round(m_total / (t_fixed * 1e-3) / 1e9, 3),
+                   "batched_delta256_ms": round(t_256, 3), "batched_bit_exact": ok_fixed and ok_256}
+    t_best, ok_best = t_fixed, ok_fixed
+    if sparams is not None:
+        for dg in dgs:
+            dg.set_sssp_policy(sparams)
+        t_learn, ok_learn, st = batched_sssp(gsrb.SSSP_DELTA_LEARNED)
+        res["sssp"].update({"batched_learned_ms": round(t_learn, 3),
+                            "batched_learned_GTEPS": round(m_total / (t_learn * 1e-3) / 1e9, 3),
+                            "batched_learned_bit_exact": ok_learn,
+                            "learned_vs_fixed_delta": round(t_fixed / t_learn, 3),
+                            "learned_deltas": sorted({int(x.delta) for x in st})})
+        t_best, ok_best = t_learn, ok_learn
+    res["sssp"].update({"batched_ms": round(t_best, 3), "batched_GTEPS": round(m_total / (t_best * 1e-3) / 1e9, 3),
+                        "batched_bit_exact": res["sssp"]["batched_bit_exact"] and ok_best,
+                        "speedup": round(t_plain / t_best, 3)})
     b.free()
     for dg in dgs:
         dg.free()
@@ -989,7 +1072,10 @@ def summarize(detail, peak):
     r = detail.get("reduce_2e24") or {}
     out["C1_reduce_2e24"] = {"us": round(r["ms"] * 1e3, 2) if "ms" in r else None, "GB_s": r.get("GB_s"),
                              "hbm_frac": r.get("hbm_frac"), "bit_exact": r.get("bit_exact"),
-                             "variant": _get(r, "cfg", "variant"),
+                             "variant": _get(r, "cfg", "variant"), "shape": "148x2x256",
+                             "ccg_us": round(r["ccg_ms"] * 1e3, 2) if r.get("ccg_ms") else None,
+                             "tuned_any_shape_hbm_frac": _get(r, "tuned_any_shape", "hbm_frac"),
+                             "single_launch_cold_us": r.get("single_launch_cold_us"),
                              "cpu_serial_GB_s": _get(r, "cpu", "serial_GB_s"), "cpu_mt_GB_s": _get(r, "cpu", "mt_GB_s")}
     if "reduce" in rg:
         out["C1_reduce_reference_programs"] = rg["reduce"]
@@ -1251,10 +1337,12 @@ def main():
                                                                  cpu=dist.rank == 0))
         params, pinfo = timed("policy", lambda: train_policy(gsrb, ctx, pol))
         detail["policy"] = pinfo
-        detail["graphs"] = timed("graphs", lambda: graph_numbers(gsrb, ctx, orc, pol, params, tune, cache,
+        sparams, spinfo = timed("sssp_policy", lambda: train_sssp_policy(gsrb, ctx, pol))
+        detail["sssp_policy"] = spinfo
+        detail["graphs"] = timed("graphs", lambda: graph_numbers(gsrb, ctx, orc, pol, params, sparams, tune, cache,
                                                                  not args.skip_pr_check,
                                                                  ref_gpu=args.reference_programs))
-        detail["batch"] = timed("batch", lambda: batch_numbers(gsrb, ctx, orc, params))
+        detail["batch"] = timed("batch", lambda: batch_numbers(gsrb, ctx, orc, params, sparams))
         detail["segments"] = timed("segments", lambda: segment_numbers(gsrb, ctx, orc, tune, cache))
         if args.reference_programs != "none":
             detail["reference_gpu"] = timed("reference_programs",

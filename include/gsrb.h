@@ -62,7 +62,7 @@ enum {
 };
 
 /* Data-kernel forms (gsrb_cfg_t.form). */
-enum { GSRB_FORM_AUTO = 0, GSRB_FORM_L2 = 1 };
+enum { GSRB_FORM_AUTO = 0, GSRB_FORM_L2 = 1, GSRB_FORM_L1 = 2 };
 
 /* Launch / schedule configuration.  Zero-initialise and call gsrb_cfg_default. */
 typedef struct gsrb_cfg {
@@ -78,8 +78,8 @@ typedef struct gsrb_cfg {
   int32_t launch_mode;   /* 0 = cooperative launch when the driver accepts it, 1 = plain launch (default)
                             (both only after the co-residency check; CCG is always cooperative) */
   int32_t wake_lines;    /* FANOUT / CLUSTER_FANOUT / HIER: wake-up lines the generation is published to (0 = 8) */
-  int32_t form;          /* scan: GSRB_FORM_AUTO (staged in shared memory when the input is 16-byte
-                            aligned and not in place) or GSRB_FORM_L2 (chunks re-read through L2) */
+  int32_t form;          /* pull PageRank: GSRB_FORM_L1 gathers x/deg through L1 (ld.ca), GSRB_FORM_AUTO and
+                            GSRB_FORM_L2 through L2 only (ld.cg); other kernels ignore it */
   int32_t reserved[4];
 } gsrb_cfg_t;
 
@@ -308,8 +308,9 @@ typedef struct gsrb_traversal_stats {
   uint64_t edges;         /* BFS: out-edges of reached vertices (the TEPS numerator);
                              SSSP: edges relaxed */
   float kernel_ms;        /* CUDA-event time of the traversal launch */
-  uint32_t launch;        /* BFS (learned, cfg NULL, launch choices set): 1 + the index of the
+  uint32_t launch;        /* BFS / SSSP (learned, cfg NULL, launch choices set): 1 + the index of the
                              launch configuration the policy picked; else 0 */
+  int32_t delta;          /* SSSP: the bucket width the traversal ran with */
 } gsrb_traversal_stats_t;
 
 /* BFS direction modes. */
@@ -356,9 +357,32 @@ gsrb_status_t gsrb_graph_trace(gsrb_graph_t g, void* h_out, uint32_t max_records
  * cfg == NULL: 2 CTAs x 512 threads per SM. */
 gsrb_status_t gsrb_bfs(gsrb_ctx_t ctx, gsrb_graph_t g, uint32_t src, int32_t* d_level, int32_t mode,
                        const gsrb_cfg_t* cfg, gsrb_traversal_stats_t* stats);
-/* SSSP distances (near-far buckets of width delta) into d_dist (int32[n]). */
+/* SSSP distances (near-far buckets of width delta) into d_dist (int32[n]).
+ * delta == GSRB_SSSP_DELTA_LEARNED: the graph's SSSP policy picks the width
+ * (and, with cfg == NULL and launch choices set, the launch configuration);
+ * GSRB_ERR_STATE without one.  The distances do not depend on either. */
+enum { GSRB_SSSP_DELTA_LEARNED = 0 };
 gsrb_status_t gsrb_sssp(gsrb_ctx_t ctx, gsrb_graph_t g, uint32_t src, int32_t* d_dist, int32_t delta,
                         const gsrb_cfg_t* cfg, gsrb_traversal_stats_t* stats);
+/* The SSSP policy (no counterpart in the reference; the reference runs every
+ * graph with DELTA = 10000, LONESTAR/apps/sssp/support.cu:10, and one launch
+ * shape): the policy network's layout (gsrb_mlp_*), its own weights, evaluated
+ * on the host once per traversal on gsrb_sssp_features of the graph and the
+ * source.  Head 2: log2 of the bucket width over the graph's mean edge weight;
+ * head 3: log2(t0 / t1), the traversal time under launch configuration 0 over
+ * that under configuration 1.  h_weights NULL: forget the policy. */
+gsrb_status_t gsrb_graph_set_sssp_policy(gsrb_graph_t g, const float* h_weights, size_t count);
+/* The policy's plan for an SSSP from src: *delta = round(2^head2 * mean weight)
+ * clamped to [1, 2^30]; *choice = head 3 > 0; scores[2] = {head 2, head 3}
+ * (any output may be NULL).  GSRB_ERR_STATE without an SSSP policy. */
+gsrb_status_t gsrb_graph_sssp_plan(gsrb_graph_t g, uint32_t src, int32_t* delta, int32_t* choice, float* scores);
+/* The 12 features of the SSSP policy: log2 of n, m, mean degree, maximum
+ * degree, the source's degree, mean / maximum / minimum edge weight (each
+ * 1 + x), symmetric (0/1), degree skew, weight spread, log2 n - 2 log2 mean
+ * degree.  The graph form reads the statistics taken when the graph was created. */
+void gsrb_sssp_features(uint32_t n, uint64_t m, uint32_t max_degree, uint32_t src_degree, double w_mean,
+                        int32_t w_min, int32_t w_max, int32_t symmetric, float* h_out12);
+gsrb_status_t gsrb_graph_sssp_features(gsrb_graph_t g, uint32_t src, float* h_out12);
 /* Pull PageRank: x0 = 1 - alpha, `iters` iterations of x = (1-alpha) + alpha * sum x_u/deg(u). */
 gsrb_status_t gsrb_pagerank(gsrb_ctx_t ctx, gsrb_graph_t g, float alpha, int32_t iters, float* d_rank,
                             const gsrb_cfg_t* cfg, gsrb_traversal_stats_t* stats);
@@ -385,7 +409,8 @@ gsrb_status_t gsrb_batch_create(gsrb_ctx_t ctx, const gsrb_graph_t* graphs, int3
 gsrb_status_t gsrb_batch_free(gsrb_batch_t b);
 /* CTA range of every instance (arrays of k, may be NULL). */
 gsrb_status_t gsrb_batch_layout(gsrb_batch_t b, uint32_t* first, uint32_t* count);
-/* Asynchronous: BFS of every instance (d_levels[i] int32[n_i]) / SSSP (d_dists[i]). */
+/* Asynchronous: BFS of every instance (d_levels[i] int32[n_i]) / SSSP (d_dists[i];
+ * delta == GSRB_SSSP_DELTA_LEARNED: every instance the width of its graph's SSSP policy). */
 gsrb_status_t gsrb_batch_bfs(gsrb_batch_t b, const uint32_t* srcs, int32_t* const* d_levels, int32_t mode);
 gsrb_status_t gsrb_batch_sssp(gsrb_batch_t b, const uint32_t* srcs, int32_t* const* d_dists, int32_t delta);
 /* Synchronous: per-instance statistics of the last batched launch (array of k). */

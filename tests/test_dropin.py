@@ -8,6 +8,11 @@ tpds22-artifact_b200/dropin/Makefile builds them from the reference sources
   "Correct sum:";
 * ``scan``: scan/main.cu:23-83 calling ``sum_scan_blelloch()``
   (scan/scan.h:16-18) and comparing with its own ``cpu_sum_scan`` -- "Match: 1";
+* ``allSyncPrims-1kernel``: Heterosync/main.cu with only its four
+  ``#include "cudaLocks*.cu"`` lines (main.cu:15-18) replaced by this library's
+  ``gsrb/cudaLocks.cuh`` -- every kernel of the program calls this library's
+  barriers, mutexes and semaphores under the reference's names, and the
+  program's own golden replay (main.cu:2987-3166) prints "PASSED!";
 * ``{bfs,sssp,pr}_gg``: LONESTAR/skelapp/skel.cu.prehip (options, .gr
   loading, copy to the GPU, output) + apps/<app>/support.cu + rt/src/csr_graph.cu,
   with this library's ``gg_main`` (skel.cu.prehip:12,61) in place of the app's
@@ -23,7 +28,7 @@ import pytest
 
 ROOT = pathlib.Path(__file__).resolve().parents[1]
 DROPIN = ROOT / "tpds22-artifact_b200" / "bin" / "dropin"
-PROGS = ["test_reduce", "scan", "bfs_gg", "sssp_gg", "pr_gg"]
+PROGS = ["test_reduce", "scan", "allSyncPrims-1kernel", "bfs_gg", "sssp_gg", "pr_gg"]
 
 pytestmark = pytest.mark.skipif(not (DROPIN / "test_reduce").exists(),
                                 reason="drop-in programs not built (needs the reference sources)")
@@ -145,3 +150,39 @@ def test_reference_skel_quiet(ctx, dropin_graphs, tmp_path):
     out = tmp_path / "none.txt"
     _run("bfs_gg", ["-q", "-o", out, path], stdin="1\n")
     assert not out.exists()
+
+
+# the reference program's syncPrim names (Heterosync/main.cu:2478-2535)
+HETEROSYNC_PRIMS = [
+    "atomicTreeBarrUniq", "atomicTreeBarrUniqLocalExch", "lfTreeBarrUniq", "lfTreeBarrUniqLocalExch",
+    "spinMutex", "spinMutexEBO", "sleepMutex", "faMutex",
+    "spinSem1", "spinSem2", "spinSem10", "spinSem120", "spinSemEBO1", "spinSemEBO2", "spinSemEBO10",
+    "spinSemEBO120", "PRspinSem1", "PRspinSem2", "PRspinSem10", "PRspinSem120",
+    "spinMutexUniq", "spinMutexEBOUniq", "sleepMutexUniq", "faMutexUniq",
+    "spinSemUniq1", "spinSemUniq2", "spinSemUniq10", "spinSemUniq120", "spinSemEBOUniq1", "spinSemEBOUniq2",
+    "spinSemEBOUniq10", "spinSemEBOUniq120",
+    "atomicTreeBarrUniqSRB", "atomicTreeBarrUniqLocalExchSRB", "atomicTreeBarrUniqNaiveSRB",
+    "atomicTreeBarrUniqLocalExchNaiveSRB", "atomicTreeBarrUniqNaiveAllSRB",
+    "atomicTreeBarrUniqLocalExchNaiveAllSRB", "atomicTreeBarrUniqHybridSRB",
+    "atomicTreeBarrUniqLocalExchHybridSRB", "atomicTreeBarrUniqCCG", "atomicTreeBarrUniqLocalExchCCG"]
+
+
+def test_dropin_heterosync_source_differs_only_in_includes():
+    # the compiled copy is the reference's main.cu with the include lines swapped
+    src = ROOT / "tpds22-artifact_b200" / "build" / "dropin" / "heterosync" / "main.cu"
+    if not src.exists():
+        pytest.skip("scratch copy not present (built elsewhere)")
+    text = src.read_text().splitlines()
+    assert sum("gsrb/cudaLocks.cuh" in line for line in text) == 1
+    assert not any(line.startswith('#include "cudaLocks') for line in text)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prim", HETEROSYNC_PRIMS)
+def test_reference_heterosync_program_on_library(ctx, prim):
+    # 2 CTAs of 32 threads per SM (co-resident), 10 loads/stores, 2 iterations;
+    # the program launches its kernel 10 times and checks its storage array
+    # against its own golden replay
+    p = _run("allSyncPrims-1kernel", [prim, 10, 2 * ctx.num_sms, 2], timeout=300)
+    assert "PASSED!" in p.stdout, (p.stdout + p.stderr)[-3000:]
+    assert re.search(r"elapsed time: [0-9.]+ ms, average: [0-9.]+ ms", p.stdout)

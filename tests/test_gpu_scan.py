@@ -109,14 +109,14 @@ def test_scan_full_size_2e28(gsrb, ctx, orc):
     assert orc.max_rel_err(got[1:], ref[1:]) <= REL_TOL_F32
 
 
-# ---- the two forms explicitly: staged in shared memory (16-byte aligned
-# input, not in place) and re-read through L2 (GSRB_FORM_L2)
-@pytest.mark.parametrize("form", [0, 1])
+# ---- every protocol at sizes around the segment boundaries, and the
+# warp-specialised kernel in place across chunk sizes (one vector to 64 Ki
+# elements) with tails of 1-3 elements
 @pytest.mark.parametrize("variant", [3, 4, 6, 8, 9, 11])
 @pytest.mark.parametrize("n", [1, 7, 4096, 16384 * 148 * 3 + 5, 3_333_333])
-def test_scan_forms_and_variants(gsrb, ctx, orc, form, variant, n):
+def test_scan_variants_segment_edges(gsrb, ctx, orc, variant, n):
     a = gsrb.uniform_i32(n + variant, n, 0, 15).astype(np.uint32)
-    c = gsrb.cfg(variant=variant, ctas_per_sm=1, threads=1024, form=form, wake_lines=4, fanin_groups=16)
+    c = gsrb.cfg(variant=variant, ctas_per_sm=1, threads=1024, wake_lines=4, fanin_groups=16, tile=16384)
     assert np.array_equal(_scan(gsrb, ctx, a, cfg=c), orc.scan_u32(a))
     f = gsrb.uniform_f32(n + 3, n)
     got = _scan(gsrb, ctx, f, f32=True, cfg=c)
@@ -125,10 +125,10 @@ def test_scan_forms_and_variants(gsrb, ctx, orc, form, variant, n):
 
 
 @pytest.mark.parametrize("k,threads,tile", [(1, 1024, 4), (1, 1024, 1000), (1, 512, 8192), (2, 512, 16384),
-                                            (2, 256, 24576), (1, 1024, 25600), (4, 256, 4096), (1, 128, 12)])
-def test_scan_staged_shapes(gsrb, ctx, orc, k, threads, tile):
-    # chunk sizes from one vector to 200 KiB of buffers, tails of 1-3 elements
+                                            (2, 256, 24576), (1, 1024, 65536), (4, 256, 4096), (1, 128, 12)])
+@pytest.mark.parametrize("inplace", [False, True])
+def test_scan_ws_shapes(gsrb, ctx, orc, k, threads, tile, inplace):
     for n in (1_000_003, 148 * k * tile + 2):
         a = gsrb.uniform_i32(n + tile, n, 0, 2**31 - 1).astype(np.uint32) * np.uint32(7)  # wraps
         c = gsrb.cfg(variant=9, ctas_per_sm=k, threads=threads, tile=tile, wake_lines=4)
-        assert np.array_equal(_scan(gsrb, ctx, a, cfg=c), orc.scan_u32(a)), n
+        assert np.array_equal(_scan(gsrb, ctx, a, cfg=c, inplace=inplace), orc.scan_u32(a)), n

@@ -268,3 +268,24 @@ def test_segments_layout(gsrb):
     assert count.tolist() == [1, 1, 8]
     with pytest.raises(gsrb.GsrbError):
         gsrb.segments_layout(np.arange(6, dtype=np.uint64), 4)  # grid < k
+
+
+def test_sssp_labels(pol):
+    # widths within 3 % of the faster configuration's best are averaged in
+    # log2(width / mean weight); the launch label is the clipped log-ratio
+    t = np.array([[9.0, 5.0, 4.0, 4.1, 4.0, 6.0],
+                  [20.0, 10.0, 8.0, 8.0, 8.0, 8.0]])
+    y2, y3 = pol.sssp_labels(t, 128.0)
+    want = np.mean([np.log2(d / 128.0) for d in (1024, 4096, 16384)])
+    assert abs(y2 - want) < 1e-9
+    assert abs(y3 - np.log2(4.0 / 8.0)) < 1e-9
+    y2, y3 = pol.sssp_labels(np.array([[100.0] * 6, [1.0] * 6]), 1.0)
+    assert y3 == 4.0  # clipped
+
+
+def test_sssp_features_host(gsrb):
+    f = np.zeros(12, np.float32)
+    gsrb.lib().gsrb_sssp_features(1 << 20, 16 << 20, 5000, 7, 128.0, 1, 255, 1, f.ctypes.data)
+    assert abs(f[0] - 20.0) < 1e-5 and abs(f[2] - np.log2(17.0)) < 1e-5
+    assert abs(f[4] - 3.0) < 1e-5 and f[8] == 1.0
+    assert abs(f[11] - (f[0] - 2 * f[2])) < 1e-5

@@ -85,7 +85,7 @@ def tune_scan(ctx, d_in, d_out, n: int, reps: int = 3):
     of writers); FLIP and CCG the single-role pipelined one."""
     g = _g()
     table = []
-    for chunk in (24576, 32768, 49152):
+    for chunk in (32768, 49152, 65536):
         for k, threads in ((1, 1024), (2, 512)):
             for cand in (dict(variant=g.BAR_FANOUT, wake_lines=4), dict(variant=g.BAR_HIER, fanin_groups=16, wake_lines=8),
                          dict(variant=g.BAR_FLIP, fanin_groups=1), dict(variant=g.BAR_CCG)):
@@ -97,23 +97,66 @@ def tune_scan(ctx, d_in, d_out, n: int, reps: int = 3):
     return table[0][1], table[0][0], table
 
 
-def tune_reduce(ctx, d_in, n: int, reps: int = 5):
+def reduce_stream_ms(ctx, bufs, n: int, out, c, passes: int = 4):
+    """Per-launch time (ms) of gsrb_reduce_i32 run back to back over the input
+    buffers in turn (launch i reads bufs[i % len(bufs)] and writes
+    out[i % len(bufs)]).  The buffers together are larger than L2, so every
+    launch reads its input from HBM.  The launches are captured once in a CUDA
+    graph and the replay is timed, so the host's call overhead is not in the
+    measured time (each launch's own device-side start-up still is).  One
+    untimed call per buffer first (it also warms the library's caches, so that
+    nothing but the launches is captured)."""
     g = _g()
-    out = ctx.array(1, np.int64)
-    table = []
-    for k, threads, stages in ((1, 1024, 6), (1, 1024, 4), (1, 512, 6), (2, 512, 3), (2, 256, 3)):
-        for cand in (dict(variant=g.BAR_FANOUT, wake_lines=4), dict(variant=g.BAR_FLIP, fanin_groups=1),
-                     dict(variant=g.BAR_CCG)):
-            c = g.cfg(ctas_per_sm=k, threads=threads, tile=stages, **cand)
+    nb = len(bufs)
+    for i in range(nb):
+        if ctx.reduce_i32(bufs[i], n, out.at(i), c):
+            return None
+    if ctx.status()[0] != 0:
+        return None
+    cg = g.CudaGraph(ctx)
+    with cg:
+        for i in range(passes * nb):
+            g.check(ctx.reduce_i32(bufs[i % nb], n, out.at(i % nb), c), "reduce (capture)")
+    try:
+        cg.launch()  # untimed replay
+        ctx.record(40)
+        cg.launch()
+        ctx.record(41)
+        t = ctx.elapsed_ms(40, 41)
+    finally:
+        cg.free()
+    if ctx.status()[0] != 0:
+        return None
+    return t / (passes * nb)
 
-            def run():
-                ctx.l2_flush()
-                return ctx.reduce_i32(d_in, n, out, c)
-            t = _median_ms(ctx, run, reps)
-            if t is not None:
-                table.append((t, dict(cand, ctas_per_sm=k, threads=threads, tile=stages)))
+
+def reduce_candidates(k: int | None = None, threads: int | None = None):
+    """The library's own barrier protocols (and grid.sync for comparison) at
+    the given shape, or over the shapes the reduce supports."""
+    g = _g()
+    shapes = [(k, threads)] if k else [(1, 1024), (1, 512), (2, 512), (2, 256), (4, 256)]
+    out = []
+    for kk, th in shapes:
+        for stages in (0, 2, 1):
+            for cand in (dict(variant=g.BAR_FANOUT, wake_lines=4), dict(variant=g.BAR_FLIP, fanin_groups=1),
+                         dict(variant=g.BAR_HIER, fanin_groups=16, wake_lines=4), dict(variant=g.BAR_CCG)):
+                out.append(dict(cand, ctas_per_sm=kk, threads=th, tile=stages))
+    return out
+
+
+def tune_reduce(ctx, bufs, n: int, out, k: int | None = None, threads: int | None = None, passes: int = 3,
+                library_barrier_only: bool = True):
+    """Fastest configuration by reduce_stream_ms; with library_barrier_only the
+    cooperative-groups barrier is timed but not chosen."""
+    g = _g()
+    table = []
+    for e in reduce_candidates(k, threads):
+        t = reduce_stream_ms(ctx, bufs, n, out, g.cfg(**e), passes)
+        if t is not None:
+            table.append((t, e))
     table.sort(key=lambda x: x[0])
-    return table[0][1], table[0][0], table
+    pick = [r for r in table if not (library_barrier_only and r[1]["variant"] == g.BAR_CCG)]
+    return pick[0][1], pick[0][0], table
 
 
 def segment_candidates(kind: str):

@@ -1016,24 +1016,33 @@ struct PrArgs {
   uint32_t* hub_done;     // [nhubs] finished chunks (monotonic over iterations)
   unsigned long long* ticket;  // block tickets (monotonic over iterations)
   uint32_t* out;
+  int32_t gather_l1;      // 1: x/deg gathers through L1 (ld.ca), 0: L2 only (ld.cg)
 };
+
+// One x/deg gather.  Through L1 the hubs' entries (read by many rows of a
+// power-law graph) hit in the SM; the buffer a gather reads was last written
+// two iterations earlier, before the grid barrier whose acquire orders it.
+__device__ __forceinline__ float pr_gather(const float* cin, uint32_t d, int l1) {
+  return l1 ? __ldca(cin + d) : __ldcg(cin + d);
+}
 
 // Sum of cin[dst[j]] over j in [j0, j1) by one warp: lanes stride the range,
 // 4 independent gathers in flight per lane, FP64 per lane, fixed-order
 // butterfly at the end (the same bits on every run).
 __device__ __forceinline__ double warp_gather_sum(const uint32_t* __restrict__ dst, const float* cin, uint32_t j0,
-                                                  uint32_t j1, uint32_t lane) {
+                                                  uint32_t j1, uint32_t lane, int l1) {
   double s = 0.0;
   uint32_t j = j0 + lane;
   for (; j + 96 < j1; j += 128) {
     const uint32_t d0 = __ldg(dst + j), d1 = __ldg(dst + j + 32), d2 = __ldg(dst + j + 64), d3 = __ldg(dst + j + 96);
-    const float c0 = __ldcg(cin + d0), c1 = __ldcg(cin + d1), c2 = __ldcg(cin + d2), c3 = __ldcg(cin + d3);
+    const float c0 = pr_gather(cin, d0, l1), c1 = pr_gather(cin, d1, l1), c2 = pr_gather(cin, d2, l1),
+                c3 = pr_gather(cin, d3, l1);
     s += (double)c0;
     s += (double)c1;
     s += (double)c2;
     s += (double)c3;
   }
-  for (; j < j1; j += 32) s += (double)__ldcg(cin + __ldg(dst + j));
+  for (; j < j1; j += 32) s += (double)pr_gather(cin, __ldg(dst + j), l1);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   return s;
@@ -1079,7 +1088,7 @@ pagerank_kernel(gsrb::GridBarrier gb, PrArgs a) {
       const uint32_t ub = __ldg(g.row + u), ue = __ldg(g.row + u + 1);
       const uint32_t j0 = ub + (c - c0) * kPrChunk;
       const uint32_t j1 = min(ue, j0 + kPrChunk);
-      const double t = warp_gather_sum(g.dst, cin, j0, j1, lane);
+      const double t = warp_gather_sum(g.dst, cin, j0, j1, lane, a.gather_l1);
       uint32_t last = 0;
       if (lane == 0) {
         a.part[c] = t;
@@ -1150,7 +1159,7 @@ pagerank_kernel(gsrb::GridBarrier gb, PrArgs a) {
 #pragma unroll
         for (int r = 0; r < kRounds; ++r) {
           const uint32_t f = f0 + 32u * r + lane;
-          val[r] = f < E ? (double)__ldcg(cin + nbr[r]) : 0.0;
+          val[r] = f < E ? (double)pr_gather(cin, nbr[r], a.gather_l1) : 0.0;
         }
 #pragma unroll
         for (int r = 0; r < kRounds; ++r) {
@@ -1575,6 +1584,14 @@ struct gsrb_graph {
   uint32_t* lb_own = nullptr;   // [m / kLbChunk + 2] queue entry owning each chunk's first edge
   uint32_t* lb_part = nullptr;  // [kLbMaxCtas] per-CTA edge totals
   bool symmetric = false;       // every edge (u, v) has its reverse (v, u)
+  // graph statistics of the SSSP policy's features (taken when the graph is created)
+  uint32_t max_degree = 0;
+  std::vector<uint32_t> h_row;  // host copy of row_start (source degrees for the host-side policy heads)
+  int32_t w_min = 0, w_max = 0;
+  double w_mean = 0.0;
+  MLPWeights sssp_host{};       // SSSP policy weights (evaluated on the host, once per traversal)
+  bool sssp_set = false;
+  int32_t last_delta = 0;       // bucket width of the last SSSP launched on this graph (0: none)
 };
 
 namespace {
@@ -1633,6 +1650,32 @@ __global__ void __launch_bounds__(256) edge_hash_kernel(DevCSR g, unsigned long 
   }
 }
 
+// Edge-weight statistics: minimum, maximum (as order-preserving unsigned keys)
+// and the int64 sum.  Grid-stride over the weights.
+__global__ void __launch_bounds__(256) edge_weight_stats_kernel(const int32_t* __restrict__ w, uint64_t m,
+                                                                unsigned long long* out) {
+  uint32_t lo = 0xffffffffu, hi = 0;
+  long long sum = 0;
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < m; j += (uint64_t)gridDim.x * blockDim.x) {
+    const int32_t x = w[j];
+    const uint32_t key = (uint32_t)x ^ 0x80000000u;  // signed order as unsigned order
+    lo = min(lo, key);
+    hi = max(hi, key);
+    sum += x;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  }
+  if (lane_id() == 0) {
+    atomicMin(out + 0, (unsigned long long)lo);
+    atomicMax(out + 1, (unsigned long long)hi);
+    atomicAdd(out + 2, (unsigned long long)sum);
+  }
+}
+
 gsrb_status_t graph_scratch(gsrb_graph* G) {
   const size_t n = G->n;
   cudaError_t e = cudaSuccess;
@@ -1658,11 +1701,13 @@ gsrb_status_t graph_scratch(gsrb_graph* G) {
   if (!e) e = dalloc(&G->lb_part, kLbMaxCtas);
   // PageRank hub chunks (degree > kPrHubDegree), built on the host from row_start
   if (!e) {
-    std::vector<uint32_t> hrow(n + 1);
+    std::vector<uint32_t>& hrow = G->h_row;
+    hrow.assign(n + 1, 0u);
     e = cudaMemcpy(hrow.data(), G->row, sizeof(uint32_t) * (n + 1), cudaMemcpyDeviceToHost);
     std::vector<uint32_t> hl, c0, ch;
     for (size_t v = 0; !e && v < n; ++v) {
       const uint32_t d = hrow[v + 1] - hrow[v];
+      if (d > G->max_degree) G->max_degree = d;
       if (d <= kPrHubDegree) continue;
       c0.push_back((uint32_t)ch.size());
       for (uint32_t j = 0; j < d; j += kPrChunk) ch.push_back((uint32_t)hl.size());
@@ -1692,6 +1737,21 @@ gsrb_status_t graph_scratch(gsrb_graph* G) {
     unsigned long long h[4] = {0, 0, 0, 0};
     if (!e) e = cudaMemcpy(h, sums, sizeof h, cudaMemcpyDeviceToHost);
     G->symmetric = h[0] == h[1] && h[2] == h[3];
+  }
+  // edge weights: minimum, maximum, mean
+  if (!e && G->w && G->m) {
+    unsigned long long* st = reinterpret_cast<unsigned long long*>(G->lb_part);
+    const unsigned long long init[3] = {0xffffffffull, 0ull, 0ull};
+    e = cudaMemcpy(st, init, sizeof init, cudaMemcpyHostToDevice);
+    if (!e) {
+      edge_weight_stats_kernel<<<1184, 256>>>(G->w, G->m, st);
+      e = cudaGetLastError();
+    }
+    unsigned long long h[3] = {0, 0, 0};
+    if (!e) e = cudaMemcpy(h, st, sizeof h, cudaMemcpyDeviceToHost);
+    G->w_min = (int32_t)((uint32_t)h[0] ^ 0x80000000u);
+    G->w_max = (int32_t)((uint32_t)h[1] ^ 0x80000000u);
+    G->w_mean = (double)(long long)h[2] / (double)G->m;
   }
   if (!e) e = cudaDeviceSynchronize();
   if (e) return cuda_err(e, "graph scratch");
@@ -1752,6 +1812,7 @@ gsrb_status_t finish_stats(gsrb_graph* G, gsrb_traversal_stats_t* st, float ms) 
     st->kernel_ms = ms;
     st->trace_records = h[4] < G->trace_cap ? h[4] : G->trace_cap;
     st->launch = 0;
+    st->delta = G->last_delta;
   }
   if (h[0]) return GSRB_ERR_OVERFLOW;
   if (h[7]) return GSRB_ERR_TIMEOUT;
@@ -1887,15 +1948,77 @@ gsrb_status_t gsrb_graph_policy_launch(gsrb_graph_t G, uint32_t src, int32_t* ch
   if (!G->mlp_set) return GSRB_ERR_STATE;
   // the first level's features, as the traversal computes them: the frontier
   // is the source, every other vertex and edge is unvisited
-  uint32_t r[2];
-  GSRB_CUDA(cudaMemcpyAsync(r, G->row + src, sizeof(r), cudaMemcpyDeviceToHost, G->ctx->stream));
-  GSRB_CUDA(cudaStreamSynchronize(G->ctx->stream));
-  const uint32_t dsrc = r[1] - r[0];
+  const uint32_t dsrc = G->h_row[src + 1] - G->h_row[src];
   float feat[kFeat], out[kOut];
   level_features(feat, G->n, G->m, 1, 1, dsrc, G->n - 1, (unsigned long long)G->m - dsrc, 1, DIR_PUSH);
   mlp_forward_host(G->mlp_host, feat, out);
   *choice = out[3] > 0.f ? 1 : 0;
   if (score) *score = out[3];
+  return GSRB_OK;
+}
+
+// The SSSP policy's 12 features of a traversal from a source: graph size,
+// degree distribution, edge-weight range and the source's degree (log-scaled).
+static void sssp_features_of(uint32_t n, uint64_t m, uint32_t max_degree, uint32_t src_degree, double w_mean,
+                             int32_t w_min, int32_t w_max, int32_t symmetric, float* f) {
+  const double nn = n ? (double)n : 1.0;
+  const double md = (double)m / nn;
+  f[0] = (float)log2(nn);
+  f[1] = (float)log2(1.0 + (double)m);
+  f[2] = (float)log2(1.0 + md);
+  f[3] = (float)log2(1.0 + (double)max_degree);
+  f[4] = (float)log2(1.0 + (double)src_degree);
+  f[5] = (float)log2(1.0 + (w_mean > 0 ? w_mean : 0.0));
+  f[6] = (float)log2(1.0 + (w_max > 0 ? (double)w_max : 0.0));
+  f[7] = (float)log2(1.0 + (w_min > 0 ? (double)w_min : 0.0));
+  f[8] = symmetric ? 1.f : 0.f;
+  f[9] = f[3] - f[2];            // degree skew
+  f[10] = f[6] - f[5];           // weight spread
+  f[11] = f[0] - 2.f * f[2];     // size against mean degree (high for meshes)
+}
+
+void gsrb_sssp_features(uint32_t n, uint64_t m, uint32_t max_degree, uint32_t src_degree, double w_mean,
+                        int32_t w_min, int32_t w_max, int32_t symmetric, float* h_out12) {
+  sssp_features_of(n, m, max_degree, src_degree, w_mean, w_min, w_max, symmetric, h_out12);
+}
+
+gsrb_status_t gsrb_graph_sssp_features(gsrb_graph_t G, uint32_t src, float* h_out12) {
+  if (!G || !h_out12 || src >= G->n) return GSRB_ERR_ARG;
+  sssp_features_of(G->n, G->m, G->max_degree, G->h_row[src + 1] - G->h_row[src], G->w_mean, G->w_min, G->w_max,
+                   G->symmetric ? 1 : 0, h_out12);
+  return GSRB_OK;
+}
+
+gsrb_status_t gsrb_graph_set_sssp_policy(gsrb_graph_t G, const float* h_weights, size_t count) {
+  if (!G) return GSRB_ERR_ARG;
+  if (!h_weights) {
+    G->sssp_set = false;
+    return GSRB_OK;
+  }
+  if (count != sizeof(MLPWeights) / sizeof(float)) return GSRB_ERR_ARG;
+  memcpy(&G->sssp_host, h_weights, sizeof(MLPWeights));
+  G->sssp_set = true;
+  return GSRB_OK;
+}
+
+gsrb_status_t gsrb_graph_sssp_plan(gsrb_graph_t G, uint32_t src, int32_t* delta, int32_t* choice, float* scores) {
+  if (!G || src >= G->n) return GSRB_ERR_ARG;
+  if (!G->sssp_set) return GSRB_ERR_STATE;
+  float feat[kFeat], out[kOut];
+  gsrb_status_t st = gsrb_graph_sssp_features(G, src, feat);
+  if (st) return st;
+  mlp_forward_host(G->sssp_host, feat, out);
+  // head 2: log2(bucket width / mean edge weight)
+  const double wm = G->w_mean >= 1.0 ? G->w_mean : 1.0;
+  double d = exp2((double)(out[2] < -30.f ? -30.f : (out[2] > 30.f ? 30.f : out[2]))) * wm;
+  if (!(d >= 1.0)) d = 1.0;
+  if (d > 1073741824.0) d = 1073741824.0;
+  if (delta) *delta = (int32_t)llround(d);
+  if (choice) *choice = out[3] > 0.f ? 1 : 0;
+  if (scores) {
+    scores[0] = out[2];
+    scores[1] = out[3];
+  }
   return GSRB_OK;
 }
 
@@ -1958,6 +2081,7 @@ gsrb_status_t gsrb_bfs(gsrb_ctx_t ctx, gsrb_graph_t G, uint32_t src, int32_t* d_
   a.out = G->flags + 4;
   a.out_edges = (unsigned long long*)((char*)G->flags + 64);
   a.solo = G->flags + 8;
+  G->last_delta = 0;
   std::lock_guard<std::mutex> g(ctx->mu);
   GSRB_CUDA(cudaMemsetAsync(G->flags, 0, 128, ctx->stream));
   gsrb::GridBarrier gb = make_barrier(ctx, c, 0, (uint32_t)grid, 0, 0);
@@ -1978,8 +2102,20 @@ gsrb_status_t gsrb_bfs(gsrb_ctx_t ctx, gsrb_graph_t G, uint32_t src, int32_t* d_
 
 gsrb_status_t gsrb_sssp(gsrb_ctx_t ctx, gsrb_graph_t G, uint32_t src, int32_t* d_dist, int32_t delta,
                         const gsrb_cfg_t* cfgin, gsrb_traversal_stats_t* stats) {
-  if (!ctx || !G || !d_dist || src >= G->n || delta <= 0) return GSRB_ERR_ARG;
+  if (!ctx || !G || !d_dist || src >= G->n || delta < 0) return GSRB_ERR_ARG;
   gsrb_cfg_t c = graph_cfg(ctx, cfgin);
+  uint32_t launch = 0;
+  if (delta == GSRB_SSSP_DELTA_LEARNED) {
+    // the SSSP policy picks the bucket width and, without a cfg, the launch
+    // configuration; both change the schedule, never the distances
+    int32_t k = 0;
+    gsrb_status_t st = gsrb_graph_sssp_plan(G, src, &delta, &k, nullptr);
+    if (st) return st;
+    if (!cfgin && G->launch_set) {
+      c = G->launch[k];
+      launch = 1u + (uint32_t)k;
+    }
+  }
   const void* fn = sssp_fn(c.variant);
   if (!fn) return GSRB_ERR_UNSUPPORTED;
   const int grid = grid_of(ctx, c);
@@ -2003,6 +2139,7 @@ gsrb_status_t gsrb_sssp(gsrb_ctx_t ctx, gsrb_graph_t G, uint32_t src, int32_t* d
   a.delta = delta;
   a.out = G->flags + 4;
   a.out_edges = (unsigned long long*)((char*)G->flags + 64);
+  G->last_delta = delta;
   std::lock_guard<std::mutex> g(ctx->mu);
   GSRB_CUDA(cudaMemsetAsync(G->flags, 0, 128, ctx->stream));
   gsrb::GridBarrier gb = make_barrier(ctx, c, 0, (uint32_t)grid, 0, 0);
@@ -2016,7 +2153,9 @@ gsrb_status_t gsrb_sssp(gsrb_ctx_t ctx, gsrb_graph_t G, uint32_t src, int32_t* d
   GSRB_CUDA(cudaEventSynchronize(ctx->events[63]));
   float ms = 0;
   GSRB_CUDA(cudaEventElapsedTime(&ms, ctx->events[62], ctx->events[63]));
-  return finish_stats(G, stats, ms);
+  st = finish_stats(G, stats, ms);
+  if (stats) stats->launch = launch;
+  return st;
 }
 
 gsrb_status_t gsrb_pagerank(gsrb_ctx_t ctx, gsrb_graph_t G, float alpha, int32_t iters, float* d_rank,
@@ -2044,6 +2183,8 @@ gsrb_status_t gsrb_pagerank(gsrb_ctx_t ctx, gsrb_graph_t G, float alpha, int32_t
   a.hub_done = G->hub_done;
   a.ticket = reinterpret_cast<unsigned long long*>(G->flags + 24);
   a.out = G->flags + 4;
+  a.gather_l1 = c.form == GSRB_FORM_L1 ? 1 : 0;
+  G->last_delta = 0;
   std::lock_guard<std::mutex> g(ctx->mu);
   GSRB_CUDA(cudaMemsetAsync(G->flags, 0, 128, ctx->stream));
   if (G->nhubs) GSRB_CUDA(cudaMemsetAsync(G->hub_done, 0, sizeof(uint32_t) * G->nhubs, ctx->stream));
@@ -2087,6 +2228,7 @@ gsrb_status_t gsrb_pagerank_residual(gsrb_ctx_t ctx, gsrb_graph_t G, float alpha
   a.overflow = G->flags;
   a.out = G->flags + 4;
   a.out_edges = (unsigned long long*)((char*)G->flags + 64);
+  G->last_delta = 0;
   std::lock_guard<std::mutex> g(ctx->mu);
   GSRB_CUDA(cudaMemsetAsync(G->flags, 0, 128, ctx->stream));
   gsrb::GridBarrier gb = make_barrier(ctx, c, 0, (uint32_t)grid, 0, 0);
@@ -2178,6 +2320,14 @@ gsrb_status_t batch_launch(gsrb_batch* B, const uint32_t* srcs, int32_t* const* 
   if (kind == 0 && param == GSRB_BFS_LEARNED)
     for (int i = 0; i < k; ++i)
       if (!B->graphs[i]->mlp_set) return GSRB_ERR_STATE;
+  // SSSP with the learned bucket width: every instance its own (host-side
+  // plan from the graph's statistics; nothing is read from the device)
+  std::vector<int32_t> deltas((size_t)k, param);
+  if (kind == 1 && param == GSRB_SSSP_DELTA_LEARNED)
+    for (int i = 0; i < k; ++i) {
+      gsrb_status_t st = gsrb_graph_sssp_plan(B->graphs[i], srcs[i], &deltas[i], nullptr, nullptr);
+      if (st) return st;
+    }
   gsrb_ctx* ctx = B->ctx;
   const void* fn = batch_fn(B->cfg.variant);
   if (!fn) return GSRB_ERR_UNSUPPORTED;
@@ -2191,8 +2341,14 @@ gsrb_status_t batch_launch(gsrb_batch* B, const uint32_t* srcs, int32_t* const* 
     d.first = B->first[i];
     d.count = B->count[i];
     d.kind = (uint32_t)kind;
-    if (kind == 0) d.bfs = bfs_args(B->graphs[i], srcs[i], outs[i], param);
-    else d.sssp = sssp_args(B->graphs[i], srcs[i], outs[i], param);
+    if (kind == 0) {
+      d.bfs = bfs_args(B->graphs[i], srcs[i], outs[i], param);
+      B->graphs[i]->last_delta = 0;
+    }
+    else {
+      d.sssp = sssp_args(B->graphs[i], srcs[i], outs[i], deltas[i]);
+      B->graphs[i]->last_delta = deltas[i];
+    }
     GSRB_CUDA(cudaMemsetAsync(B->graphs[i]->flags, 0, 128, ctx->stream));
   }
   GSRB_CUDA(cudaMemcpyAsync(B->d_desc, B->h_desc, sizeof(BatchDesc) * k, cudaMemcpyHostToDevice, ctx->stream));
@@ -2298,7 +2454,7 @@ gsrb_status_t gsrb_batch_bfs(gsrb_batch_t B, const uint32_t* srcs, int32_t* cons
 }
 
 gsrb_status_t gsrb_batch_sssp(gsrb_batch_t B, const uint32_t* srcs, int32_t* const* d_dists, int32_t delta) {
-  if (delta <= 0) return GSRB_ERR_ARG;
+  if (delta < 0) return GSRB_ERR_ARG;
   return batch_launch(B, srcs, d_dists, 1, delta);
 }
 

@@ -30,6 +30,19 @@ struct gsrb_ctx {
   void* flush = nullptr;
   size_t flush_bytes = 0;
   cudaEvent_t events[64] = {};
+  // co-resident capacity per (kernel, block, dynamic smem, cluster): the
+  // occupancy query and the shared-memory attribute cost microseconds of host
+  // time before every persistent launch, so each shape is asked once
+  struct Coresident {
+    const void* fn;
+    int block;
+    size_t smem;
+    int cluster;
+    int ctas;
+  };
+  std::mutex occ_mu;
+  Coresident occ[64] = {};
+  int occ_n = 0;
 };
 
 namespace gsrbrt {

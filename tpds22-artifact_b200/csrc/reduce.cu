@@ -77,7 +77,6 @@ reduce_i32_kernel(gsrb::GridBarrier gb, const int32_t* __restrict__ in, uint64_t
   __shared__ long long warp_buf[32];
   __shared__ uint64_t full[kMaxStages], empty[kMaxStages];
   gsrb::GridSync<V> bar;
-  const bool ok0 = bar.init(gb, &bsh);
   const uint32_t tid = threadIdx.x, T = blockDim.x, lane = tid & 31u, nwarps = T >> 5;
   const uint64_t G = gridDim.x;
   uint64_t chunk = (n + G - 1) / G;
@@ -99,14 +98,6 @@ reduce_i32_kernel(gsrb::GridBarrier gb, const int32_t* __restrict__ in, uint64_t
   const uint32_t nst = (uint32_t)((nbytes + kStageBytes - 1) / kStageBytes);
   const unsigned char* src = reinterpret_cast<const unsigned char*>(p);
 
-  if (tid == 0) {
-    for (uint32_t i = 0; i < nbuf; ++i) {
-      gsrb::ptx::mbar_init(&full[i], 1);
-      gsrb::ptx::mbar_init(&empty[i], nwarps);
-    }
-    gsrb::ptx::fence_mbar_init();
-  }
-  __syncthreads();
   auto bytes_of = [&](uint32_t k) {
     return (uint32_t)min((uint64_t)kStageBytes, nbytes - (uint64_t)k * kStageBytes);
   };
@@ -115,9 +106,24 @@ reduce_i32_kernel(gsrb::GridBarrier gb, const int32_t* __restrict__ in, uint64_t
     gsrb::ptx::mbar_arrive_expect_tx(&full[buf], bytes_of(k));
     gsrb::ptx::bulk_g2s(stage + (size_t)buf * kStageBytes, src + (size_t)k * kStageBytes, bytes_of(k), &full[buf]);
   };
-  if (tid == 0 && ok0)
-    for (uint32_t k = 0; k < nst && k < nbuf; ++k) issue(k);
+  // The first copies go out before the barrier's set-up reads (two dependent
+  // L2 round trips): they only read the input.  Whatever the set-up decides,
+  // every issued copy is waited for below before the CTA leaves.
+  uint32_t issued = 0;
+  if (tid == 0) {
+    for (uint32_t i = 0; i < nbuf; ++i) {
+      gsrb::ptx::mbar_init(&full[i], 1);
+      gsrb::ptx::mbar_init(&empty[i], nwarps);
+    }
+    gsrb::ptx::fence_mbar_init();
+    for (; issued < nst && issued < nbuf; ++issued) issue(issued);
+  }
+  const bool ok0 = bar.init(gb, &bsh);  // its __syncthreads also publishes the mbarrier set-up
   bool ok = ok0;
+  if (!ok0 && tid == 0) {
+    // refused to start (a recorded error): leave no copy in flight
+    for (uint32_t k = 0; k < issued; ++k) mbar_wait_bounded(&full[k % nbuf], (k / nbuf) & 1u, gb);
+  }
   if (ok0) {
     // No CTA-wide barrier per stage: each warp frees a stage on `empty` when
     // it has read its part; thread 0 refills a stage once every warp has.

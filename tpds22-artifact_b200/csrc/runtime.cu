@@ -18,6 +18,10 @@ std::atomic<uint64_t> g_launches{0};
 
 gsrb_status_t cuda_err(cudaError_t e, const char* what) {
   if (getenv("GSRB_VERBOSE")) fprintf(stderr, "[gsrb] %s failed: %s\n", what, cudaGetErrorString(e));
+  // a failed call that did not break the context leaves its code as the
+  // thread's last error: clear it, so that the next entry point's own checks
+  // do not report this failure again (a sticky error stays and is reported)
+  (void)cudaGetLastError();
   if (e == cudaErrorMemoryAllocation) return GSRB_ERR_NOMEM;
   if (e == cudaErrorCooperativeLaunchTooLarge) return GSRB_ERR_NOT_CORESIDENT;
   return GSRB_ERR_CUDA;
@@ -105,9 +109,42 @@ gsrb::GridBarrier make_barrier(gsrb_ctx* ctx, const gsrb_cfg_t& c, int slot, uin
   return gb;
 }
 
+static gsrb_status_t coresident_query(gsrb_ctx* ctx, const void* fn, int block, size_t smem, int cluster,
+                                      int* ctas);
+
 gsrb_status_t coresident_ctas(gsrb_ctx* ctx, const void* fn, int block, size_t smem, int cluster,
                               int* ctas) {
-  if (smem > 48 * 1024) GSRB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  {
+    std::lock_guard<std::mutex> g(ctx->occ_mu);
+    for (int i = 0; i < ctx->occ_n; ++i) {
+      const gsrb_ctx::Coresident& e = ctx->occ[i];
+      if (e.fn == fn && e.block == block && e.smem == smem && e.cluster == cluster) {
+        *ctas = e.ctas;
+        return GSRB_OK;
+      }
+    }
+  }
+  gsrb_status_t st = coresident_query(ctx, fn, block, smem, cluster, ctas);
+  if (st) return st;
+  std::lock_guard<std::mutex> g(ctx->occ_mu);
+  // a full table starts over (the shapes in use are few)
+  if (ctx->occ_n == (int)(sizeof(ctx->occ) / sizeof(ctx->occ[0]))) ctx->occ_n = 0;
+  ctx->occ[ctx->occ_n++] = {fn, block, smem, cluster, *ctas};
+  return GSRB_OK;
+}
+
+static gsrb_status_t coresident_query(gsrb_ctx* ctx, const void* fn, int block, size_t smem, int cluster,
+                                      int* ctas) {
+  // raise the kernel's dynamic shared-memory limit to what the device allows
+  // next to the kernel's static shared memory (a limit set to this launch's
+  // size could be below a later, cached shape's)
+  if (smem > 48 * 1024) {
+    cudaFuncAttributes fa;
+    GSRB_CUDA(cudaFuncGetAttributes(&fa, fn));
+    int lim = ctx->max_smem_optin - (int)fa.sharedSizeBytes;
+    if (lim < (int)smem) lim = (int)smem;  // too large: the call below reports it
+    GSRB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+  }
   if (cluster <= 1) {
     int nb = 0;
     GSRB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, block, smem));

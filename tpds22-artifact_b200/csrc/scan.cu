@@ -550,227 +550,6 @@ scan_ws_kernel(gsrb::GridBarrier gb, const typename ScanT<F32>::Elem* __restrict
   bar.finish();
 }
 
-// ---------------------------------------------------------------------------
-// Shared-memory-staged form (16-byte aligned input).  Each CTA keeps `nbuf`
-// chunk buffers in shared memory; thread 0 fills them with bulk copies
-// (cp.async.bulk global->shared, completion on a "full" mbarrier per buffer,
-// no multicast) up to nbuf - 1 segments ahead of the one being scanned.  Per
-// segment s: every warp sums its slice of the staged chunk, the CTA publishes
-// its partial and syncs on the grid barrier, reads the partials of the CTAs
-// before it, rescans its slice from shared memory and streams it out; the
-// buffer is then refilled with segment s + nbuf.  HBM sees each element read
-// once and written once and nothing is re-read through L2; the bulk copies of
-// the next segments stay in flight across the barrier's latency.
-constexpr uint32_t kSmMaxBufs = 4;
-constexpr uint32_t kSmPiece = 16384;  // bytes per bulk copy (several in flight per buffer)
-
-// Bounded wait on an mbarrier phase; records a timeout in the barrier's status
-// word and returns false when the deadline passes.
-__device__ __forceinline__ bool sm_mbar_wait(uint64_t* mbar, uint32_t parity, const gsrb::GridBarrier& gb,
-                                             uint32_t where) {
-  uint64_t t0 = 0;
-  for (uint32_t it = 0;; ++it) {
-    if (gsrb::ptx::mbar_try_wait(mbar, parity)) return true;
-    if ((it & 63u) == 63u) {
-      const uint64_t now = gsrb::ptx::globaltimer_ns();
-      if (t0 == 0) t0 = now;
-      else if (now - t0 > gb.timeout_ns) {
-        gsrb::detail::record_error(gb, gsrb::GSRB_DEV_TIMEOUT, where);
-        return false;
-      }
-    }
-  }
-}
-
-template <int V, bool F32>
-__global__ void __launch_bounds__(1024, 1)
-scan_sm_kernel(gsrb::GridBarrier gb, const typename ScanT<F32>::Elem* __restrict__ in,
-               typename ScanT<F32>::Elem* __restrict__ out, uint64_t n, uint32_t chunk, uint32_t nbuf,
-               unsigned long long* __restrict__ partials, int vec_out) {
-  using Elem = typename ScanT<F32>::Elem;
-  using Acc = typename ScanT<F32>::Acc;
-  using Vec = typename ScanT<F32>::Vec;
-  extern __shared__ __align__(128) unsigned char sm_raw[];
-  __shared__ gsrb::BarrierShared bsh;
-  __shared__ uint64_t full[kSmMaxBufs];
-  __shared__ Acc s_wsum[32], s_red[2][32], s_bcast[2];
-  __shared__ uint32_t s_fail;
-
-  const uint32_t tid = threadIdx.x, lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
-  const uint32_t G = gridDim.x, b = blockIdx.x;
-  const uint64_t pol_drop = l2_policy_evict_first();
-  Elem* stage = reinterpret_cast<Elem*>(sm_raw);
-  gsrb::GridSync<V> bar;
-  bool ok = bar.init(gb, &bsh);
-  const uint64_t seg = (uint64_t)G * chunk;
-  const uint64_t nseg = (n + seg - 1) / seg;
-
-  // thread 0: stage this CTA's chunk of segment s into buffer s % nbuf
-  auto issue = [&](uint64_t s) {
-    const uint32_t buf = (uint32_t)(s % nbuf);
-    const TileGeom t = tile_of(s, n, G, chunk, b);
-    Elem* dst = stage + (size_t)buf * chunk;
-    const uint32_t vbytes = (t.cnt >> 2) * 16u;
-    // the 0-3 elements past the last whole vector with plain loads
-    for (uint32_t e = t.cnt & ~3u; e < t.cnt; ++e) dst[e] = in[t.beg + e];
-    if (vbytes == 0) {
-      gsrb::ptx::mbar_arrive(&full[buf]);
-      return;
-    }
-    gsrb::ptx::mbar_arrive_expect_tx(&full[buf], vbytes);
-    const unsigned char* src = reinterpret_cast<const unsigned char*>(in + t.beg);
-    for (uint32_t o = 0; o < vbytes; o += kSmPiece)
-      gsrb::ptx::bulk_g2s(reinterpret_cast<unsigned char*>(dst) + o, src + o, min(kSmPiece, vbytes - o), &full[buf]);
-  };
-
-  if (tid == 0) {
-    for (uint32_t i = 0; i < nbuf; ++i) gsrb::ptx::mbar_init(&full[i], 1);
-    gsrb::ptx::fence_mbar_init();
-    s_fail = ok ? 0u : 1u;
-  }
-  __syncthreads();
-  uint64_t issued = 0;  // thread 0: segments whose copies were issued
-  if (tid == 0 && ok)
-    for (; issued < nseg && issued < nbuf; ++issued) issue(issued);
-
-  Acc carry = Acc(0);
-  uint64_t s = 0;
-  for (; ok && s < nseg; ++s) {
-    const uint32_t buf = (uint32_t)(s % nbuf);
-    const uint32_t par = (uint32_t)((s / nbuf) & 1u);
-    const TileGeom t = tile_of(s, n, G, chunk, b);
-    const Elem* src = stage + (size_t)buf * chunk;
-    // every thread observes the buffer's completion itself (acquire of the
-    // async-proxy writes); the tail elements were written before the
-    // __syncthreads that ended the previous segment
-    if (!sm_mbar_wait(&full[buf], par, gb, 0xfffffff3u)) s_fail = 1u;
-    const uint32_t nvec = (t.cnt + 3u) >> 2;
-    const uint32_t vpw = (nvec + nw - 1) / nw;
-    const uint32_t v0 = min(nvec, w * vpw), v1 = min(nvec, v0 + vpw);
-    auto vec_at = [&](uint32_t v) {
-      Vec x;
-      const uint32_t e = 4u * v;
-      if (e + 3u < t.cnt) {
-        x = *reinterpret_cast<const Vec*>(src + e);
-      } else {
-        Elem y[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) y[k] = (e + k < t.cnt) ? src[e + k] : Elem(0);
-        x.x = y[0];
-        x.y = y[1];
-        x.z = y[2];
-        x.w = y[3];
-      }
-      return x;
-    };
-    // chunk sum: warp totals -> exclusive warp offsets, the CTA's partial
-    Acc lsum = Acc(0);
-    for (uint32_t v = v0 + lane; v < v1; v += 32u) lsum += vsum(vec_at(v));
-    const Acc wt = warp_sum(lsum);
-    if (lane == 0) s_wsum[w] = wt;
-    __syncthreads();
-    if (s_fail) {
-      ok = false;
-      break;
-    }
-    if (tid == 0) {
-      Acc run = Acc(0);
-      for (uint32_t i = 0; i < nw; ++i) {
-        const Acc x = s_wsum[i];
-        s_wsum[i] = run;
-        run += x;
-      }
-      __stcg(&partials[(s & 1) * G + b], (unsigned long long)acc_bits(run));
-    }
-    ok = bar.sync();
-    if (!ok) break;
-    // offset = carry + sum of the partials of the CTAs before b
-    Acc pre = Acc(0), tot = Acc(0);
-    for (uint32_t j = tid; j < G; j += blockDim.x) {
-      Acc x;
-      acc_from(__ldcg(&partials[(s & 1) * G + j]), x);
-      tot += x;
-      if (j < b) pre += x;
-    }
-    pre = warp_sum(pre);
-    tot = warp_sum(tot);
-    if (lane == 0) {
-      s_red[0][w] = pre;
-      s_red[1][w] = tot;
-    }
-    __syncthreads();
-    if (tid == 0) {
-      Acc p = Acc(0), q = Acc(0);
-      for (uint32_t i = 0; i < nw; ++i) {
-        p += s_red[0][i];
-        q += s_red[1][i];
-      }
-      s_bcast[0] = p;
-      s_bcast[1] = q;
-    }
-    __syncthreads();
-    Acc run = carry + s_bcast[0] + s_wsum[w];
-    carry += s_bcast[1];
-    // rescan the slice from shared memory, 32 vectors (128 elements) per round
-    for (uint32_t r0 = v0; r0 < v1; r0 += 32u) {
-      const uint32_t v = r0 + lane;
-      const Vec x = v < v1 ? vec_at(v) : Vec{};
-      const Elem a0 = x.x, a1 = a0 + x.y, a2 = a1 + x.z, a3 = a2 + x.w;
-      const Elem lt = a3;
-      Elem incl = lt;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const Elem y = shfl_up(incl, o);
-        if ((int)lane >= o) incl += y;
-      }
-      const Acc e0 = run + Acc(incl - lt);
-      Vec y;
-      y.x = Elem(e0);
-      y.y = Elem(e0 + Acc(a0));
-      y.z = Elem(e0 + Acc(a1));
-      y.w = Elem(e0 + Acc(a2));
-      const uint32_t e = 4u * v;
-      if (v < v1) {
-        if (vec_out && e + 3u < t.cnt) {
-          st_hint(reinterpret_cast<Vec*>(out + t.beg + e), y, pol_drop);
-        } else {
-          const Elem ys[4] = {y.x, y.y, y.z, y.w};
-#pragma unroll
-          for (int q = 0; q < 4; ++q)
-            if (e + q < t.cnt) out[t.beg + e + q] = ys[q];
-        }
-      }
-      run += Acc(shfl_idx(incl, 31));
-    }
-    // every thread is done with the buffer (and with s_wsum): refill it
-    __syncthreads();
-    if (tid == 0 && issued < nseg) issue(issued++);
-  }
-  // leave no bulk copy in flight into this CTA's shared memory
-  if (tid == 0) {
-    for (uint64_t k = s; k < issued; ++k) {
-      const uint32_t buf = (uint32_t)(k % nbuf);
-      const uint32_t par = (uint32_t)((k / nbuf) & 1u);
-      if (!sm_mbar_wait(&full[buf], par, gb, 0xfffffff4u)) break;
-    }
-  }
-  __syncthreads();
-  bar.finish();
-}
-
-template <bool F32>
-const void* scan_sm_fn_t(int variant) {
-  switch (variant) {
-    case gsrb::V_SOFT2: return (const void*)scan_sm_kernel<gsrb::V_SOFT2, F32>;
-    case gsrb::V_FLAT: return (const void*)scan_sm_kernel<gsrb::V_FLAT, F32>;
-    case gsrb::V_CCG: return (const void*)scan_sm_kernel<gsrb::V_CCG, F32>;
-    case gsrb::V_FLIP: return (const void*)scan_sm_kernel<gsrb::V_FLIP, F32>;
-    case gsrb::V_FANOUT: return (const void*)scan_sm_kernel<gsrb::V_FANOUT, F32>;
-    case gsrb::V_HIER: return (const void*)scan_sm_kernel<gsrb::V_HIER, F32>;
-    default: return nullptr;
-  }
-}
-
 template <bool F32>
 const void* scan_ws_fn_t(int variant) {
   switch (variant) {
@@ -798,8 +577,6 @@ const void* scan_fn_t(int variant) {
 }
 
 constexpr uint32_t kDefaultChunk = 32768;  // elements per CTA per segment (128 KiB; a segment of 148 is 19 MiB)
-constexpr uint32_t kDefaultSmChunk = 16384;  // staged form: 64 KiB per buffer, three buffers per SM
-constexpr size_t kSmBudget = 200u * 1024u;   // staged form: shared memory per SM for the buffers
 
 gsrb_status_t scan_launch(gsrb_ctx_t ctx, const void* d_in, void* d_out, size_t n, const gsrb_cfg_t* cfgin,
                           bool f32) {
@@ -815,6 +592,13 @@ gsrb_status_t scan_launch(gsrb_ctx_t ctx, const void* d_in, void* d_out, size_t 
   }
   if (c.threads % 128 || c.threads > 1024) return GSRB_ERR_ARG;
   if (n == 0) return GSRB_OK;
+  // barriers with a thread-level split protocol run the warp-specialised form
+  const void* fn = f32 ? scan_ws_fn_t<true>(c.variant) : scan_ws_fn_t<false>(c.variant);
+  if (!fn) fn = f32 ? scan_fn_t<true>(c.variant) : scan_fn_t<false>(c.variant);
+  if (!fn) return GSRB_ERR_UNSUPPORTED;
+  uint32_t tile = c.tile > 0 ? (uint32_t)c.tile : kDefaultChunk;
+  tile = (tile + 3) & ~3u;
+  const size_t smem = 0;
   const int grid = grid_of(ctx, c);
   if (grid % c.cluster) return GSRB_ERR_ARG;
   void* part = nullptr;
@@ -825,29 +609,6 @@ gsrb_status_t scan_launch(gsrb_ctx_t ctx, const void* d_in, void* d_out, size_t 
   unsigned long long* partials = (unsigned long long*)part;
   int in_bulk = ((uintptr_t)d_in & 15u) == 0;
   int out_bulk = ((uintptr_t)d_out & 15u) == 0;
-  // the shared-memory-staged form needs bulk copies (16-byte aligned input)
-  // and is not used in place (the rescan would race with the refills' sources)
-  const void* fn = nullptr;
-  if (c.form != GSRB_FORM_L2 && in_bulk && d_in != d_out && c.cluster == 1)
-    fn = f32 ? scan_sm_fn_t<true>(c.variant) : scan_sm_fn_t<false>(c.variant);
-  uint32_t chunk = c.tile > 0 ? (uint32_t)c.tile : kDefaultSmChunk;
-  chunk = (chunk + 3) & ~3u;
-  const uint32_t kps = c.ctas_per_sm > 0 ? (uint32_t)c.ctas_per_sm : 1u;
-  uint32_t nbuf = (uint32_t)((kSmBudget / kps) / ((size_t)chunk * sizeof(uint32_t)));
-  if (nbuf > kSmMaxBufs) nbuf = kSmMaxBufs;
-  if (nbuf < 2) fn = nullptr;  // chunk too large for two buffers per CTA: the L2 forms
-  if (fn) {
-    const size_t smem = (size_t)nbuf * chunk * sizeof(uint32_t);
-    void* args[] = {&gb, (void*)&d_in, &d_out, &n64, &chunk, &nbuf, &partials, &out_bulk};
-    return launch_persistent(ctx, fn, grid, c.threads, smem, c.cluster, coop_of(c), args);
-  }
-  // barriers with a thread-level split protocol run the warp-specialised form
-  fn = f32 ? scan_ws_fn_t<true>(c.variant) : scan_ws_fn_t<false>(c.variant);
-  if (!fn) fn = f32 ? scan_fn_t<true>(c.variant) : scan_fn_t<false>(c.variant);
-  if (!fn) return GSRB_ERR_UNSUPPORTED;
-  uint32_t tile = c.tile > 0 ? (uint32_t)c.tile : kDefaultChunk;
-  tile = (tile + 3) & ~3u;
-  const size_t smem = 0;
   void* args[] = {&gb, (void*)&d_in, &d_out, &n64, &tile, &partials, &in_bulk, &out_bulk};
   return launch_persistent(ctx, fn, grid, c.threads, smem, c.cluster, coop_of(c), args);
 }

@@ -52,6 +52,8 @@ BAR_LOCKFREE = 12
 BAR_NONE = 99
 FORM_AUTO = 0
 FORM_L2 = 1
+FORM_L1 = 2
+SSSP_DELTA_LEARNED = 0
 VARIANT_NAMES = {
     BAR_CLUSTER: "gsrb_cluster",
     BAR_CLUSTER_ALLPOLL: "gsrb_cluster_allpoll",
@@ -166,6 +168,11 @@ _SIGS = {
     "gsrb_graph_info": (C.c_int32, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
     "gsrb_graph_is_symmetric": (C.c_int32, [_P, C.POINTER(C.c_int32)]),
     "gsrb_graph_set_policy": (C.c_int32, [_P, _P, C.c_size_t]),
+    "gsrb_graph_set_sssp_policy": (C.c_int32, [_P, _P, C.c_size_t]),
+    "gsrb_graph_sssp_plan": (C.c_int32, [_P, C.c_uint32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _P]),
+    "gsrb_graph_sssp_features": (C.c_int32, [_P, C.c_uint32, _P]),
+    "gsrb_sssp_features": (None, [C.c_uint32, C.c_uint64, C.c_uint32, C.c_uint32, C.c_double, C.c_int32,
+                                  C.c_int32, C.c_int32, _P]),
     "gsrb_graph_set_launch_choices": (C.c_int32, [_P, C.POINTER(Cfg), C.POINTER(Cfg)]),
     "gsrb_graph_policy_launch": (C.c_int32, [_P, C.c_uint32, C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
     "gsrb_graph_trace": (C.c_int32, [_P, _P, C.c_uint32, C.POINTER(C.c_uint32)]),
@@ -202,7 +209,7 @@ BFS_FLAG_LB = 0x100  # OR-ed into a mode: load-balanced expansion of large push 
 class TraversalStats(C.Structure):
     _fields_ = [("levels", C.c_uint32), ("aux", C.c_uint32), ("decisions", C.c_uint32),
                 ("trace_records", C.c_uint32), ("edges", C.c_uint64), ("kernel_ms", C.c_float),
-                ("launch", C.c_uint32)]
+                ("launch", C.c_uint32), ("delta", C.c_int32)]
 
 
 TRACE_DTYPE = np.dtype([("level", "<u4"), ("dir", "<u4"), ("nf", "<u4"), ("nu", "<u4"), ("mf", "<u8"),
@@ -269,6 +276,13 @@ def _ptr(a: np.ndarray) -> int:
     return a.ctypes.data
 
 
+class ElementRef:
+    """A device address inside a DeviceArray (not an allocation of its own)."""
+
+    def __init__(self, ptr: int, dtype):
+        self.ptr, self.dtype = ptr, np.dtype(dtype)
+
+
 class DeviceArray:
     """A device allocation with a numpy dtype and shape (plumbing only)."""
 
@@ -299,6 +313,11 @@ class DeviceArray:
     def zero(self):
         check(_lib().gsrb_memset(self.ctx.h, self.ptr, 0, self.nbytes), "memset")
         return self
+
+    def at(self, i: int) -> "ElementRef":
+        """The device address of element i (for entry points that take a pointer)."""
+        assert 0 <= i < self.size
+        return ElementRef(self.ptr + i * self.dtype.itemsize, self.dtype)
 
     def free(self):
         if self.ptr:
@@ -486,6 +505,27 @@ class DeviceGraph:
         for learned traversals run without a cfg (None, None: forget them)."""
         check(_lib().gsrb_graph_set_launch_choices(self.h, C.byref(c0) if c0 is not None else None,
                                                    C.byref(c1) if c1 is not None else None), "set_launch_choices")
+
+    def set_sssp_policy(self, weights: np.ndarray | None):
+        """Weights of the SSSP policy (None: forget it); gsrb_sssp with delta
+        SSSP_DELTA_LEARNED then runs the width (and launch) it plans."""
+        if weights is None:
+            check(_lib().gsrb_graph_set_sssp_policy(self.h, None, 0), "set_sssp_policy")
+            return
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        check(_lib().gsrb_graph_set_sssp_policy(self.h, w.ctypes.data, w.size), "set_sssp_policy")
+
+    def sssp_plan(self, src: int = 0):
+        """(bucket width, launch choice, head 2, head 3) of the SSSP policy for a traversal from src."""
+        d, k = C.c_int32(), C.c_int32()
+        sc = np.zeros(2, np.float32)
+        check(_lib().gsrb_graph_sssp_plan(self.h, src, C.byref(d), C.byref(k), sc.ctypes.data), "sssp_plan")
+        return int(d.value), int(k.value), float(sc[0]), float(sc[1])
+
+    def sssp_features(self, src: int = 0) -> np.ndarray:
+        out = np.zeros(12, np.float32)
+        check(_lib().gsrb_graph_sssp_features(self.h, src, out.ctypes.data), "sssp_features")
+        return out
 
     def policy_launch(self, src: int = 0):
         """(choice, head 3) of the policy for a BFS from src."""

@@ -253,3 +253,68 @@ def save(path, params: np.ndarray):
 
 def load(path) -> np.ndarray:
     return np.load(path).astype(np.float32)
+
+
+# ---------------------------------------------------------------- SSSP policy
+# The SSSP policy uses the same network layout with its own weights, evaluated
+# on the host once per traversal (gsrb_graph_sssp_plan):
+#   head 2: log2(bucket width / mean edge weight)   (squared error)
+#   head 3: log2(t0 / t1) over the two launch configurations (squared error)
+# Labels come from timed SSSP runs of each training graph: every width of
+# SSSP_DELTAS under both launch configurations.  Heads 0-1 are masked out.
+SSSP_DELTAS = (64, 256, 1024, 4096, 16384, 65536)
+SSSP_SOURCES = 8
+SSSP_NEAR_BEST = 1.03
+
+
+def sssp_times(ctx, dgraph, cfgs, src: int = 0, deltas=SSSP_DELTAS, reps: int = 2) -> np.ndarray:
+    """t[k, j]: fastest of `reps` SSSP kernel times (ms) under launch
+    configuration k and bucket width deltas[j]."""
+    g = _g()
+    out = ctx.array(dgraph.n, np.int32)
+    t = np.full((len(cfgs), len(deltas)), np.inf)
+    for k, c in enumerate(cfgs):
+        for j, d in enumerate(deltas):
+            for _ in range(reps):
+                rc, st = dgraph.sssp(src, out, int(d), c)
+                g.check(rc, "sssp (policy labels)")
+                t[k, j] = min(t[k, j], float(st.kernel_ms))
+    out.free()
+    return t
+
+
+def sssp_labels(t: np.ndarray, mean_w: float, deltas=SSSP_DELTAS):
+    """(head 2 label, head 3 label) from a time table: the launch label is the
+    log-ratio of the two configurations' best times; the width label the mean
+    log2(width / mean weight) of the widths within 3 % of the best under the
+    faster configuration (the time is flat over a range of widths)."""
+    best_k = t.min(axis=1)
+    k = int(np.argmin(best_k))
+    near = [j for j in range(t.shape[1]) if t[k, j] <= SSSP_NEAR_BEST * best_k[k]]
+    y2 = float(np.mean([np.log2(deltas[j] / max(mean_w, 1.0)) for j in near]))
+    y3 = float(np.clip(np.log2(max(best_k[0], 1e-6) / max(best_k[1], 1e-6)), -4.0, 4.0))
+    return y2, y3
+
+
+def sssp_collect(ctx, dgraph, cfgs=None, src: int = 0, reps: int = 2):
+    """Training rows of one graph: the SSSP features of SSSP_SOURCES sources
+    (src and a seeded sample), all with the graph's labels."""
+    cfgs = cfgs or launch_candidates()
+    t = sssp_times(ctx, dgraph, cfgs, src, reps=reps)
+    f0 = dgraph.sssp_features(src)
+    mean_w = float(2.0 ** f0[5] - 1.0)
+    y2, y3 = sssp_labels(t, mean_w)
+    rng = np.random.default_rng(int(dgraph.n) * 7919 + int(dgraph.m))
+    srcs = [src] + [int(x) for x in rng.integers(0, dgraph.n, SSSP_SOURCES - 1)]
+    X = np.stack([dgraph.sssp_features(s) for s in srcs]).astype(np.float32)
+    Y = np.zeros((len(srcs), 4), np.float32)
+    M = np.zeros((len(srcs), 4), np.float32)
+    Y[:, 2], Y[:, 3] = y2, y3
+    M[:, 2], M[:, 3] = 1.0, LAUNCH_WEIGHT / 4.0
+    return X, Y, M, {"times_ms": t, "mean_w": mean_w, "y2": y2, "y3": y3}
+
+
+def sssp_train(ctx, X, Y, M, steps: int = 3000, lr: float = 3e-3, seed: int = 2023):
+    """Adam on the GPU (gsrb_mlp_train); returns (params, loss history)."""
+    g = _g()
+    return g.mlp_train(ctx, g.mlp_init(seed), X, Y, M, steps=steps, lr=lr)
