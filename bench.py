@@ -922,9 +922,11 @@ def reference_gpu_numbers(gsrb, ctx, mode="quick"):
     out = {"programs": "baseline/_ref, the reference's sources compiled for sm_100a", "mode": mode,
            "slow_shapes_recorded": REF_SLOW_SHAPES}
     iters = 10000 if mode == "full" else 1000
-    # Heterosync barriers: one barrier per iteration, NUM_LDST = 1, 10 launches averaged
+    # Heterosync barriers: one barrier per iteration, NUM_LDST = 1, 10 launches
+    # averaged; quick mode at full residency only (each run of the program also
+    # spends seconds in its cudaLocksInit, one cudaMemset per mutex word)
     het = []
-    for k in (1, 8):
+    for k in ((1, 8) if mode == "full" else (8,)):
         ntb = 148 * k
         row = {"ctas": ntb, "threads": 32, "iterations": iters}
         for name, prim in (("gsrb", "atomicTreeBarrUniqSRB"), ("gcpusrb", "atomicTreeBarrUniqNaiveSRB"),
