@@ -599,6 +599,15 @@ def graph_numbers(gsrb, ctx, orc, pol, params, sparams, tune, cache, verify_pr=T
               "serial_edges_per_s": round(rm.nedges / t_pr1, 1), "mt_ms_per_iter": round(t_prm * 1e3, 2),
               "mt_edges_per_s": round(rm.nedges / t_prm, 1), "threads": thr,
               "sample": "5 of the 50 FP64 pull iterations, per-iteration time"}
+    # the gather floor: one edge-parallel pass with nothing but the x/deg gathers
+    floor_l1, floor_l2 = dg.probe_gather(True), dg.probe_gather(False)
+    per_iter = st.kernel_ms / 50
+    res["rmat22"]["pagerank_gather_floor"] = {
+        "pass_ms_l1": round(floor_l1, 4), "pass_ms_l2": round(floor_l2, 4), "iteration_ms": round(per_iter, 4),
+        "frac_of_gather_floor": round(floor_l1 / per_iter, 4),
+        "floor_hbm_frac": round(per_iter_bytes / (floor_l1 * 1e-3) / 1e9 / hbm_peak()[0], 4),
+        "note": "an edge-parallel pass gathering x/deg at every edge (no per-vertex sums): the most a pull "
+                "iteration can reach on this graph; frac = floor / iteration time"}
     res["rmat22"]["pagerank"] = {"iters": 50, "ms": round(st.kernel_ms, 3),
                                  "edges_per_s": round(50 * rm.nedges / (st.kernel_ms * 1e-3), 1),
                                  "GB_s_algorithmic": round(50 * per_iter_bytes / (st.kernel_ms * 1e-3) / 1e9, 1),
@@ -1078,6 +1087,7 @@ def summarize(detail, peak):
                              "ccg_us": round(r["ccg_ms"] * 1e3, 2) if r.get("ccg_ms") else None,
                              "tuned_any_shape_hbm_frac": _get(r, "tuned_any_shape", "hbm_frac"),
                              "single_launch_cold_us": r.get("single_launch_cold_us"),
+                             "dram_traffic_per_launch": profile_traffic("reduce_i32_kernel_2e24"),
                              "cpu_serial_GB_s": _get(r, "cpu", "serial_GB_s"), "cpu_mt_GB_s": _get(r, "cpu", "mt_GB_s")}
     if "reduce" in rg:
         out["C1_reduce_reference_programs"] = rg["reduce"]
@@ -1111,6 +1121,8 @@ def summarize(detail, peak):
         pr = g.get("pagerank") or {}
         if pr:
             e["pr50_ms"], e["pr_hbm_frac"], e["pr_l1"] = pr.get("ms"), pr.get("hbm_frac"), pr.get("l1_vs_fp64")
+            e["pr_frac_of_gather_floor"] = _get(g, "pagerank_gather_floor", "frac_of_gather_floor")
+            e["pr_gather_floor_hbm_frac"] = _get(g, "pagerank_gather_floor", "floor_hbm_frac")
         e["cpu_bfs_serial_GTEPS"] = _get(b, "cpu", "serial_GTEPS")
         e["cpu_bfs_mt_GTEPS"] = _get(b, "cpu", "mt_GTEPS")
         e["cpu_sssp_serial_GTEPS"] = _get(ss, "cpu", "serial_GTEPS")

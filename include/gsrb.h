@@ -78,7 +78,7 @@ typedef struct gsrb_cfg {
   int32_t launch_mode;   /* 0 = cooperative launch when the driver accepts it, 1 = plain launch (default)
                             (both only after the co-residency check; CCG is always cooperative) */
   int32_t wake_lines;    /* FANOUT / CLUSTER_FANOUT / HIER: wake-up lines the generation is published to (0 = 8) */
-  int32_t form;          /* pull PageRank: GSRB_FORM_L1 gathers x/deg through L1 (ld.ca), GSRB_FORM_AUTO and
+  int32_t form;          /* pull PageRank: GSRB_FORM_AUTO and GSRB_FORM_L1 gather x/deg through L1 (ld.ca),
                             GSRB_FORM_L2 through L2 only (ld.cg); other kernels ignore it */
   int32_t reserved[4];
 } gsrb_cfg_t;
@@ -152,7 +152,7 @@ gsrb_status_t gsrb_probe_l2_atomics(gsrb_ctx_t ctx, int32_t ctas, int32_t iters,
  * cp.async.bulk (cfg->tile = stages, 0 = as many as fit, at most 6), one grid
  * barrier, CTA 0 combines the partials in a fixed order.  cfg == NULL: one
  * 1024-thread CTA per SM.  Replaces reduce_kernel/reduce() of
- * Reduce/reduce_gsrb.cu:289-404 (API Reduce/reduce.cuh:47).  Asynchronous. */
+ * Reduce/reduce_gsrb.cu:289-404 (API Reduce/reduce.cuh:19).  Asynchronous. */
 gsrb_status_t gsrb_reduce_i32(gsrb_ctx_t ctx, const int32_t* d_in, size_t n, int64_t* d_out,
                               const gsrb_cfg_t* cfg);
 
@@ -386,6 +386,12 @@ gsrb_status_t gsrb_graph_sssp_features(gsrb_graph_t g, uint32_t src, float* h_ou
 /* Pull PageRank: x0 = 1 - alpha, `iters` iterations of x = (1-alpha) + alpha * sum x_u/deg(u). */
 gsrb_status_t gsrb_pagerank(gsrb_ctx_t ctx, gsrb_graph_t g, float alpha, int32_t iters, float* d_rank,
                             const gsrb_cfg_t* cfg, gsrb_traversal_stats_t* stats);
+/* The gather floor of a pull pass over g (no counterpart in the reference):
+ * one edge-parallel launch that gathers an FP32 value at every edge's
+ * destination (the pull PageRank's x/deg reads without its per-vertex
+ * bookkeeping), through L1 (l1 != 0) or L2 only; *ms = its time, mean of 10
+ * back-to-back launches.  Synchronous.  The roofline of the pull PageRank. */
+gsrb_status_t gsrb_probe_gather(gsrb_ctx_t ctx, gsrb_graph_t g, int32_t l1, float* ms);
 /* The reference's push-residual PageRank (apps/pr/kernel_gsrb.cu:298-508):
  * p = 1 - alpha, residuals seeded with (1 - alpha) * alpha * sum 1/outdeg, then
  * rounds of "take the residual, add it to p, push alpha * res / outdeg along

@@ -2,7 +2,7 @@
 // reference headers) so that the reference's own drivers link against libgsrb
 // unchanged:
 //   int  reduce(const int* arr, unsigned N, unsigned threads_per_block)
-//        Reduce/reduce.cuh:47 -- host array in, int sum out, prints
+//        Reduce/reduce.cuh:19 -- host array in, int sum out, prints
 //        "time (ms) is %f" like Reduce/reduce_gsrb.cu:396
 //   void sum_scan_blelloch(unsigned* d_out, unsigned* d_in, size_t numElems)
 //        scan/scan.h:16-18 -- device pointers, exclusive uint32 scan, prints

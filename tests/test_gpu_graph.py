@@ -64,17 +64,27 @@ def test_sssp_distances_exact(gsrb, ctx, orc, graphs, name, delta):
 
 
 @pytest.mark.parametrize("name", ["tiny", "rmat12", "rmat16", "grid64", "isolated"])
-def test_pagerank_l1(gsrb, ctx, orc, graphs, name):
+@pytest.mark.parametrize("form", [0, 1, 2])  # x/deg gathers: through L1 (default and explicit), L2 only
+def test_pagerank_l1(gsrb, ctx, orc, graphs, name, form):
     g = graphs[name]
     dg = ctx.graph(g)
     out = ctx.array(g.nnodes, np.float32)
-    rc, st = dg.pagerank(out, 0.85, 50)
+    rc, st = dg.pagerank(out, 0.85, 50, gsrb.cfg(variant=gsrb.BAR_FANOUT, ctas_per_sm=2, threads=512,
+                                                  wake_lines=4, form=form))
     gsrb.check(rc, "pagerank")
     assert st.levels == 50
     ref = orc.pagerank(g, 0.85, 50)
     got = out.download()
     assert orc.normalized_l1(got, ref) <= PR_L1_TOL
     assert np.max(np.abs(got - ref) / ref) < 1e-5
+
+
+@pytest.mark.parametrize("name", ["rmat12", "grid64"])
+def test_gather_probe(gsrb, ctx, graphs, name):
+    dg = ctx.graph(graphs[name])
+    assert dg.probe_gather(True) > 0.0 and dg.probe_gather(False) > 0.0
+    assert ctx.status()[0] == 0
+    dg.free()
 
 
 @pytest.mark.parametrize("name", ["tiny", "rmat12", "rmat16", "grid64", "isolated"])

@@ -1,7 +1,7 @@
 // Persistent barrier-stepped sum reduction of int32 into int64.
 //
 // Reference: reduce_kernel / reduce() in Reduce/reduce_gsrb.cu:289-404 (API
-// Reduce/reduce.cuh:47): one element per thread, grid = ceil(N / tpb) CTAs (so
+// Reduce/reduce.cuh:19): one element per thread, grid = ceil(N / tpb) CTAs (so
 // N is limited to the co-resident thread count, 148*2048 on B200), a
 // shared-memory tree per level and one grid barrier per level, int accumulation.
 //

@@ -169,6 +169,7 @@ _SIGS = {
     "gsrb_graph_is_symmetric": (C.c_int32, [_P, C.POINTER(C.c_int32)]),
     "gsrb_graph_set_policy": (C.c_int32, [_P, _P, C.c_size_t]),
     "gsrb_graph_set_sssp_policy": (C.c_int32, [_P, _P, C.c_size_t]),
+    "gsrb_probe_gather": (C.c_int32, [_P, _P, C.c_int32, C.POINTER(C.c_float)]),
     "gsrb_graph_sssp_plan": (C.c_int32, [_P, C.c_uint32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _P]),
     "gsrb_graph_sssp_features": (C.c_int32, [_P, C.c_uint32, _P]),
     "gsrb_sssp_features": (None, [C.c_uint32, C.c_uint64, C.c_uint32, C.c_uint32, C.c_double, C.c_int32,
@@ -521,6 +522,13 @@ class DeviceGraph:
         sc = np.zeros(2, np.float32)
         check(_lib().gsrb_graph_sssp_plan(self.h, src, C.byref(d), C.byref(k), sc.ctypes.data), "sssp_plan")
         return int(d.value), int(k.value), float(sc[0]), float(sc[1])
+
+    def probe_gather(self, l1: bool = True) -> float:
+        """ms of one edge-parallel pass gathering an FP32 value per edge (the
+        pull PageRank's gather floor on this graph)."""
+        t = C.c_float()
+        check(_lib().gsrb_probe_gather(self.ctx.h, self.h, 1 if l1 else 0, C.byref(t)), "probe_gather")
+        return float(t.value)
 
     def sssp_features(self, src: int = 0) -> np.ndarray:
         out = np.zeros(12, np.float32)
