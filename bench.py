@@ -288,27 +288,55 @@ def barrier_table(gsrb, ctx, tune, tuned_cache):
 
 
 def semaphore_numbers(gsrb, ctx):
+    """Acquires/s of the priority semaphore (148 x 8 CTAs, one writer per 10
+    readers, 100 increments per hold, 2 holds per CTA) beside the reference's
+    protocols restated, and the bound the critical sections themselves set:
+    with one CTA and no semaphore (GSRB_SEM_NONE) a writer's hold takes T_w and
+    a reader's T_r, writers exclude everyone and at most S readers overlap, so
+    no semaphore can finish W writer and R reader holds faster than
+    W * T_w + R * T_r / S."""
+    iters, incs, every, k = 2, 100, 11, 8
+
+    def bare(writer_every, r1=100, r2=1100):
+        # the call's own set-up (lock state allocation, record init) is in both
+        # timings: the difference over r2 - r1 holds is the holds alone
+        c = gsrb.cfg(ctas_per_sm=1, threads=256, grid_override=1)
+        cnt = ctx.array(8, np.uint32).zero()
+        ts = []
+        for reps in (r1, r2, r1, r2):
+            cnt.zero()
+            ctx.record(6)
+            gsrb.check(ctx.semaphore_bench(c, gsrb.SEM_NONE, 1, writer_every, reps, incs, cnt), "semaphore probe")
+            ctx.record(7)
+            ts.append(ctx.elapsed_ms(6, 7))
+        return max(1e-6, (min(ts[1], ts[3]) - min(ts[0], ts[2])) / (r2 - r1))
+
+    t_w, t_r = bare(1), bare(0)
+    grid = k * ctx.num_sms
+    writers = len([b for b in range(grid) if b % every == 0])
     out = []
     for S in (1, 2, 10, 120):
-        row = {"S": S}
-        for name, kind, k in (("native_priority", gsrb.SEM_PRIORITY, 8), ("ref_priority", gsrb.SEM_REF_PRIORITY, 8),
-                              ("ref_spin_k2", gsrb.SEM_REF_SPIN, 2)):
+        bound_ms = writers * iters * t_w + (grid - writers) * iters * t_r / S
+        rate_bound = grid * iters / (bound_ms * 1e-3)
+        row = {"S": S, "critical_section_bound_acq_per_s": round(rate_bound, 1)}
+        for name, kind in (("native_priority", gsrb.SEM_PRIORITY), ("ref_priority", gsrb.SEM_REF_PRIORITY),
+                           ("ref_spin", gsrb.SEM_REF_SPIN)):
             c = gsrb.cfg(ctas_per_sm=k, threads=256, timeout_ms=5000)
             cnt = ctx.array(8, np.uint32).zero()
-            iters = 2
             ctx.record(6)
-            st = ctx.semaphore_bench(c, kind, S, 11, iters, 100, cnt)
+            st = ctx.semaphore_bench(c, kind, S, every, iters, incs, cnt)
             ctx.record(7)
             ms = ctx.elapsed_ms(6, 7)
             W, R, inside, maxr, viol, acq, tmo, _ = cnt.download().tolist()
-            grid = k * ctx.num_sms
-            writers = len([b for b in range(grid) if b % 11 == 0])
-            exact = (st == 0 and W == writers * iters * 100 and R == (grid - writers) * iters * 100 and viol == 0
+            exact = (st == 0 and W == writers * iters * incs and R == (grid - writers) * iters * incs and viol == 0
                      and maxr <= S)
-            row[name] = {"acquires_per_s": round(acq / (ms * 1e-3), 1), "ms": round(ms, 3), "exact": exact,
-                         "ctas": grid}
+            rate = acq / (ms * 1e-3)
+            row[name] = {"acquires_per_s": round(rate, 1), "ms": round(ms, 3), "exact": exact, "ctas": grid,
+                         "frac_of_bound": round(rate / rate_bound, 4)}
         out.append(row)
-    return out
+    return {"rows": out, "writer_hold_us": round(t_w * 1e3, 3), "reader_hold_us": round(t_r * 1e3, 3),
+            "shape": f"{grid} CTAs x 256 threads, 1 writer per {every - 1} readers, {incs} increments per hold, "
+                     f"{iters} holds per CTA"}
 
 
 # --------------------------------------------------------------- data kernels
@@ -1076,9 +1104,12 @@ def summarize(detail, peak):
     if "heterosync_barrier" in rg:
         out["C2_barrier_reference_programs"] = {f"k{r['ctas'] // 148}": {k: v for k, v in r.items() if k.endswith("_ns")}
                                                 for r in rg["heterosync_barrier"]}
-    sem = detail.get("semaphore") or []
+    sem = (detail.get("semaphore") or {}).get("rows") or []
     out["C2_semaphore"] = {f"S{r['S']}": {"acq_per_s": _get(r, "native_priority", "acquires_per_s"),
+                                          "frac_of_critical_section_bound": _get(r, "native_priority",
+                                                                                 "frac_of_bound"),
                                           "ref_protocol_acq_per_s": _get(r, "ref_priority", "acquires_per_s"),
+                                          "ref_spin_acq_per_s": _get(r, "ref_spin", "acquires_per_s"),
                                           "exact": _get(r, "native_priority", "exact")} for r in sem}
     r = detail.get("reduce_2e24") or {}
     out["C1_reduce_2e24"] = {"us": round(r["ms"] * 1e3, 2) if "ms" in r else None, "GB_s": r.get("GB_s"),

@@ -253,13 +253,16 @@ enum {
   GSRB_SEM_REF_EBO = 1,           /* ... with exponential backoff */
   GSRB_SEM_REF_PRIORITY = 2,      /* reference TPDS'22 priority semaphore protocol */
   GSRB_SEM_REF_PRIORITY_EBO = 3,  /* ... with exponential backoff */
-  GSRB_SEM_PRIORITY = 4           /* B200-native priority semaphore (wait-free posts, writer queue) */
+  GSRB_SEM_PRIORITY = 4,          /* B200-native priority semaphore (wait-free posts, writer queue) */
+  GSRB_SEM_NONE = 5               /* no semaphore: the critical sections alone (on one CTA, the timing
+                                     that bounds any semaphore's throughput; counts are not exact on more) */
 };
 /* Mutex kinds for gsrb_mutex_bench. */
 enum { GSRB_MUTEX_SPIN = 0, GSRB_MUTEX_EBO = 1, GSRB_MUTEX_FA = 2, GSRB_MUTEX_SLEEP = 3 };
 
 /* Semaphore microbenchmark: grid = cfg CTAs; CTA b is a
- * writer when b % writer_every == 0; each CTA acquires `iters` times and adds 1
+ * writer when writer_every > 0 and b % writer_every == 0 (writer_every = 0: no
+ * writers); each CTA acquires `iters` times and adds 1
  * to a shared counter `incs` times per acquire (writers: plain read-modify-write
  * of W; readers: atomic add to R).  d_counters: 8 uint32, zeroed by the caller:
  * [W, R, inside, max_readers, violations, acquires, timeouts, 0].  Synchronous.

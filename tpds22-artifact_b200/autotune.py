@@ -162,13 +162,15 @@ def tune_reduce(ctx, bufs, n: int, out, k: int | None = None, threads: int | Non
 def segment_candidates(kind: str):
     """Shapes and sub-grid protocols for the batched segment calls (protocols
     whose state does not depend on the team size; for the scan also the round
-    length, 0 = 4 tiles of 16 x threads)."""
+    length: 1, 2, 4 (= 0, the default) or 8 tiles of 16 x threads per CTA -- a
+    short round keeps the round and its prefetched successor in L2 for the
+    rescan, a long one pays fewer barriers)."""
     g = _g()
     out = []
     for k, threads in ((2, 512), (4, 256), (8, 128), (2, 256), (1, 1024)):
         for cand in (dict(variant=g.BAR_FANOUT, wake_lines=4), dict(variant=g.BAR_FLIP, fanin_groups=1),
                      dict(variant=g.BAR_FLAT)):
-            for tile in ((0, 8 * 16 * threads) if kind == "scan" else (0,)):
+            for tile in ((16 * threads, 2 * 16 * threads, 0, 8 * 16 * threads) if kind == "scan" else (0,)):
                 out.append(dict(cand, ctas_per_sm=k, threads=threads, tile=tile))
     return out
 

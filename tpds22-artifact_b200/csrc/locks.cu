@@ -132,11 +132,13 @@ template <int KIND>
 __global__ void __launch_bounds__(256)
 semaphore_bench_kernel(uint32_t* rec, const void* statbuf, int writer_every, int iters, int incs,
                        uint64_t timeout_ns, uint32_t spin_ns, Counters* c) {
-  const bool writer = (blockIdx.x % (uint32_t)writer_every) == 0;
+  const bool writer = writer_every > 0 && (blockIdx.x % (uint32_t)writer_every) == 0;
   const uint32_t cap = rec[3] - 1;
   for (int it = 0; it < iters; ++it) {
-    bool ok;
-    if (KIND == GSRB_SEM_PRIORITY)
+    bool ok = true;
+    if (KIND == GSRB_SEM_NONE)
+      ok = true;  // the critical section alone (its timing is the semaphore's bound)
+    else if (KIND == GSRB_SEM_PRIORITY)
       ok = gsrb::psem_wait(gsrb::PrioritySem{rec}, writer, statbuf, timeout_ns, spin_ns);
     else
       ok = gsrb::refsem_wait(gsrb::RefSem{rec}, writer, rec[3], KIND == GSRB_SEM_REF_PRIORITY ||
@@ -162,7 +164,9 @@ semaphore_bench_kernel(uint32_t* rec, const void* statbuf, int writer_every, int
       atomicAdd(&c->acquires, 1u);
       __threadfence();
     }
-    if (KIND == GSRB_SEM_PRIORITY) {
+    if (KIND == GSRB_SEM_NONE) {
+      __syncthreads();
+    } else if (KIND == GSRB_SEM_PRIORITY) {
       gsrb::psem_post(gsrb::PrioritySem{rec}, writer);
     } else {
       if (!gsrb::refsem_post(gsrb::RefSem{rec}, writer, rec[3], KIND == GSRB_SEM_REF_PRIORITY ||
@@ -249,6 +253,7 @@ const void* sem_fn(int kind) {
     case GSRB_SEM_REF_PRIORITY: return (const void*)semaphore_bench_kernel<GSRB_SEM_REF_PRIORITY>;
     case GSRB_SEM_REF_PRIORITY_EBO: return (const void*)semaphore_bench_kernel<GSRB_SEM_REF_PRIORITY_EBO>;
     case GSRB_SEM_PRIORITY: return (const void*)semaphore_bench_kernel<GSRB_SEM_PRIORITY>;
+    case GSRB_SEM_NONE: return (const void*)semaphore_bench_kernel<GSRB_SEM_NONE>;
     default: return nullptr;
   }
 }
@@ -334,7 +339,7 @@ gsrb_status_t gsrb_locks_status(gsrb_locks_t L, uint32_t* code) {
 
 gsrb_status_t gsrb_semaphore_bench(gsrb_ctx_t ctx, const gsrb_cfg_t* cfgin, int32_t kind, uint32_t capacity,
                                    int32_t writer_every, int32_t iters, int32_t incs, uint32_t* d_counters) {
-  if (!ctx || !d_counters || capacity < 1 || capacity > 60000 || writer_every < 1 || iters < 0 || incs < 0)
+  if (!ctx || !d_counters || capacity < 1 || capacity > 60000 || writer_every < 0 || iters < 0 || incs < 0)
     return GSRB_ERR_ARG;
   const void* fn = sem_fn(kind);
   if (!fn) return GSRB_ERR_ARG;

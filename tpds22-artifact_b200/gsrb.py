@@ -201,7 +201,7 @@ _SIGS = {
 }
 
 # semaphore / mutex kinds, BFS modes
-SEM_REF_SPIN, SEM_REF_EBO, SEM_REF_PRIORITY, SEM_REF_PRIORITY_EBO, SEM_PRIORITY = range(5)
+SEM_REF_SPIN, SEM_REF_EBO, SEM_REF_PRIORITY, SEM_REF_PRIORITY_EBO, SEM_PRIORITY, SEM_NONE = range(6)
 MUTEX_SPIN, MUTEX_EBO, MUTEX_FA, MUTEX_SLEEP = range(4)
 BFS_PUSH, BFS_HEURISTIC, BFS_LEARNED, BFS_PULL, BFS_TOPO = range(5)
 BFS_FLAG_LB = 0x100  # OR-ed into a mode: load-balanced expansion of large push levels
