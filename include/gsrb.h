@@ -254,8 +254,8 @@ enum {
   GSRB_SEM_REF_PRIORITY = 2,      /* reference TPDS'22 priority semaphore protocol */
   GSRB_SEM_REF_PRIORITY_EBO = 3,  /* ... with exponential backoff */
   GSRB_SEM_PRIORITY = 4,          /* B200-native priority semaphore (wait-free posts, writer queue) */
-  GSRB_SEM_NONE = 5               /* no semaphore: the critical sections alone (on one CTA, the timing
-                                     that bounds any semaphore's throughput; counts are not exact on more) */
+  GSRB_SEM_NONE = 5               /* no semaphore: the critical sections alone (on one CTA, what a hold
+                                     costs by itself; counts are not exact on more CTAs) */
 };
 /* Mutex kinds for gsrb_mutex_bench. */
 enum { GSRB_MUTEX_SPIN = 0, GSRB_MUTEX_EBO = 1, GSRB_MUTEX_FA = 2, GSRB_MUTEX_SLEEP = 3 };
