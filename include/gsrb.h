@@ -80,7 +80,12 @@ typedef struct gsrb_cfg {
   int32_t wake_lines;    /* FANOUT / CLUSTER_FANOUT / HIER: wake-up lines the generation is published to (0 = 8) */
   int32_t form;          /* pull PageRank: GSRB_FORM_AUTO and GSRB_FORM_L1 gather x/deg through L1 (ld.ca),
                             GSRB_FORM_L2 through L2 only (ld.cg); other kernels ignore it */
-  int32_t reserved[4];
+  int32_t overlap;       /* gsrb_reduce_i32 only, plain launches only: 1 = the launch may start, and read
+                            d_in, while the kernel before it on the stream is still running (programmatic
+                            dependent launch); it touches no other memory until that kernel has finished.
+                            Set it only when that kernel does not write d_in -- e.g. in a chain of
+                            reductions over inputs that were all ready before the chain began.  0 = off */
+  int32_t reserved[3];
 } gsrb_cfg_t;
 
 void gsrb_cfg_default(gsrb_cfg_t* cfg);

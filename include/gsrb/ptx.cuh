@@ -213,5 +213,17 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// ---- programmatic dependent launch ---------------------------------------------
+// Wait until the grids this one depends on (the previous kernel on the stream,
+// when this grid was launched with programmatic stream serialisation) have
+// completed and their memory operations are visible.  A no-op otherwise.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// Let the next grid on the stream (if launched with programmatic stream
+// serialisation) be scheduled once every CTA of this grid has executed this or
+// exited.  It gives that grid no memory visibility: it still waits with griddep_wait.
+__device__ __forceinline__ void griddep_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 }  // namespace ptx
 }  // namespace gsrb

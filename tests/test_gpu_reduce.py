@@ -61,3 +61,58 @@ def test_reduce_other_shapes(gsrb, ctx, orc, k, threads, stages):
     a = gsrb.uniform_i32(99, 7_777_777, 0, 127)
     c = gsrb.cfg(ctas_per_sm=k, threads=threads, cluster=2, tile=stages)
     assert _reduce(gsrb, ctx, a, c) == orc.sum_i32(a)
+
+
+# protocols of chained launches (cfg.overlap = 1): (variant, cluster, extra cfg)
+CHAIN = [(9, 1, dict(wake_lines=4)), (8, 1, dict(fanin_groups=1)), (11, 1, dict(fanin_groups=16, wake_lines=4)),
+         (0, 2, {}), (3, 1, {}), (4, 1, {})]
+
+
+@pytest.mark.parametrize("variant,cluster,extra", CHAIN)
+@pytest.mark.parametrize("graph", [False, True])
+def test_reduce_chained_launches(gsrb, ctx, orc, variant, cluster, extra, graph):
+    # A chain of reductions over distinct inputs of uneven sizes, each launch
+    # allowed to start (and read its input) while the previous one finishes;
+    # they share the barrier state and the partials, which a launch touches only
+    # after the previous one has completed.  Every result bit-exact, three times
+    # over (a chain also follows the previous chain's last launch).
+    sizes = [1 << 22, 3_000_001, 17, 0, 1 << 20, 5_555_555, 1 << 22, 1]
+    arrays = [gsrb.uniform_i32(1000 + i, n, -1000, 1000) for i, n in enumerate(sizes)]
+    bufs = [ctx.to_device(a) if a.size else ctx.array(1, np.int32).zero() for a in arrays]
+    out = ctx.array(len(sizes), np.int64)
+    c = gsrb.cfg(variant=variant, ctas_per_sm=2, threads=256, cluster=cluster, overlap=1, **extra)
+    want = [orc.sum_i32(a) for a in arrays]
+
+    def chain():
+        for i, n in enumerate(sizes):
+            gsrb.check(ctx.reduce_i32(bufs[i], n, out.at(i), c), f"chained reduce {i}")
+
+    cg = None
+    if graph:
+        chain()  # warm the library's caches outside the capture
+        cg = gsrb.CudaGraph(ctx)
+        with cg:
+            chain()
+    try:
+        for rep in range(3):
+            out.upload(np.full(len(sizes), -1, np.int64))
+            if cg:
+                cg.launch()
+            else:
+                chain()
+            ctx.check_status("chained reduce")
+            assert out.download().tolist() == want, f"rep {rep}"
+    finally:
+        if cg:
+            cg.free()
+    for b in bufs:
+        b.free()
+
+
+def test_reduce_overlap_refused_for_cooperative_launch(gsrb, ctx):
+    # a chained launch is a plain launch; grid.sync's cooperative launch refuses it
+    a = ctx.to_device(np.ones(1000, np.int32))
+    out = ctx.array(1, np.int64)
+    c = gsrb.cfg(variant=gsrb.BAR_CCG, ctas_per_sm=2, threads=256, overlap=1)
+    assert ctx.reduce_i32(a, 1000, out, c) == gsrb.ERR_UNSUPPORTED
+    a.free()

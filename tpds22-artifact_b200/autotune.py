@@ -130,9 +130,12 @@ def reduce_stream_ms(ctx, bufs, n: int, out, c, passes: int = 4):
     return t / (passes * nb)
 
 
-def reduce_candidates(k: int | None = None, threads: int | None = None):
+def reduce_candidates(k: int | None = None, threads: int | None = None, overlap: bool = False):
     """The library's own barrier protocols (and grid.sync for comparison) at
-    the given shape, or over the shapes the reduce supports."""
+    the given shape, or over the shapes the reduce supports.  overlap: also
+    the chained form of the plain-launch protocols (cfg.overlap = 1: a launch
+    may start streaming its input while the previous reduction on the stream
+    finishes; valid when that reduction does not write this one's input)."""
     g = _g()
     shapes = [(k, threads)] if k else [(1, 1024), (1, 512), (2, 512), (2, 256), (4, 256)]
     out = []
@@ -141,16 +144,19 @@ def reduce_candidates(k: int | None = None, threads: int | None = None):
             for cand in (dict(variant=g.BAR_FANOUT, wake_lines=4), dict(variant=g.BAR_FLIP, fanin_groups=1),
                          dict(variant=g.BAR_HIER, fanin_groups=16, wake_lines=4), dict(variant=g.BAR_CCG)):
                 out.append(dict(cand, ctas_per_sm=kk, threads=th, tile=stages))
+                if overlap and cand["variant"] != g.BAR_CCG:
+                    out.append(dict(cand, ctas_per_sm=kk, threads=th, tile=stages, overlap=1))
     return out
 
 
 def tune_reduce(ctx, bufs, n: int, out, k: int | None = None, threads: int | None = None, passes: int = 3,
-                library_barrier_only: bool = True):
+                library_barrier_only: bool = True, overlap: bool = False):
     """Fastest configuration by reduce_stream_ms; with library_barrier_only the
-    cooperative-groups barrier is timed but not chosen."""
+    cooperative-groups barrier is timed but not chosen; overlap: the chained
+    form is a candidate too."""
     g = _g()
     table = []
-    for e in reduce_candidates(k, threads):
+    for e in reduce_candidates(k, threads, overlap):
         t = reduce_stream_ms(ctx, bufs, n, out, g.cfg(**e), passes)
         if t is not None:
             table.append((t, e))

@@ -74,9 +74,12 @@ gsrb::GridBarrier make_barrier(gsrb_ctx* ctx, const gsrb_cfg_t& c, int slot, uin
 // than the co-resident capacity; attaches the cluster dimension.  coop:
 // 2 = cooperative launch required (GSRB_BAR_CCG), 1 = cooperative when the
 // driver accepts it, 0 = plain launch (safe: co-residency was checked and every
-// device wait is bounded).
+// device wait is bounded).  pdl (plain launches only): launch with programmatic
+// stream serialisation, so that the kernel may start while the one before it on
+// the stream is still running (it must call ptx::griddep_wait before touching
+// anything that kernel uses).
 gsrb_status_t launch_persistent(gsrb_ctx* ctx, const void* fn, int grid, int block, size_t smem,
-                                int cluster, int coop, void** args);
+                                int cluster, int coop, void** args, bool pdl = false);
 inline int coop_of(const gsrb_cfg_t& c) {
   if (c.variant == gsrb::V_CCG) return 2;
   return c.launch_mode == 1 ? 0 : 1;

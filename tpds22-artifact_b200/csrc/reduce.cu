@@ -71,7 +71,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* mbar, uint32_t parit
 template <int V>
 __global__ void __launch_bounds__(1024)
 reduce_i32_kernel(gsrb::GridBarrier gb, const int32_t* __restrict__ in, uint64_t n,
-                  long long* __restrict__ partials, long long* __restrict__ out, uint32_t nbuf) {
+                  long long* __restrict__ partials, long long* __restrict__ out, uint32_t nbuf, uint32_t pdl) {
   extern __shared__ __align__(128) unsigned char stage[];
   __shared__ gsrb::BarrierShared bsh;
   __shared__ long long warp_buf[32];
@@ -106,6 +106,11 @@ reduce_i32_kernel(gsrb::GridBarrier gb, const int32_t* __restrict__ in, uint64_t
     gsrb::ptx::mbar_arrive_expect_tx(&full[buf], bytes_of(k));
     gsrb::ptx::bulk_g2s(stage + (size_t)buf * kStageBytes, src + (size_t)k * kStageBytes, bytes_of(k), &full[buf]);
   };
+  // Chained launches (pdl): the next reduction on the stream may be scheduled
+  // as soon as every CTA of this one runs; its CTAs take the SM slots this
+  // grid's CTAs free when they leave, so its stream overlaps this grid's
+  // barrier and combine.  It reads only its own input before griddep_wait.
+  if (pdl) gsrb::ptx::griddep_launch_dependents();
   // The first copies go out before the barrier's set-up reads (two dependent
   // L2 round trips): they only read the input.  Whatever the set-up decides,
   // every issued copy is waited for below before the CTA leaves.
@@ -118,7 +123,13 @@ reduce_i32_kernel(gsrb::GridBarrier gb, const int32_t* __restrict__ in, uint64_t
     gsrb::ptx::fence_mbar_init();
     for (; issued < nst && issued < nbuf; ++issued) issue(issued);
   }
-  const bool ok0 = bar.init(gb, &bsh);  // its __syncthreads also publishes the mbarrier set-up
+  // Without pdl the barrier set-up comes first (its __syncthreads also
+  // publishes the mbarrier set-up).  With pdl it waits until the previous grid
+  // on the stream has finished (that grid may still use the barrier state and
+  // the partials), so it comes after this CTA's stream.
+  bool ok0 = true;
+  if (!pdl) ok0 = bar.init(gb, &bsh);
+  else __syncthreads();
   bool ok = ok0;
   if (!ok0 && tid == 0) {
     // refused to start (a recorded error): leave no copy in flight
@@ -143,6 +154,10 @@ reduce_i32_kernel(gsrb::GridBarrier gb, const int32_t* __restrict__ in, uint64_t
         issue(k + nbuf);
       }
     }
+  }
+  if (pdl) {
+    gsrb::ptx::griddep_wait();
+    ok = bar.init(gb, &bsh) && ok;
   }
   const long long bsum = block_sum_i64(acc, warp_buf);
   if (tid == 0) partials[blockIdx.x] = bsum;
@@ -228,6 +243,10 @@ extern "C" gsrb_status_t gsrb_reduce_i32(gsrb_ctx_t ctx, const int32_t* d_in, si
   long long* out = (long long*)d_out;
   const size_t smem = gsrb_reduce_smem_for(c);
   uint32_t nbuf = (uint32_t)(smem / kStageBytes);
-  void* args[] = {&gb, &d_in, &n64, &partials, &out, &nbuf};
-  return launch_persistent(ctx, fn, grid, c.threads, smem, c.cluster, coop_of(c), args);
+  // chained launch: plain launches only (a cooperative launch is refused)
+  const bool pdl = c.overlap != 0 && coop_of(c) == 0;
+  if (c.overlap != 0 && !pdl) return GSRB_ERR_UNSUPPORTED;
+  uint32_t pdl32 = pdl ? 1u : 0u;
+  void* args[] = {&gb, &d_in, &n64, &partials, &out, &nbuf, &pdl32};
+  return launch_persistent(ctx, fn, grid, c.threads, smem, c.cluster, coop_of(c), args, pdl);
 }

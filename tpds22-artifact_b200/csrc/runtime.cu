@@ -171,8 +171,9 @@ static gsrb_status_t coresident_query(gsrb_ctx* ctx, const void* fn, int block, 
 }
 
 gsrb_status_t launch_persistent(gsrb_ctx* ctx, const void* fn, int grid, int block, size_t smem,
-                                int cluster, int coop, void** args) {
+                                int cluster, int coop, void** args, bool pdl) {
   if (grid <= 0 || block <= 0 || block > 1024) return GSRB_ERR_ARG;
+  if (pdl && coop > 0) return GSRB_ERR_UNSUPPORTED;
   if (cluster < 1) cluster = 1;
   if (grid % cluster) return GSRB_ERR_ARG;
   int cap = 0;
@@ -189,8 +190,13 @@ gsrb_status_t launch_persistent(gsrb_ctx* ctx, const void* fn, int grid, int blo
   cfg.blockDim = dim3((unsigned)block, 1, 1);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = ctx->stream;
-  cudaLaunchAttribute attr[2];
+  cudaLaunchAttribute attr[3];
   unsigned na = 0;
+  if (pdl) {
+    attr[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[na].val.programmaticStreamSerializationAllowed = 1;
+    ++na;
+  }
   if (cluster > 1) {
     attr[na].id = cudaLaunchAttributeClusterDimension;
     attr[na].val.clusterDim.x = (unsigned)cluster;

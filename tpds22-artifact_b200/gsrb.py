@@ -93,7 +93,8 @@ class Cfg(C.Structure):
         ("launch_mode", C.c_int32),
         ("wake_lines", C.c_int32),
         ("form", C.c_int32),
-        ("reserved", C.c_int32 * 4),
+        ("overlap", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
     def as_dict(self):
