@@ -1,7 +1,8 @@
 """The benchmark configurations themselves, as parity tests.
 
 * C1: the sum of 2^24 int32 U[0,127] on exactly 148 x 2 CTAs x 256 threads,
-  under each of the library's own barrier protocols, bit-exact;
+  under each of the library's own barrier protocols, bit-exact, and the
+  chained stream of such reductions that the bench times;
 * C2: the barrier at full residency (148 x 8 x 256) -- 10,000-episode
   accounting and 10^5 message-passing episodes with no stale read -- and the
   priority semaphore at S in {1, 2, 10, 120}, one writer per 10 readers, 100
@@ -47,6 +48,33 @@ def test_c1_reduce_2e24_on_148x2x256(gsrb, ctx, orc, c1_input, variant):
     ctx.check_status("reduce")
     assert int(out.download()[0]) == orc.sum_i32(a)
     d.free()
+
+
+@pytest.mark.parametrize("stages", [1, 2, 0])
+def test_c1_chained_stream_of_2e24_reductions(gsrb, ctx, orc, stages):
+    # the C1 workload as the bench times it: eight 2^24 inputs reduced in turn
+    # by chained launches (cfg.overlap) on 148 x 2 x 256, replayed from a CUDA
+    # graph twice; every sum bit-exact
+    arrays = [gsrb.uniform_i32(SEED + i, 1 << 24, 0, 127) for i in range(8)]
+    bufs = [ctx.to_device(a) for a in arrays]
+    out = ctx.array(8, np.int64)
+    c = gsrb.cfg(variant=gsrb.BAR_FANOUT, ctas_per_sm=2, threads=256, wake_lines=4, tile=stages, overlap=1)
+    for i in range(8):  # warm the library's caches outside the capture
+        gsrb.check(ctx.reduce_i32(bufs[i], 1 << 24, out.at(i), c), "reduce")
+    cg = gsrb.CudaGraph(ctx)
+    with cg:
+        for i in range(8):
+            gsrb.check(ctx.reduce_i32(bufs[i], 1 << 24, out.at(i), c), "reduce (capture)")
+    try:
+        for _ in range(2):
+            out.upload(np.full(8, -1, np.int64))
+            cg.launch()
+            ctx.check_status("chained reduce")
+            assert out.download().tolist() == [orc.sum_i32(a) for a in arrays]
+    finally:
+        cg.free()
+    for b in bufs:
+        b.free()
 
 
 # ------------------------------------------------------------------- C2
