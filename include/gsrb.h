@@ -62,7 +62,7 @@ enum {
 };
 
 /* Data-kernel forms (gsrb_cfg_t.form). */
-enum { GSRB_FORM_AUTO = 0, GSRB_FORM_L2 = 1, GSRB_FORM_L1 = 2 };
+enum { GSRB_FORM_AUTO = 0, GSRB_FORM_L2 = 1, GSRB_FORM_L1 = 2, GSRB_FORM_REG = 3 };
 
 /* Launch / schedule configuration.  Zero-initialise and call gsrb_cfg_default. */
 typedef struct gsrb_cfg {
@@ -79,7 +79,10 @@ typedef struct gsrb_cfg {
                             (both only after the co-residency check; CCG is always cooperative) */
   int32_t wake_lines;    /* FANOUT / CLUSTER_FANOUT / HIER: wake-up lines the generation is published to (0 = 8) */
   int32_t form;          /* pull PageRank: GSRB_FORM_AUTO and GSRB_FORM_L1 gather x/deg through L1 (ld.ca),
-                            GSRB_FORM_L2 through L2 only (ld.cg); other kernels ignore it */
+                            GSRB_FORM_L2 through L2 only (ld.cg).  Segmented scans: GSRB_FORM_REG keeps
+                            each round's chunk in registers from its sum to its rescan (GSRB_BAR_FANOUT);
+                            other forms stage tiles through shared memory and re-read L2.  Other kernels
+                            ignore it */
   int32_t overlap;       /* gsrb_reduce_i32 only, plain launches only: 1 = the launch may start, and read
                             d_in, while the kernel before it on the stream is still running (programmatic
                             dependent launch); it touches no other memory until that kernel has finished.
@@ -205,7 +208,7 @@ gsrb_status_t gsrb_scan_f32(gsrb_ctx_t ctx, const float* d_in, float* d_out, siz
  * (slot 1 + i).  The layout is computed on the device from the launch
  * parameters, so nothing is copied per call and calls can be captured
  * (gsrb_capture_begin/end).  cfg == NULL: GSRB_BAR_FANOUT, 2 x 512 threads per
- * SM for the reduce, 4 x 256 for the scan; cfg->variant must be GSRB_BAR_FANOUT, GSRB_BAR_FLIP or GSRB_BAR_FLAT; grid
+ * SM for the reduce, 4 x 256 and GSRB_FORM_REG for the scan; cfg->variant must be GSRB_BAR_FANOUT, GSRB_BAR_FLIP or GSRB_BAR_FLAT; grid
  * >= k.  Asynchronous; a bounded wait that ran out is reported by
  * gsrb_ctx_status. */
 /* d_out[i] = int64 sum of segment i (0 for an empty segment), bit-exact. */
@@ -215,7 +218,12 @@ gsrb_status_t gsrb_reduce_i32_segments(gsrb_ctx_t ctx, const int32_t* d_in, cons
  * at 0), written at the same offsets of d_out.  Not in place.  A segment is
  * scanned in rounds of cfg->tile elements per CTA (rounded up to whole tiles of
  * 16 x threads; 0 = 4 tiles), chunk sums and one sub-grid barrier per round, so
- * that the rescan re-reads L2. */
+ * that the rescan re-reads L2.  With cfg->form = GSRB_FORM_REG (GSRB_BAR_FANOUT
+ * only) the CTA's threads form 2-4 groups that take the rounds in turn and keep
+ * their chunk in registers from its sum to its rescan: cfg->tile is then the
+ * chunk, threads x 4 x (16 vectors a lane when ctas_per_sm x threads <= 512,
+ * else 8) divided by the number of groups (0 = two groups); other values
+ * return GSRB_ERR_ARG. */
 gsrb_status_t gsrb_scan_u32_segments(gsrb_ctx_t ctx, const uint32_t* d_in, uint32_t* d_out, const uint64_t* h_off,
                                      int32_t k, const gsrb_cfg_t* cfg);
 /* The same for FP32: chunk sums and carries in FP64, each tile scanned in FP32

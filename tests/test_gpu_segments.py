@@ -178,3 +178,113 @@ def test_segments_graph_replay(gsrb, ctx, orc):
         ctx.check_status("replay")
         assert out.download().tolist() == want
     cg.free()
+
+
+# ---- register-resident rounds (cfg.form = FORM_REG, fan-out sub-grid barrier):
+# groups of each CTA take the rounds in turn and keep their chunk in registers
+# from its sum to its rescan.  Shapes: (CTAs/SM, threads, groups); the chunk is
+# threads x 4 x (16 vectors a lane when CTAs/SM x threads <= 512, else 8) / groups.
+REG_SHAPES = [(1, 512, 2), (1, 512, 4), (2, 256, 2), (4, 128, 2), (1, 1024, 2), (1, 1024, 4), (1, 768, 3),
+              (1, 64, 2), (2, 512, 4)]
+
+
+def _reg_cfg(gsrb, k, threads, groups):
+    per = threads * (16 if threads * k <= 512 else 8) * 4
+    return gsrb.cfg(variant=9, ctas_per_sm=k, threads=threads, form=gsrb.FORM_REG, tile=per // groups, wake_lines=4)
+
+
+class _At:
+    """A device address inside an array, with its element type."""
+
+    def __init__(self, arr, elems):
+        self.ptr = arr.ptr + 4 * elems
+        self.dtype = arr.dtype
+
+
+@pytest.mark.parametrize("k_sm,threads,groups", REG_SHAPES)
+@pytest.mark.parametrize("k", [1, 7, 64, 127])
+def test_scan_segments_reg_exact(gsrb, ctx, orc, k_sm, threads, groups, k):
+    off = _uneven_offsets(500 + k, k)
+    a = gsrb.uniform_i32(0x5EED2022 + k, int(off[-1]), 0, 2**31 - 1).astype(np.uint32) * np.uint32(3)  # wraps
+    got = _scan_segments(gsrb, ctx, a, off, _reg_cfg(gsrb, k_sm, threads, groups))
+    assert np.array_equal(got, _want_scan(orc, a, off))
+
+
+@pytest.mark.parametrize("in_off,out_off", [(0, 0), (1, 1), (3, 3), (1, 0), (0, 2), (2, 3)])
+def test_scan_segments_reg_alignment_and_tiny_segments(gsrb, ctx, orc, in_off, out_off):
+    # segments start at every alignment; input and output at the same or a
+    # different 16-byte phase (128-bit stores only when they match)
+    lens = np.array([0, 1, 2, 3, 5, 7, 9, 0, 1, 100_003, 3, 1 << 20, 6, 8, 4, 2, 1, 777_777], np.uint64)
+    off = np.concatenate([[0], np.cumsum(lens)]).astype(np.uint64)
+    n = int(off[-1])
+    u = gsrb.uniform_i32(9, n, 0, 2**31 - 1).astype(np.uint32) * np.uint32(7)
+    buf = np.zeros(n + 8, np.uint32)
+    buf[in_off:in_off + n] = u
+    d = ctx.to_device(buf)
+    out = ctx.array(n + 8, np.uint32)
+    for shape in ((1, 512, 2), (2, 256, 4), (1, 1024, 2)):
+        out.zero()
+        c = _reg_cfg(gsrb, *shape)
+        gsrb.check(ctx.scan_u32_segments(_At(d, in_off), _At(out, out_off), off, c), "scan_u32_segments")
+        ctx.check_status("scan_u32_segments")
+        full = out.download()
+        assert np.array_equal(full[out_off:out_off + n], _want_scan(orc, u, off)), shape
+        # nothing outside the output range is written
+        assert not full[:out_off].any() and not full[out_off + n:].any()
+
+
+@pytest.mark.parametrize("k", [1, 9, 127])
+def test_scan_f32_segments_reg_tolerance_and_mixed_sign(gsrb, ctx, orc, k):
+    off = _uneven_offsets(600 + k, k, hi=1 << 19)
+    c = _reg_cfg(gsrb, 1, 512, 2)
+    for mixed in (False, True):
+        a = gsrb.uniform_f32(0xC0FFEE + k, int(off[-1]))
+        if mixed:
+            a = (a * np.float32(2.0) - np.float32(1.0)).astype(np.float32)
+        d = ctx.to_device(a) if a.size else ctx.array(1, np.float32)
+        out = ctx.array(max(a.size, 1), np.float32).zero()
+        gsrb.check(ctx.scan_segments(d, out, off, c), "scan_f32_segments")
+        ctx.check_status("scan_f32_segments")
+        got = out.download()[: a.size].astype(np.float64)
+        for i in range(k):
+            s0, e0 = int(off[i]), int(off[i + 1])
+            if e0 == s0:
+                continue
+            seg = a[s0:e0].astype(np.float64)
+            want = np.concatenate([[0.0], np.cumsum(seg)[:-1]])
+            mass = np.concatenate([[0.0], np.cumsum(np.abs(seg))[:-1]])
+            assert got[s0] == 0.0
+            assert np.all(np.abs(got[s0:e0] - want) <= REL_TOL_F32 * mass + 1e-30), (i, mixed)
+
+
+def test_scan_segments_reg_many_rounds_and_replay(gsrb, ctx, orc):
+    # small chunks: tens of rounds per segment, the round sums' buffers reused
+    # many times; then the same call replayed from a CUDA graph
+    off = np.array([0, 1_000_003, 1_000_004, 1_700_000, 3_000_001], np.uint64)
+    a = gsrb.uniform_i32(21, int(off[-1]), 0, 2**31 - 1).astype(np.uint32) * np.uint32(5)
+    want = _want_scan(orc, a, off)
+    c = _reg_cfg(gsrb, 1, 128, 4)
+    assert np.array_equal(_scan_segments(gsrb, ctx, a, off, c), want)
+    d = ctx.to_device(a)
+    out = ctx.array(a.size, np.uint32)
+    gsrb.check(ctx.scan_u32_segments(d, out, off, c))
+    cg = gsrb.CudaGraph(ctx)
+    with cg:
+        gsrb.check(ctx.scan_u32_segments(d, out, off, c))
+    for _ in range(2):
+        out.zero()
+        cg.launch()
+        ctx.check_status("replay")
+        assert np.array_equal(out.download(), want)
+    cg.free()
+
+
+def test_scan_segments_reg_bad_cfg(gsrb, ctx):
+    u = ctx.array(64, np.uint32)
+    o = ctx.array(64, np.uint32)
+    off = np.array([0, 64], np.uint64)
+    assert ctx.scan_u32_segments(u, o, off, gsrb.cfg(variant=8, ctas_per_sm=1, threads=512,
+                                                     form=gsrb.FORM_REG)) == gsrb.ERR_UNSUPPORTED
+    for tile in (1000, 512 * 64 * 2, 512 * 64 // 8):  # not threads x 64 / (2..4)
+        c = gsrb.cfg(variant=9, ctas_per_sm=1, threads=512, form=gsrb.FORM_REG, tile=tile)
+        assert ctx.scan_u32_segments(u, o, off, c) == gsrb.ERR_ARG

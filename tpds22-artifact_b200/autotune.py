@@ -170,7 +170,8 @@ def segment_candidates(kind: str):
     whose state does not depend on the team size; for the scan also the round
     length: 1, 2, 4 (= 0, the default) or 8 tiles of 16 x threads per CTA -- a
     short round keeps the round and its prefetched successor in L2 for the
-    rescan, a long one pays fewer barriers)."""
+    rescan, a long one pays fewer barriers), and the register-resident form
+    that keeps each round's chunk in registers."""
     g = _g()
     out = []
     for k, threads in ((2, 512), (4, 256), (8, 128), (2, 256), (1, 1024)):
@@ -178,6 +179,14 @@ def segment_candidates(kind: str):
                      dict(variant=g.BAR_FLAT)):
             for tile in ((16 * threads, 2 * 16 * threads, 0, 8 * 16 * threads) if kind == "scan" else (0,)):
                 out.append(dict(cand, ctas_per_sm=k, threads=threads, tile=tile))
+    if kind == "scan":
+        # register-resident rounds (fan-out only): two groups a CTA; the chunk
+        # is threads x 4 x (16 vectors a lane when an SM holds <= 512 of the
+        # launch's threads, else 8) / 2
+        for k, threads in ((4, 256), (2, 512), (4, 128), (2, 256)):
+            per = threads * (16 if k * threads <= 512 else 8) * 4
+            out.append(dict(variant=g.BAR_FANOUT, wake_lines=4, ctas_per_sm=k, threads=threads, form=g.FORM_REG,
+                            tile=per // 2))
     return out
 
 

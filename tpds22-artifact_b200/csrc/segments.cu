@@ -359,6 +359,254 @@ scan_segments_kernel(SegParams p, const T* __restrict__ in, T* __restrict__ out,
   bar.finish();
 }
 
+// ---------------------------------------------------------------------------
+// Register-resident scan of segments (cfg.form = GSRB_FORM_REG; fan-out
+// sub-grid barrier).  The CTA's threads form NG groups that take the team's
+// rounds in turn (group g: rounds g, g + NG, ...).  In a round every CTA of the
+// team takes one chunk of GT x D x 4 elements (GT threads a group, D 128-bit
+// vectors a lane), which the group loads once into registers, sums, publishes
+// and -- after the segment's barrier of that round -- scans and writes from the
+// same registers: no element is read twice and nothing waits in L2 between a
+// read and a re-read.  While one group waits for its round's barrier the
+// others load or write theirs.  Chunks sit on a vector grid anchored at the
+// first position at or before the segment's start where `in` is 16-byte
+// aligned, so whole vectors are loaded with 128-bit loads (the elements of a
+// vector outside the segment read as zero and are not written); outputs go
+// out as 128-bit stores when `out` has the same alignment as `in`, else as
+// scalars.
+//
+// Ordering (every wait bounded):
+//  * the group of round j arrives at j only after this CTA passed the barrier
+//    of round j-1 (s_passed);
+//  * the group of round j takes the team's running total from the group of
+//    round j-1 (s_carry, sequence s_cseq) and hands on total + sum(j);
+//  * round sums rotate over NG + 2 buffers of one word per CTA: the sum of
+//    round j is written after this CTA passed j-1, so every CTA of the team
+//    arrived at j-1, which its group of j-1 did after reading the sums of
+//    j-1-NG and older; the last user of buffer j % (NG + 2) was j-NG-2;
+//  * a group's control flow is uniform: its leader decides (s_gfail) before a
+//    named barrier of the group that every thread of the group then passes.
+constexpr uint32_t kRegMaxGroups = 4;  // named barriers 1..4
+
+__device__ __forceinline__ void group_sync(uint32_t id, uint32_t nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// Bounded wait for a shared counter written by another group of the CTA.
+__device__ __forceinline__ bool group_wait_ge(const volatile uint32_t* p, uint32_t target,
+                                              const gsrb::GridBarrier& gb) {
+  uint64_t t0 = 0;
+  for (uint32_t it = 0;; ++it) {
+    if ((int32_t)(*p - target) >= 0) {
+      __threadfence_block();
+      return true;
+    }
+    if ((it & 63u) == 63u) {
+      if (gsrb::ptx::ld_relaxed_gpu(&gb.slot->status) != 0u) return false;
+      const uint64_t now = gsrb::ptx::globaltimer_ns();
+      if (t0 == 0) t0 = now;
+      else if (now - t0 > gb.timeout_ns) {
+        gsrb::detail::record_error(gb, gsrb::GSRB_DEV_TIMEOUT, 0xfffffff3u);
+        return false;
+      }
+    }
+  }
+}
+
+template <typename T> struct RegT;
+template <> struct RegT<uint32_t> {
+  using Vec = uint4;
+  // read once: streaming (evict-first) loads and stores
+  __device__ static __forceinline__ uint4 ld(const uint32_t* p) { return __ldcs(reinterpret_cast<const uint4*>(p)); }
+  __device__ static __forceinline__ void st(uint32_t* p, uint4 v) { __stcs(reinterpret_cast<uint4*>(p), v); }
+  // one lane's outputs: exclusive prefix before its first element e0 plus its
+  // local inclusive prefixes a0..a2 (uint32 wraps: exact in any order)
+  __device__ static __forceinline__ uint4 out(uint32_t e0, uint32_t a0, uint32_t a1, uint32_t a2) {
+    return make_uint4(e0, e0 + a0, e0 + a1, e0 + a2);
+  }
+};
+template <> struct RegT<float> {
+  using Vec = float4;
+  __device__ static __forceinline__ float4 ld(const float* p) { return __ldcs(reinterpret_cast<const float4*>(p)); }
+  __device__ static __forceinline__ void st(float* p, float4 v) { __stcs(reinterpret_cast<float4*>(p), v); }
+  // FP32: the FP64 prefix rounded once, the lane's local prefixes added in FP32
+  __device__ static __forceinline__ float4 out(double e0, float a0, float a1, float a2) {
+    const float b = (float)e0;
+    return make_float4(b, b + a0, b + a1, b + a2);
+  }
+};
+
+template <typename T>
+__device__ __forceinline__ T shfl_up_t(T v, int o) { return __shfl_up_sync(0xffffffffu, v, o); }
+template <typename T>
+__device__ __forceinline__ T shfl_idx_t(T v, int l) { return __shfl_sync(0xffffffffu, v, l); }
+
+template <typename T, int D, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1)
+scan_segments_reg_kernel(SegParams p, const T* __restrict__ in, T* __restrict__ out,
+                         typename ScanT<T>::Acc* __restrict__ partials, uint32_t ngroups) {
+  using Acc = typename ScanT<T>::Acc;
+  using Vec = typename RegT<T>::Vec;
+  __shared__ gsrb::BarrierShared bsh;
+  __shared__ Acc s_wt[kRegMaxGroups][32];  // warp totals -> exclusive warp offsets
+  __shared__ Acc s_red[kRegMaxGroups][2][32];
+  __shared__ Acc s_base[kRegMaxGroups];
+  __shared__ uint32_t s_gfail[kRegMaxGroups];
+  __shared__ volatile uint32_t s_passed, s_cseq, s_fail;
+  __shared__ volatile Acc s_carry;
+  __shared__ uint32_t s_epoch0;
+
+  const uint32_t tid = threadIdx.x, lane = tid & 31u;
+  const uint32_t NG = ngroups, GT = blockDim.x / NG, GW = GT >> 5;
+  const uint32_t g = tid / GT, gt = tid - g * GT, gw = gt >> 5;
+  const bool leader = gt == 0;
+  const uint32_t NB = NG + 2;
+  const uint64_t C = (uint64_t)GT * D * 4u;  // elements of one CTA's chunk
+  const SegTeam t = seg_team(p);
+  const gsrb::GridBarrier gb = seg_barrier(p, t);
+  gsrb::GridSync<gsrb::V_FANOUT> bar;
+  const bool ok0 = bar.init(gb, &bsh);
+  if (tid == 0) {
+    s_epoch0 = bar.epoch;
+    s_passed = 0;
+    s_cseq = 0;
+    s_carry = Acc(0);
+    s_fail = ok0 ? 0u : 1u;
+  }
+  __syncthreads();
+  const uint32_t epoch0 = s_epoch0;
+  const uint64_t o0 = p.off[t.seg], o1 = p.off[t.seg + 1];
+  // Positions are relative to the vector grid's origin, lo (0..3) elements
+  // before the segment's start, where `in` is 16-byte aligned: the segment is
+  // [lo, hi), and relative position u is element o0 + (u - lo).
+  const uint32_t ia = (uint32_t)((reinterpret_cast<uintptr_t>(in) >> 2) & 3u);
+  const uint64_t lo = (o0 + ia) & 3u, hi = o1 - o0 + lo;
+  const bool vec_in = (reinterpret_cast<uintptr_t>(in) & 3u) == 0;
+  const bool vec_out = vec_in && (reinterpret_cast<uintptr_t>(out) & 3u) == 0 &&
+                       ((reinterpret_cast<uintptr_t>(out) >> 2) & 3u) == ia;
+  const uint64_t R = C * t.count;
+  const uint32_t rounds = o1 > o0 ? (uint32_t)((hi + R - 1) / R) : 0u;
+  const uint32_t me = t.rank;
+
+  for (uint32_t j = g; j < rounds; j += NG) {
+    // A. this group's chunk of round j into registers, and its sum
+    const uint64_t cb = ((uint64_t)j * t.count + t.rank) * C;  // chunk base (relative, vector-aligned)
+    const uint32_t v0 = gw * 32u * D + lane;
+    Vec x[D];
+#pragma unroll
+    for (uint32_t k = 0; k < D; ++k) {
+      const uint64_t u = cb + 4ull * (v0 + 32u * k);
+      if (vec_in && u >= lo && u + 4 <= hi) {
+        x[k] = RegT<T>::ld(in + o0 + (u - lo));
+      } else {
+        T y[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) y[q] = (u + q >= lo && u + q < hi) ? __ldg(in + o0 + (u + q - lo)) : T(0);
+        x[k].x = y[0];
+        x[k].y = y[1];
+        x[k].z = y[2];
+        x[k].w = y[3];
+      }
+    }
+    Acc lsum = Acc(0);
+#pragma unroll
+    for (uint32_t k = 0; k < D; ++k) lsum += ScanT<T>::vsum(x[k]);
+    const Acc wt = warp_sum(lsum);
+    if (lane == 0) s_wt[g][gw] = wt;
+    group_sync(1u + g, GT);
+    // B. leader: warp offsets, the round's sum, arrival after j-1 was passed, barrier of j
+    if (leader) {
+      bool ok = s_fail == 0u;
+      Acc run = Acc(0);
+      for (uint32_t i = 0; i < GW; ++i) {
+        const Acc y = s_wt[g][i];
+        s_wt[g][i] = run;
+        run += y;
+      }
+      if (ok && j > 0) ok = group_wait_ge(&s_passed, j, gb);
+      if (ok) {
+        __stcg(&partials[(j % NB) * gridDim.x + t.first + t.rank], run);
+        gsrb::detail::fanout_arrive(gb, t.count, epoch0 + j);
+        ok = gsrb::detail::fanout_wait(gb, me, epoch0 + j, j);
+      }
+      if (ok) {
+        __threadfence_block();
+        s_passed = j + 1u;
+      } else {
+        s_fail = 1u;
+      }
+      s_gfail[g] = ok ? 0u : 1u;
+    }
+    group_sync(1u + g, GT);
+    if (s_gfail[g]) break;  // uniform: written by the leader before the group barrier
+    // C. offset = running total + the round's sums of the CTAs before this one
+    Acc pre = Acc(0), tot = Acc(0);
+    const Acc* part = partials + (j % NB) * gridDim.x + t.first;
+    for (uint32_t r = gt; r < t.count; r += GT) {
+      const Acc y = __ldcg(part + r);
+      tot += y;
+      if (r < t.rank) pre += y;
+    }
+    pre = warp_sum(pre);
+    tot = warp_sum(tot);
+    if (lane == 0) {
+      s_red[g][0][gw] = pre;
+      s_red[g][1][gw] = tot;
+    }
+    group_sync(1u + g, GT);
+    if (leader) {
+      Acc pp = Acc(0), qq = Acc(0);
+      for (uint32_t i = 0; i < GW; ++i) {
+        pp += s_red[g][0][i];
+        qq += s_red[g][1][i];
+      }
+      const bool ok = j == 0 || group_wait_ge(&s_cseq, j, gb);  // running total of rounds < j handed on
+      const Acc cin = j == 0 ? Acc(0) : Acc(s_carry);
+      s_base[g] = cin + pp;
+      s_carry = cin + qq;
+      __threadfence_block();
+      s_cseq = j + 1u;
+      if (!ok) s_fail = 1u;
+      s_gfail[g] = ok ? 0u : 1u;
+    }
+    group_sync(1u + g, GT);
+    if (s_gfail[g]) break;
+    // D. scan the registers and write the segment's elements
+    Acc run = s_base[g] + s_wt[g][gw];
+#pragma unroll
+    for (uint32_t k = 0; k < D; ++k) {
+      const uint64_t u = cb + 4ull * (v0 + 32u * k);
+      const Vec xv = x[k];
+      const T a0 = xv.x, a1 = a0 + xv.y, a2 = a1 + xv.z, a3 = a2 + xv.w;
+      T incl = a3;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const T y = shfl_up_t(incl, o);
+        if ((int)lane >= o) incl += y;
+      }
+      const Vec y = RegT<T>::out(run + Acc(incl - a3), a0, a1, a2);
+      if (vec_out && u >= lo && u + 4 <= hi) {
+        RegT<T>::st(out + o0 + (u - lo), y);
+      } else {
+        const T ys[4] = {y.x, y.y, y.z, y.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (u + q >= lo && u + q < hi) out[o0 + (u + q - lo)] = ys[q];
+      }
+      run += Acc(shfl_idx_t(incl, 31));
+    }
+  }
+  __syncthreads();
+  bar.finish();
+}
+
+// 16 vectors a lane when an SM holds at most 512 of the launch's threads
+// (about 128 registers a thread), else 8 (64 registers, 1024 threads an SM)
+template <typename T>
+const void* scan_segments_reg_fn(bool wide) {
+  return wide ? (const void*)scan_segments_reg_kernel<T, 16, 512> : (const void*)scan_segments_reg_kernel<T, 8, 1024>;
+}
+
 const void* reduce_segments_fn(int v) {
   switch (v) {  // sub-grid protocols whose state does not depend on the team size
     case gsrb::V_FLAT: return (const void*)reduce_segments_kernel<gsrb::V_FLAT>;
@@ -426,6 +674,28 @@ gsrb_status_t scan_segments(gsrb_ctx* ctx, const T* d_in, T* d_out, const uint64
   if (st) return st;
   using Acc = typename ScanT<T>::Acc;
   void* part = nullptr;
+  if (!cfgin) c.form = GSRB_FORM_REG;  // default: fan-out, 4 x 256, two groups of 4096-element chunks
+  if (c.form == GSRB_FORM_REG) {
+    // register-resident rounds (fan-out sub-grid barrier only): cfg->tile =
+    // elements of a CTA's chunk, threads x 4 x (16 vectors a lane when an
+    // SM holds at most 512 of the launch's threads, else 8) divided by 2..4
+    // groups (0 = two groups)
+    if (c.variant != gsrb::V_FANOUT) return GSRB_ERR_UNSUPPORTED;
+    const bool wide = c.threads * c.ctas_per_sm <= 512;
+    const uint32_t per = (uint32_t)c.threads * (wide ? 16u : 8u) * 4u;
+    uint32_t ng = 2;
+    if (c.tile > 0) {
+      if (per % (uint32_t)c.tile) return GSRB_ERR_ARG;
+      ng = per / (uint32_t)c.tile;
+    }
+    if (ng < 2 || ng > kRegMaxGroups || (c.threads / ng) % 32) return GSRB_ERR_ARG;
+    st = scratch(ctx, sizeof(Acc) * (kRegMaxGroups + 2) * (size_t)grid, &part);
+    if (st) return st;
+    Acc* partials = (Acc*)part;
+    const void* rf = scan_segments_reg_fn<T>(wide);
+    void* args[] = {&p, &d_in, &d_out, &partials, &ng};
+    return launch_persistent(ctx, rf, grid, c.threads, 0, 1, coop_of(c), args);
+  }
   st = scratch(ctx, sizeof(Acc) * 2 * (size_t)grid, &part);
   if (st) return st;
   Acc* partials = (Acc*)part;

@@ -53,6 +53,7 @@ BAR_NONE = 99
 FORM_AUTO = 0
 FORM_L2 = 1
 FORM_L1 = 2
+FORM_REG = 3
 SSSP_DELTA_LEARNED = 0
 VARIANT_NAMES = {
     BAR_CLUSTER: "gsrb_cluster",
