@@ -1148,15 +1148,22 @@ pagerank_kernel(gsrb::GridBarrier gb, PrArgs a) {
 #pragma unroll
         for (int r = 0; r < kRounds; ++r) {
           const uint32_t f = f0 + 32u * r + lane;
-          // owner = the last lane whose exclusive prefix is <= f
-          uint32_t lo = 0;
+          // owner = the last lane whose exclusive prefix is <= f; the search
+          // carries that prefix along (lane 0's is 0), so it costs no shuffle
+          uint32_t lo = 0, oe = 0;
 #pragma unroll
           for (uint32_t step = 16; step > 0; step >>= 1) {
             const uint32_t x = __shfl_sync(0xffffffffu, excl, lo + step);
-            if (x <= f) lo += step;
+            if (x <= f) {
+              lo += step;
+              oe = x;
+            }
           }
-          own[r] = lo;
-          const uint32_t ob = __shfl_sync(0xffffffffu, b, lo), oe = __shfl_sync(0xffffffffu, excl, lo);
+          // the lane (of this round) where the owner's segment begins: the
+          // segmented scan below compares lanes against it instead of
+          // shuffling owners
+          own[r] = oe > f0 + 32u * r ? oe - (f0 + 32u * r) : 0u;
+          const uint32_t ob = __shfl_sync(0xffffffffu, b, lo);
           nbr[r] = f < E ? __ldg(g.dst + ob + (f - oe)) : 0u;
         }
 #pragma unroll
@@ -1168,13 +1175,13 @@ pagerank_kernel(gsrb::GridBarrier gb, PrArgs a) {
         for (int r = 0; r < kRounds; ++r) {
           const uint32_t rb = f0 + 32u * r;
           if (rb >= E) break;  // warp-uniform
-          // segmented inclusive scan keyed by owner (owners ascend with the lane)
+          // segmented inclusive scan: lane l - o belongs to the same owner
+          // as lane l exactly when l - o is not before the owner's first lane
           double x = val[r];
 #pragma unroll
           for (int o = 1; o < 32; o <<= 1) {
             const double y = __shfl_up_sync(0xffffffffu, x, o);
-            const uint32_t ko = __shfl_up_sync(0xffffffffu, own[r], o);
-            if ((int)lane >= o && ko == own[r]) x += y;
+            if ((int)lane - o >= (int)own[r]) x += y;
           }
           // this lane's vertex: its segment in this round ends at flat index
           // min(excl + d, rb + 32, E) - 1
