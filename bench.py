@@ -592,8 +592,11 @@ def train_sssp_policy(gsrb, ctx, pol):
     """SSSP policy from timed runs of training graphs (not the evaluated ones):
     every width of policy.SSSP_DELTAS under both launch candidates."""
     graphs = [gsrb.rmat(s, 16, seed=SEED + 2000 + s) for s in (14, 16, 18, 20, 21)]
+    # grids up to 2^21 vertices: on meshes the best width grows with the
+    # diameter (fewer rounds), so the network must see large ones
     graphs += [gsrb.grid2d(w, h, seed=SEED + 2100 + w + h, wlo=1, whi=1000)
-               for w, h in ((256, 256), (1024, 64), (512, 512), (1024, 1024), (2048, 256))]
+               for w, h in ((256, 256), (1024, 64), (512, 512), (1024, 1024), (2048, 256), (2048, 1024),
+                            (4096, 512))]
     X, Y, M, rows = [], [], [], []
     t0 = time.time()
     for g in graphs:
