@@ -1031,15 +1031,29 @@ __device__ __forceinline__ float pr_gather(const float* cin, uint32_t d, int l1)
 
 // Sum of cin[dst[j]] over j in [j0, j1) by one warp: lanes stride the range,
 // 4 independent gathers in flight per lane, FP64 per lane, fixed-order
-// butterfly at the end (the same bits on every run).
+// butterfly at the end (the same bits on every run).  The destinations of the
+// next 128 edges are loaded while this step's gathers are in flight, so a
+// step costs one dependent round trip (the gather), not two.
 __device__ __forceinline__ double warp_gather_sum(const uint32_t* __restrict__ dst, const float* cin, uint32_t j0,
                                                   uint32_t j1, uint32_t lane, int l1) {
   double s = 0.0;
   uint32_t j = j0 + lane;
+  uint32_t d0 = 0, d1 = 0, d2 = 0, d3 = 0;
+  if (j + 96 < j1) {
+    d0 = __ldg(dst + j);
+    d1 = __ldg(dst + j + 32);
+    d2 = __ldg(dst + j + 64);
+    d3 = __ldg(dst + j + 96);
+  }
   for (; j + 96 < j1; j += 128) {
-    const uint32_t d0 = __ldg(dst + j), d1 = __ldg(dst + j + 32), d2 = __ldg(dst + j + 64), d3 = __ldg(dst + j + 96);
     const float c0 = pr_gather(cin, d0, l1), c1 = pr_gather(cin, d1, l1), c2 = pr_gather(cin, d2, l1),
                 c3 = pr_gather(cin, d3, l1);
+    if (j + 224 < j1) {
+      d0 = __ldg(dst + j + 128);
+      d1 = __ldg(dst + j + 160);
+      d2 = __ldg(dst + j + 192);
+      d3 = __ldg(dst + j + 224);
+    }
     s += (double)c0;
     s += (double)c1;
     s += (double)c2;
