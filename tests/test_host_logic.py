@@ -102,6 +102,43 @@ def test_autotune_candidates_and_cfg_roundtrip(gsrb, tune):
         assert {c["variant"] for c in sc} == {gsrb.BAR_FANOUT, gsrb.BAR_FLIP, gsrb.BAR_FLAT}
         assert all(c["ctas_per_sm"] * c["threads"] <= 2048 for c in sc)
     assert {c["tile"] for c in tune.segment_candidates("reduce")} == {0}
+    # the scan's register-resident candidates: fan-out, two groups, a chunk of
+    # threads x 4 x (16 vectors a lane at <= 512 threads an SM, else 8) / 2
+    reg = [c for c in tune.segment_candidates("scan") if c.get("form") == gsrb.FORM_REG]
+    assert reg and all(c["variant"] == gsrb.BAR_FANOUT for c in reg)
+    for c in reg:
+        per = c["threads"] * (16 if c["ctas_per_sm"] * c["threads"] <= 512 else 8) * 4
+        assert c["tile"] * 2 == per
+    # the reduce tuner's chained candidates exist only on request and never for grid.sync
+    assert not any(c.get("overlap") for c in tune.reduce_candidates(2, 256))
+    chained = [c for c in tune.reduce_candidates(2, 256, overlap=True) if c.get("overlap")]
+    assert chained and all(c["variant"] != gsrb.BAR_CCG for c in chained)
+
+
+def test_bench_tail_summary_fits_the_tail():
+    # the JSON line ends with one compact summary of every configuration, so a
+    # reader that keeps only the last 1500 characters still sees them all
+    import json
+    bench = _mod("bench_under_test", ROOT / "bench.py")
+    cf = {"C1_reduce_2e24": {"us": 9.68, "hbm_frac": 1.06, "unchained_hbm_frac": 0.66, "single_launch_cold_us": 20.5,
+                             "bit_exact": True, "cpu_mt_GB_s": 57.2},
+          "C2_barrier_k8": {f"F{f}": {"x_ccg": 1.1} for f in (0, 64, 1024)},
+          "C2_barrier_reference_programs": {"k8": {"gsrb_ns": 24144.4, "gcpusrb_ns": 21390.7, "ccg_ns": 4188.8,
+                                                   "atomic_tree_ns": 43595.4, "native_fanout_ns": 2237.0,
+                                                   "native_flip_ns": 3299.3}},
+          "C2_semaphore": {f"S{k}": {"acq_per_s": 123456.7} for k in (1, 2, 10, 120)},
+          "C3_scan_2e28": {"u32_hbm_frac": 0.775, "f32_hbm_frac": 0.755, "u32_bit_exact": True, "cpu_mt_GB_s": 35.1},
+          "C4_rmat22": {"bfs_learned_GTEPS": 271.1, "bfs_learned_vs_plain": 7.8, "sssp_GTEPS": 19.8,
+                        "pr_frac_of_gather_floor": 0.613, "bfs_bit_exact": True, "sssp_bit_exact": True},
+          "C4_grid2048": {"bfs_heuristic_ms": 29.8, "sssp_ms": 60.5},
+          "C5_batch64": {"bfs_learned_vs_plain": 46.8, "bfs_learned_vs_heuristic": 1.04, "sssp_speedup": 4.1,
+                         "bit_exact": True},
+          "C5_segments64": {"reduce_hbm_frac": 0.648, "scan_hbm_frac": 0.555}}
+    t = bench.tail_summary(cf)
+    assert set(t) >= {"C1_reduce", "C2_barrier_k8_x_ccg", "C3_scan", "C4_rmat22", "C5_batch64",
+                      "C5_segments64_hbm_frac"}
+    assert t["C1_reduce"]["hbm_frac"] == 1.06 and t["C4_rmat22"]["exact"] is True
+    assert len(json.dumps({"summary": t})) < 1400
 
 
 def _bench_env():
