@@ -214,7 +214,9 @@ def tune_bfs(ctx, dgraph, src: int, mode: int, reps: int = 2):
     g = _g()
     out = ctx.array(dgraph.n, np.int32)
     table = []
-    for k, threads in ((1, 512), (2, 256), (2, 512), (4, 256)):
+    # small grids matter on meshes (one SM's worth of CTAs of 256 threads
+    # runs the 2048^2 grid's 4095 levels fastest: fewer barrier participants)
+    for k, threads in ((1, 512), (2, 256), (2, 512), (4, 256), (1, 256), (1, 128)):
         for cand in (dict(variant=g.BAR_FANOUT, wake_lines=4), dict(variant=g.BAR_FLIP, fanin_groups=1),
                      dict(variant=g.BAR_HIER, fanin_groups=16, wake_lines=8), dict(variant=g.BAR_CCG)):
             c = g.cfg(ctas_per_sm=k, threads=threads, **cand)
