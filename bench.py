@@ -614,6 +614,16 @@ def train_sssp_policy(gsrb, ctx, pol):
                     "loss_first": float(hist[0]), "loss_last": float(hist[-1])}
 
 
+def _tuning_note(gsrb, best, table):
+    """The tuned launch (the library's own barriers only) and, beside it, the
+    fastest shape under grid.sync, from the tuner's timing table."""
+    ccg = [r for r in table if r[1]["variant"] == gsrb.BAR_CCG]
+    own = [r for r in table if r[1]["variant"] != gsrb.BAR_CCG]
+    return {"cfg": best, "tuning_ms": round(own[0][0], 3) if own else None,
+            "grid_sync_best_ms": round(ccg[0][0], 3) if ccg else None,
+            "grid_sync_best_cfg": ccg[0][1] if ccg else None}
+
+
 def graph_numbers(gsrb, ctx, orc, pol, params, sparams, tune, cache, verify_pr=True, ref_gpu="quick"):
     res = {}
     t0 = time.time()
@@ -621,8 +631,9 @@ def graph_numbers(gsrb, ctx, orc, pol, params, sparams, tune, cache, verify_pr=T
     res["rmat22"] = {"n": rm.nnodes, "m": rm.nedges, "max_degree": int(rm.degrees().max()),
                      "gen_s": round(time.time() - t0, 1)}
     dg = ctx.graph(rm)
-    best, _, _ = tune.tune_bfs(ctx, dg, 0, gsrb.BFS_HEURISTIC, reps=1)
+    best, _, ttab = tune.tune_bfs(ctx, dg, 0, gsrb.BFS_HEURISTIC, reps=1)
     cache["bfs_rmat"] = best
+    res["rmat22"]["launch_tuning"] = _tuning_note(gsrb, best, ttab)
     cfg = tune.cfg_from(best)
     res["rmat22"]["bfs"] = bfs_runs(gsrb, ctx, orc, dg, rm, params, cfg, launch=pol.launch_candidates(), cpu=True)
     dg.set_sssp_policy(sparams)
@@ -678,10 +689,10 @@ def graph_numbers(gsrb, ctx, orc, pol, params, sparams, tune, cache, verify_pr=T
     del rm
     gr = gsrb.grid2d(2048, 2048, seed=SEED, wlo=1, whi=1000)
     dg = ctx.graph(gr)
-    best, _, _ = tune.tune_bfs(ctx, dg, 0, gsrb.BFS_PUSH, reps=1)
+    best, _, ttab = tune.tune_bfs(ctx, dg, 0, gsrb.BFS_PUSH, reps=1)
     cache["bfs_grid"] = best
     cfg = tune.cfg_from(best)
-    res["grid2048"] = {"n": gr.nnodes, "m": gr.nedges,
+    res["grid2048"] = {"n": gr.nnodes, "m": gr.nedges, "launch_tuning": _tuning_note(gsrb, best, ttab),
                        "bfs": bfs_runs(gsrb, ctx, orc, dg, gr, params, cfg, reps=2, launch=pol.launch_candidates(),
                                        cpu=True)}
     dg.set_sssp_policy(sparams)

@@ -210,7 +210,9 @@ def tune_segments(ctx, kind: str, d_in, d_out, offsets, reps: int = 3):
     return table[0][1], table[0][0], table
 
 
-def tune_bfs(ctx, dgraph, src: int, mode: int, reps: int = 2):
+def tune_bfs(ctx, dgraph, src: int, mode: int, reps: int = 2, library_barrier_only: bool = True):
+    """Fastest launch shape and barrier for a BFS; with library_barrier_only
+    the cooperative-groups barrier is timed but not chosen."""
     g = _g()
     out = ctx.array(dgraph.n, np.int32)
     table = []
@@ -230,7 +232,8 @@ def tune_bfs(ctx, dgraph, src: int, mode: int, reps: int = 2):
             if ts:
                 table.append((statistics.median(ts), dict(cand, ctas_per_sm=k, threads=threads)))
     table.sort(key=lambda x: x[0])
-    return table[0][1], table[0][0], table
+    pick = [r for r in table if not (library_barrier_only and r[1]["variant"] == g.BAR_CCG)]
+    return pick[0][1], pick[0][0], table
 
 
 def load_cache(path=CACHE) -> dict:
