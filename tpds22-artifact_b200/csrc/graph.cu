@@ -346,6 +346,7 @@ __device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const B
   unsigned long long edges = dsrc;
   uint32_t dir = DIR_PUSH, prev_nf = 1;
   bool fallback = a.mode != GSRB_BFS_LEARNED;
+  uint32_t fb_level = 0;  // level at which the policy fell back (0 = never)
   float pred = __int_as_float(0x7fc00000);
   uint32_t L = 1;
   uint32_t decisions = 0;
@@ -367,7 +368,10 @@ __device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const B
     // ---- choose the level's direction (identical in every CTA)
     if (!fallback && L > 1 && pred == pred) {
       const float actual = log2f(1.f + (float)nf);
-      if (fabsf(actual - pred) > 1.f) fallback = true;  // missed by more than 2x
+      if (fabsf(actual - pred) > 1.f) {  // missed by more than 2x
+        fallback = true;
+        fb_level = L;
+      }
     }
     uint32_t nd = DIR_PUSH;
     if (a.mode == GSRB_BFS_PULL) {
@@ -576,13 +580,10 @@ __device__ __forceinline__ void bfs_run(gsrb::GridSync<V>& bar, bool ok, const B
     a.out[3] = ok ? 0u : 1u;
     *a.out_edges = edges;
   }
-  if (team.cta == 0 && threadIdx.x == 0 && a.mode == GSRB_BFS_LEARNED) {
-    // first level at which the policy fell back (0 = never); recomputed from the trace
-    uint32_t fb = 0;
-    for (uint32_t i = 0; i + 1 < L && i < a.trace_cap; ++i)
-      if (a.trace[i].fallback) { fb = a.trace[i].level; break; }
-    a.out[1] = fb;
-  }
+  // first level at which the policy fell back (0 = never), kept in a
+  // register: scanning the trace for it here cost one thread a dependent load
+  // per level (about 1 ms on a 4095-level mesh)
+  if (team.cta == 0 && threadIdx.x == 0 && a.mode == GSRB_BFS_LEARNED) a.out[1] = fb_level;
 }
 
 constexpr int kGraphMaxThreads = 1024;
