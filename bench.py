@@ -29,7 +29,8 @@ measured on the same device in the same run (disable with --no-extras):
 host cores: the reference has no CPU barrier, so this is the oracle's port of
 its sense-reversing barrier run by host threads (same metric and unit).
 Multi-GPU: the barrier does not shard (replicas only): every rank runs the
-same workload on its own GPU and the reported time is the max over ranks.
+same workload on its own GPU and the reported time is the max over ranks; the
+other configurations are measured at N = 1 only.
 """
 from __future__ import annotations
 
@@ -949,8 +950,13 @@ def _ref_run(prog, args, stdin=None, timeout=180):
     """Runs one of the reference's own programs (recompiled for sm_100a) and
     returns (time in ms it printed, stdout).  Only co-resident shapes are
     passed: the GSRB forms spin without a bound."""
+    # the program sees only this process's GPU (the LOCAL_RANK-th visible one)
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    devs = [d for d in vis.split(",") if d] if vis else [str(local)]
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES=devs[min(local, len(devs) - 1)] if vis else devs[0])
     p = subprocess.run([str(REF_BIN / prog)] + [str(a) for a in args], input=stdin, capture_output=True,
-                       text=True, timeout=timeout)
+                       text=True, timeout=timeout, env=env)
     if p.returncode != 0:
         raise RuntimeError(f"{prog} rc {p.returncode}: {(p.stdout + p.stderr)[-300:]}")
     for rx in _TIME_RE:
@@ -1426,7 +1432,9 @@ def main():
             }
     detail = {"headline": dict(line), "autotune_top5": [{"ns": t, "cfg": cand} for t, cand in tune_table[:5]]}
 
-    if not args.no_extras:
+    # the other configurations are measured at one GPU only: with N > 1 every
+    # GPU would repeat them (replicas) while all N are held
+    if not args.no_extras and dist.world == 1:
         orc = load_oracle()
         pol = _load("gsrb_policy", PKG / "policy.py")
         extras_t0 = time.time()
