@@ -631,13 +631,18 @@ struct RelaxSink {
   long long T;                  // near threshold
   WarpRes* res;                 // the warp's near-queue reservation
   uint32_t near_cap;            // near-queue capacity in slots (holes included)
+  bool precheck;                // read a distance before claiming it (large rounds)
 };
 
 // Relax four edges per lane at once: edge r of the lane is j[r] (where bit r of
 // `act` is set), leaving a vertex at distance du[r].  Every dependent step is
 // issued for all four before the next (destinations and weights, distance
-// probes, the atomicMin claims, the stamps, the degrees of vertices entering
-// the near queue), and the warp reserves queue space once per step.
+// probes, the atomicMin claims, the stamps), and the warp reserves queue space
+// once per step.  The row range of a destination (its degree, for the queue
+// it enters) is loaded alongside its stamp exchange; in small rounds
+// (!s.precheck) the distance probe is skipped -- the atomicMin itself tells
+// whether the edge improves -- and the row range goes out with the claim.
+// The same claims land either way, so distances are the same.
 // Warp-synchronous.
 __device__ __forceinline__ void sssp_relax4e(const SsspArgs& a, const long long* du, const uint32_t* j, uint32_t act,
                                              const RelaxSink& s, unsigned long long& my_edges) {
@@ -651,13 +656,31 @@ __device__ __forceinline__ void sssp_relax4e(const SsspArgs& a, const long long*
     nd[r] = on ? du[r] + (long long)__ldg(g.w + j[r]) : (long long)kInf;
     my_edges += on ? 1u : 0u;
   }
-  int32_t cur[4];
-#pragma unroll
-  for (int r = 0; r < 4; ++r) cur[r] = nd[r] < (long long)kInf ? __ldcg(a.dist + v[r]) : kInf;
   bool imp[4];
+  uint32_t rb[4], re[4];
+  if (s.precheck) {
+    int32_t cur[4];
 #pragma unroll
-  for (int r = 0; r < 4; ++r)
-    imp[r] = nd[r] < (long long)cur[r] && nd[r] < (long long)atomicMin(a.dist + v[r], (int32_t)nd[r]);
+    for (int r = 0; r < 4; ++r) cur[r] = nd[r] < (long long)kInf ? __ldcg(a.dist + v[r]) : kInf;
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+      imp[r] = nd[r] < (long long)cur[r] && nd[r] < (long long)atomicMin(a.dist + v[r], (int32_t)nd[r]);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      rb[r] = imp[r] && nd[r] < s.T ? __ldg(g.row + v[r]) : 0u;
+      re[r] = imp[r] && nd[r] < s.T ? __ldg(g.row + v[r] + 1) : 0u;
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const bool on = nd[r] < (long long)kInf;
+      rb[r] = on && nd[r] < s.T ? __ldg(g.row + v[r]) : 0u;
+      re[r] = on && nd[r] < s.T ? __ldg(g.row + v[r] + 1) : 0u;
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+      imp[r] = nd[r] < (long long)kInf && nd[r] < (long long)atomicMin(a.dist + v[r], (int32_t)nd[r]);
+  }
   bool to_near[4], to_far[4];
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
@@ -666,7 +689,7 @@ __device__ __forceinline__ void sssp_relax4e(const SsspArgs& a, const long long*
   }
   uint32_t d[4];
 #pragma unroll
-  for (int r = 0; r < 4; ++r) d[r] = to_near[r] ? __ldg(g.row + v[r] + 1) - __ldg(g.row + v[r]) : 0u;
+  for (int r = 0; r < 4; ++r) d[r] = to_near[r] ? re[r] - rb[r] : 0u;
   bool reg[4], big[4];
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
@@ -859,7 +882,8 @@ __device__ __forceinline__ void sssp_run(gsrb::GridSync<V>& bar, bool ok, const 
     // near-queue reservations in chunks of 64 slots when the queue (2n slots)
     // can hold the holes of every warp
     WarpRes res{0ull, 0u, 63ull * team.nwarps() <= g.n ? 64u : 0u};
-    const RelaxSink sink{qout, hout, &c->n_reg, &c->n_big, fout, fc, stamp, fgen, T, &res, 2u * g.n};
+    const RelaxSink sink{qout, hout, &c->n_reg, &c->n_big, fout, fc, stamp, fgen, T, &res, 2u * g.n,
+                         nf > kPushPrecheckFrontier};
     // vertex lists relaxed edge-balanced: edge prefix, first edge, distance
     ListSmem& L_ = list_smem();
     uint32_t* s_lp = L_.p;
@@ -909,11 +933,15 @@ __device__ __forceinline__ void sssp_run(gsrb::GridSync<V>& bar, bool ok, const 
       for (uint32_t base = gw * 32u; base < nreg; base += nwarps * 32u) {
         const uint32_t i = base + lane;
         uint32_t u = 0, b = 0, e = 0;
+        int32_t du0 = 0;
         if (i < nreg) {
           u = __ldcg(qin + i);
           if (u != kHole) {
+            // the distance is read alongside the row range (one round trip):
+            // a later decrease in this round re-queues the vertex anyway
             b = __ldg(g.row + u);
             e = __ldg(g.row + u + 1);
+            du0 = __ldcg(a.dist + u);
           }
         }
         const uint32_t deg = e - b;
@@ -929,14 +957,13 @@ __device__ __forceinline__ void sssp_run(gsrb::GridSync<V>& bar, bool ok, const 
         while (coop) {
           const int src = __ffs(coop) - 1;
           coop &= coop - 1;
-          const uint32_t uu = __shfl_sync(0xffffffffu, u, src);
           const uint32_t bb = __shfl_sync(0xffffffffu, b, src), ee = __shfl_sync(0xffffffffu, e, src);
-          const long long du = (long long)__ldcg(a.dist + uu);
+          const long long du = (long long)__shfl_sync(0xffffffffu, du0, src);
           for (uint32_t j0 = bb; j0 < ee; j0 += 128) sssp_relax4(a, du, j0 + lane, 32u, ee, sink, my_edges);
         }
         const uint32_t mine = deg <= kWarpDegree ? deg : 0u;
         const uint32_t kmax = warp_max_u32(mine);
-        const long long du = mine ? (long long)__ldcg(a.dist + u) : 0;
+        const long long du = mine ? (long long)du0 : 0;
         for (uint32_t k0 = 0; k0 < kmax; k0 += 4) sssp_relax4(a, du, b + k0, 1u, b + mine, sink, my_edges);
       }
       __syncthreads();
