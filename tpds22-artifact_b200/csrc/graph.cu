@@ -1309,12 +1309,20 @@ __device__ __forceinline__ void prr_push4e(const PrrArgs& a, const float* upd, c
       cross[r] = prev + upd[r] > a.eps && prev < a.eps;
     }
   }
+  // the row range of a candidate goes out with its stamp exchange (one round
+  // trip instead of two; unused when the exchange finds it already queued)
+  uint32_t rb[4], re[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    rb[r] = cross[r] ? __ldg(g.row + w[r]) : 0u;
+    re[r] = cross[r] ? __ldg(g.row + w[r] + 1) : 0u;
+  }
 #pragma unroll
   for (int r = 0; r < 4; ++r) cross[r] = cross[r] && atomicExch(a.mark + w[r], s.stamp) != s.stamp;
   bool reg[4], big[4];
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
-    const uint32_t d = cross[r] ? __ldg(g.row + w[r] + 1) - __ldg(g.row + w[r]) : 0u;
+    const uint32_t d = cross[r] ? re[r] - rb[r] : 0u;
     reg[r] = cross[r] && d <= kBigDegree;
     big[r] = cross[r] && d > kBigDegree;
     pushes += cross[r] ? 1u : 0u;
