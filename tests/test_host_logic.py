@@ -326,3 +326,15 @@ def test_sssp_features_host(gsrb):
     assert abs(f[0] - 20.0) < 1e-5 and abs(f[2] - np.log2(17.0)) < 1e-5
     assert abs(f[4] - 3.0) < 1e-5 and f[8] == 1.0
     assert abs(f[11] - (f[0] - 2 * f[2])) < 1e-5
+
+
+def test_bench_tuning_note_keeps_grid_sync_beside(gsrb):
+    # the graphs' launch tuning reports the library's own pick and grid.sync's
+    # best shape beside it, from the tuner's sorted table
+    bench = _mod("bench_under_test", ROOT / "bench.py")
+    table = [(26.5, dict(variant=gsrb.BAR_CCG, ctas_per_sm=1, threads=256)),
+             (27.3, dict(variant=gsrb.BAR_FLIP, fanin_groups=1, ctas_per_sm=1, threads=256)),
+             (30.4, dict(variant=gsrb.BAR_FLIP, fanin_groups=1, ctas_per_sm=2, threads=256))]
+    note = bench._tuning_note(gsrb, table[1][1], table)
+    assert note["cfg"]["variant"] == gsrb.BAR_FLIP and note["tuning_ms"] == 27.3
+    assert note["grid_sync_best_ms"] == 26.5 and note["grid_sync_best_cfg"]["ctas_per_sm"] == 1
